@@ -1,0 +1,324 @@
+// Device V-cycle of a smoothed-aggregation hierarchy (gfem/linalg.py:156-195).
+//
+// Per level: Chebyshev smoothing of D^-1 A over [rho/30, rho] with degree 2
+// (3 operator products per call, the first one on a zero guess is skipped since
+// A*0 = 0), residual, restriction R = P^T, recursion, prolongation, and
+// post-smoothing.  The coarsest level is solved in FP64 with the inverse of the
+// regularised dense Cholesky factor formed on the host (two triangular solves in
+// the reference, gfem/linalg.py:179-181; the product is the same up to rounding).
+//
+// CSR products run with a group of 4-32 lanes per row (chosen from the mean row
+// length) and a fixed shuffle tree, so results are deterministic.  The Chebyshev
+// step is fused into the row loop: x += d, r -= dinv*(A d), d' = a d + b r.
+// Level 0 can instead be smoothed with the current matrix-free tangent
+// (gfem/solvers.py:311-314), in which case the products go through the
+// element kernel and the vector updates through small elementwise kernels.
+#include "internal.h"
+#include "solver.h"
+
+namespace exfem {
+
+enum SpmvMode { SP_SET = 0, SP_ADD = 1, SP_RES = 2, SP_RESINIT = 3, SP_CHEB = 4 };
+
+template <class T, int LANES, int MODE>
+__global__ void __launch_bounds__(256)
+spmv_kernel(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
+            const T* __restrict__ val, const T* __restrict__ x, T* __restrict__ y,
+            const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ d2,
+            T* __restrict__ xo, T c1, T c2, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  constexpr int GPW = 32 / LANES;  // row groups per warp
+  const int lane = threadIdx.x & (LANES - 1);
+  const int grp = (threadIdx.x & 31) / LANES;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = warp * GPW; base < n; base += nwarps * GPW) {
+    const int64_t row = base + grp;
+    T s = T(0);
+    if (row < n) {
+      const int64_t k1 = ptr[row + 1];
+      for (int64_t k = ptr[row] + lane; k < k1; k += LANES) s += val[k] * x[idx[k]];
+    }
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LANES);
+    if (row < n && lane == 0) {
+      if (MODE == SP_SET) {
+        y[row] = s;
+      } else if (MODE == SP_ADD) {
+        y[row] += s;
+      } else if (MODE == SP_RES) {
+        y[row] = b[row] - s;
+      } else if (MODE == SP_RESINIT) {
+        const T r = dinv[row] * (b[row] - s);
+        y[row] = r;
+        d2[row] = r * c1;
+      } else {  // SP_CHEB: x is the direction d
+        const T d = x[row];
+        xo[row] += d;
+        const T r = y[row] - dinv[row] * s;
+        y[row] = r;
+        d2[row] = c1 * d + c2 * r;
+      }
+    }
+  }
+}
+
+template <class T, int MODE>
+static int spmv_lanes(const Csr64& A, const T* val, const T* x, T* y, const T* b, const T* dinv, T* d2,
+                      T* xo, T c1, T c2, const int* skip, cudaStream_t s) {
+  if (A.n == 0) return EXFEM_OK;
+  const double avg = A.n ? (double)A.nnz / (double)A.n : 0.0;
+  const int threads = 256;
+  const int64_t warps_needed = (A.n + 7) / 8;
+  const unsigned grid = grid_for((size_t)warps_needed * 32, threads, 148u * 24u);
+#define EXF_SP(L) spmv_kernel<T, L, MODE><<<grid, threads, 0, s>>>(A.n, A.ptr.p, A.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, skip)
+  if (avg <= 8) EXF_SP(4);
+  else if (avg <= 24) EXF_SP(8);
+  else if (avg <= 64) EXF_SP(16);
+  else EXF_SP(32);
+#undef EXF_SP
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
+template <class T>
+static const T* csr_vals(const Csr64& A);
+template <> const double* csr_vals<double>(const Csr64& A) { return A.v64.p; }
+template <> const float* csr_vals<float>(const Csr64& A) { return A.v32.p; }
+
+// ---------------------------------------------------------------- elementwise kernels
+template <class T>
+__global__ void cheb_init0_kernel(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv,
+                                  T* __restrict__ x, T* __restrict__ r, T* __restrict__ d, T ith,
+                                  const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T ri = dinv[i] * b[i];
+    x[i] = T(0);
+    r[i] = ri;
+    d[i] = ri * ith;
+  }
+}
+
+template <class T>
+__global__ void cheb_update_kernel(int64_t n, T* __restrict__ x, const T* __restrict__ d, T* __restrict__ r,
+                                   const T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ d2,
+                                   T c1, T c2, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T di = d[i];
+    x[i] += di;
+    const T ri = r[i] - dinv[i] * Ad[i];
+    r[i] = ri;
+    d2[i] = c1 * di + c2 * ri;
+  }
+}
+
+template <class T>
+__global__ void resinit_kernel(int64_t n, const T* __restrict__ b, const T* __restrict__ Ax,
+                               const T* __restrict__ dinv, T* __restrict__ r, T* __restrict__ d, T ith,
+                               const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T ri = dinv[i] * (b[i] - Ax[i]);
+    r[i] = ri;
+    d[i] = ri * ith;
+  }
+}
+
+template <class T>
+__global__ void sub_kernel(int64_t n, const T* __restrict__ b, T* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = b[i] - y[i];
+}
+
+template <class T>
+__global__ void add_kernel(int64_t n, const T* __restrict__ d, T* __restrict__ x, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += d[i];
+}
+
+// x = Ainv * b, FP64 arithmetic, one warp per row
+template <class T>
+__global__ void coarse_kernel(int64_t nc, const double* __restrict__ Ainv, const T* __restrict__ b,
+                              T* __restrict__ x, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= nc) return;
+  double s = 0.0;
+  for (int64_t j = lane; j < nc; j += 32) s += Ainv[row * nc + j] * (double)b[j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[row] = (T)s;
+}
+
+// ---------------------------------------------------------------- V-cycle driver
+template <class T>
+static T* lvbuf(AmgLevel& L, int k);
+template <> double* lvbuf<double>(AmgLevel& L, int k) { return L.w64[k].p; }
+template <> float* lvbuf<float>(AmgLevel& L, int k) { return L.w32[k].p; }
+template <class T>
+static const T* lvdinv(AmgLevel& L);
+template <> const double* lvdinv<double>(AmgLevel& L) { return L.dinv64.p; }
+template <> const float* lvdinv<float>(AmgLevel& L) { return L.dinv32.p; }
+
+int amg_prepare(exfem_amg_s* h, int dtype) {
+  int st;
+  for (auto& Lp : h->levels) {
+    AmgLevel& L = *Lp;
+    const int64_t nb = std::max<int64_t>(L.n, 1);
+    for (int k = 0; k < AmgLevel::NW; ++k) {
+      if (dtype == EXFEM_F64 && L.w64[k].n < (size_t)nb && (st = L.w64[k].alloc(nb))) return st;
+      if (dtype == EXFEM_F32 && L.w32[k].n < (size_t)nb && (st = L.w32[k].alloc(nb))) return st;
+    }
+  }
+  const int64_t nb = std::max<int64_t>(h->nc, 1);
+  if (dtype == EXFEM_F64) {
+    if (h->cb64.n < (size_t)nb && (st = h->cb64.alloc(nb))) return st;
+    if (h->cx64.n < (size_t)nb && (st = h->cx64.alloc(nb))) return st;
+  } else {
+    if (h->cb32.n < (size_t)nb && (st = h->cb32.alloc(nb))) return st;
+    if (h->cx32.n < (size_t)nb && (st = h->cx32.alloc(nb))) return st;
+  }
+  return EXFEM_OK;
+}
+
+template <class T>
+static int coarse_solve(exfem_amg_s* h, const T* b, T* x, const int* skip, cudaStream_t s) {
+  if (h->nc == 0) return EXFEM_OK;
+  const int threads = 128;
+  coarse_kernel<T><<<(unsigned)((h->nc * 32 + threads - 1) / threads), threads, 0, s>>>(h->nc, h->Ainv.p, b, x, skip);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
+template <class T>
+static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0Op<T>* op0,
+                        const int* skip, cudaStream_t s) {
+  if (l == h->levels.size()) return coarse_solve<T>(h, b, x, skip, s);
+  AmgLevel& L = *h->levels[l];
+  const bool mf = (l == 0 && op0 && op0->apply);
+  const T* dinv = (l == 0 && op0 && op0->dinv) ? op0->dinv : lvdinv<T>(L);
+  const int64_t n = L.n;
+  T* r = lvbuf<T>(L, AmgLevel::WR);
+  T* d = lvbuf<T>(L, AmgLevel::WD);
+  T* d2 = lvbuf<T>(L, AmgLevel::WD2);
+  T* t = lvbuf<T>(L, AmgLevel::WTMP);
+  const double lmax = L.rho, lmin = L.rho / 30.0;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double ca[8], cb[8];
+  {
+    double rh = 1.0 / sigma;
+    for (int j = 0; j < h->degree; ++j) {
+      const double rn = 1.0 / (2.0 * sigma - rh);
+      ca[j] = rn * rh;
+      cb[j] = 2.0 * rn / delta;
+      rh = rn;
+    }
+  }
+  const T ith = (T)(1.0 / theta);
+  const unsigned eg = grid_for(n, 256);
+  const T* vals = csr_vals<T>(L.A);
+  int st;
+  auto smooth_steps = [&]() -> int {
+    for (int j = 0; j < h->degree; ++j) {
+      if (mf) {
+        if ((st = op0->apply(op0->ctx, d, t, skip, s))) return st;
+        cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], skip);
+        EX_LAUNCH_CHECK();
+      } else {
+        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s))) return st;
+      }
+      std::swap(d, d2);
+    }
+    add_kernel<T><<<eg, 256, 0, s>>>(n, d, x, skip);
+    EX_LAUNCH_CHECK();
+    return EXFEM_OK;
+  };
+  // pre-smoothing from x = 0
+  cheb_init0_kernel<T><<<eg, 256, 0, s>>>(n, b, dinv, x, r, d, ith, skip);
+  EX_LAUNCH_CHECK();
+  if ((st = smooth_steps())) return st;
+  // residual and restriction
+  if (mf) {
+    if ((st = op0->apply(op0->ctx, x, t, skip, s))) return st;
+    sub_kernel<T><<<eg, 256, 0, s>>>(n, b, t, skip);
+    EX_LAUNCH_CHECK();
+  } else {
+    if ((st = spmv_lanes<T, SP_RES>(L.A, vals, x, t, b, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  }
+  T* bc;
+  T* xc;
+  if (l + 1 < h->levels.size()) {
+    AmgLevel& C = *h->levels[l + 1];
+    bc = lvbuf<T>(C, AmgLevel::WB);
+    xc = lvbuf<T>(C, AmgLevel::WX);
+  } else {
+    if constexpr (sizeof(T) == 8) { bc = (T*)h->cb64.p; xc = (T*)h->cx64.p; }
+    else { bc = (T*)h->cb32.p; xc = (T*)h->cx32.p; }
+  }
+  if ((st = spmv_lanes<T, SP_SET>(L.R, csr_vals<T>(L.R), t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  if ((st = vcycle_level<T>(h, l + 1, bc, xc, nullptr, skip, s))) return st;
+  if ((st = spmv_lanes<T, SP_ADD>(L.P, csr_vals<T>(L.P), xc, x, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  // post-smoothing from the corrected x
+  if (mf) {
+    if ((st = op0->apply(op0->ctx, x, t, skip, s))) return st;
+    resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, skip);
+    EX_LAUNCH_CHECK();
+  } else {
+    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), skip, s))) return st;
+  }
+  return smooth_steps();
+}
+
+template <class T>
+int amg_vcycle(exfem_amg_s* h, const T* b, T* x, const Level0Op<T>* op0, const int* skip, cudaStream_t s) {
+  if (h->levels.empty()) {
+    if (h->nc == 0) { set_error("empty AMG hierarchy"); return EXFEM_ERR_ARG; }
+    return coarse_solve<T>(h, b, x, skip, s);
+  }
+  int st;
+  if ((st = amg_prepare(h, sizeof(T) == 8 ? EXFEM_F64 : EXFEM_F32))) return st;
+  return vcycle_level<T>(h, 0, b, x, op0, skip, s);
+}
+
+template int amg_vcycle<double>(exfem_amg_s*, const double*, double*, const Level0Op<double>*, const int*, cudaStream_t);
+template int amg_vcycle<float>(exfem_amg_s*, const float*, float*, const Level0Op<float>*, const int*, cudaStream_t);
+
+// ---------------------------------------------------------------- upload
+static int upload_csr(Csr64& M, int64_t n, int64_t ncols, const int64_t* ptr, const int32_t* idx, const double* val) {
+  M.n = n;
+  M.ncols = ncols;
+  M.nnz = ptr[n];
+  int st;
+  if ((st = M.ptr.upload(ptr, n + 1))) return st;
+  if ((st = M.idx.upload(idx, M.nnz))) return st;
+  if ((st = M.v64.upload(val, M.nnz))) return st;
+  std::vector<float> v32(val, val + M.nnz);
+  for (int64_t k = 0; k < M.nnz; ++k) v32[k] = (float)val[k];
+  return M.v32.upload(v32.data(), M.nnz);
+}
+
+int amg_add_level(exfem_amg_s* h, int64_t n, int64_t nc, const int64_t* Ap, const int32_t* Ai, const double* Av,
+                  const int64_t* Pp, const int32_t* Pi, const double* Pv, const int64_t* Rp, const int32_t* Ri,
+                  const double* Rv, const double* dinv, double rho) {
+  auto L = std::make_unique<AmgLevel>();
+  L->n = n;
+  L->nc = nc;
+  L->rho = rho;
+  int st;
+  if ((st = upload_csr(L->A, n, n, Ap, Ai, Av))) return st;
+  if ((st = upload_csr(L->P, n, nc, Pp, Pi, Pv))) return st;
+  if ((st = upload_csr(L->R, nc, n, Rp, Ri, Rv))) return st;
+  if ((st = L->dinv64.upload(dinv, n))) return st;
+  std::vector<float> d32(dinv, dinv + n);
+  if ((st = L->dinv32.upload(d32.data(), n))) return st;
+  h->levels.push_back(std::move(L));
+  return EXFEM_OK;
+}
+
+}  // namespace exfem

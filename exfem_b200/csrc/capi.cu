@@ -1,0 +1,460 @@
+// extern "C" entry points of libexfem_b200 (declared in include/exfem_b200.h).
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+
+#include "solver.h"
+
+namespace exfem {
+
+static thread_local std::string g_err;
+
+void set_error(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+int cuda_status(cudaError_t e, const char* what, const char* file, int line) {
+  set_error("%s failed (%s:%d): %s", what, file, line, cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? EXFEM_ERR_OOM : EXFEM_ERR_CUDA;
+}
+
+int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan, int& vmax);
+int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& colour, int& ncolour);
+int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg);
+int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters, double* relres, cudaStream_t st);
+int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, double inner_tol, int max_pass,
+                 int maxiter, int* iters, int* passes, double* relres, cudaStream_t st);
+int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st);
+int solver_alloc(exfem_solver_s* S);
+
+static int set_material(exfem_block_s* b, const exfem_material* m) {
+  EX_ARG(m, "material is NULL");
+  EX_ARG(m->kind == EXFEM_LINEAR_ELASTIC || m->kind == EXFEM_J2, "unknown material kind %d", m->kind);
+  EX_ARG(m->E > 0 && m->nu > -1.0 && m->nu < 0.5, "invalid elastic constants E=%g nu=%g", m->E, m->nu);
+  b->mat_in = *m;
+  MatDev& d = b->mat;
+  memset(&d, 0, sizeof(d));
+  d.kind = m->kind;
+  d.mu = m->E / (2.0 * (1.0 + m->nu));                        // gfem/materials.py:18-19
+  d.lam = m->E * m->nu / ((1.0 + m->nu) * (1.0 - 2.0 * m->nu));
+  d.K = d.lam + 2.0 * d.mu / 3.0;                             // gfem/materials.py:245
+  d.Hk = m->Hk;
+  if (m->kind == EXFEM_J2) {
+    EX_ARG(m->ntab >= 2 && m->ntab <= EXFEM_MAX_TABLE, "J2 table needs 2..%d rows, got %d", EXFEM_MAX_TABLE, m->ntab);
+    for (int i = 1; i < m->ntab; ++i)
+      EX_ARG(m->ep_tab[i] >= m->ep_tab[i - 1], "J2 table plastic strains must be non-decreasing");
+    d.ntab = m->ntab;
+    for (int i = 0; i < m->ntab; ++i) {
+      d.ep[i] = m->ep_tab[i];
+      d.sy[i] = m->sy_tab[i];
+    }
+  }
+  return EXFEM_OK;
+}
+
+static int init_tangent(exfem_block_s* b) {
+  if (b->mat.kind != EXFEM_J2) return EXFEM_OK;
+  const size_t n = (size_t)b->ne * b->ngp * 8;
+  std::vector<double> t(n, 0.0);
+  std::vector<float> t32(n, 0.0f);
+  for (size_t i = 0; i < n; i += 8) {
+    t[i + 6] = 1.0;
+    t32[i + 6] = 1.0f;
+  }
+  int s;
+  if ((s = b->tan64.upload(t.data(), n))) return s;
+  return b->tan32.upload(t32.data(), n);
+}
+
+}  // namespace exfem
+
+using namespace exfem;
+
+static cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
+
+template <class T>
+static int mf_apply_cb(void* ctx, const T* x, T* y, const int* skip, cudaStream_t s) {
+  return launch_mf_matvec<T>((exfem_block_s*)ctx, x, y, skip, s);
+}
+
+// graphs cannot be captured on the legacy default stream: such calls run on a
+// private stream ordered after and before the caller's stream with events
+struct StreamGuard {
+  cudaStream_t user, work = nullptr;
+  cudaEvent_t ev = nullptr;
+  bool own = false;
+  int init(void* s) {
+    user = (cudaStream_t)s;
+    if (user != nullptr && user != cudaStreamLegacy) { work = user; return EXFEM_OK; }
+    EX_CUDA(cudaStreamCreateWithFlags(&work, cudaStreamNonBlocking));
+    EX_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    own = true;
+    EX_CUDA(cudaEventRecord(ev, user));
+    EX_CUDA(cudaStreamWaitEvent(work, ev, 0));
+    return EXFEM_OK;
+  }
+  ~StreamGuard() {
+    if (own) {
+      cudaEventRecord(ev, work);
+      cudaStreamWaitEvent(user, ev, 0);
+      cudaEventDestroy(ev);
+      cudaStreamDestroy(work);
+    }
+  }
+};
+
+
+extern "C" {
+
+int exfem_version(void) { return 1000; }
+const char* exfem_last_error(void) { return g_err.c_str(); }
+
+int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const double* X_host, int64_t ne,
+                       const int32_t* conn_host, exfem_block* out) {
+  EX_ARG(out, "out is NULL");
+  *out = nullptr;
+  EX_ARG(etype == EXFEM_C3D8 || etype == EXFEM_C3D10, "unknown element type %d", etype);
+  EX_ARG(nn >= 0 && ne >= 0, "negative sizes");
+  EX_ARG(nn == 0 || X_host, "X is NULL");
+  EX_ARG(ne == 0 || conn_host, "conn is NULL");
+  EX_ARG(3 * nn < (int64_t)INT32_MAX, "too many nodes for int32 DOF indices");
+  auto b = std::make_unique<exfem_block_s>();
+  cudaGetDevice(&b->device);
+  b->etype = etype;
+  b->nnode = etype == EXFEM_C3D8 ? 8 : 10;
+  b->ngp = etype == EXFEM_C3D8 ? 8 : 4;
+  b->nd = 3 * b->nnode;
+  b->ne = ne;
+  b->nn = nn;
+  int s;
+  if ((s = set_material(b.get(), mat))) return s;
+  b->nstate = mat->kind == EXFEM_J2 ? 19 : 1;
+  if ((s = host_gather_plan(nn, ne, b->nnode, conn_host, b->plan_host, b->vmax))) return s;
+  std::vector<int32_t> colours;
+  if ((s = host_colouring(nn, ne, b->nnode, conn_host, colours, b->ncolour))) return s;
+  b->colour_host = colours;
+  // elements grouped by colour, ascending element index within a colour
+  b->colour_ptr.assign(b->ncolour + 1, 0);
+  for (int64_t e = 0; e < ne; ++e) ++b->colour_ptr[colours[e] + 1];
+  for (int c = 0; c < b->ncolour; ++c) b->colour_ptr[c + 1] += b->colour_ptr[c];
+  std::vector<int32_t> elems(ne);
+  {
+    std::vector<int64_t> pos(b->colour_ptr.begin(), b->colour_ptr.end() - 1);
+    for (int64_t e = 0; e < ne; ++e) elems[pos[colours[e]]++] = (int32_t)e;
+  }
+  // straight-edge check for C3D10 (mid-node at the edge midpoint)
+  b->affine = 1;
+  if (etype == EXFEM_C3D10) {
+    static const int E[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+    for (int64_t e = 0; e < ne && b->affine; ++e) {
+      const int32_t* c = conn_host + e * 10;
+      for (int k = 0; k < 6; ++k) {
+        const double* p = X_host + 3 * (int64_t)c[E[k][0]];
+        const double* q = X_host + 3 * (int64_t)c[E[k][1]];
+        const double* m = X_host + 3 * (int64_t)c[4 + k];
+        double L = 0.0, d = 0.0;
+        for (int i = 0; i < 3; ++i) {
+          L += (q[i] - p[i]) * (q[i] - p[i]);
+          const double r = m[i] - 0.5 * (p[i] + q[i]);
+          d += r * r;
+        }
+        if (d > 1e-20 * L) { b->affine = 0; break; }
+      }
+    }
+  }
+  if ((s = b->X.upload(X_host, 3 * nn))) return s;
+  if ((s = b->conn.upload(conn_host, ne * b->nnode))) return s;
+  if ((s = b->plan.upload(b->plan_host.data(), b->plan_host.size()))) return s;
+  if ((s = b->colour_elems.upload(elems.data(), elems.size()))) return s;
+  if ((s = build_geometry(b.get()))) return s;
+  if ((s = init_tangent(b.get()))) return s;
+  // element-vector scratch (force assembly, stored-Ke products, diagonals); allocated
+  // here so that no later call allocates inside a captured CUDA graph
+  if ((s = b->ys.alloc(std::max<int64_t>(ne * b->nnode * 3, 1)))) return s;
+  *out = b.release();
+  return EXFEM_OK;
+}
+
+int exfem_block_destroy(exfem_block b) {
+  delete b;
+  return EXFEM_OK;
+}
+
+int exfem_block_query(exfem_block b, int64_t* ne, int64_t* nn, int* nnode, int* ngp, int* nstate, int* vmax,
+                      int* ncolour, int* affine, int64_t* device_bytes) {
+  EX_ARG(b, "block is NULL");
+  if (ne) *ne = b->ne;
+  if (nn) *nn = b->nn;
+  if (nnode) *nnode = b->nnode;
+  if (ngp) *ngp = b->ngp;
+  if (nstate) *nstate = b->nstate;
+  if (vmax) *vmax = b->vmax;
+  if (ncolour) *ncolour = b->ncolour;
+  if (affine) *affine = b->affine;
+  if (device_bytes)
+    *device_bytes = (int64_t)(b->X.bytes() + b->conn.bytes() + b->scale.bytes() + b->plan.bytes() +
+                              b->colour_elems.bytes() + b->fixed.bytes() + b->node_fixed.bytes() +
+                              b->geo64.bytes() + b->geo32.bytes() + b->tan64.bytes() + b->tan32.bytes() +
+                              b->ys.bytes());
+  return EXFEM_OK;
+}
+
+int exfem_block_gather_plan(exfem_block b, int32_t* plan_host) {
+  EX_ARG(b && plan_host, "NULL argument");
+  memcpy(plan_host, b->plan_host.data(), b->plan_host.size() * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_block_colours(exfem_block b, int32_t* colour_host) {
+  EX_ARG(b && colour_host, "NULL argument");
+  memcpy(colour_host, b->colour_host.data(), b->colour_host.size() * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_block_set_scale(exfem_block b, const double* scale_host) {
+  EX_ARG(b, "block is NULL");
+  int s;
+  if (scale_host) {
+    if ((s = b->scale.upload(scale_host, b->ne))) return s;
+  } else {
+    b->scale.release();
+  }
+  ++b->bc_gen;
+  return build_geometry(b);
+}
+
+int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
+  EX_ARG(b, "block is NULL");
+  int s;
+  ++b->bc_gen;
+  if (!fixed_host) {
+    b->fixed.release();
+    b->node_fixed.release();
+    return EXFEM_OK;
+  }
+  std::vector<uint8_t> f(fixed_host, fixed_host + b->ndof()), nf(b->nn, 0);
+  for (int64_t n = 0; n < b->nn; ++n)
+    for (int c = 0; c < 3; ++c) {
+      f[3 * n + c] = f[3 * n + c] ? 1 : 0;
+      nf[n] |= (uint8_t)(f[3 * n + c] << c);
+    }
+  if (b->fixed.n == (size_t)b->ndof()) {
+    EX_CUDA(cudaMemcpy(b->fixed.p, f.data(), f.size(), cudaMemcpyHostToDevice));
+    EX_CUDA(cudaMemcpy(b->node_fixed.p, nf.data(), nf.size(), cudaMemcpyHostToDevice));
+    return EXFEM_OK;
+  }
+  if ((s = b->fixed.upload(f.data(), f.size()))) return s;
+  return b->node_fixed.upload(nf.data(), nf.size());
+}
+
+int exfem_internal_force(exfem_block b, const double* u, const double* state_old, double* state_new, double* fe,
+                         double* f, int assembly, void* stream) {
+  EX_ARG(b && u && f, "NULL argument");
+  EX_ARG(b->mat.kind != EXFEM_J2 || state_old, "J2 material needs state_old");
+  EX_ARG(assembly == EXFEM_ASSEMBLE_GATHER || assembly == EXFEM_ASSEMBLE_COLOUR, "unknown assembly %d", assembly);
+  int s;
+  if (!fe) {
+    if (b->ys.n < (size_t)(b->ne * b->nnode * 3) && (s = b->ys.alloc(b->ne * b->nnode * 3))) return s;
+    fe = b->ys.p;
+  }
+  if ((s = launch_force(b, FORCE_FULL, u, state_old, state_new, fe, nullptr, nullptr, nullptr, as_stream(stream)))) return s;
+  if (b->mat.kind == EXFEM_J2) ++b->tan_gen;
+  if (assembly == EXFEM_ASSEMBLE_GATHER) return launch_gather_assemble(b, fe, f, nullptr, nullptr, as_stream(stream));
+  return launch_colour_assemble(b, fe, f, as_stream(stream));
+}
+
+int exfem_element_stiffness(exfem_block b, const double* u, const double* state_old, int dtype, void* Ke, void* stream) {
+  EX_ARG(b && u && Ke, "NULL argument");
+  EX_ARG(b->mat.kind != EXFEM_J2 || state_old, "J2 material needs state_old");
+  return launch_stiffness(b, u, state_old, dtype, Ke, nullptr, as_stream(stream));
+}
+
+int exfem_tangent_update(exfem_block b, const double* u, const double* state_old, void* stream) {
+  EX_ARG(b && u, "NULL argument");
+  if (b->mat.kind != EXFEM_J2) return EXFEM_OK;
+  EX_ARG(state_old, "J2 material needs state_old");
+  ++b->tan_gen;
+  return launch_force(b, FORCE_TANGENT, u, state_old, nullptr, nullptr, nullptr, nullptr, nullptr, as_stream(stream));
+}
+
+int exfem_tangent_matvec(exfem_block b, int dtype, const void* v, void* y, int apply_bc, void* stream) {
+  EX_ARG(b && v && y, "NULL argument");
+  if (dtype == EXFEM_F64)
+    return launch_mf_matvec<double>(b, (const double*)v, (double*)y, nullptr, as_stream(stream), apply_bc != 0);
+  if (dtype == EXFEM_F32)
+    return launch_mf_matvec<float>(b, (const float*)v, (float*)y, nullptr, as_stream(stream), apply_bc != 0);
+  set_error("tangent matvec supports F64 and F32, got %d", dtype);
+  return EXFEM_ERR_ARG;
+}
+
+int exfem_tangent_diagonal(exfem_block b, double* diag, void* stream) {
+  EX_ARG(b && diag, "NULL argument");
+  return launch_mf_diagonal(b, diag, as_stream(stream));
+}
+
+int exfem_ebe_matvec(exfem_block b, const double* Ke, const double* v, double* y, int apply_bc, void* stream) {
+  EX_ARG(b && Ke && v && y, "NULL argument");
+  return launch_ebe_matvec(b, Ke, v, y, nullptr, as_stream(stream), apply_bc != 0);
+}
+
+int exfem_ebe_diagonal(exfem_block b, const double* Ke, double* diag, void* stream) {
+  EX_ARG(b && Ke && diag, "NULL argument");
+  return launch_ebe_diagonal(b, Ke, diag, as_stream(stream));
+}
+
+int exfem_stresses(exfem_block b, const double* u, const double* state, double* S, double* mises, double* peeq,
+                   void* stream) {
+  EX_ARG(b && u, "NULL argument");
+  EX_ARG(b->mat.kind != EXFEM_J2 || state, "J2 material needs a state");
+  return launch_force(b, FORCE_STRESS, u, state, nullptr, nullptr, S, mises, peeq, as_stream(stream));
+}
+
+// ---------------------------------------------------------------- AMG
+int exfem_amg_create(exfem_amg* out) {
+  EX_ARG(out, "out is NULL");
+  *out = new exfem_amg_s();
+  return EXFEM_OK;
+}
+
+int exfem_amg_destroy(exfem_amg h) {
+  delete h;
+  return EXFEM_OK;
+}
+
+int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc, const int64_t* A_ptr, const int32_t* A_idx,
+                        const double* A_val, const int64_t* P_ptr, const int32_t* P_idx, const double* P_val,
+                        const int64_t* R_ptr, const int32_t* R_idx, const double* R_val, const double* dinv,
+                        double rho) {
+  EX_ARG(h && A_ptr && P_ptr && R_ptr && dinv, "NULL argument");
+  EX_ARG(n > 0 && nc > 0, "empty level");
+  EX_ARG(h->levels.empty() || h->levels.back()->nc == n, "level size %lld does not match the previous coarse size",
+         (long long)n);
+  EX_ARG(rho > 0 && std::isfinite(rho), "invalid spectral bound %g", rho);
+  return amg_add_level(h, n, nc, A_ptr, A_idx, A_val, P_ptr, P_idx, P_val, R_ptr, R_idx, R_val, dinv, rho);
+}
+
+int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv) {
+  EX_ARG(h && Ainv, "NULL argument");
+  EX_ARG(h->levels.empty() || h->levels.back()->nc == nc, "coarse size mismatch");
+  h->nc = nc;
+  return h->Ainv.upload(Ainv, (size_t)(nc * nc));
+}
+
+int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0, const void* dinv0,
+                     void* stream) {
+  EX_ARG(h && r && z, "NULL argument");
+  EX_ARG(!level0 || dinv0, "a level-0 block needs dinv0");
+  if (dtype == EXFEM_F64) {
+    Level0Op<double> op;
+    if (level0) { op.apply = &mf_apply_cb<double>; op.ctx = level0; op.dinv = (const double*)dinv0; }
+    return amg_vcycle<double>(h, (const double*)r, (double*)z, level0 ? &op : nullptr, nullptr, as_stream(stream));
+  }
+  if (dtype == EXFEM_F32) {
+    Level0Op<float> op;
+    if (level0) { op.apply = &mf_apply_cb<float>; op.ctx = level0; op.dinv = (const float*)dinv0; }
+    return amg_vcycle<float>(h, (const float*)r, (float*)z, level0 ? &op : nullptr, nullptr, as_stream(stream));
+  }
+  set_error("V-cycle supports F64 and F32, got %d", dtype);
+  return EXFEM_ERR_ARG;
+}
+
+// ---------------------------------------------------------------- solvers
+int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out) {
+  EX_ARG(b && out, "NULL argument");
+  *out = nullptr;
+  EX_ARG(op_kind >= EXFEM_OP_EBE_F64 && op_kind <= EXFEM_OP_MF_F32, "unknown operator kind %d", op_kind);
+  EX_ARG(pc_kind >= EXFEM_PC_NONE && pc_kind <= EXFEM_PC_AMG, "unknown preconditioner %d", pc_kind);
+  EX_ARG(pc_kind != EXFEM_PC_AMG || amg, "AMG preconditioner needs a hierarchy");
+  EX_ARG(pc_kind != EXFEM_PC_AMG || amg->levels.empty() || amg->levels[0]->n == b->ndof(),
+         "hierarchy level 0 has %lld rows, block has %lld DOFs", (long long)(amg->levels.empty() ? 0 : amg->levels[0]->n),
+         (long long)b->ndof());
+  auto S = std::make_unique<exfem_solver_s>();
+  S->blk = b;
+  S->amg = amg;
+  S->op = op_kind;
+  S->pc = pc_kind;
+  S->n = b->ndof();
+  int s;
+  if ((s = solver_alloc(S.get()))) return s;
+  *out = S.release();
+  return EXFEM_OK;
+}
+
+int exfem_solver_destroy(exfem_solver s) {
+  delete s;
+  return EXFEM_OK;
+}
+
+int exfem_solver_set_ke(exfem_solver s, const double* Ke) {
+  EX_ARG(s, "solver is NULL");
+  s->Ke = Ke;
+  s->diag_ready = false;
+  return EXFEM_OK;
+}
+
+int exfem_solver_refresh_diagonal(exfem_solver s, void* stream) {
+  EX_ARG(s, "solver is NULL");
+  return solver_refresh_diagonal(s, as_stream(stream));
+}
+
+int exfem_solver_set_graph(exfem_solver s, int enable, int chunk) {
+  EX_ARG(s, "solver is NULL");
+  EX_ARG(chunk >= 1 && chunk <= 1024, "chunk must be in 1..1024");
+  for (auto& g : s->gexec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  s->use_graph = enable ? 1 : 0;
+  s->chunk = chunk;
+  return EXFEM_OK;
+}
+
+int exfem_solver_pcg(exfem_solver s, const double* b, double* x, double tol, int maxiter, int* iters, double* relres,
+                     void* stream) {
+  EX_ARG(s && b && x, "NULL argument");
+  EX_ARG(tol >= 0 && maxiter >= 0, "invalid tolerance or iteration limit");
+  StreamGuard g;
+  int st;
+  if ((st = g.init(stream))) return st;
+  return solver_pcg(s, b, x, tol, maxiter, iters, relres, g.work);
+}
+
+int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, double inner_tol, int max_pass,
+                       int maxiter, int* iters, int* passes, double* relres, void* stream) {
+  EX_ARG(s && b && x, "NULL argument");
+  EX_ARG(tol >= 0 && inner_tol > 0 && max_pass >= 1 && maxiter >= 0, "invalid refinement parameters");
+  StreamGuard g;
+  int st;
+  if ((st = g.init(stream))) return st;
+  return solver_mixed(s, b, x, tol, inner_tol, max_pass, maxiter, iters, passes, relres, g.work);
+}
+
+// ---------------------------------------------------------------- host builders
+int exfem_host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* plan, int* vmax) {
+  EX_ARG(conn && vmax, "NULL argument");
+  std::vector<int32_t> p;
+  int v = 0, s;
+  if ((s = host_gather_plan(nn, ne, nnode, conn, p, v))) return s;
+  *vmax = v;
+  if (plan) memcpy(plan, p.data(), p.size() * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* colour, int* ncolour) {
+  EX_ARG(conn && colour && ncolour, "NULL argument");
+  std::vector<int32_t> c;
+  int s;
+  if ((s = host_colouring(nn, ne, nnode, conn, c, *ncolour))) return s;
+  memcpy(colour, c.data(), c.size() * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
+  EX_ARG(ptr && idx && agg && nagg, "NULL argument");
+  return host_standard_aggregation(n, ptr, idx, agg, *nagg);
+}
+
+}  // extern "C"

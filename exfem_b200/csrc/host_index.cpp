@@ -1,0 +1,127 @@
+// Host-side index builders of the exfem_b200 library (no device work).
+//
+//  * gather plan (gfem/model.py:241-261): for every node, the flat element
+//    slots elem*nnode + local that touch it, in increasing slot order (the
+//    reference's stable argsort by node), padded with the sentinel ne*nnode to
+//    the maximum valence.  Built here with a counting sort; bit-identical.
+//  * greedy element colouring (no counterpart in the reference): elements in
+//    index order take the smallest colour unused by every element that shares a
+//    node with them.
+//  * standard aggregation for smoothed aggregation (Vanek, Mandel & Brezina,
+//    "Algebraic multigrid by smoothed aggregation", 1996; PyAMG's default
+//    'standard' aggregation, which the reference calls through
+//    pyamg.smoothed_aggregation_solver at gfem/linalg.py:113-116):
+//      pass 1: every node whose strong neighbours are all unaggregated seeds an
+//              aggregate with them; nodes with no neighbour stay unaggregated;
+//      pass 2: remaining nodes join the first neighbouring pass-1 aggregate;
+//      pass 3: still-unaggregated nodes seed new aggregates with their
+//              unaggregated neighbours.
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace exfem {
+
+int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan,
+                     int& vmax) {
+  std::vector<int32_t> cnt(nn, 0);
+  const int64_t nslot = ne * nnode;
+  for (int64_t k = 0; k < nslot; ++k) {
+    const int32_t n = conn[k];
+    if (n < 0 || n >= nn) {
+      set_error("connectivity entry %d at slot %lld is outside [0, %lld)", n, (long long)k, (long long)nn);
+      return EXFEM_ERR_ARG;
+    }
+    ++cnt[n];
+  }
+  int32_t m = 1;
+  for (int64_t n = 0; n < nn; ++n) m = cnt[n] > m ? cnt[n] : m;
+  vmax = m;
+  if (nslot >= (int64_t)INT32_MAX) {
+    set_error("gather plan needs int64 slots (ne*nnode >= 2^31)");
+    return EXFEM_ERR_UNSUPPORTED;
+  }
+  plan.assign((size_t)nn * vmax, (int32_t)nslot);
+  std::fill(cnt.begin(), cnt.end(), 0);
+  for (int64_t k = 0; k < nslot; ++k) {
+    const int32_t n = conn[k];
+    plan[(size_t)n * vmax + cnt[n]++] = (int32_t)k;
+  }
+  return EXFEM_OK;
+}
+
+int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& colour,
+                   int& ncolour) {
+  constexpr int W = 4;  // 256 colours
+  std::vector<uint64_t> used((size_t)nn * W, 0);
+  colour.assign(ne, 0);
+  ncolour = 0;
+  for (int64_t e = 0; e < ne; ++e) {
+    uint64_t m[W] = {0, 0, 0, 0};
+    for (int a = 0; a < nnode; ++a) {
+      const int64_t n = conn[e * nnode + a];
+      for (int w = 0; w < W; ++w) m[w] |= used[n * W + w];
+    }
+    int c = 0;
+    while (c < 64 * W && ((m[c >> 6] >> (c & 63)) & 1ull)) ++c;
+    if (c >= 64 * W) {
+      set_error("element colouring needs more than %d colours", 64 * W);
+      return EXFEM_ERR_UNSUPPORTED;
+    }
+    colour[e] = c;
+    if (c + 1 > ncolour) ncolour = c + 1;
+    for (int a = 0; a < nnode; ++a) {
+      const int64_t n = conn[e * nnode + a];
+      used[n * W + (c >> 6)] |= (1ull << (c & 63));
+    }
+  }
+  return EXFEM_OK;
+}
+
+int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg) {
+  constexpr int32_t UNSET = -2, ISOLATED = -1;
+  std::vector<uint8_t> seeded(n, 0);  // 1 = member of a pass-1 aggregate
+  for (int64_t i = 0; i < n; ++i) agg[i] = UNSET;
+  int32_t next = 0;
+  for (int64_t i = 0; i < n; ++i) {  // pass 1
+    if (agg[i] != UNSET) continue;
+    bool has_nb = false, free_nbs = true;
+    for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+      const int64_t j = idx[k];
+      if (j == i) continue;
+      has_nb = true;
+      if (agg[j] != UNSET) { free_nbs = false; break; }
+    }
+    if (!has_nb) {
+      agg[i] = ISOLATED;
+    } else if (free_nbs) {
+      agg[i] = next;
+      seeded[i] = 1;
+      for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+        agg[idx[k]] = next;
+        seeded[idx[k]] = 1;
+      }
+      ++next;
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {  // pass 2
+    if (agg[i] != UNSET) continue;
+    for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) {
+      const int64_t j = idx[k];
+      if (j != i && seeded[j]) { agg[i] = agg[j]; break; }
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {  // pass 3
+    if (agg[i] != UNSET) continue;
+    agg[i] = next;
+    for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+      if (agg[idx[k]] == UNSET) agg[idx[k]] = next;
+    ++next;
+  }
+  nagg = next;
+  return EXFEM_OK;
+}
+
+}  // namespace exfem

@@ -1,0 +1,74 @@
+// Internal handle layouts and cross-file launchers of the exfem_b200 library.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "element_math.cuh"
+
+struct exfem_block_s {
+  int device = 0;
+  int etype = 0, nnode = 0, ngp = 0, nstate = 1, nd = 0;
+  int64_t ne = 0, nn = 0;
+  exfem::MatDev mat{};
+  exfem_material mat_in{};
+  // mesh
+  exfem::DevBuf<double> X;            // (nn, 3)
+  exfem::DevBuf<int32_t> conn;        // (ne, nnode)
+  exfem::DevBuf<double> scale;        // (ne), empty = 1
+  // index maps
+  int vmax = 0;
+  exfem::DevBuf<int32_t> plan;        // (nn, vmax), sentinel ne*nnode
+  std::vector<int32_t> plan_host;
+  int ncolour = 0;
+  std::vector<int64_t> colour_ptr;    // (ncolour+1) into colour_elems
+  exfem::DevBuf<int32_t> colour_elems;
+  std::vector<int32_t> colour_host;
+  // boundary conditions
+  exfem::DevBuf<uint8_t> fixed;       // (ndof) 1 = prescribed; empty = all free
+  exfem::DevBuf<uint8_t> node_fixed;  // (nn) bit c set = dof c prescribed
+  // matrix-free operator data
+  int affine = 1;
+  exfem::DevBuf<double> geo64;        // (ne, geo_stride)
+  exfem::DevBuf<float> geo32;
+  int plastic_tangent = 0;            // 1 once tangent data differs from elastic
+  exfem::DevBuf<double> tan64;        // (ne, ngp, 8)
+  exfem::DevBuf<float> tan32;
+  // generations: tangent data and boundary-condition buffers (solvers compare)
+  uint64_t tan_gen = 0, bc_gen = 0;
+  // scratch
+  exfem::DevBuf<double> ys;           // (ne*nnode*3) element vectors for gather assembly
+  int64_t ndof() const { return 3 * nn; }
+};
+
+namespace exfem {
+
+struct Csr64 {  // device CSR, FP64 values and an FP32 copy
+  int64_t n = 0, ncols = 0, nnz = 0;
+  DevBuf<int64_t> ptr;
+  DevBuf<int32_t> idx;
+  DevBuf<double> v64;
+  DevBuf<float> v32;
+};
+
+// element kernels (element_ops.cu)
+int launch_force(exfem_block_s* b, int mode, const double* u, const double* st_old, double* st_new,
+                 double* fe, double* S, double* mises, double* peeq, cudaStream_t s);
+int launch_gather_assemble(exfem_block_s* b, const double* ys, double* f, const double* v_opa,
+                           const int* skip, cudaStream_t s);
+int build_geometry(exfem_block_s* b);
+int launch_stiffness(exfem_block_s* b, const double* u, const double* st_old, int dtype, void* Ke,
+                     double* ediag, cudaStream_t s, const double* tan_in = nullptr);
+int launch_colour_assemble(exfem_block_s* b, const double* fe, double* f, cudaStream_t s);
+int launch_ebe_matvec(exfem_block_s* b, const double* Ke, const double* v, double* y,
+                      const int* skip, cudaStream_t s, bool bc = true);
+int launch_ebe_diagonal(exfem_block_s* b, const double* Ke, double* diag, cudaStream_t s);
+// matrix-free operator (matfree.cu)
+template <class T>
+int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaStream_t s, bool bc = true);
+int launch_mf_diagonal(exfem_block_s* b, double* diag, cudaStream_t s);
+
+// reductions and vector kernels (krylov.cu)
+enum ModeForce { FORCE_FULL = 0, FORCE_TANGENT = 1, FORCE_STRESS = 2 };
+
+}  // namespace exfem

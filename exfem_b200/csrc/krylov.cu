@@ -1,0 +1,464 @@
+// PCG and mixed-precision iterative refinement on the device.
+//
+// PCG follows gfem/linalg.py:21-47 exactly: x0 = 0, r = b, z = M(r), p = z,
+// loop while r.r > tol^2 max(b.b, 1e-300) and k < maxiter: Ap = A p,
+// alpha = rz / p.Ap, x += alpha p, r -= alpha Ap, rr = r.r, z = M(r),
+// beta = r.z / rz, p = z + beta p.  All dot products accumulate in FP64 with a
+// fixed two-level reduction order (deterministic), and all step scalars live in
+// device memory as FP64, so the host never sits in the loop: iterations are
+// issued in chunks (captured once as a CUDA graph), every kernel first reads the
+// device "done" flag, and the host reads the flag once per chunk.
+//
+// Mixed refinement follows gfem/solvers.py:344-384 (_LinearSystem._mixed): an
+// FP32 inner PCG on the normalised residual, the correction accumulated in FP64,
+// and the FP64 residual b - A x recomputed with the FP64 operator each pass.
+#include "solver.h"
+
+namespace exfem {
+
+constexpr int RT = 256;          // reduction block size
+constexpr int RED_MAX_BLOCKS = 296;
+
+enum Fin { FIN_BB = 0, FIN_RZ0, FIN_RR0, FIN_ALPHA, FIN_RR, FIN_BETA, FIN_STORE };
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void fin_apply(int F, double s, PcgScal* sc, double* out) {
+  switch (F) {
+    case FIN_BB:
+      sc->bb = s;
+      sc->tol2 = sc->spare * fmax(s, 1e-300);
+      break;
+    case FIN_RZ0: sc->rz = s; break;
+    case FIN_RR0:
+      sc->rr = s;
+      sc->done = !(s > sc->tol2 && sc->k < sc->maxiter);
+      break;
+    case FIN_ALPHA:
+      sc->pAp = s;
+      sc->alpha = sc->rz / s;
+      break;
+    case FIN_RR: sc->rr = s; break;
+    case FIN_BETA:
+      sc->beta = s / sc->rz;
+      sc->rz = s;
+      sc->k += 1;
+      sc->done = !(sc->rr > sc->tol2 && sc->k < sc->maxiter);
+      break;
+    default: *out = s;
+  }
+}
+
+// block partial sums + last-block final sum in index order
+__device__ __forceinline__ void block_finish(double v, double* partial, unsigned* counter, int F,
+                                             PcgScal* sc, double* out) {
+  __shared__ double sw[RT / 32];
+  __shared__ int last;
+  v = warp_sum(v);
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < RT / 32; ++w) t += sw[w];
+    partial[blockIdx.x] = t;
+    __threadfence();
+    const unsigned tk = atomicAdd(counter, 1u);
+    last = (tk == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+    double t = 0.0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += 32) t += ((volatile double*)partial)[i];
+    t = warp_sum(t);
+    if (threadIdx.x == 0) {
+      fin_apply(F, t, sc, out);
+      *counter = 0u;
+    }
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(RT)
+dot_kernel(int64_t n, const T* __restrict__ a, const T* __restrict__ b, double* partial, unsigned* counter,
+           PcgScal* sc, double* out, int F, int check_done) {
+  if (check_done && sc->done) return;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n; i += (int64_t)gridDim.x * RT)
+    acc += (double)a[i] * (double)b[i];
+  block_finish(acc, partial, counter, F, sc, out);
+}
+
+template <class T>
+__global__ void __launch_bounds__(RT)
+update_xr_kernel(int64_t n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                 const T* __restrict__ Ap, double* partial, unsigned* counter, PcgScal* sc) {
+  if (sc->done) return;
+  const T alpha = (T)sc->alpha;
+  double acc = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n; i += (int64_t)gridDim.x * RT) {
+    x[i] += alpha * p[i];
+    const T ri = r[i] - alpha * Ap[i];
+    r[i] = ri;
+    acc += (double)ri * (double)ri;
+  }
+  block_finish(acc, partial, counter, FIN_RR, sc, nullptr);
+}
+
+template <class T>
+__global__ void update_p_kernel(int64_t n, T* __restrict__ p, const T* __restrict__ z, const PcgScal* sc) {
+  if (sc->done) return;
+  const T beta = (T)sc->beta;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = z[i] + beta * p[i];
+}
+
+template <class TS, class TD>
+__global__ void convert_kernel(int64_t n, const TS* __restrict__ s, TD* __restrict__ d, double scale,
+                               const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = (TD)((double)s[i] * scale);
+}
+
+template <class T>
+__global__ void mask_kernel(int64_t n, const uint8_t* __restrict__ fixed, const T* __restrict__ v,
+                            T* __restrict__ out, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = fixed[i] ? T(0) : v[i];
+}
+
+template <class T>
+__global__ void pc_out_kernel(int64_t n, const uint8_t* __restrict__ fixed, const T* __restrict__ r,
+                              T* __restrict__ z, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (fixed[i]) z[i] = r[i];
+}
+
+template <class T>
+__global__ void jacobi_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r, T* __restrict__ z,
+                              const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = dinv[i] * r[i];
+}
+
+__global__ void dinv_kernel(int64_t n, const double* __restrict__ d, const uint8_t* __restrict__ fixed,
+                            double* __restrict__ d64, float* __restrict__ d32) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const bool fx = fixed && fixed[i];
+    const double v = fx ? 1.0 : (fabs(d[i]) > 0.0 ? 1.0 / d[i] : 1.0);
+    d64[i] = v;
+    d32[i] = (float)v;
+  }
+}
+
+__global__ void axpy_f32_kernel(int64_t n, double* __restrict__ x, const float* __restrict__ d, double sc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += (double)d[i] * sc;
+}
+
+__global__ void sub64_kernel(int64_t n, const double* __restrict__ b, const double* __restrict__ t,
+                             double* __restrict__ r) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    r[i] = b[i] - t[i];
+}
+
+__global__ void init_scal_kernel(PcgScal* sc, double tol, int maxiter) {
+  sc->rz = sc->pAp = sc->rr = sc->bb = sc->alpha = sc->beta = 0.0;
+  sc->spare = tol * tol;
+  sc->tol2 = 0.0;
+  sc->k = 0;
+  sc->maxiter = maxiter;
+  sc->done = 0;
+}
+
+// ---------------------------------------------------------------- helpers
+static unsigned red_grid(int64_t n) {
+  int64_t g = (n + RT * 4 - 1) / (RT * 4);
+  if (g < 1) g = 1;
+  if (g > RED_MAX_BLOCKS) g = RED_MAX_BLOCKS;
+  return (unsigned)g;
+}
+
+template <class T>
+static int dot(exfem_solver_s* S, const T* a, const T* b, int F, double* out, int check_done, cudaStream_t st) {
+  dot_kernel<T><<<red_grid(S->n), RT, 0, st>>>(S->n, a, b, S->partial.p, S->counter.p, S->scal.p, out, F, check_done);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
+static double* ws64(exfem_solver_s* S, int k) {
+  DevBuf<double>* v[] = {&S->x64, &S->r64, &S->z64, &S->p64, &S->Ap64, &S->b64, &S->t64};
+  return v[k]->p;
+}
+static float* ws32(exfem_solver_s* S, int k) {
+  DevBuf<float>* v[] = {&S->x32, &S->r32, &S->z32, &S->p32, &S->Ap32, &S->b32, &S->t32};
+  return v[k]->p;
+}
+enum { WX = 0, WR, WZ, WP, WAP, WB, WT };
+template <class T> static T* ws(exfem_solver_s* S, int k);
+template <> double* ws<double>(exfem_solver_s* S, int k) { return ws64(S, k); }
+template <> float* ws<float>(exfem_solver_s* S, int k) { return ws32(S, k); }
+template <class T> static const T* sdinv(exfem_solver_s* S);
+template <> const double* sdinv<double>(exfem_solver_s* S) { return S->dinv64.p; }
+template <> const float* sdinv<float>(exfem_solver_s* S) { return S->dinv32.p; }
+
+template <class T>
+static int op_apply(exfem_solver_s* S, const T* v, T* y, const int* skip, cudaStream_t st) {
+  if constexpr (sizeof(T) == 8) {
+    if (S->op == EXFEM_OP_EBE_F64) {
+      if (!S->Ke) { set_error("solver: stored-Ke operator without Ke (call exfem_solver_set_ke)"); return EXFEM_ERR_ARG; }
+      return launch_ebe_matvec(S->blk, S->Ke, v, y, skip, st);
+    }
+    return launch_mf_matvec<double>(S->blk, v, y, skip, st);
+  } else {
+    return launch_mf_matvec<float>(S->blk, v, y, skip, st);
+  }
+}
+
+template <class T>
+static int op0_apply(void* ctx, const T* x, T* y, const int* skip, cudaStream_t st) {
+  return op_apply<T>((exfem_solver_s*)ctx, x, y, skip, st);
+}
+
+template <class T>
+static int pc_apply(exfem_solver_s* S, const T* r, T* z, const int* skip, cudaStream_t st) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  if (S->pc == EXFEM_PC_NONE) {
+    EX_CUDA(cudaMemcpyAsync(z, r, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+    return EXFEM_OK;
+  }
+  if (S->pc == EXFEM_PC_JACOBI) {
+    jacobi_kernel<T><<<eg, 256, 0, st>>>(n, sdinv<T>(S), r, z, skip);
+    EX_LAUNCH_CHECK();
+    return EXFEM_OK;
+  }
+  const uint8_t* fixed = S->blk->fixed.p;
+  const T* rin = r;
+  if (fixed) {
+    T* t = ws<T>(S, WT);
+    mask_kernel<T><<<eg, 256, 0, st>>>(n, fixed, r, t, skip);
+    EX_LAUNCH_CHECK();
+    rin = t;
+  }
+  Level0Op<T> op0;
+  op0.apply = &op0_apply<T>;
+  op0.ctx = S;
+  op0.dinv = sdinv<T>(S);
+  int s;
+  if ((s = amg_vcycle<T>(S->amg, rin, z, &op0, skip, st))) return s;
+  if (fixed) {
+    pc_out_kernel<T><<<eg, 256, 0, st>>>(n, fixed, r, z, skip);
+    EX_LAUNCH_CHECK();
+  }
+  return EXFEM_OK;
+}
+
+template <class T>
+static int pcg_iteration(exfem_solver_s* S, cudaStream_t st) {
+  const int* skip = &S->scal.p->done;
+  T *x = ws<T>(S, WX), *r = ws<T>(S, WR), *z = ws<T>(S, WZ), *p = ws<T>(S, WP), *Ap = ws<T>(S, WAP);
+  int s;
+  if ((s = op_apply<T>(S, p, Ap, skip, st))) return s;
+  if ((s = dot<T>(S, p, Ap, FIN_ALPHA, nullptr, 1, st))) return s;
+  update_xr_kernel<T><<<red_grid(S->n), RT, 0, st>>>(S->n, x, r, p, Ap, S->partial.p, S->counter.p, S->scal.p);
+  EX_LAUNCH_CHECK();
+  if ((s = pc_apply<T>(S, r, z, skip, st))) return s;
+  if ((s = dot<T>(S, r, z, FIN_BETA, nullptr, 1, st))) return s;
+  update_p_kernel<T><<<grid_for(S->n, 256), 256, 0, st>>>(S->n, p, z, S->scal.p);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
+int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
+  int s;
+  if (S->op == EXFEM_OP_EBE_F64) {
+    if (!S->Ke) { set_error("solver: stored-Ke operator without Ke"); return EXFEM_ERR_ARG; }
+    s = launch_ebe_diagonal(S->blk, S->Ke, S->diag64.p, st);
+  } else {
+    s = launch_mf_diagonal(S->blk, S->diag64.p, st);
+  }
+  if (s) return s;
+  dinv_kernel<<<grid_for(S->n, 256), 256, 0, st>>>(S->n, S->diag64.p, S->blk->fixed.p, S->dinv64.p, S->dinv32.p);
+  EX_LAUNCH_CHECK();
+  S->diag_ready = true;
+  S->diag_tan_gen = S->blk->tan_gen;
+  S->diag_bc_gen = S->blk->bc_gen;
+  return EXFEM_OK;
+}
+
+// PCG on workspace vectors b (WB) -> x (WX) in precision T
+template <class T>
+static int pcg_run(exfem_solver_s* S, double tol, int maxiter, int* iters, double* relres, cudaStream_t st) {
+  const int64_t n = S->n;
+  const int gi = sizeof(T) == 8 ? 0 : 1;
+  int s;
+  if (S->pc == EXFEM_PC_AMG && !S->amg) { set_error("solver: AMG preconditioner without hierarchy"); return EXFEM_ERR_ARG; }
+  if (S->pc == EXFEM_PC_AMG && (s = amg_prepare(S->amg, sizeof(T) == 8 ? EXFEM_F64 : EXFEM_F32))) return s;
+  const bool stale = !S->diag_ready || S->diag_tan_gen != S->blk->tan_gen || S->diag_bc_gen != S->blk->bc_gen;
+  if (stale && S->pc != EXFEM_PC_NONE && (s = solver_refresh_diagonal(S, st))) return s;
+  T *x = ws<T>(S, WX), *r = ws<T>(S, WR), *z = ws<T>(S, WZ), *p = ws<T>(S, WP), *b = ws<T>(S, WB);
+  init_scal_kernel<<<1, 1, 0, st>>>(S->scal.p, tol, maxiter);
+  EX_LAUNCH_CHECK();
+  EX_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, st));
+  EX_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+  if ((s = dot<T>(S, b, b, FIN_BB, nullptr, 0, st))) return s;
+  if ((s = pc_apply<T>(S, r, z, nullptr, st))) return s;
+  EX_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+  if ((s = dot<T>(S, r, z, FIN_RZ0, nullptr, 0, st))) return s;
+  if ((s = dot<T>(S, r, r, FIN_RR0, nullptr, 0, st))) return s;
+  const int chunk = S->chunk > 0 ? S->chunk : 8;
+  if (S->use_graph) {
+    const double* keptr = S->op == EXFEM_OP_EBE_F64 ? S->Ke : nullptr;
+    if (S->graph_bc_gen != S->blk->bc_gen) {
+      for (auto& ge : S->gexec)
+        if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+      S->graph_bc_gen = S->blk->bc_gen;
+    }
+    if (S->gexec[gi] && S->g_Ke[gi] != keptr) {
+      cudaGraphExecDestroy(S->gexec[gi]);
+      S->gexec[gi] = nullptr;
+    }
+    if (!S->gexec[gi]) {
+      cudaGraph_t g;
+      EX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      int cs = EXFEM_OK;
+      for (int i = 0; i < chunk && !cs; ++i) cs = pcg_iteration<T>(S, st);
+      cudaError_t ce = cudaStreamEndCapture(st, &g);
+      if (cs) { if (ce == cudaSuccess) cudaGraphDestroy(g); return cs; }
+      EX_CUDA(ce);
+      ce = cudaGraphInstantiate(&S->gexec[gi], g, 0);
+      cudaGraphDestroy(g);
+      EX_CUDA(ce);
+      S->g_Ke[gi] = keptr;
+    }
+  }
+  const int max_chunks = maxiter / chunk + 2;
+  for (int c = 0; c < max_chunks; ++c) {
+    EX_CUDA(cudaMemcpyAsync(S->h_scal, S->scal.p, sizeof(PcgScal), cudaMemcpyDeviceToHost, st));
+    EX_CUDA(cudaStreamSynchronize(st));
+    if (S->h_scal->done) break;
+    if (S->use_graph) {
+      EX_CUDA(cudaGraphLaunch(S->gexec[gi], st));
+    } else {
+      for (int i = 0; i < chunk; ++i)
+        if ((s = pcg_iteration<T>(S, st))) return s;
+    }
+  }
+  EX_CUDA(cudaMemcpyAsync(S->h_scal, S->scal.p, sizeof(PcgScal), cudaMemcpyDeviceToHost, st));
+  EX_CUDA(cudaStreamSynchronize(st));
+  const PcgScal& h = *S->h_scal;
+  if (iters) *iters = h.k;
+  const double rel = sqrt(h.rr / fmax(h.bb, 1e-300));
+  if (relres) *relres = rel;
+  return (std::isfinite(rel) && rel <= 1e-3) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
+}
+
+int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters,
+               double* relres, cudaStream_t st) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  int s;
+  if (S->op == EXFEM_OP_MF_F32) {
+    convert_kernel<double, float><<<eg, 256, 0, st>>>(n, b, S->b32.p, 1.0, nullptr);
+    EX_LAUNCH_CHECK();
+    s = pcg_run<float>(S, tol, maxiter, iters, relres, st);
+    if (s < 0) return s;
+    convert_kernel<float, double><<<eg, 256, 0, st>>>(n, S->x32.p, x, 1.0, nullptr);
+    EX_LAUNCH_CHECK();
+    return s;
+  }
+  EX_CUDA(cudaMemcpyAsync(S->b64.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  s = pcg_run<double>(S, tol, maxiter, iters, relres, st);
+  if (s < 0) return s;
+  EX_CUDA(cudaMemcpyAsync(x, S->x64.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  return s;
+}
+
+static int norm64(exfem_solver_s* S, const double* v, double* out, cudaStream_t st) {
+  int s;
+  if ((s = dot<double>(S, v, v, FIN_STORE, S->dscr.p, 0, st))) return s;
+  double h;
+  EX_CUDA(cudaMemcpyAsync(&h, S->dscr.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  EX_CUDA(cudaStreamSynchronize(st));
+  *out = sqrt(h);
+  return EXFEM_OK;
+}
+
+int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, double inner_tol, int max_pass,
+                 int maxiter, int* iters, int* passes, double* relres, cudaStream_t st) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  if (S->op == EXFEM_OP_EBE_F64) {
+    set_error("mixed refinement needs a matrix-free operator (EXFEM_OP_MF_F32)");
+    return EXFEM_ERR_ARG;
+  }
+  // r64 holds the FP64 residual, x the FP64 solution; t64 is scratch for A64(x)
+  int s;
+  EX_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+  EX_CUDA(cudaMemcpyAsync(S->r64.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  double bn;
+  if ((s = norm64(S, b, &bn, st))) return s;
+  if (bn == 0.0) bn = 1.0;
+  int its = 0, p = 0;
+  double rn = bn;
+  for (p = 0; p < max_pass; ++p) {
+    double sc;
+    if ((s = norm64(S, S->r64.p, &sc, st))) return s;
+    if (sc == 0.0) sc = 1.0;
+    convert_kernel<double, float><<<eg, 256, 0, st>>>(n, S->r64.p, S->b32.p, 1.0 / sc, nullptr);
+    EX_LAUNCH_CHECK();
+    int k = 0;
+    double rr;
+    s = pcg_run<float>(S, inner_tol, maxiter, &k, &rr, st);
+    if (s < 0) return s;
+    its += k;
+    axpy_f32_kernel<<<eg, 256, 0, st>>>(n, x, S->x32.p, sc);
+    EX_LAUNCH_CHECK();
+    if ((s = launch_mf_matvec<double>(S->blk, x, S->Ap64.p, nullptr, st))) return s;
+    sub64_kernel<<<eg, 256, 0, st>>>(n, b, S->Ap64.p, S->r64.p);
+    EX_LAUNCH_CHECK();
+    if ((s = norm64(S, S->r64.p, &rn, st))) return s;
+    if (!std::isfinite(rn)) break;
+    if (rn <= tol * bn) { ++p; break; }
+  }
+  if (iters) *iters = its;
+  if (passes) *passes = p;
+  if (relres) *relres = rn / bn;
+  return (std::isfinite(rn) && rn <= tol * bn) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
+}
+
+int solver_alloc(exfem_solver_s* S) {
+  const int64_t n = S->n;
+  int s;
+  DevBuf<double>* v64[] = {&S->x64, &S->r64, &S->z64, &S->p64, &S->Ap64, &S->b64, &S->t64, &S->dinv64, &S->diag64};
+  for (auto* v : v64)
+    if ((s = v->alloc(std::max<int64_t>(n, 1)))) return s;
+  DevBuf<float>* v32[] = {&S->x32, &S->r32, &S->z32, &S->p32, &S->Ap32, &S->b32, &S->t32, &S->dinv32};
+  for (auto* v : v32)
+    if ((s = v->alloc(std::max<int64_t>(n, 1)))) return s;
+  if ((s = S->partial.alloc(RED_MAX_BLOCKS))) return s;
+  if ((s = S->dscr.alloc(4))) return s;
+  if ((s = S->counter.alloc(1))) return s;
+  EX_CUDA(cudaMemset(S->counter.p, 0, sizeof(unsigned)));
+  if ((s = S->scal.alloc(1))) return s;
+  EX_CUDA(cudaMallocHost(&S->h_scal, sizeof(PcgScal)));
+  return EXFEM_OK;
+}
+
+}  // namespace exfem
+
+exfem_solver_s::~exfem_solver_s() {
+  for (auto& g : gexec)
+    if (g) cudaGraphExecDestroy(g);
+  if (h_scal) cudaFreeHost(h_scal);
+}

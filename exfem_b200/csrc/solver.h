@@ -1,0 +1,74 @@
+// AMG hierarchy and solver handle layouts (internal).
+#pragma once
+#include <algorithm>
+#include <memory>
+#include <vector>
+
+#include "internal.h"
+
+namespace exfem {
+
+struct AmgLevel {
+  enum { WB = 0, WX = 1, WR = 2, WD = 3, WD2 = 4, WTMP = 5, NW = 6 };
+  int64_t n = 0, nc = 0;
+  double rho = 1.0;
+  Csr64 A, P, R;
+  DevBuf<double> dinv64;
+  DevBuf<float> dinv32;
+  DevBuf<double> w64[NW];
+  DevBuf<float> w32[NW];
+};
+
+// level-0 operator override: y = A0(x) and its inverse diagonal
+template <class T>
+struct Level0Op {
+  int (*apply)(void* ctx, const T* x, T* y, const int* skip, cudaStream_t s) = nullptr;
+  void* ctx = nullptr;
+  const T* dinv = nullptr;
+};
+
+template <class T>
+int amg_vcycle(exfem_amg_s* h, const T* b, T* x, const Level0Op<T>* op0, const int* skip, cudaStream_t s);
+int amg_prepare(exfem_amg_s* h, int dtype);
+int amg_add_level(exfem_amg_s* h, int64_t n, int64_t nc, const int64_t* Ap, const int32_t* Ai, const double* Av,
+                  const int64_t* Pp, const int32_t* Pi, const double* Pv, const int64_t* Rp, const int32_t* Ri,
+                  const double* Rv, const double* dinv, double rho);
+
+// device scalars of one PCG run (FP64 step scalars and dot products)
+struct PcgScal {
+  double rz, pAp, rr, bb, tol2, alpha, beta, spare;
+  int k, maxiter, done, pad;
+};
+
+}  // namespace exfem
+
+struct exfem_amg_s {
+  int degree = 2;
+  std::vector<std::unique_ptr<exfem::AmgLevel>> levels;
+  int64_t nc = 0;
+  exfem::DevBuf<double> Ainv;
+  exfem::DevBuf<double> cb64, cx64;
+  exfem::DevBuf<float> cb32, cx32;
+};
+
+struct exfem_solver_s {
+  exfem_block_s* blk = nullptr;
+  exfem_amg_s* amg = nullptr;
+  int op = EXFEM_OP_MF_F32, pc = EXFEM_PC_AMG;
+  const double* Ke = nullptr;
+  int64_t n = 0;
+  // workspace
+  exfem::DevBuf<double> x64, r64, z64, p64, Ap64, b64, t64, dinv64, diag64;
+  exfem::DevBuf<float> x32, r32, z32, p32, Ap32, b32, t32, dinv32;
+  exfem::DevBuf<double> partial, dscr;
+  exfem::DevBuf<unsigned> counter;
+  exfem::DevBuf<exfem::PcgScal> scal;
+  exfem::PcgScal* h_scal = nullptr;  // pinned
+  bool diag_ready = false;
+  uint64_t diag_tan_gen = 0, diag_bc_gen = 0, graph_bc_gen = 0;
+  // CUDA graphs of `chunk` PCG iterations, one per precision
+  int use_graph = 1, chunk = 8;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  const double* g_Ke[2] = {nullptr, nullptr};
+  ~exfem_solver_s();
+};

@@ -1,0 +1,380 @@
+"""Linear algebra of the hot path (drop-in for ``gfem.linalg``).
+
+* ``pcg(A, b, M, x0, tol, maxiter) -> (x, k, relres)`` (gfem/linalg.py:21-47).
+  With ``A`` a :class:`NativeSolver` the whole loop runs in the library (device
+  scalars, graph-captured iteration chunks); with plain callables it runs the
+  same recurrence over torch device vectors.
+* ``rigid_body_modes`` (linalg.py:80-98), ``bc_matrix`` (213-217), ``Direct``
+  (199-210, SuperLU on the host, a reference solver for parity), ``csr_to_device``
+  / ``csr_mv`` (51-77).
+* ``AMG(A, X, max_coarse=300, degree=2, presmooth=1, rot_mask=None)``
+  (linalg.py:102-195).  The hierarchy is set up once on the host, as in the
+  reference, then copied to HBM (FP64 and FP32 values) and applied by the
+  library's device V-cycle.  The reference calls PyAMG's
+  ``smoothed_aggregation_solver`` with a BSR matrix, rigid-body near-null space,
+  symmetric strength with theta = 0, standard aggregation, Jacobi prolongation
+  smoothing with omega = 4/3 and local (Gershgorin row-sum) weighting, and
+  ``max_coarse = 300``.  PyAMG is not available here, so this module contains a
+  project-written smoothed-aggregation set-up with those same choices (Vanek,
+  Mandel & Brezina 1996): nodal-block strength graph, 3-pass standard
+  aggregation (native, ``exfem_host_standard_aggregation``), tentative
+  prolongator by per-aggregate orthonormalisation of the near-null space,
+  one Jacobi smoothing step, Galerkin coarse operators R A P with R = P^T.  The
+  reference's own per-level data follow unchanged: inverse diagonal, spectral
+  bound by 15 power iterations from a seed-0 Gaussian vector times 1.1, and a
+  dense Cholesky coarse solve with 1e-13 regularisation.
+"""
+import ctypes as C
+import time
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_ptr
+
+
+# ------------------------------------------------------------------ PCG
+def pcg(A, b, M=None, x0=None, tol=1e-8, maxiter=2000):
+    """Preconditioned CG (gfem/linalg.py:21-47).  ``A`` may be a NativeSolver."""
+    if isinstance(A, NativeSolver):
+        return A.pcg(b, tol=tol, maxiter=maxiter)
+    M = M or (lambda r: r)
+    x = torch.zeros_like(b) if x0 is None else x0.clone()
+    r = b - A(x)
+    z = M(r)
+    p = z.clone()
+    rz = torch.dot(r, z)
+    bn2 = torch.clamp(torch.dot(b, b), min=1e-300)
+    tol2 = tol * tol * bn2
+    rr = torch.dot(r, r)
+    k = 0
+    while bool(rr > tol2) and k < maxiter:
+        Ap = A(p)
+        alpha = rz / torch.dot(p, Ap)
+        x = x + alpha * p
+        r = r - alpha * Ap
+        rr = torch.dot(r, r)
+        z = M(r)
+        rz_new = torch.dot(r, z)
+        p = z + (rz_new / rz) * p
+        rz = rz_new
+        k += 1
+    return x, k, torch.sqrt(rr / bn2)
+
+
+# ------------------------------------------------------------------ CSR helpers
+def csr_to_device(A, ell_max_ratio=2.0):
+    """Device CSR (torch sparse) of a host matrix; the ELL/CSR choice of the
+    reference (linalg.py:51-70) is a JAX gather strategy and has no effect here."""
+    A = A.tocsr()
+    A.sort_indices()
+    t = torch.sparse_csr_tensor(torch.as_tensor(A.indptr, dtype=torch.int64), torch.as_tensor(A.indices, dtype=torch.int64),
+                                torch.as_tensor(A.data), size=A.shape, device="cuda")
+    return dict(csr=t, n=A.shape[0])
+
+
+def csr_mv(M, x, n=None):
+    return (M["csr"] @ x.reshape(-1, 1)).reshape(-1)
+
+
+def rigid_body_modes(X, rot_mask=None):                                # linalg.py:80-98
+    X = np.asarray(X)
+    n = len(X)
+    t = np.ones(n) if rot_mask is None else (~np.asarray(rot_mask)).astype(float)
+    c = (X - X[t > 0].mean(0)) * t[:, None]
+    B = np.zeros((3 * n, 6))
+    for i in range(3):
+        B[i::3, i] = t
+    x, y, z = c[:, 0], c[:, 1], c[:, 2]
+    B[0::3, 3], B[1::3, 3] = -y, x
+    B[1::3, 4], B[2::3, 4] = -z, y
+    B[0::3, 5], B[2::3, 5] = z, -x
+    return B
+
+
+def bc_matrix(A, free):                                                # linalg.py:213-217
+    D = sp.diags(np.asarray(free, float))
+    return (D @ A @ D + sp.diags(1.0 - np.asarray(free, float))).tocsr()
+
+
+class Direct:                                                          # linalg.py:199-210
+    """Host sparse direct solve (SuperLU); a parity reference, not the hot path."""
+
+    def __init__(self, A):
+        self.n = A.shape[0]
+        try:
+            self.lu = spla.splu(A.tocsc(), permc_spec="COLAMD")
+            self._solve = self.lu.solve
+        except RuntimeError:
+            self._solve = spla.factorized(A.tocsc())
+
+    def solve(self, b):
+        return self._solve(np.asarray(b))
+
+
+def ops_assemble(ops, ndof):
+    """Host CSR of element operators [(dofs, Ke)] (gfem/model.py:176-192)."""
+    rows, cols, vals = [], [], []
+    for d, K in ops:
+        d = np.asarray(d.cpu() if isinstance(d, torch.Tensor) else d, dtype=np.int64)
+        K = np.asarray(K.detach().cpu().double() if isinstance(K, torch.Tensor) else K)
+        nd = d.shape[1]
+        rows.append(np.repeat(d, nd, axis=1).ravel())
+        cols.append(np.tile(d, (1, nd)).ravel())
+        vals.append(K.reshape(len(d), -1).ravel())
+    if not rows:
+        return sp.csr_matrix((ndof, ndof))
+    A = sp.coo_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))),
+                      shape=(ndof, ndof)).tocsr()
+    A.sum_duplicates()
+    return A
+
+
+# ------------------------------------------------------------------ smoothed aggregation (host set-up)
+def _strength_graph(A, bs):
+    """Nodal strength graph of A with bs x bs blocks; theta = 0 keeps every block
+    with a nonzero entry (explicit zeros removed first)."""
+    A = A.tocoo()
+    keep = A.data != 0
+    r, c = A.row[keep] // bs, A.col[keep] // bs
+    nb = A.shape[0] // bs
+    S = sp.csr_matrix((np.ones(len(r)), (r, c)), shape=(nb, nb))
+    S.sum_duplicates()
+    S.sort_indices()
+    return S
+
+
+def _aggregate(S):
+    n = S.shape[0]
+    ptr_ = np.ascontiguousarray(S.indptr.astype(np.int64))
+    idx = np.ascontiguousarray(S.indices.astype(np.int32))
+    agg = np.empty(n, np.int32)
+    nagg = C.c_int64()
+    check(lib.exfem_host_standard_aggregation(n, ptr_.ctypes.data, idx.ctypes.data, agg.ctypes.data, C.byref(nagg)))
+    return agg, int(nagg.value)
+
+
+def _fit_candidates(agg, nagg, B, bs, drop=1e-10):
+    """Tentative prolongator T (n x nagg*K) and coarse near-null space Bc (nagg*K x K):
+    per aggregate, modified Gram-Schmidt of the near-null-space rows of its DOFs;
+    columns that vanish (relative norm < drop) are zeroed."""
+    n, K = B.shape
+    node = np.arange(n) // bs
+    a_of = agg[node]
+    member = a_of >= 0
+    dofs = np.nonzero(member)[0]
+    order = np.argsort(a_of[dofs], kind="stable")
+    dofs = dofs[order]
+    a_sorted = a_of[dofs]
+    counts = np.bincount(a_sorted, minlength=nagg)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    Bc = np.zeros((nagg * K, K))
+    Ti, Tj, Tv = [], [], []
+    for m in np.unique(counts[counts > 0]):
+        aggs = np.nonzero(counts == m)[0]
+        rows = dofs[starts[aggs][:, None] + np.arange(m)[None, :]]          # (g, m)
+        Q = B[rows].copy()                                                  # (g, m, K)
+        R = np.zeros((len(aggs), K, K))
+        n0 = np.linalg.norm(Q, axis=1) + 1e-300                             # (g, K)
+        for j in range(K):
+            for i in range(j):
+                rij = np.einsum("gm,gm->g", Q[:, :, i], Q[:, :, j])
+                R[:, i, j] = rij
+                Q[:, :, j] -= rij[:, None] * Q[:, :, i]
+            nj = np.linalg.norm(Q[:, :, j], axis=1)
+            ok = nj > drop * n0[:, j]
+            R[:, j, j] = np.where(ok, nj, 0.0)
+            Q[:, :, j] = np.where(ok[:, None], Q[:, :, j] / np.where(ok, nj, 1.0)[:, None], 0.0)
+        for g, a in enumerate(aggs):
+            Bc[a * K:(a + 1) * K] = R[g]
+        Ti.append(np.repeat(rows, K, axis=1).ravel())
+        Tj.append((aggs[:, None, None] * K + np.arange(K)[None, None, :]).repeat(m, axis=1).reshape(len(aggs), -1).ravel())
+        Tv.append(Q.reshape(len(aggs), -1).ravel())
+    T = sp.csr_matrix((np.concatenate(Tv), (np.concatenate(Ti), np.concatenate(Tj))), shape=(n, nagg * K))
+    T.eliminate_zeros()
+    return T, Bc
+
+
+def sa_hierarchy(A, B, bs=3, max_coarse=300, max_levels=10, omega=4.0 / 3.0):
+    """Smoothed-aggregation hierarchy: list of (A, P) and the coarsest matrix."""
+    A = A.tocsr()
+    A.eliminate_zeros()
+    levels = []
+    while A.shape[0] > max_coarse and len(levels) < max_levels - 1:
+        S = _strength_graph(A, bs)
+        agg, nagg = _aggregate(S)
+        if nagg == 0:
+            break
+        T, Bc = _fit_candidates(agg, nagg, B, bs)
+        D = np.asarray(abs(A).sum(axis=1)).ravel()
+        Dinv = np.where(D != 0, 1.0 / np.where(D != 0, D, 1.0), 0.0)
+        P = (T - omega * (sp.diags(Dinv) @ (A @ T))).tocsr()
+        P.eliminate_zeros()
+        R = P.T.tocsr()
+        Ac = (R @ A @ P).tocsr()
+        Ac.eliminate_zeros()
+        levels.append((A, P))
+        if Ac.shape[0] >= A.shape[0]:
+            A = Ac
+            break
+        A, B, bs = Ac, Bc, B.shape[1]
+    return levels, A
+
+
+def _rho(A, dinv, it=15):                                              # linalg.py:138-146
+    x = np.random.default_rng(0).standard_normal(A.shape[0])
+    lam = 1.0
+    for _ in range(it):
+        y = dinv * (A @ x)
+        lam = np.linalg.norm(y) / max(np.linalg.norm(x), 1e-300)
+        x = y / max(np.linalg.norm(y), 1e-300)
+    return 1.1 * lam
+
+
+def _csr_parts(M):
+    M = M.tocsr()
+    M.sort_indices()
+    return (np.ascontiguousarray(M.indptr.astype(np.int64)), np.ascontiguousarray(M.indices.astype(np.int32)),
+            np.ascontiguousarray(M.data.astype(np.float64)))
+
+
+class AMG:
+    """Smoothed-aggregation AMG: host set-up, device V-cycle (gfem/linalg.py:102-195)."""
+
+    def __init__(self, A, X=None, max_coarse=300, degree=2, presmooth=1, rot_mask=None):
+        t0 = time.time()
+        A = A.tocsr()
+        n = A.shape[0]
+        if X is not None and n == 3 * len(X):
+            B, bs = rigid_body_modes(X, rot_mask), 3
+        else:
+            B, bs = np.ones((n, 1)), 1
+        sa_levels, Ac = sa_hierarchy(A, B, bs, max_coarse)
+        self.levels = []
+        for Al, P in sa_levels:
+            d = Al.diagonal()
+            dinv = np.where(np.abs(d) > 0, 1.0 / np.where(d == 0, 1, d), 0.0)
+            self.levels.append(dict(A=Al, P=P, R=P.T.tocsr(), dinv=dinv, rho=float(_rho(Al, dinv)),
+                                    n=Al.shape[0], nc=P.shape[1]))
+        Acd = Ac.toarray()
+        Acd = 0.5 * (Acd + Acd.T)
+        try:
+            Lc = np.linalg.cholesky(Acd + 1e-13 * np.abs(Acd).max() * np.eye(len(Acd)))
+        except np.linalg.LinAlgError:
+            w, V = np.linalg.eigh(Acd)
+            Lc = np.linalg.cholesky(V @ np.diag(np.maximum(w, 1e-12 * w.max())) @ V.T)
+        self.coarse = Lc
+        Linv = np.linalg.inv(Lc)
+        self.coarse_inv = np.ascontiguousarray(Linv.T @ Linv)
+        self.degree, self.presmooth = degree, presmooth
+        nnz = [lv["A"].nnz for lv in self.levels] + [int(np.count_nonzero(Acd))]
+        self.sizes = [lv["n"] for lv in self.levels] + [Acd.shape[0]]
+        self.complexity = float(sum(nnz) / max(nnz[0], 1))
+        self.nlevels = len(self.sizes)
+        self.setup_time = time.time() - t0
+        self._upload()
+
+    def _upload(self):
+        _lib.require_cuda()
+        h = C.c_void_p()
+        check(lib.exfem_amg_create(C.byref(h)))
+        self._h = h
+        for lv in self.levels:
+            Ap, Ai, Av = _csr_parts(lv["A"])
+            Pp, Pi, Pv = _csr_parts(lv["P"])
+            Rp, Ri, Rv = _csr_parts(lv["R"])
+            dinv = np.ascontiguousarray(lv["dinv"], dtype=np.float64)
+            check(lib.exfem_amg_add_level(h, lv["n"], lv["nc"], Ap.ctypes.data, Ai.ctypes.data, Av.ctypes.data,
+                                          Pp.ctypes.data, Pi.ctypes.data, Pv.ctypes.data, Rp.ctypes.data,
+                                          Ri.ctypes.data, Rv.ctypes.data, dinv.ctypes.data, lv["rho"]))
+        check(lib.exfem_amg_set_coarse(h, self.coarse_inv.shape[0], self.coarse_inv.ctypes.data))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.exfem_amg_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        return f"AMG levels={self.nlevels} sizes={self.sizes} op.complexity={self.complexity:.2f}"
+
+    def params(self):
+        return dict(handle=self._h)
+
+    def vcycle(self, r, level0=None, dinv0=None):
+        """z = M(r): one device V-cycle in r's precision (FP64 or FP32); ``level0``
+        is an optional Block whose matrix-free tangent smooths level 0 with the
+        inverse diagonal ``dinv0`` (gfem/solvers.py:311-314)."""
+        r = r.contiguous()
+        code = _lib.F64 if r.dtype == torch.float64 else _lib.F32
+        z = torch.empty_like(r)
+        check(lib.exfem_amg_vcycle(self._h, code, ptr(r), ptr(z), level0.handle if level0 is not None else None,
+                                   ptr(dinv0.to(r.dtype).contiguous()) if dinv0 is not None else None, stream_ptr()))
+        return z
+
+    def make(self):
+        """precond(params, r, A0=None, dinv0=None) as in gfem/linalg.py:156-195;
+        ``A0`` may be a Block (matrix-free level 0) or None (stored level-0 matrix)."""
+        def precond(p, r, A0=None, dinv0=None):
+            if A0 is not None and not hasattr(A0, "handle"):
+                raise NotImplementedError("level-0 override must be a Block (matrix-free tangent)")
+            return self.vcycle(r, A0, dinv0)
+        return precond
+
+
+# ------------------------------------------------------------------ native solver
+class NativeSolver:
+    """PCG / mixed-precision refinement in the library for one block.
+
+    op: "ebe64" (stored Ke, FP64), "mf64" (matrix-free FP64), "mf32" (matrix-free
+    FP32); pc: "none", "jacobi", "amg"."""
+
+    OPS = {"ebe64": _lib.OP_EBE_F64, "mf64": _lib.OP_MF_F64, "mf32": _lib.OP_MF_F32}
+    PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG}
+
+    def __init__(self, block, op="mf32", pc="amg", amg=None, graph=True, chunk=8):
+        self.block, self.amg = block, amg
+        self.op, self.pc = op, pc
+        h = C.c_void_p()
+        check(lib.exfem_solver_create(block.handle, self.OPS[op], self.PCS[pc],
+                                      amg.handle if amg is not None else None, C.byref(h)))
+        self._h = h
+        check(lib.exfem_solver_set_graph(h, 1 if graph else 0, chunk))
+        self._Ke = None
+        self.last_iters = 0
+        self.last_passes = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.exfem_solver_destroy(h)
+            self._h = None
+
+    def set_ke(self, Ke):
+        self._Ke = Ke.contiguous()
+        check(lib.exfem_solver_set_ke(self._h, ptr(self._Ke)))
+
+    def pcg(self, b, tol=1e-8, maxiter=2000):
+        b = b.to(torch.float64).contiguous()
+        x = torch.empty_like(b)
+        k, rr = C.c_int(), C.c_double()
+        check(lib.exfem_solver_pcg(self._h, ptr(b), ptr(x), float(tol), int(maxiter), C.byref(k), C.byref(rr),
+                                   stream_ptr()))
+        self.last_iters = k.value
+        return x, k.value, rr.value
+
+    def mixed(self, b, tol=1e-8, inner_tol=2e-5, max_pass=12, maxiter=20000):
+        b = b.to(torch.float64).contiguous()
+        x = torch.empty_like(b)
+        k, p, rr = C.c_int(), C.c_int(), C.c_double()
+        check(lib.exfem_solver_mixed(self._h, ptr(b), ptr(x), float(tol), float(inner_tol), int(max_pass),
+                                     int(maxiter), C.byref(k), C.byref(p), C.byref(rr), stream_ptr()))
+        self.last_iters, self.last_passes = k.value, p.value
+        return x, k.value, p.value, rr.value

@@ -1,0 +1,309 @@
+"""Model and element blocks on the GPU (drop-in for the solid-block part of ``gfem.model``).
+
+Layout (gfem/model.py:1-11): one block = one element type + one material; every
+element kernel is one launch over all elements of a block.  Each ``Block`` owns a
+library handle holding, in HBM, the node coordinates, the connectivity, the
+gather plan (bit-identical to gfem/model.py:241-261), an element colouring, the
+per-element geometry streams of the matrix-free operator (FP32 and FP64) and,
+for J2, the per-Gauss-point consistent-tangent data.
+
+Public methods keep the reference's names and argument meaning:
+``Model.internal_force(u, states, fields) -> (f, new_states)`` (model.py:466-477),
+``element_stiffness`` (479-483), ``stiffness_ops -> [(dofs, Ke)]`` (485-486),
+``tangent_jvp(u, states, v, fields)`` (488-490), ``matvec``/``diagonal``
+(495-499), ``stresses`` (530-539), ``gather`` (421-429), ``init_state`` (380-381);
+``Block.force``/``Block.stiff`` accept the reference's per-element gathered
+arrays (model.py:70-111, 146-147).  Arrays are torch CUDA FP64 tensors (numpy
+inputs are moved to the device).  There is no CPU path.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib, ptr, stream_ptr
+
+
+def _dev(x, dtype=torch.float64):
+    if isinstance(x, torch.Tensor):
+        return x.to(device="cuda", dtype=dtype).contiguous()
+    return torch.as_tensor(np.asarray(x), dtype=dtype, device="cuda").contiguous()
+
+
+class Block:
+    """Element block bound to node coordinates ``X`` (library handle)."""
+
+    def __init__(self, conn, etype, material, X, name="block"):
+        _lib.require_cuda()
+        self.conn = np.ascontiguousarray(np.asarray(conn, dtype=np.int32))
+        self.etype, self.material, self.name = etype, material, name
+        self.ne = int(self.conn.shape[0])
+        X = np.ascontiguousarray(np.asarray(X, dtype=np.float64))
+        self.nn = int(X.shape[0])
+        if self.ne and self.conn.shape[1] != etype.nnode:
+            raise ValueError(f"{etype.name} needs {etype.nnode} nodes per element, got {self.conn.shape[1]}")
+        h = C.c_void_p()
+        m = material.to_c()
+        check(lib.exfem_block_create(etype.code, C.byref(m), self.nn, X.ctypes.data, self.ne,
+                                     self.conn.ctypes.data if self.ne else None, C.byref(h)))
+        self._h = h
+        self._scale_key = None
+        self._fixed_key = None
+        self.conn_dev = torch.as_tensor(self.conn, device="cuda")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            lib.exfem_block_destroy(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---------------- info and index maps
+    def query(self):
+        ne, nn, vmax, ncol, aff, nb = C.c_int64(), C.c_int64(), C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        nnode, ngp, ns = C.c_int(), C.c_int(), C.c_int()
+        check(lib.exfem_block_query(self._h, C.byref(ne), C.byref(nn), C.byref(nnode), C.byref(ngp), C.byref(ns),
+                                    C.byref(vmax), C.byref(ncol), C.byref(aff), C.byref(nb)))
+        return dict(ne=ne.value, nn=nn.value, nnode=nnode.value, ngp=ngp.value, nstate=ns.value,
+                    vmax=vmax.value, ncolour=ncol.value, affine=bool(aff.value), device_bytes=nb.value)
+
+    def gather_plan(self):
+        q = self.query()
+        out = np.empty((self.nn, q["vmax"]), np.int32)
+        check(lib.exfem_block_gather_plan(self._h, out.ctypes.data))
+        return out
+
+    def colours(self):
+        out = np.empty(self.ne, np.int32)
+        check(lib.exfem_block_colours(self._h, out.ctypes.data))
+        return out
+
+    def init_state(self):                                              # model.py:154-155
+        return torch.zeros((self.ne, self.etype.ngp, self.material.nstate), dtype=torch.float64, device="cuda")
+
+    def dofs(self):                                                    # model.py:157-158
+        return (self.conn_dev.long()[:, :, None] * 3 + torch.arange(3, device="cuda")).reshape(self.ne, -1)
+
+    # ---------------- parameters
+    def set_scale(self, scale):
+        """Per-element stiffness scale (fields["scale"], model.py:449-463)."""
+        if scale is None:
+            if self._scale_key is not None:
+                check(lib.exfem_block_set_scale(self._h, None))
+                self._scale_key = None
+            return
+        s = np.ascontiguousarray(np.asarray(scale.cpu() if isinstance(scale, torch.Tensor) else scale,
+                                            dtype=np.float64).reshape(-1))
+        key = (s.size, hash(s.tobytes()))
+        if key != self._scale_key:
+            check(lib.exfem_block_set_scale(self._h, s.ctypes.data))
+            self._scale_key = key
+
+    def set_fixed(self, fixed):
+        """Prescribed-DOF mask (ndof of this block's node set) used by opA."""
+        if fixed is None:
+            if self._fixed_key is not None:
+                check(lib.exfem_block_set_fixed(self._h, None))
+                self._fixed_key = None
+            return
+        f = np.ascontiguousarray(np.asarray(fixed).astype(np.uint8).reshape(-1))
+        key = hash(f.tobytes())
+        if key != self._fixed_key:
+            check(lib.exfem_block_set_fixed(self._h, f.ctypes.data))
+            self._fixed_key = key
+
+    # ---------------- kernels on global vectors
+    def internal_force(self, u, state, assembly=_lib.ASSEMBLE_GATHER, fe=None):
+        u = _dev(u)
+        j2 = self.material.nstate > 1
+        s_old = _dev(state) if j2 else None
+        s_new = torch.empty_like(s_old) if j2 else None
+        f = torch.empty(3 * self.nn, dtype=torch.float64, device="cuda")
+        check(lib.exfem_internal_force(self._h, ptr(u), ptr(s_old), ptr(s_new), ptr(fe), ptr(f), assembly,
+                                       stream_ptr()))
+        return f, (s_new if j2 else state)
+
+    def stiffness(self, u, state, dtype=torch.float64):
+        code = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.bfloat16: _lib.BF16}[dtype]
+        u = _dev(u)
+        s_old = _dev(state) if self.material.nstate > 1 else None
+        nd = self.etype.nd
+        Ke = torch.empty((self.ne, nd, nd), dtype=dtype, device="cuda")
+        check(lib.exfem_element_stiffness(self._h, ptr(u), ptr(s_old), code, ptr(Ke), stream_ptr()))
+        return Ke
+
+    def tangent_update(self, u, state):
+        if self.material.nstate > 1:
+            check(lib.exfem_tangent_update(self._h, ptr(_dev(u)), ptr(_dev(state)), stream_ptr()))
+
+    def tangent_matvec(self, v, out=None, apply_bc=True):
+        v = v.contiguous()
+        code = _lib.F64 if v.dtype == torch.float64 else _lib.F32
+        y = torch.empty_like(v) if out is None else out
+        check(lib.exfem_tangent_matvec(self._h, code, ptr(v), ptr(y), 1 if apply_bc else 0, stream_ptr()))
+        return y
+
+    def tangent_diagonal(self):
+        d = torch.empty(3 * self.nn, dtype=torch.float64, device="cuda")
+        check(lib.exfem_tangent_diagonal(self._h, ptr(d), stream_ptr()))
+        return d
+
+    def ebe_matvec(self, Ke, v, apply_bc=True):
+        v = _dev(v)
+        y = torch.empty_like(v)
+        check(lib.exfem_ebe_matvec(self._h, ptr(Ke.contiguous()), ptr(v), ptr(y), 1 if apply_bc else 0, stream_ptr()))
+        return y
+
+    def ebe_diagonal(self, Ke):
+        d = torch.empty(3 * self.nn, dtype=torch.float64, device="cuda")
+        check(lib.exfem_ebe_diagonal(self._h, ptr(Ke.contiguous()), ptr(d), stream_ptr()))
+        return d
+
+    def cauchy(self, u, state):
+        S = torch.empty((self.ne, 3, 3), dtype=torch.float64, device="cuda")
+        mises = torch.empty(self.ne, dtype=torch.float64, device="cuda")
+        peeq = torch.empty(self.ne, dtype=torch.float64, device="cuda")
+        s = _dev(state) if self.material.nstate > 1 else None
+        check(lib.exfem_stresses(self._h, ptr(_dev(u)), ptr(s), ptr(S), ptr(mises), ptr(peeq), stream_ptr()))
+        return S, mises, peeq
+
+    # ---------------- reference per-element signatures (model.py:70-111)
+    @staticmethod
+    def _disjoint(etype, material, Xe):
+        ne, nnode = Xe.shape[0], Xe.shape[1]
+        conn = np.arange(ne * nnode, dtype=np.int32).reshape(ne, nnode)
+        return Block(conn, etype, material, np.asarray(Xe.detach().cpu() if isinstance(Xe, torch.Tensor) else Xe,
+                                                       dtype=np.float64).reshape(-1, 3))
+
+    def force(self, Xe, ue, se=None, Te=None, scv=None):
+        """Element forces from gathered arrays Xe, ue (ne, nnode, 3): (fe, s_new)."""
+        b = Block._disjoint(self.etype, self.material, Xe)
+        if scv is not None:
+            b.set_scale(np.asarray(torch.as_tensor(scv)[:, 0].cpu()))
+        st = se if se is not None else b.init_state()
+        fe = torch.empty((b.ne, self.etype.nnode, 3), dtype=torch.float64, device="cuda")
+        _, sn = b.internal_force(_dev(ue).reshape(-1), st, fe=fe)
+        return fe, sn
+
+    def stiff(self, Xe, ue, se=None, Te=None, scv=None):
+        """Element tangents from gathered arrays: Ke (ne, nd, nd)."""
+        b = Block._disjoint(self.etype, self.material, Xe)
+        if scv is not None:
+            b.set_scale(np.asarray(torch.as_tensor(scv)[:, 0].cpu()))
+        st = se if se is not None else b.init_state()
+        return b.stiffness(_dev(ue).reshape(-1), st)
+
+
+class Model:
+    """Nodes + element blocks (gfem/model.py:270-539, solid blocks)."""
+
+    def __init__(self, nodes):
+        self.X = np.ascontiguousarray(np.asarray(nodes, dtype=np.float64))
+        self.nn = int(self.X.shape[0])
+        self.ndof = 3 * self.nn
+        self.blocks = []
+        self.nsets, self.elsets, self.surfaces = {}, {}, {}
+        self.constraints, self.interactions = [], []
+        self.rot_of = {}
+        self.T0 = None
+
+    def add_block(self, conn, etype, material, name=None):
+        b = Block(conn, etype, material, self.X, name or f"block{len(self.blocks)}")
+        self.blocks.append(b)
+        return b
+
+    def init_state(self):
+        return [b.init_state() for b in self.blocks]
+
+    def gather(self):
+        if len(self.blocks) != 1:
+            raise NotImplementedError("gather plan export covers single-block models")
+        return self.blocks[0].gather_plan()
+
+    def dof(self, nodes, d):
+        return np.asarray(nodes, dtype=np.int64).ravel() * 3 + d
+
+    def rot_mask(self):
+        return np.zeros(self.nn, bool)
+
+    @property
+    def nelem(self):
+        return sum(b.ne for b in self.blocks)
+
+    def default_fields(self):
+        return dict(scale=[None] * len(self.blocks))
+
+    def _apply_fields(self, fields):
+        sc = (fields or {}).get("scale") or [None] * len(self.blocks)
+        for b, s in zip(self.blocks, sc):
+            b.set_scale(s)
+
+    # ---------- global operators
+    def internal_force(self, u, states, fields=None, assembly=_lib.ASSEMBLE_GATHER):
+        self._apply_fields(fields)
+        u = _dev(u)
+        f, new = None, []
+        for b, s in zip(self.blocks, states):
+            fb, sn = b.internal_force(u, s, assembly)
+            f = fb if f is None else f + fb
+            new.append(sn)
+        if f is None:
+            f = torch.zeros(self.ndof, dtype=torch.float64, device="cuda")
+        return f, new
+
+    def element_stiffness(self, u, states, fields=None, dtype=torch.float64):
+        self._apply_fields(fields)
+        u = _dev(u)
+        return [b.stiffness(u, s, dtype) for b, s in zip(self.blocks, states)]
+
+    def stiffness_ops(self, u, states, fields=None):
+        return list(zip([b.dofs() for b in self.blocks], self.element_stiffness(u, states, fields)))
+
+    def tangent_update(self, u, states, fields=None):
+        self._apply_fields(fields)
+        u = _dev(u)
+        for b, s in zip(self.blocks, states):
+            b.tangent_update(u, s)
+
+    def tangent_jvp(self, u, states, v, fields=None):
+        """K(u) v with the matrix-free tangent (no boundary conditions applied)."""
+        self.tangent_update(u, states, fields)
+        v = _dev(v)
+        out = None
+        for b in self.blocks:
+            y = b.tangent_matvec(v, apply_bc=False)
+            out = y if out is None else out + y
+        return out
+
+    def matvec(self, Kes, v):
+        v = _dev(v)
+        out = None
+        for b, K in zip(self.blocks, Kes):
+            y = b.ebe_matvec(K, v, apply_bc=False)
+            out = y if out is None else out + y
+        return out
+
+    def diagonal(self, Kes):
+        out = None
+        for b, K in zip(self.blocks, Kes):
+            d = b.ebe_diagonal(K)
+            out = d if out is None else out + d
+        return out
+
+    def stresses(self, u, states, fields=None):
+        self._apply_fields(fields)
+        out = []
+        for b, s in zip(self.blocks, states):
+            S, mises, peeq = b.cauchy(u, s)
+            out.append(dict(S=S, MISES=mises, PEEQ=peeq))
+        return out
+
+    def summary(self):
+        lines = [f"{self.nn} nodes, {self.nelem} elements, {self.ndof} dofs"]
+        for b in self.blocks:
+            lines.append(f"  {b.name}: {b.ne} x {b.etype.name}, {b.material.describe()}")
+        return "\n".join(lines)

@@ -1,0 +1,357 @@
+"""Quasi-static Newton procedure over the device hot path (drop-in for the
+``StaticSolver`` part of ``gfem.solvers``).
+
+* ``Monitor``, ``Step``, ``State`` — gfem/solvers.py:24-95 (the fields the
+  static procedure uses).
+* ``_Setup`` — gfem/solvers.py:104-217 for MPC-free, amplitude-free steps:
+  fixed mask, prescribed values ramped from the step's start state, load groups
+  summed with ``np.add.at``, precomputed load vectors (``dloads``).
+* ``_LinearSystem`` — gfem/solvers.py:235-477.  Methods:
+    "direct"  host sparse LU of the assembled tangent (a reference solver);
+    "amg"     plain FP64 path: FP64 operator (stored Ke, or matrix-free with
+              ``tangent="mf"``) + FP64 AMG V-cycle, PCG in the library;
+    "jacobi"  FP64 operator + Jacobi PCG;
+    "mixed"   FP32 matrix-free operator + FP32 V-cycle (FP64 coarse solve)
+              inside FP64 iterative refinement with an FP64 matrix-free residual
+              (solvers.py:344-384);
+    "auto"    direct up to 20000 DOFs, else amg (the reference's GPU rule).
+  The hierarchy is built on the first solve of a step from the assembled FP64
+  tangent, frozen across Newton iterations and increments, and rebuilt when the
+  PCG iteration count exceeds 4x the first one (solvers.py:442-470); level 0 is
+  always smoothed with the current operator (solvers.py:311-314).
+* ``StaticSolver`` — gfem/solvers.py:481-683: automatic incrementation (x1.5
+  growth after <= 5 iterations, x0.25 cutback), tangent predictor, Newton with
+  the reference convergence test and a 4-step backtracking line search.
+
+``tangent="ebe"`` stores element tangents Ke (the reference default);
+``tangent="mf"`` (alias "jvp") keeps the tangent matrix-free: the force kernel
+leaves per-Gauss-point consistent-tangent data in HBM and every product is
+evaluated element by element (the B200 replacement of ``Model.tangent_jvp``).
+"""
+import time
+
+import numpy as np
+import torch
+
+from . import linalg
+from .linalg import NativeSolver
+
+
+class Monitor:                                                          # solvers.py:24-45
+    def __init__(self, verbose=True):
+        self.verbose = verbose
+        self.stop = False
+
+    def log(self, msg):
+        if self.verbose:
+            print(msg, flush=True)
+
+    def iteration(self, **kw):
+        pass
+
+    def increment(self, **kw):
+        pass
+
+    def frame(self, t, u, states, **kw):
+        pass
+
+    def should_stop(self):
+        return self.stop
+
+
+class Step:                                                             # solvers.py:48-80
+    def __init__(self, name="Step-1", kind="static", time_period=1.0, dt_init=None, dt_min=None, dt_max=None,
+                 max_inc=1000, bcs=(), loads=(), dloads=(), **kw):
+        self.name, self.kind, self.T = name, kind, float(time_period)
+        self.dt_init = dt_init or self.T
+        self.dt_min = dt_min if dt_min is not None else 1e-5 * self.T
+        self.dt_max = dt_max or self.T
+        self.max_inc = max_inc
+        self.bcs, self.loads, self.dloads = list(bcs), list(loads), list(dloads)
+        self.output_every = kw.get("output_every", 1)
+
+
+class State:                                                            # solvers.py:83-95
+    def __init__(self, model):
+        self.u = torch.zeros(model.ndof, dtype=torch.float64, device="cuda")
+        self.states = model.init_state()
+        self.fext = torch.zeros(model.ndof, dtype=torch.float64, device="cuda")
+        self.time = 0.0
+        self.reactions = torch.zeros(model.ndof, dtype=torch.float64, device="cuda")
+
+
+def _ramp(t, T):                                                        # solvers.py:220-221
+    return min(max(t / T, 0.0), 1.0) if T > 0 else 1.0
+
+
+class _Setup:                                                           # solvers.py:104-217
+    def __init__(self, model, step, state):
+        nd = model.ndof
+        self.step = step
+        self.fixed = np.zeros(nd, bool)
+        self.target = np.zeros(nd)
+        for bc in step.bcs:
+            nodes, dof, val = bc[:3]
+            d = model.dof(nodes, dof)
+            self.fixed[d] = True
+            self.target[d] = val
+        g = np.zeros(nd)
+        for ld in step.loads:
+            nodes, dof, val = ld[:3]
+            np.add.at(g, model.dof(nodes, dof), val)
+        for dl in step.dloads:
+            vec = dl[0] if isinstance(dl, (tuple, list)) else dl
+            g += np.asarray(vec.cpu() if isinstance(vec, torch.Tensor) else vec, float)
+        self.group = torch.as_tensor(g, device="cuda")
+        self.fprev = state.fext
+        self.ustart = state.u.clone()
+        self.free_np = (~self.fixed).astype(float)
+        self.free = torch.as_tensor(self.free_np, device="cuda")
+        self.fixed_j = torch.as_tensor(self.fixed, device="cuda")
+        self.target_j = torch.as_tensor(self.target, device="cuda")
+
+    def fext(self, t):
+        r = _ramp(t, self.step.T)
+        return self.fprev * (1 - r) + self.group * r
+
+    def fext_final(self):
+        return self.fext(self.step.T)
+
+    def prescribed(self, t):
+        r = _ramp(t, self.step.T)
+        tgt = self.ustart + (self.target_j - self.ustart) * r
+        return torch.where(self.fixed_j, tgt, torch.zeros_like(tgt))
+
+
+class _LinearSystem:                                                    # solvers.py:235-477
+    """Solves (free K free + fixed I) x = b with the chosen back-end."""
+
+    def __init__(self, model, method="auto", tangent="ebe", cg_tol=1e-9, cg_maxiter=20000, monitor=None,
+                 graph=True):
+        self.m = model
+        if method == "auto":
+            method = "direct" if model.ndof <= 20000 else "amg"
+        if method not in ("direct", "amg", "jacobi", "mixed"):
+            raise ValueError(f"unknown linear solver {method!r}")
+        if len(model.blocks) != 1:
+            raise NotImplementedError("the device linear solvers cover single-block models")
+        self.method = method
+        self.tangent = "mf" if tangent in ("mf", "jvp") or method == "mixed" else "ebe"
+        self.cg_tol, self.cg_maxiter = cg_tol, cg_maxiter
+        self.mon = monitor or Monitor(False)
+        self.graph = graph
+        self.amg = None
+        self.amg_iters0 = None
+        self.last_iters = 0
+        self.last_passes = 0
+        self._solvers = {}
+
+    def reset(self):
+        self.amg = None
+        self.amg_iters0 = None
+        self._solvers = {}
+
+    def _solver(self, op, pc):
+        key = (op, pc, id(self.amg))
+        s = self._solvers.get(key)
+        if s is None:
+            s = NativeSolver(self.m.blocks[0], op, pc, self.amg if pc == "amg" else None, graph=self.graph)
+            self._solvers = {k: v for k, v in self._solvers.items() if k[2] == id(self.amg)}
+            self._solvers[key] = s
+        return s
+
+    def assemble(self, ops, setup):
+        A = linalg.ops_assemble(ops, self.m.ndof)
+        return linalg.bc_matrix(A, setup.free_np)
+
+    def _setup_ops(self, ops, ctx):
+        """Element tangents for assembly: the stored ops, or a stiffness evaluation at
+        the matrix-free operator's state."""
+        if isinstance(ops, list):
+            return ops
+        u, s, fields = ctx
+        return self.m.stiffness_ops(u, s, fields)
+
+    def _build_amg(self, ops, setup, ctx):
+        t0 = time.time()
+        A = self.assemble(self._setup_ops(ops, ctx), setup)
+        self.amg = linalg.AMG(A, self.m.X)
+        self.amg_iters0 = None
+        self._solvers = {}
+        self.mon.log(f"    {self.amg.info()}  setup {time.time() - t0:.2f}s")
+
+    def solve(self, ops, b, setup, jvp_args=None, rebuild=False):
+        """ops: [(dofs, Ke)] (tangent="ebe") or None with jvp_args = (u, states, fields)
+        (tangent="mf"; the block's tangent data must be current)."""
+        blk = self.m.blocks[0]
+        blk.set_fixed(setup.fixed)
+        b = b.to(torch.float64)
+        if self.method == "direct":
+            A = self.assemble(self._setup_ops(ops, jvp_args), setup)
+            x = linalg.Direct(A).solve(b.cpu().numpy())
+            self.last_iters = 1
+            return torch.as_tensor(x, device="cuda")
+        if self.method in ("amg", "mixed") and (self.amg is None or rebuild):
+            self._build_amg(ops, setup, jvp_args)
+        if self.method == "mixed":
+            S = self._solver("mf32", "amg")
+            x, k, p, rel = S.mixed(b, tol=self.cg_tol, maxiter=self.cg_maxiter)
+            self.last_iters, self.last_passes = k, p
+            if not np.isfinite(rel) or rel > max(self.cg_tol * 10, 1e-3):
+                self.mon.log(f"    warning: mixed refinement not converged ({k} it, {p} passes, rel.res {rel:.2e})")
+            return x
+        op = "ebe64" if self.tangent == "ebe" else "mf64"
+        pc = "jacobi" if self.method == "jacobi" else "amg"
+        S = self._solver(op, pc)
+        if op == "ebe64":
+            S.set_ke(ops[0][1])
+        x, k, rr = S.pcg(b, tol=self.cg_tol, maxiter=self.cg_maxiter)
+        if pc == "amg":
+            if self.amg_iters0 is None:
+                self.amg_iters0 = max(k, 5)
+            elif k > 4 * self.amg_iters0 and not rebuild:
+                return self.solve(ops, b, setup, jvp_args, rebuild=True)
+        self.last_iters = k
+        if not np.isfinite(rr) or rr > 1e-3:
+            self.mon.log(f"    warning: PCG not converged ({k} it, rel.res {rr:.2e})")
+        return x
+
+
+class StaticSolver:                                                     # solvers.py:481-683
+    def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
+                 cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True):
+        self.m, self.rtol, self.max_iter = model, rtol, max_iter
+        self.mon = monitor or Monitor(verbose)
+        self.line_search = line_search
+        self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph)
+        self.newton_iterations = 0
+
+    def _fields(self, scale=None):
+        return dict(scale=scale)
+
+    def _fint(self, u, s, fields):
+        return self.m.internal_force(u, s, fields)
+
+    def _ops(self, u, s, fields):
+        if self.lin.tangent == "mf":
+            self.m.tangent_update(u, s, fields)
+            return None
+        return self.m.stiffness_ops(u, s, fields)
+
+    def _linsolve(self, u, s, fields, b, setup):
+        ops = self._ops(u, s, fields)
+        return self.lin.solve(ops, b, setup, (u, s, fields) if ops is None else None)
+
+    def solve(self, step, u0=None, states=None, fext0=None, callback=None, state=None, scale=None):
+        m = self.m
+        st = state or State(m)
+        if u0 is not None:
+            st.u = torch.as_tensor(u0, dtype=torch.float64, device="cuda")
+        if states is not None:
+            st.states = states
+        if fext0 is not None:
+            st.fext = torch.as_tensor(fext0, dtype=torch.float64, device="cuda")
+        setup = _Setup(m, step, st)
+        self.setup = setup
+        self.lin.reset()
+        u, states = st.u, st.states
+        t, dt, inc, history = 0.0, min(step.dt_init, step.T), 0, []
+        t0 = time.time()
+        total = 0
+        self.qref = 0.0
+        fields = self._fields(scale)
+        while t < step.T * (1 - 1e-12):
+            if self.mon.should_stop():
+                self.mon.log("  stopped by user")
+                break
+            inc += 1
+            if inc > step.max_inc:
+                raise RuntimeError("max increments exceeded")
+            dt = min(dt, step.T - t)
+            tn = t + dt
+            fext = setup.fext(tn)
+            ut = torch.where(setup.fixed_j, setup.prescribed(tn), u)
+            try:
+                ut = self._predictor(u, states, ut, fext, fields, setup)
+                ok, it, ui, s_try, rh = self._newton(ut, states, fext, fields, setup, inc)
+            except FloatingPointError:
+                ok, it, ui, s_try, rh = False, 0, u, states, []
+            total += it
+            if ok:
+                u, states, t = ui, s_try, tn
+                history.append((t, it))
+                self.mon.log(f"  inc {inc:4d}  t={t:.4g}  dt={dt:.3g}  iters={it}  lin={self.lin.last_iters}")
+                self.mon.increment(step=step.name, inc=inc, t=t, dt=dt, iters=it, ok=True)
+                if callback:
+                    callback(t, u, states)
+                if it <= 5:
+                    dt = min(dt * 1.5, step.dt_max)
+            else:
+                dt *= 0.25
+                self.mon.log(f"  inc {inc:4d}  cutback -> dt={dt:.3g}")
+                self.mon.increment(step=step.name, inc=inc, t=t, dt=dt, iters=it, ok=False)
+                if dt < step.dt_min:
+                    raise RuntimeError("time increment smaller than minimum")
+        self.mon.log(f"  step '{step.name}' done: {inc} incs, {total} iterations, {time.time() - t0:.2f}s")
+        fint, _ = self._fint(u, states, fields)
+        reactions = (fint - setup.fext(step.T)) * setup.fixed_j
+        fe = setup.fext_final()
+        st.u, st.states, st.fext = u, states, fe
+        st.time += step.T
+        st.reactions = reactions
+        self.newton_iterations = total
+        return u, states, dict(history=history, reactions=reactions, fext=fe, state=st, iterations=total,
+                               increments=inc)
+
+    def _predictor(self, uc, s_old, ut, fext, fields, setup):           # solvers.py:607-624
+        delta = ut - uc
+        fint, _ = self._fint(uc, s_old, fields)
+        if self.lin.tangent == "mf":
+            Kd = self.m.tangent_jvp(uc, s_old, delta, fields)
+        else:
+            ops = self._ops(uc, s_old, fields)
+            Kd = self.m.matvec([K for _, K in ops], delta)
+        r = setup.free * (fint + Kd - fext)
+        rn = float(torch.linalg.norm(r))
+        self.qref = max(self.qref, rn)
+        if rn == 0.0:
+            return ut
+        du = self._linsolve(uc, s_old, fields, -r, setup)
+        return ut + setup.free * du
+
+    def _residual(self, u, s_old, fext, fields, setup):                # solvers.py:626-630
+        fint, s_new = self._fint(u, s_old, fields)
+        return setup.free * (fint - fext), fint, s_new
+
+    def _newton(self, u, s_old, fext, fields, setup, inc):              # solvers.py:632-683
+        hist = []
+        dut = 0.0
+        fn_t = float(torch.linalg.norm(fext))
+        for it in range(1, self.max_iter + 1):
+            r, fint, s_new = self._residual(u, s_old, fext, fields, setup)
+            rt = float(torch.linalg.norm(r))
+            ft = float(torch.linalg.norm(fint))
+            ref = max(fn_t, ft, 1e-3 * self.qref, 1e-30)
+            self.qref = max(self.qref, fn_t, ft)
+            ratio = rt / ref
+            hist.append(ratio)
+            self.mon.iteration(inc=inc, it=it, residual=ratio, du=dut)
+            if not np.isfinite(rt):
+                return False, it, u, s_old, hist
+            ut_n = float(torch.linalg.norm(u))
+            small_du = dut <= 1e-2 * max(ut_n, 1e-30)
+            if ratio <= self.rtol * 1e-2 or (it > 1 and ratio <= self.rtol and small_du):
+                return True, it - 1, u, s_new, hist
+            du = self._linsolve(u, s_old, fields, -r, setup)
+            alpha = 1.0
+            if self.line_search:
+                rn = rt
+                for _ in range(4):
+                    ut = u + alpha * du
+                    r2 = self._residual(ut, s_old, fext, fields, setup)[0]
+                    if float(torch.linalg.norm(r2)) < rn or alpha < 0.2:
+                        break
+                    alpha *= 0.5
+            u = u + alpha * du
+            dut = float(torch.linalg.norm(alpha * du))
+        return False, self.max_iter, u, s_old, hist

@@ -1,0 +1,205 @@
+/*
+ * exfem_b200 — C ABI of the B200 structural hot path (element force / tangent
+ * kernels, element-by-element matvecs, smoothed-aggregation V-cycle, PCG and
+ * mixed-precision refinement) behind the interfaces of EXFEM's ``gfem`` 0.3.0.
+ *
+ * Conventions (all entry points):
+ *   - plain C types only; no exceptions cross the boundary;
+ *   - every call returns an int status: EXFEM_OK (0), EXFEM_NOT_CONVERGED (1,
+ *     results still written), or a negative error; exfem_last_error() gives a
+ *     message for the calling host thread;
+ *   - device pointers passed in are borrowed for the duration of the call and
+ *     owned by the caller; host pointers are read before the call returns;
+ *   - "stream" is a cudaStream_t passed as void*; NULL means the legacy default
+ *     stream; work is stream ordered and calls return without a device sync
+ *     unless they must read a device scalar (solvers, which say so);
+ *   - handles (block, amg, solver) own their device memory and are not thread
+ *     safe: one host thread per handle;
+ *   - DOF numbering is node-interleaved, dof = 3*node + component, as in the
+ *     reference (gfem/model.py:157-158).
+ */
+#ifndef EXFEM_B200_H
+#define EXFEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  EXFEM_OK = 0,
+  EXFEM_NOT_CONVERGED = 1,
+  EXFEM_ERR_ARG = -1,
+  EXFEM_ERR_CUDA = -2,
+  EXFEM_ERR_OOM = -3,
+  EXFEM_ERR_TIMEOUT = -4,
+  EXFEM_ERR_NONFINITE = -5,
+  EXFEM_ERR_UNSUPPORTED = -6
+};
+
+/* element types: gfem/elements.py:124-125 (HEX8, fbar=True -> B-bar for small
+ * strain) and gfem/elements.py:177-179 (TET10); ELEMENTS map 194-197 */
+enum { EXFEM_C3D8 = 0, EXFEM_C3D10 = 1 };
+/* materials: gfem/materials.py:56-68 LinearElastic, 228-302 J2Plasticity */
+enum { EXFEM_LINEAR_ELASTIC = 0, EXFEM_J2 = 1 };
+/* arithmetic types of buffers passed as void* */
+enum { EXFEM_F64 = 0, EXFEM_F32 = 1, EXFEM_BF16 = 2 };
+/* assembly of element vectors into nodal vectors */
+enum { EXFEM_ASSEMBLE_GATHER = 0, EXFEM_ASSEMBLE_COLOUR = 1 };
+/* linear-operator kinds of a solver */
+enum { EXFEM_OP_EBE_F64 = 0, EXFEM_OP_MF_F64 = 1, EXFEM_OP_MF_F32 = 2 };
+/* preconditioners of a solver */
+enum { EXFEM_PC_NONE = 0, EXFEM_PC_JACOBI = 1, EXFEM_PC_AMG = 2 };
+
+#define EXFEM_MAX_TABLE 32
+
+/* Material parameters.  Mirrors the constructor arguments of
+ * gfem/materials.py:56-68 (LinearElastic(E, nu)) and 236-256
+ * (J2Plasticity(E, nu, table, Hk)).  For J2, (sy_tab, ep_tab) is the hardening
+ * table *after* the reference's extension (one-row tables become perfect
+ * plasticity, and a last point at eps_p = 1e6 continues the final slope). */
+typedef struct {
+  int kind;
+  double E, nu;
+  double Hk;
+  int ntab;
+  double sy_tab[EXFEM_MAX_TABLE];
+  double ep_tab[EXFEM_MAX_TABLE];
+} exfem_material;
+
+typedef struct exfem_block_s* exfem_block;
+typedef struct exfem_amg_s* exfem_amg;
+typedef struct exfem_solver_s* exfem_solver;
+
+/* ------------------------------------------------------------ library */
+int exfem_version(void);
+const char* exfem_last_error(void);
+
+/* ------------------------------------------------------------ blocks
+ * One element block = one element type + one material over a node set
+ * (gfem/model.py:21-26 Block.__init__, :362-365 Model.add_block).  Creation
+ * uploads coordinates and connectivity, builds the atomic-free gather plan
+ * (gfem/model.py:241-261, bit-identical), a greedy element colouring, and the
+ * per-element geometry streams of the matrix-free operator. */
+int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const double* X_host,
+                       int64_t ne, const int32_t* conn_host, exfem_block* out);
+int exfem_block_destroy(exfem_block b);
+/* sizes: ne, nn, nnode, ngp, nstate, gather-plan width vmax, colour count,
+ * affine (1 if every C3D10 has straight edges), device bytes held */
+int exfem_block_query(exfem_block b, int64_t* ne, int64_t* nn, int* nnode, int* ngp, int* nstate,
+                      int* vmax, int* ncolour, int* affine, int64_t* device_bytes);
+/* index maps, copied to host: gather plan (nn, vmax) int32 with sentinel ne*nnode
+ * (gfem/model.py:241-261); element colours (ne,) */
+int exfem_block_gather_plan(exfem_block b, int32_t* plan_host);
+int exfem_block_colours(exfem_block b, int32_t* colour_host);
+/* per-element stiffness scale (gfem/model.py:449-463, fields["scale"]); NULL = 1 */
+int exfem_block_set_scale(exfem_block b, const double* scale_host);
+/* prescribed-DOF mask (ndof bytes, 1 = fixed): operators apply the reference's
+ * opA, y = free*K(free*v) + fixed*v (gfem/solvers.py:257-267); NULL = all free */
+int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host);
+
+/* ------------------------------------------------------------ element kernels (FP64)
+ * Internal force f(u) with new Gauss-point states (gfem/model.py:466-477
+ * Model.internal_force over Block.force 70-81).  u, f: (ndof); state_old,
+ * state_new: (ne, ngp, nstate) or NULL for the linear-elastic material;
+ * fe: optional (ne, nnode, 3) element forces.  assembly = EXFEM_ASSEMBLE_GATHER
+ * reduces through the gather plan (reference order), EXFEM_ASSEMBLE_COLOUR by
+ * a colour-by-colour scatter; both are deterministic.  Also refreshes the
+ * block's per-Gauss-point consistent-tangent data at (u, state_old). */
+int exfem_internal_force(exfem_block b, const double* u, const double* state_old,
+                         double* state_new, double* fe, double* f, int assembly, void* stream);
+/* Element tangents Ke (ne, 3*nnode, 3*nnode) row-major in dtype F64/F32/BF16
+ * (gfem/model.py:83-111 Block.stiff, 479-483 Model.element_stiffness). */
+int exfem_element_stiffness(exfem_block b, const double* u, const double* state_old, int dtype,
+                            void* Ke, void* stream);
+/* Refresh only the per-Gauss-point tangent data of the matrix-free operator at
+ * (u, state_old) — what ``jax.jvp`` re-derives on every product in
+ * gfem/model.py:488-490 (Model.tangent_jvp). */
+int exfem_tangent_update(exfem_block b, const double* u, const double* state_old, void* stream);
+/* Matrix-free tangent product with the block's current tangent data, dtype F64
+ * or F32: y = opA(v) when apply_bc != 0 (gfem/solvers.py:257-267), else the bare
+ * y = K(u) v of Model.tangent_jvp (gfem/model.py:488-490), which it replaces. */
+int exfem_tangent_matvec(exfem_block b, int dtype, const void* v, void* y, int apply_bc, void* stream);
+/* Diagonal of the matrix-free tangent (FP64, ndof); fixed DOFs get 1. */
+int exfem_tangent_diagonal(exfem_block b, double* diag, void* stream);
+/* Stored-tangent EbE product with Ke (ne, nd, nd) FP64 and reference-order
+ * gather assembly: y = opA(v) when apply_bc != 0 (gfem/model.py:264-267
+ * gather_matvec within opA, gfem/solvers.py:257-267), else y = K v
+ * (gfem/model.py:162-166 ops_matvec). */
+int exfem_ebe_matvec(exfem_block b, const double* Ke, const double* v, double* y, int apply_bc, void* stream);
+/* Diagonal of stored Ke (gfem/model.py:169-173 ops_diagonal), FP64 (ndof). */
+int exfem_ebe_diagonal(exfem_block b, const double* Ke, double* diag, void* stream);
+/* Volume-averaged Cauchy stress (ne, 3, 3), von Mises (ne) and PEEQ (ne)
+ * (gfem/model.py:530-539 Model.stresses over Block.cauchy 129-137). */
+int exfem_stresses(exfem_block b, const double* u, const double* state, double* S,
+                   double* mises, double* peeq, void* stream);
+
+/* ------------------------------------------------------------ AMG hierarchy
+ * Device copy of a smoothed-aggregation hierarchy set up on the host
+ * (gfem/linalg.py:103-136 AMG.__init__/params).  Levels are added fine to
+ * coarse as CSR (int64 indptr, int32 indices, FP64 data): level matrix A
+ * (n x n), prolongator P (n x nc), restriction R = P^T (nc x n), Jacobi
+ * inverse diagonal dinv (n) and the Chebyshev bound rho.  The coarsest matrix is
+ * given densely; its regularised Cholesky factor's inverse is formed on the
+ * host (gfem/linalg.py:126-133). */
+int exfem_amg_create(exfem_amg* out);
+int exfem_amg_destroy(exfem_amg h);
+int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc,
+                        const int64_t* A_ptr, const int32_t* A_idx, const double* A_val,
+                        const int64_t* P_ptr, const int32_t* P_idx, const double* P_val,
+                        const int64_t* R_ptr, const int32_t* R_idx, const double* R_val,
+                        const double* dinv, double rho);
+int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv_dense);
+/* One V-cycle z = M(r) (gfem/linalg.py:156-195, Chebyshev degree 2 over
+ * [rho/30, rho]) in dtype F64 or F32; the coarse solve is FP64 in both.  When
+ * level0 is a block, level 0 is smoothed with that block's matrix-free tangent
+ * and the given inverse diagonal dinv0 (same dtype) instead of the stored level
+ * matrix (gfem/solvers.py:311-314). */
+int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0,
+                     const void* dinv0, void* stream);
+
+/* ------------------------------------------------------------ solvers
+ * A solver binds an operator (EXFEM_OP_*) of a block, a preconditioner
+ * (EXFEM_PC_*; an AMG handle for EXFEM_PC_AMG) and device workspace.
+ * EXFEM_OP_EBE_F64 needs exfem_solver_set_ke before solving. */
+int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out);
+int exfem_solver_destroy(exfem_solver s);
+int exfem_solver_set_ke(exfem_solver s, const double* Ke);
+/* Refresh the Jacobi / level-0 inverse diagonal from the current operator
+ * (gfem/solvers.py:312-313 dinv0). Called automatically by the first solve. */
+int exfem_solver_refresh_diagonal(exfem_solver s, void* stream);
+/* Use CUDA graphs for the PCG iteration loop (default on) and the number of
+ * iterations captured per graph launch. */
+int exfem_solver_set_graph(exfem_solver s, int enable, int chunk);
+/* PCG in the operator's precision with FP64 scalars and dot products
+ * (gfem/linalg.py:21-47): x0 = 0, stop when r.r <= tol^2 b.b or k >= maxiter.
+ * b, x: FP64 device (ndof).  Synchronises the stream to read the iteration count.
+ * Returns EXFEM_NOT_CONVERGED when relres > 1e-3 or is not finite (the
+ * reference's warning condition, gfem/solvers.py:472-473). */
+int exfem_solver_pcg(exfem_solver s, const double* b, double* x, double tol, int maxiter,
+                     int* iters, double* relres, void* stream);
+/* FP32 inner PCG (tolerance inner_tol) inside FP64 iterative refinement with an
+ * FP64 matrix-free residual, at most max_pass passes, until
+ * ||b - A x|| <= tol ||b|| (gfem/solvers.py:344-384 _LinearSystem._mixed). */
+int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, double inner_tol,
+                       int max_pass, int maxiter, int* iters, int* passes, double* relres,
+                       void* stream);
+
+/* ------------------------------------------------------------ host index builders
+ * Host-side, no device work.  Gather plan of one connectivity exactly as
+ * gfem/model.py:241-261 (plan must hold nn*vmax entries; call with plan = NULL to
+ * get vmax); greedy colouring; standard aggregation of a symmetric strength
+ * graph (CSR pattern) for the smoothed-aggregation set-up. */
+int exfem_host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* plan,
+                           int* vmax);
+int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* colour,
+                         int* ncolour);
+int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx,
+                                    int32_t* agg, int64_t* nagg);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXFEM_B200_H */

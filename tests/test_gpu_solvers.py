@@ -1,0 +1,201 @@
+"""Device AMG V-cycle, PCG, mixed refinement and the Newton loop against the oracle.
+
+Bars: the device V-cycle equals the oracle's restatement of gfem/linalg.py:156-195
+on the same hierarchy to 1e-12 (FP64); converged displacements agree with the
+oracle's direct solve to 1e-8 relative (the plain FP64 path at cg_tol 1e-10, and
+the mixed FP32/FP64 path at tol 1e-9); the J2 Newton loop reproduces the
+oracle's per-increment Newton iteration counts; the reference's analytic checks
+(tests/test_verification.py:27-36, 39-52, 66-83) hold on the device path.
+"""
+import numpy as np
+import pytest
+import torch
+
+from helpers import cantilever_bcs, jittered_box, rel_err, tet10_box
+from oracle import fem as ofem
+from oracle import linalg as olin
+from oracle import solvers as osol
+
+pytestmark = pytest.mark.gpu
+
+E, NU = 210000.0, 0.3
+
+
+def _config1():
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = mesh.box_hex(100.0, 20.0, 20.0, 20, 4, 4)
+    fix, tip, bcs, loads = cantilever_bcs(X, 100.0)
+    pm = xf.Model(X)
+    pm.add_block(c, xf.HEX8, xf.LinearElastic(E, NU))
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.LinearElastic(E, NU))
+    return X, c, bcs, loads, pm, om
+
+
+def _oracle_direct(om, bcs, loads):
+    st = osol.Step(bcs=bcs, loads=loads)
+    u, s, info = osol.StaticSolver(om, rtol=1e-6).solve(st)
+    return u
+
+
+def test_vcycle_matches_oracle(cuda):
+    import exfem_b200 as xf
+    X, c, bcs, loads, pm, om = _config1()
+    setup = osol.Setup(om, osol.Step(bcs=bcs, loads=loads))
+    ops = [(d, K.numpy()) for d, K in om.stiffness_ops(torch.zeros(om.ndof), om.init_state())]
+    A = olin.bc_matrix(ofem.ops_assemble(ops, om.ndof), setup.free)
+    amg = xf.AMG(A, X)
+    assert amg.nlevels >= 2
+    levels = [dict(A=lv["A"], dinv=lv["dinv"], rho=lv["rho"], P=lv["P"], R=lv["R"]) for lv in amg.levels]
+    b = np.random.default_rng(0).standard_normal(om.ndof) * setup.free
+    zo = olin.vcycle(levels, amg.coarse, b)
+    zp = amg.vcycle(torch.as_tensor(b, device="cuda"))
+    assert rel_err(zp, zo) < 1e-12
+    z32 = amg.vcycle(torch.as_tensor(b, device="cuda", dtype=torch.float32))
+    assert rel_err(z32.double(), zo) < 1e-4
+    # level 0 smoothed with the matrix-free tangent (gfem/solvers.py:311-314)
+    blk = pm.blocks[0]
+    blk.set_fixed(setup.fixed)
+    blk.tangent_update(torch.zeros(pm.ndof, device="cuda"), pm.init_state()[0])
+    d = blk.tangent_diagonal().cpu().numpy()
+    dinv0 = np.where(setup.free > 0, 1.0 / np.where(np.abs(d) > 0, d, 1.0), 1.0)
+    A0 = lambda v: A @ v                                        # the same operator, assembled
+    zo0 = olin.vcycle(levels, amg.coarse, b, A0=A0, dinv0=dinv0)
+    zp0 = amg.vcycle(torch.as_tensor(b, device="cuda"), blk, torch.as_tensor(dinv0, device="cuda"))
+    assert rel_err(zp0, zo0) < 1e-11
+    blk.set_fixed(None)
+
+
+@pytest.mark.parametrize("method,tangent", [("amg", "ebe"), ("amg", "mf"), ("mixed", "mf"), ("jacobi", "ebe")])
+def test_config1_linear_solve(cuda, method, tangent):
+    import exfem_b200 as xf
+    X, c, bcs, loads, pm, om = _config1()
+    uo = _oracle_direct(om, bcs, loads)
+    st = xf.Step(bcs=bcs, loads=loads)
+    tol = 1e-10 if method != "mixed" else 1e-9
+    up, s, info = xf.StaticSolver(pm, rtol=1e-6, linear_solver=method, tangent=tangent, cg_tol=tol,
+                                  verbose=False).solve(st)
+    err = rel_err(up, uo)
+    assert err < (1e-8 if method != "jacobi" else 1e-7), err
+
+
+def test_graph_and_eager_pcg_agree(cuda):
+    import exfem_b200 as xf
+    X, c, bcs, loads, pm, om = _config1()
+    res = []
+    for graph in (True, False):
+        st = xf.Step(bcs=bcs, loads=loads)
+        s = xf.StaticSolver(pm, rtol=1e-6, linear_solver="amg", cg_tol=1e-10, verbose=False, graph=graph)
+        u, _, _ = s.solve(st)
+        res.append((u.cpu().numpy(), s.lin.last_iters))
+    assert res[0][1] == res[1][1]
+    np.testing.assert_array_equal(res[0][0], res[1][0])       # deterministic reductions
+
+
+def test_j2_newton_counts_match_oracle(cuda):
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = jittered_box(100.0, 20.0, 20.0, 10, 2, 2, frac=0.1, seed=1)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > 100.0 - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)] + [(tip, 2, -2.0)]
+    table = [[250.0, 0.0], [1250.0, 1.0]]
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.J2Plasticity(E, NU, table))
+    uo, so, io = osol.StaticSolver(om, rtol=1e-6).solve(osol.Step(bcs=bcs, dt_init=0.2, dt_max=0.2))
+    pm = xf.Model(X)
+    pm.add_block(c, xf.HEX8, xf.J2Plasticity(E, NU, table))
+    for method, tangent in (("amg", "ebe"), ("mixed", "mf")):
+        up, sp, ip = xf.StaticSolver(pm, rtol=1e-6, linear_solver=method, tangent=tangent, cg_tol=1e-10,
+                                     verbose=False).solve(xf.Step(bcs=bcs, dt_init=0.2, dt_max=0.2))
+        assert [h[1] for h in ip["history"]] == [h[1] for h in io["history"]], (method, ip["history"], io["history"])
+        assert rel_err(up, uo) < 1e-7
+        mo = om.stresses(torch.as_tensor(uo), so)[0]["MISES"]
+        mp = pm.stresses(up, sp)[0]["MISES"]
+        assert rel_err(mp, mo) < 1e-6
+        assert float(so[0][..., 9].max()) > 0
+
+
+@pytest.mark.parametrize("etype", ["C3D8", "C3D10"])
+def test_patch_linear(cuda, etype):
+    """tests/test_verification.py:27-36 on the device path."""
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    Ev = 200e3
+    X, c = mesh.box_hex(1, 1, 1, 2, 2, 2)
+    if etype == "C3D10":
+        X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+    m = xf.Model(X)
+    m.add_block(c, xf.ELEMENTS[etype], xf.LinearElastic(Ev, NU))
+    w = lambda f: mesh.nodes_where(X, f)
+    bcs = [(w(lambda x, y, z: x < 1e-9), 0, 0.0), (w(lambda x, y, z: y < 1e-9), 1, 0.0),
+           (w(lambda x, y, z: z < 1e-9), 2, 0.0), (w(lambda x, y, z: x > 1 - 1e-9), 0, 1e-3)]
+    u, s, info = xf.StaticSolver(m, linear_solver="amg", cg_tol=1e-12, verbose=False).solve(xf.Step(bcs=bcs))
+    S = m.stresses(u, s)[0]["S"].cpu().numpy()
+    assert np.allclose(S[:, 0, 0], Ev * 1e-3, rtol=1e-6)
+    assert np.allclose(S[:, 1, 1], 0, atol=1e-6 * Ev)
+    U = u.cpu().numpy().reshape(-1, 3)
+    assert np.allclose(U[:, 1].min(), -NU * 1e-3, rtol=1e-6)
+
+
+def test_j2_uniaxial_hardening(cuda):
+    """tests/test_verification.py:39-52 on the device path."""
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    Ev, sy, H = 200e3, 250.0, 2000.0
+    X, c = mesh.box_hex(1, 1, 1, 1, 1, 1)
+    m = xf.Model(X)
+    m.add_block(c, xf.HEX8, xf.J2Plasticity(Ev, NU, [[sy, 0.0], [sy + H * 0.1, 0.1]]))
+    w = lambda f: mesh.nodes_where(X, f)
+    bcs = [(w(lambda x, y, z: x < 1e-9), 0, 0.0), (w(lambda x, y, z: y < 1e-9), 1, 0.0),
+           (w(lambda x, y, z: z < 1e-9), 2, 0.0), (w(lambda x, y, z: x > 1 - 1e-9), 0, 0.01)]
+    u, s, info = xf.StaticSolver(m, linear_solver="amg", cg_tol=1e-12, verbose=False).solve(
+        xf.Step(bcs=bcs, dt_init=0.1, dt_max=0.1))
+    r = m.stresses(u, s)[0]
+    sxx = float(r["S"][0, 0, 0])
+    eps, ey = 0.01, sy / Ev
+    expected = sy + Ev * H / (Ev + H) * (eps - ey)
+    assert abs(sxx - expected) / expected < 1e-4
+    assert abs(float(r["PEEQ"][0]) - (eps - sxx / Ev)) < 1e-6
+
+
+def test_tet10_cantilever_vs_beam_theory(cuda):
+    """tests/test_verification.py:66-83 on the device path."""
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    Ev, L, h = 200e3, 10.0, 1.0
+    X, c = mesh.box_hex(L, h, h, 20, 2, 2)
+    X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+    m = xf.Model(X)
+    m.add_block(c, xf.TET10, xf.LinearElastic(Ev, NU))
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > L - 1e-9)
+    st = xf.Step(bcs=[(fix, d, 0.0) for d in range(3)], loads=[(tip, 1, -1.0 / len(tip))])
+    u, s, info = xf.StaticSolver(m, linear_solver="mixed", cg_tol=1e-10, verbose=False).solve(st)
+    I = h ** 4 / 12
+    d_beam = L ** 3 / (3 * Ev * I) + L / (5 / 6 * Ev / (2 * (1 + NU)) * h * h)
+    d = -float(u.cpu().numpy().reshape(-1, 3)[tip, 1].mean())
+    assert abs(d - d_beam) / d_beam < 0.03
+    R = info["reactions"].cpu().numpy().reshape(-1, 3)[:, 1].sum()
+    assert abs(R - 1.0) < 1e-6
+
+
+def test_tet10_mixed_vs_direct(cuda):
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = tet10_box(1.0, 1.0, 1.0, 4, 4, 4, frac=0.1, seed=2)
+    rng = np.random.default_rng(3)
+    sc = np.exp(rng.uniform(0, np.log(10), size=len(c)))
+    fix = mesh.nodes_where(X, lambda x, y, z: z < 1e-9)
+    top = mesh.nodes_where(X, lambda x, y, z: z > 1 - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)]
+    loads = [(top, 2, 1.0 / len(top))]
+    om = ofem.Model(X)
+    om.add_block(c, ofem.TET10, ofem.LinearElastic(1000.0, 0.3))
+    uo, _, _ = osol.StaticSolver(om, rtol=1e-6, scale=[sc]).solve(osol.Step(bcs=bcs, loads=loads))
+    pm = xf.Model(X)
+    pm.add_block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3))
+    up, _, _ = xf.StaticSolver(pm, rtol=1e-6, linear_solver="mixed", cg_tol=1e-10, verbose=False).solve(
+        xf.Step(bcs=bcs, loads=loads), scale=[sc])
+    assert rel_err(up, uo) < 1e-8
