@@ -1,0 +1,339 @@
+"""Benchmark of the structural hot path on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (``config.workload``): the C3D10 mesh of the mixed-precision scale case
+— a unit cube split into 80x80x80 hexahedra, each into 6 Kuhn tetrahedra with
+straight-edged quadratic mid-nodes (3,072,000 C3D10, 4,173,281 nodes,
+12,519,843 DOF), interior nodes jittered +-10% of h from a seed, linear elastic
+with per-element E log-uniform in [1, 10] GPa, nu = 0.3, z = 0 clamped.  Synthetic
+data, generated here.  One step = one FP32 matrix-free tangent product
+y = opA(v) over the whole mesh (the operator inside the mixed FP32/FP64 PCG).
+
+value  = DOF x products / s with inputs resident in HBM (CUDA events on the
+         launching stream, K steps between synchronisations; the per-step stream
+         is 600 MB, larger than the 126 MB L2, so no flush is needed);
+e2e    = the same metric through the C ABI with host buffers: every step copies v
+         from pinned host memory, runs the product and copies y back;
+roofline = algorithmic bytes per product (8*ndof + ne*(16*nnode + 4), FP32
+         vectors, int32 connectivity, centroid-relative FP32 element coordinates
+         and one modulus per element) / measured step time, against the measured
+         HBM copy bandwidth;
+solve  = solves/s and p50/p99 latency of the cantilever of the small plain-method
+         case (C3D8 20x4x4, 1,575 DOF) by the mixed FP32/FP64 AMG-PCG path and by
+         the plain FP64 path, with the relative displacement error between them;
+cpu_baseline = the CPU oracle (restated reference, torch FP64 forward-mode AD of
+         the internal force = the reference's Model.tangent_jvp) on a 30^3-hex
+         C3D10 sub-mesh with all host threads.
+
+Multi-GPU: replicas only — every rank runs the same workload on its own GPU;
+value is the sum over ranks divided by the slowest rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DOF·matvec/s, solves/s, p50/p99 latency at 1e-8 rel err vs plain FP64 path"
+UNIT = "DOF·matvec/s"
+WORKLOAD = "C3D10 80^3x6 unit cube (3,072,000 el, 12,519,843 DOF), FP32 matrix-free tangent product"
+# DRAM bytes per product of the dominant kernel from one ncu capture
+# (profiles/mf_matvec_c3d10_config3.md); None until measured
+TRAFFIC_BYTES = None
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_config3(n=80, seed=0):
+    from exfem_b200 import mesh
+    X, c = mesh.box_hex(1.0, 1.0, 1.0, n, n, n)
+    X = mesh.jitter_interior(X, 1.0 / n, 0.1, seed)
+    X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+    rng = np.random.default_rng(seed + 1)
+    scale = np.exp(rng.uniform(np.log(1.0), np.log(10.0), size=len(c)))
+    return X, c, scale
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["clock sampling unavailable"])
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 8 for k in range(4) if r[4 + k] == "Active"})
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                    reasons=reasons, samples=len(sm))
+
+
+class CpuOracleProduct:
+    """The CPU oracle's matrix-free product (FP64 forward-mode AD JVP of the
+    internal force, the restated Model.tangent_jvp) on a bounded C3D10 sub-mesh
+    with all host threads."""
+
+    def __init__(self, n=30):
+        import torch
+        from exfem_b200 import mesh
+        from oracle import fem as ofem
+        self.cores = os.cpu_count()
+        torch.set_num_threads(self.cores)
+        X, c = mesh.box_hex(1.0, 1.0, 1.0, n, n, n)
+        X = mesh.jitter_interior(X, 1.0 / n, 0.1, 0)
+        X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+        self.m = ofem.Model(X)
+        self.m.add_block(c, ofem.TET10, ofem.LinearElastic(1000.0, 0.3), chunk=1 << 20)
+        self.scale = [np.exp(np.random.default_rng(1).uniform(0, np.log(10.0), size=len(c)))]
+        self.u = torch.zeros(self.m.ndof, dtype=torch.float64)
+        self.v = torch.randn(self.m.ndof, dtype=torch.float64, generator=torch.Generator().manual_seed(0))
+        self.s = self.m.init_state()
+        self.ndof = self.m.ndof
+        self.sample = (f"C3D10 {n}^3x6 sub-mesh of the same construction ({len(c)} el, {self.m.ndof} DOF), "
+                       f"FP64 AD JVP of the internal force (restated Model.tangent_jvp), torch threads={self.cores}")
+
+    def step(self):
+        self.m.tangent_jvp(self.u, self.s, self.v, self.scale)
+
+
+def cpu_baseline(steps=3, n=30):
+    """(DOF·matvec/s, info) of the CPU oracle product, timed after one warm-up."""
+    p = CpuOracleProduct(n)
+    p.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        p.step()
+    dt = (time.perf_counter() - t0) / steps
+    return p.ndof / dt, dict(cores=p.cores, kind="port", sample=p.sample + f", {steps} products")
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    if n_gpus > 1 or int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        rank, world = dist.get_rank(), dist.get_world_size()
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", rank)))
+        return rank, world, dist
+    torch.cuda.set_device(0)
+    return 0, 1, None
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle port on the host cores, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    p = CpuOracleProduct()
+    for _ in range(max(args.warmup, 1)):
+        p.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        p.step()
+    dt = (time.perf_counter() - t0) / args.steps
+    value = p.ndof / dt
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=dt * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
+                data="synthetic", impl="reference",
+                config=dict(workload=WORKLOAD, sample=p.sample),
+                cpu_baseline=dict(value=value, unit=UNIT, cores=p.cores, kind="port", sample=p.sample),
+                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def solve_section(reps=10):
+    """Config-1 cantilever: mixed FP32/FP64 path vs plain FP64 path."""
+    import torch
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = mesh.box_hex(100.0, 20.0, 20.0, 20, 4, 4)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > 100.0 - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)]
+    loads = [(tip, 2, -1000.0 / len(tip))]
+    m = xf.Model(X)
+    m.add_block(c, xf.HEX8, xf.LinearElastic(210000.0, 0.3))
+    out = {}
+    sols = {}
+    for name, kw in (("plain_fp64", dict(linear_solver="amg", tangent="ebe", graph=False)),
+                     ("mixed", dict(linear_solver="mixed", tangent="mf", graph=True))):
+        s = xf.StaticSolver(m, rtol=1e-6, cg_tol=1e-10 if name == "plain_fp64" else 1e-9, verbose=False, **kw)
+        u, _, _ = s.solve(xf.Step(bcs=bcs, loads=loads))          # warm-up, builds the hierarchy
+        lat = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            u, _, _ = s.solve(xf.Step(bcs=bcs, loads=loads))
+            torch.cuda.synchronize()
+            lat.append(time.perf_counter() - t0)
+        sols[name] = u
+        lat = np.array(lat) * 1e3
+        out[name] = dict(solves_per_s=float(1e3 / lat.mean()), p50_ms=float(np.percentile(lat, 50)),
+                         p99_ms=float(np.percentile(lat, 99)), pcg_iters=s.lin.last_iters)
+    err = float((sols["mixed"] - sols["plain_fp64"]).abs().max() / sols["plain_fp64"].abs().max())
+    out["rel_err_mixed_vs_fp64"] = err
+    out["case"] = "C3D8 20x4x4 cantilever, 1,575 DOF, full StaticSolver.solve incl. host AMG set-up reuse"
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=80, help="hexahedra per cube edge (80 = the scale case)")
+    ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import ctypes as C
+    import torch
+    import exfem_b200 as xf
+    from exfem_b200 import _lib
+    from exfem_b200.model import Model
+
+    rank, world, dist = dist_setup(args.gpus)
+    X, c, scale = build_config3(args.n)
+    m = Model(X)
+    blk = m.add_block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3))
+    blk.set_scale(scale)
+    fixed = np.zeros(m.ndof, bool)
+    base = np.nonzero(X[:, 2] < 1e-9)[0]
+    for d in range(3):
+        fixed[base * 3 + d] = True
+    blk.set_fixed(fixed)
+    ne, nn, ndof = len(c), len(X), m.ndof
+    stream = torch.cuda.current_stream()
+    v = torch.randn(ndof, dtype=torch.float32, device="cuda", generator=torch.Generator("cuda").manual_seed(rank))
+    y = torch.empty_like(v)
+    h = blk.handle
+    launch = lambda: _lib.check(_lib.lib.exfem_tangent_matvec(h, _lib.F32, v.data_ptr(), y.data_ptr(), 1,
+                                                               stream.cuda_stream))
+    for _ in range(max(args.warmup, 3)):
+        launch()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    vh = v.cpu().pin_memory()
+    yh = torch.empty(ndof, dtype=torch.float32).pin_memory()
+    vd = torch.empty_like(v)
+    lib = _lib.lib
+
+    def e2e_step():
+        vd.copy_(vh, non_blocking=True)
+        _lib.check(lib.exfem_tangent_matvec(h, _lib.F32, vd.data_ptr(), y.data_ptr(), 1, stream.cuda_stream))
+        yh.copy_(y, non_blocking=True)
+
+    for _ in range(3):
+        e2e_step()
+    torch.cuda.synchronize()
+    esteps = max(5, args.steps // 5)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(esteps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1) / esteps
+    if dist:
+        t = torch.tensor([e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+
+    solve = None
+    if rank == 0 and not args.no_solve:
+        solve = solve_section()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cv, ci = cpu_baseline()
+        cpu = dict(value=cv, unit=UNIT, cores=ci["cores"], kind=ci["kind"], sample=ci["sample"])
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    value = world * ndof / (ms * 1e-3)
+    alg_bytes = 8 * ndof + ne * (16 * 10 + 4)
+    pk, pk_src = peaks()
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    line = dict(
+        metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+        ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+        data="synthetic",
+        config=dict(workload=WORKLOAD, ne=ne, nodes=nn, ndof=ndof, parallelism=f"replicas x{world}",
+                    l2="per-step stream 600 MB > 126 MB L2, no flush", seed=0),
+        e2e=dict(value=world * ndof / (e_ms * 1e-3), unit=UNIT, h2d_bytes_per_step=4 * ndof,
+                 d2h_bytes_per_step=4 * ndof, ms_per_step=e_ms),
+        roofline=dict(bound="hbm", achieved=achieved, peak=pk, unit="GB/s", frac=achieved / pk,
+                      traffic=TRAFFIC_BYTES, peak_source=f"{pk_src} (MEASURED_PEAKS.json hbm_gbs)",
+                      algorithmic_bytes_per_step=alg_bytes),
+        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve)
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()
