@@ -53,6 +53,8 @@ _SIGS = {
                            C.POINTER(I32), C.POINTER(I32), C.POINTER(I32), C.POINTER(I64)], C.c_int),
     "exfem_block_gather_plan": ([VP, P], C.c_int),
     "exfem_block_colours": ([VP, P], C.c_int),
+    "exfem_block_tile_info": ([VP, C.POINTER(I64), C.POINTER(I64), C.POINTER(I32)], C.c_int),
+    "exfem_block_tile_maps": ([VP, P, P, P, P], C.c_int),
     "exfem_block_set_scale": ([VP, P], C.c_int),
     "exfem_block_set_fixed": ([VP, P], C.c_int),
     "exfem_internal_force": ([VP, P, P, P, P, P, C.c_int, VP], C.c_int),

@@ -1,6 +1,6 @@
 """Build ``libexfem_b200.so`` in-tree for sm_100a with nvcc.
 
-    python -m exfem_b200.build [--verbose] [--ptxas]
+    python exfem_b200/build.py [--verbose] [--ptxas]
 
 Every ``csrc/*.cu`` and ``csrc/*.cpp`` file is compiled to an object under
 ``exfem_b200/_build/`` (in parallel, skipped when the object is newer than the

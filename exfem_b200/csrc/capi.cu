@@ -26,6 +26,9 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line) {
 int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan, int& vmax);
 int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& colour, int& ncolour);
 int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg);
+int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
+                   std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
+                   int& maxu);
 int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters, double* relres, cudaStream_t st);
 int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, double inner_tol, int max_pass,
                  int maxiter, int* iters, int* passes, double* relres, cudaStream_t st);
@@ -59,13 +62,16 @@ static int set_material(exfem_block_s* b, const exfem_material* m) {
 
 static int init_tangent(exfem_block_s* b) {
   if (b->mat.kind != EXFEM_J2) return EXFEM_OK;
-  const size_t n = (size_t)b->ne * b->ngp * 8;
+  // elastic tangent data (c1 = 1) in the tile-major layout, padding included
+  const int W = b->ngp * 8;
+  const size_t n = (size_t)b->ntile * MF_TILE * W;
   std::vector<double> t(n, 0.0);
   std::vector<float> t32(n, 0.0f);
-  for (size_t i = 0; i < n; i += 8) {
-    t[i + 6] = 1.0;
-    t32[i + 6] = 1.0f;
-  }
+  for (int64_t e = 0; e < b->ntile * MF_TILE; ++e)
+    for (int g = 0; g < b->ngp; ++g) {
+      t[tile_index(e, g * 8 + 6, W)] = 1.0;
+      t32[tile_index(e, g * 8 + 6, W)] = 1.0f;
+    }
   int s;
   if ((s = b->tan64.upload(t.data(), n))) return s;
   return b->tan32.upload(t32.data(), n);
@@ -167,6 +173,28 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
       }
     }
   }
+  {
+    std::vector<int32_t> tp, tn;
+    std::vector<uint16_t> te, tq;
+    if ((s = host_tile_maps(nn, ne, b->nnode, conn_host, MF_TILE, tp, tn, te, tq, b->maxu))) return s;
+    b->ntile = (int64_t)tp.size() - 1;
+    if ((s = b->tile_ptr.upload(tp.data(), tp.size()))) return s;
+    if ((s = b->tile_nodes.upload(tn.data(), std::max<size_t>(tn.size(), 1)))) return s;
+    if ((s = b->tile_nend.upload(te.data(), std::max<size_t>(te.size(), 1)))) return s;
+    if ((s = b->tile_perm.upload(tq.data(), std::max<size_t>(tq.size(), 1)))) return s;
+    {  // forward map of the slot lists: list position of every slot's node
+      std::vector<uint16_t> li(tq.size(), 0);
+      const int NS = b->nnode * MF_TILE;
+      for (int64_t t = 0; t < b->ntile; ++t) {
+        int q = 0;
+        for (int k = 0; k < tp[t + 1] - tp[t]; ++k)
+          for (; q < te[tp[t] + k]; ++q) li[t * NS + tq[t * NS + q]] = (uint16_t)k;
+      }
+      if ((s = b->lidx.upload(li.data(), std::max<size_t>(li.size(), 1)))) return s;
+    }
+    if ((s = b->dev_err.alloc(1))) return s;
+    EX_CUDA(cudaMemset(b->dev_err.p, 0, sizeof(int)));
+  }
   if ((s = b->X.upload(X_host, 3 * nn))) return s;
   if ((s = b->conn.upload(conn_host, ne * b->nnode))) return s;
   if ((s = b->plan.upload(b->plan_host.data(), b->plan_host.size()))) return s;
@@ -213,6 +241,33 @@ int exfem_block_gather_plan(exfem_block b, int32_t* plan_host) {
 int exfem_block_colours(exfem_block b, int32_t* colour_host) {
   EX_ARG(b && colour_host, "NULL argument");
   memcpy(colour_host, b->colour_host.data(), b->colour_host.size() * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_block_tile_info(exfem_block b, int64_t* ntile, int64_t* nlist, int* maxu) {
+  EX_ARG(b, "block is NULL");
+  if (ntile) *ntile = b->ntile;
+  if (nlist) {
+    int32_t last = 0;
+    if (b->ntile) EX_CUDA(cudaMemcpy(&last, b->tile_ptr.p + b->ntile, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    *nlist = last;
+  }
+  if (maxu) *maxu = b->maxu;
+  return EXFEM_OK;
+}
+
+int exfem_block_tile_maps(exfem_block b, int32_t* ptr_host, int32_t* nodes_host, uint16_t* nend_host,
+                          uint16_t* perm_host) {
+  EX_ARG(b, "block is NULL");
+  int64_t nl = 0;
+  int st;
+  if ((st = exfem_block_tile_info(b, nullptr, &nl, nullptr))) return st;
+  if (ptr_host) EX_CUDA(cudaMemcpy(ptr_host, b->tile_ptr.p, (b->ntile + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (nodes_host && nl) EX_CUDA(cudaMemcpy(nodes_host, b->tile_nodes.p, nl * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (nend_host && nl) EX_CUDA(cudaMemcpy(nend_host, b->tile_nend.p, nl * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+  if (perm_host && b->ntile)
+    EX_CUDA(cudaMemcpy(perm_host, b->tile_perm.p, (size_t)b->ntile * b->nnode * MF_TILE * sizeof(uint16_t),
+                       cudaMemcpyDeviceToHost));
   return EXFEM_OK;
 }
 

@@ -128,6 +128,17 @@ __host__ __device__ constexpr double tet10_dN(int g, int a, int i) {
                         tet_L(g, tet_edge(a - 4, 0)) * tet_dL(tet_edge(a - 4, 1), i));
 }
 
+// ---------------------------------------------------------------- tile-major streams
+// Per-element streams of the matrix-free operator (geometry, J2 tangent data,
+// tile-local node indices) are stored tile-major ("AoSoA"): tiles of MF_TILE
+// consecutive elements, and inside a tile component k of element l at
+// k*MF_TILE + l.  A tile's stream is one contiguous block (one bulk copy), and a
+// warp reading component k of its 32 elements touches 128 contiguous bytes.
+constexpr int MF_TILE = 128;
+__host__ __device__ __forceinline__ int64_t tile_index(int64_t e, int k, int width) {
+  return ((e / MF_TILE) * width + k) * MF_TILE + (e % MF_TILE);
+}
+
 // ---------------------------------------------------------------- element traits
 template <int ET> struct ElemTraits;
 template <> struct ElemTraits<EXFEM_C3D8> {

@@ -107,10 +107,10 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
       if (MODE != FORCE_STRESS) {
         if (tan64)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan64[(e * NG + g) * 8 + k] = tn[k];
+          for (int k = 0; k < 8; ++k) tan64[tile_index(e, g * 8 + k, NG * 8)] = tn[k];
         if (tan32)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan32[(e * NG + g) * 8 + k] = (float)tn[k];
+          for (int k = 0; k < 8; ++k) tan32[tile_index(e, g * 8 + k, NG * 8)] = (float)tn[k];
       }
       if (MODE == FORCE_FULL) {
         const double vol = detJ * sc;
@@ -177,10 +177,10 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
       if (MODE != FORCE_STRESS) {
         if (tan64)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan64[(e * NG + g) * 8 + k] = tn[k];
+          for (int k = 0; k < 8; ++k) tan64[tile_index(e, g * 8 + k, NG * 8)] = tn[k];
         if (tan32)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan32[(e * NG + g) * 8 + k] = (float)tn[k];
+          for (int k = 0; k < 8; ++k) tan32[tile_index(e, g * 8 + k, NG * 8)] = (float)tn[k];
       }
       if (MODE == FORCE_FULL) {
         const double vol = detJ / 24.0 * sc;
@@ -369,17 +369,20 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
   }
 #pragma unroll
   for (int k = 0; k < GS; ++k) {
-    g64[e * GS + k] = out[k];
-    g32[e * GS + k] = (float)out[k];
+    g64[tile_index(e, k, GS)] = out[k];
+    g32[tile_index(e, k, GS)] = (float)out[k];
   }
 }
 
 int build_geometry(exfem_block_s* b) {
   const int GS = b->etype == EXFEM_C3D8 ? ElemTraits<EXFEM_C3D8>::geo_stride : ElemTraits<EXFEM_C3D10>::geo_stride;
   int st;
-  if (b->geo64.n != (size_t)(b->ne * GS)) {
-    if ((st = b->geo64.alloc(b->ne * GS))) return st;
-    if ((st = b->geo32.alloc(b->ne * GS))) return st;
+  const int64_t padded = b->ntile * MF_TILE * GS;
+  if (b->geo64.n != (size_t)padded) {
+    if ((st = b->geo64.alloc(padded))) return st;
+    if ((st = b->geo32.alloc(padded))) return st;
+    EX_CUDA(cudaMemset(b->geo64.p, 0, b->geo64.bytes()));
+    EX_CUDA(cudaMemset(b->geo32.p, 0, b->geo32.bytes()));
   }
   if (b->ne == 0) return EXFEM_OK;
   const int threads = 128;
@@ -473,7 +476,7 @@ stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __rest
     const double* st = st_old ? st_old + (e * NG + g) * ns : zero_state;
     double sig[6], tn[8];
     if (tan_in) {
-      for (int k = 0; k < 8; ++k) tn[k] = tan_in[(e * NG + g) * 8 + k];
+      for (int k = 0; k < 8; ++k) tn[k] = tan_in[tile_index(e, g * 8 + k, NG * 8)];
     } else {
       material_stress(mat, H, st, nullptr, sig, tn);
     }

@@ -16,6 +16,7 @@
 //      pass 2: remaining nodes join the first neighbouring pass-1 aggregate;
 //      pass 3: still-unaggregated nodes seed new aggregates with their
 //              unaggregated neighbours.
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -76,6 +77,52 @@ int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::
       const int64_t n = conn[e * nnode + a];
       used[n * W + (c >> 6)] |= (1ull << (c & 63));
     }
+  }
+  return EXFEM_OK;
+}
+
+// Element-tile maps of the matrix-free operator.  Tiles are `tile` consecutive
+// elements; a slot of a tile is s = a*tile + l (local node a of the tile's
+// element l).  Per tile: the sorted distinct nodes it touches; for each of them,
+// in node order, its slots in increasing slot order, concatenated into `perm`
+// (tile-major, padded to nnode*tile entries per tile); and `nend`, the end of
+// each node's run in perm (aligned with the node list).
+int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
+                   std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
+                   int& maxu) {
+  const int64_t ntile = (ne + tile - 1) / tile;
+  const int nslot = nnode * tile;
+  ptr.assign(ntile + 1, 0);
+  nodes.clear();
+  nend.clear();
+  perm.assign((size_t)ntile * nslot, 0);
+  std::vector<int64_t> stamp(nn, -1);
+  std::vector<int32_t> pos(nn, 0), cnt, start;
+  std::vector<int32_t> list;
+  maxu = 0;
+  for (int64_t t = 0; t < ntile; ++t) {
+    list.clear();
+    const int64_t e0 = t * tile, e1 = std::min<int64_t>(ne, e0 + tile);
+    for (int64_t k = e0 * nnode; k < e1 * nnode; ++k) {
+      const int32_t n = conn[k];
+      if (stamp[n] != t) { stamp[n] = t; list.push_back(n); }
+    }
+    std::sort(list.begin(), list.end());
+    const int nu = (int)list.size();
+    for (int i = 0; i < nu; ++i) pos[list[i]] = i;
+    cnt.assign(nu, 0);
+    for (int a = 0; a < nnode; ++a)
+      for (int64_t e = e0; e < e1; ++e) ++cnt[pos[conn[e * nnode + a]]];
+    start.assign(nu + 1, 0);
+    for (int i = 0; i < nu; ++i) start[i + 1] = start[i] + cnt[i];
+    uint16_t* pm = perm.data() + (size_t)t * nslot;
+    for (int i = 0; i < nu; ++i) cnt[i] = start[i];
+    for (int a = 0; a < nnode; ++a)                      // increasing slot order
+      for (int64_t e = e0; e < e1; ++e) pm[cnt[pos[conn[e * nnode + a]]]++] = (uint16_t)(a * tile + (e - e0));
+    nodes.insert(nodes.end(), list.begin(), list.end());
+    for (int i = 0; i < nu; ++i) nend.push_back((uint16_t)start[i + 1]);
+    ptr[t + 1] = (int32_t)nodes.size();
+    maxu = std::max<int>(maxu, nu);
   }
   return EXFEM_OK;
 }

@@ -27,8 +27,17 @@ struct exfem_block_s {
   // boundary conditions
   exfem::DevBuf<uint8_t> fixed;       // (ndof) 1 = prescribed; empty = all free
   exfem::DevBuf<uint8_t> node_fixed;  // (nn) bit c set = dof c prescribed
-  // matrix-free operator data
+  // matrix-free operator data: tiles of MF_TILE consecutive elements, each with
+  // the sorted list of distinct nodes it touches and per-slot local indices
   int affine = 1;
+  int64_t ntile = 0;
+  int maxu = 0;                       // largest distinct-node count of a tile
+  exfem::DevBuf<int32_t> tile_ptr;    // (ntile+1)
+  exfem::DevBuf<int32_t> tile_nodes;  // concatenated sorted node lists
+  exfem::DevBuf<uint16_t> lidx;       // tile-major (ntile, nnode*MF_TILE): list position of each slot's node
+  exfem::DevBuf<uint16_t> tile_nend;  // per listed node: end of its slot run in tile_perm
+  exfem::DevBuf<uint16_t> tile_perm;  // tile-major (ntile, nnode*MF_TILE) slots grouped by node
+  exfem::DevBuf<int> dev_err;         // set by bounded waits that give up
   exfem::DevBuf<double> geo64;        // (ne, geo_stride)
   exfem::DevBuf<float> geo32;
   int plastic_tangent = 0;            // 1 once tangent data differs from elastic

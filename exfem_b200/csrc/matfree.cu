@@ -1,30 +1,65 @@
 // Matrix-free element-by-element tangent product y = opA(v) in FP32 or FP64.
 //
-// This replaces the reference's forward-mode AD product K(u) v
-// (gfem/model.py:488-490 Model.tangent_jvp) and its stored-Ke product
-// (gfem/model.py:264-267) inside opA (gfem/solvers.py:257-267):
-//     y = free * K (free * v) + fixed * v.
-// Per element the kernel reads a geometry stream (C3D8: the 7 modal coordinate
-// vectors, i.e. coordinates with the centroid removed, plus the stiffness scale;
-// C3D10 with straight edges: the constant inverse Jacobian and scaled volume),
-// gathers v at the element nodes, evaluates the B-bar (C3D8) or standard (C3D10)
-// strain at every Gauss point, applies the elastic law or the stored J2
-// consistent tangent, and scatters the element vector with atomic adds.
+// Replaces the reference's forward-mode AD product K(u) v (gfem/model.py:488-490
+// Model.tangent_jvp) and its stored-Ke product (gfem/model.py:264-267) inside
+// opA (gfem/solvers.py:257-267):  y = free * K (free * v) + fixed * v.
+//
+// Work unit: a tile of MF_TILE = 128 consecutive elements, one CTA of 128 threads
+// per tile, persistent over tiles.  Per tile:
+//   1. element streams (geometry, tile-local node indices, J2 tangent data) are
+//      one contiguous block each in the tile-major layout; in the FP32 kernel a
+//      single thread moves them into shared memory with bulk TMA copies
+//      (cp.async.bulk, mbarrier completion), double buffered so that the copy of
+//      the next tile overlaps the work on this one;
+//   2. v is gathered once per distinct node of the tile (masked by the fixed-DOF
+//      bits) into shared memory — ~3 distinct nodes per element instead of 8/10
+//      node slots;
+//   3. one thread per element evaluates the element product from shared memory
+//      (C3D8: modal B-bar form; C3D10: constant inverse Jacobian of the
+//      straight-edged element) and accumulates it into per-node shared-memory
+//      sums;
+//   4. one global reduction per distinct node (an 8-byte vector reduction plus a
+//      scalar one) adds the tile's sums into y (initialised to fixed*v by a
+//      separate pass).
+// Geometry: C3D8 stores the 7 modal coordinate vectors (coordinates with the
+// centroid removed) and the stiffness scale; C3D10 stores the inverse Jacobian
+// and scaled volume, formed in FP64 from the nodal coordinates and rounded once.
 #include "internal.h"
 
 namespace exfem {
 
-template <class T>
-__device__ __forceinline__ void mf_stress(bool j2, const T* __restrict__ tn, T lam, T mu, T Kb,
-                                          const T (&e)[6], T (&s)[6]) {
-  if (j2) {
-    T t[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) t[k] = tn[k];
-    tangent_stress(Kb, mu, t, e, s);
-  } else {
-    elastic_stress(lam, mu, e, s);
-  }
+// ---------------------------------------------------------------- async-copy helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: gives up after ~2^24 polls, records the failure and returns false
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+  for (int i = 0; i < (1 << 24); ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  if (err) atomicExch(err, 1);
+  return false;
 }
 
 template <class T>
@@ -35,39 +70,31 @@ __device__ __forceinline__ void matmul3t(const T (&A)[9], const T (&B)[9], T (&C
     for (int j = 0; j < 3; ++j) C[3 * i + j] = A[3 * i] * B[j] + A[3 * i + 1] * B[3 + j] + A[3 * i + 2] * B[6 + j];
 }
 
-template <class T, int ET, bool J2>
-__global__ void __launch_bounds__(128)
-mf_matvec_kernel(int64_t ne, const T* __restrict__ geo, const int32_t* __restrict__ conn,
-                 const T* __restrict__ tan, const uint8_t* __restrict__ nfix, const T* __restrict__ v,
-                 T* __restrict__ y, T lam, T mu, T Kb, const int* __restrict__ skip) {
-  using Tr = ElemTraits<ET>;
-  constexpr int NN = Tr::nnode, NG = Tr::ngp, GS = Tr::geo_stride;
-  if (skip && *skip) return;
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= ne) return;
-  int nod[NN];
-  uint8_t fx[NN];
+// stress at a Gauss point from the strain: elastic or the stored J2 tangent
+// (tn points to component 0 of this element/point, stride MF_TILE)
+template <class T, bool J2>
+__device__ __forceinline__ void mf_stress(const T* tn, T lam, T mu, T Kb, const T (&e)[6], T (&s)[6]) {
+  if constexpr (J2) {
+    T t[8];
 #pragma unroll
-  for (int a = 0; a < NN; ++a) {
-    nod[a] = __ldg(conn + e * NN + a);
-    fx[a] = nfix ? __ldg(nfix + nod[a]) : (uint8_t)0;
+    for (int k = 0; k < 8; ++k) t[k] = tn[k * MF_TILE];
+    tangent_stress(Kb, mu, t, e, s);
+  } else {
+    elastic_stress(lam, mu, e, s);
   }
-  T va[NN][3];
-#pragma unroll
-  for (int a = 0; a < NN; ++a)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) va[a][c] = ((fx[a] >> c) & 1) ? T(0) : __ldg(v + 3 * (int64_t)nod[a] + c);
-  T g[GS];
-#pragma unroll
-  for (int k = 0; k < GS; ++k) g[k] = __ldg(geo + e * GS + k);
-  T f[NN][3];
+}
+
+// element product f = Ke v_e from the element's streams (strided by MF_TILE)
+template <class T, int ET, bool J2>
+__device__ __forceinline__ void element_product(const T* g, const T* tn, const T (&va)[ElemTraits<ET>::nnode][3],
+                                                T lam, T mu, T Kb, T (&f)[ElemTraits<ET>::nnode][3]) {
   if constexpr (ET == EXFEM_C3D8) {
     T cm[7][3], um[7][3];
 #pragma unroll
     for (int k = 0; k < 7; ++k)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) cm[k][c] = g[3 * k + c];
-    const T sc = g[21];
+      for (int c = 0; c < 3; ++c) cm[k][c] = g[(3 * k + c) * MF_TILE];
+    const T sc = g[21 * MF_TILE];
     hex_to_modal(va, um);
     T J0[9], iJ0[9], G0[9], H0[9];
 #pragma unroll
@@ -98,7 +125,7 @@ mf_matvec_kernel(int64_t ne, const T* __restrict__ geo, const int32_t* __restric
       H[8] += bb;
       T ee[6], s[6];
       sym_from_grad(H, ee);
-      mf_stress<T>(J2, J2 ? tan + (e * NG + q) * 8 : nullptr, lam, mu, Kb, ee, s);
+      mf_stress<T, J2>(tn + q * 8 * MF_TILE, lam, mu, Kb, ee, s);
       const T vol = detJ * sc;
       const T t = vol * (s[0] + s[1] + s[2]) * T(1.0 / 3.0);
       tacc += t;
@@ -116,19 +143,14 @@ mf_matvec_kernel(int64_t ne, const T* __restrict__ geo, const int32_t* __restric
     for (int c = 0; c < 3; ++c)
 #pragma unroll
       for (int i = 0; i < 3; ++i) Fm[i][c] += tacc * iJ0[3 * i + c];
-    T fo[8][3];
-    hex_from_modal(Fm, fo);
-#pragma unroll
-    for (int a = 0; a < 8; ++a)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) f[a][c] = fo[a][c];
+    hex_from_modal(Fm, f);
   } else {
     T iJ[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) iJ[k] = g[k];
-    const T vol = g[9];
+    for (int k = 0; k < 9; ++k) iJ[k] = g[k * MF_TILE];
+    const T vol = g[9 * MF_TILE];
 #pragma unroll
-    for (int a = 0; a < NN; ++a) f[a][0] = f[a][1] = f[a][2] = T(0);
+    for (int a = 0; a < 10; ++a) f[a][0] = f[a][1] = f[a][2] = T(0);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       T G[9];
@@ -147,7 +169,7 @@ mf_matvec_kernel(int64_t ne, const T* __restrict__ geo, const int32_t* __restric
       matmul3t(G, iJ, H);
       T ee[6], s[6];
       sym_from_grad(H, ee);
-      mf_stress<T>(J2, J2 ? tan + (e * NG + q) * 8 : nullptr, lam, mu, Kb, ee, s);
+      mf_stress<T, J2>(tn + q * 8 * MF_TILE, lam, mu, Kb, ee, s);
       const T r[3][3] = {{vol * s[0], vol * s[3], vol * s[5]},
                          {vol * s[3], vol * s[1], vol * s[4]},
                          {vol * s[5], vol * s[4], vol * s[2]}};
@@ -167,11 +189,138 @@ mf_matvec_kernel(int64_t ne, const T* __restrict__ geo, const int32_t* __restric
         }
     }
   }
+}
+
+template <class T, int ET, bool J2>
+struct TileLayout {
+  using Tr = ElemTraits<ET>;
+  static constexpr int NN = Tr::nnode, NG = Tr::ngp, GS = Tr::geo_stride, NSLOT = NN * MF_TILE;
+  static constexpr uint32_t GEO_B = GS * MF_TILE * sizeof(T);
+  static constexpr uint32_t LIDX_B = NSLOT * sizeof(uint16_t);
+  static constexpr uint32_t TAN_B = J2 ? NG * 8 * MF_TILE * sizeof(T) : 0;
+  static constexpr uint32_t STAGE_B = GEO_B + LIDX_B + TAN_B;
+  static_assert(GEO_B % 16 == 0 && LIDX_B % 16 == 0 && TAN_B % 16 == 0, "bulk copies need 16-byte multiples");
+};
+
+// add a node's three components into y (12-byte stride): one 8-byte vector
+// reduction for the aligned pair and one scalar reduction
+__device__ __forceinline__ void red_node(float* y, int64_t n, float a, float b, float c, uint8_t bits) {
+  float* p = y + 3 * n;
+  if (bits) {
+    if (!(bits & 1)) atomicAdd(p, a);
+    if (!(bits & 2)) atomicAdd(p + 1, b);
+    if (!(bits & 4)) atomicAdd(p + 2, c);
+  } else if ((n & 1) == 0) {
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
+    atomicAdd(p + 2, c);
+  } else {
+    atomicAdd(p, a);
+    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p + 1), "f"(b), "f"(c) : "memory");
+  }
+}
+__device__ __forceinline__ void red_node(double* y, int64_t n, double a, double b, double c, uint8_t bits) {
+  double* p = y + 3 * n;
+  if (!(bits & 1)) atomicAdd(p, a);
+  if (!(bits & 2)) atomicAdd(p + 1, b);
+  if (!(bits & 4)) atomicAdd(p + 2, c);
+}
+
+template <class T, int ET, bool J2, bool TMA>
+__global__ void __launch_bounds__(MF_TILE)
+mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint16_t* __restrict__ lidx,
+               const T* __restrict__ tan, const int32_t* __restrict__ tptr, const int32_t* __restrict__ tnodes,
+               const uint8_t* __restrict__ nfix, const T* __restrict__ v, T* __restrict__ y, T lam, T mu, T Kb,
+               int maxu, const int* __restrict__ skip, int* __restrict__ err) {
+  using L = TileLayout<T, ET, J2>;
+  constexpr int NN = L::NN, NG = L::NG, GS = L::GS, NSLOT = L::NSLOT;
+  if (skip && *skip) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ __align__(8) uint64_t bar[2];
+  const int tid = threadIdx.x;
+  // element of the tile handled by this thread: lanes of a warp take every 4th
+  // element, so the elements that share corner nodes (neighbours in the mesh
+  // order) fall into different warps and their shared-memory additions to the
+  // same node rarely collide inside one warp instruction
+  const int lt = 4 * (tid & 31) + (tid >> 5);
+  T* xs = reinterpret_cast<T*>(smem + (TMA ? 2 * L::STAGE_B : 0));  // gathered v, node-major per component
+  T* ys = xs + 3 * maxu;                                              // accumulated products
+  auto stage_geo = [&](int s) { return reinterpret_cast<T*>(smem + s * L::STAGE_B); };
+  auto stage_lidx = [&](int s) { return reinterpret_cast<uint16_t*>(smem + s * L::STAGE_B + L::GEO_B); };
+  auto stage_tan = [&](int s) { return reinterpret_cast<T*>(smem + s * L::STAGE_B + L::GEO_B + L::LIDX_B); };
+  auto issue = [&](int64_t t, int s) {
+    fence_proxy_async();
+    mbar_expect_tx(&bar[s], L::STAGE_B);
+    bulk_g2s(stage_geo(s), geo + t * (GS * MF_TILE), L::GEO_B, &bar[s]);
+    bulk_g2s(stage_lidx(s), lidx + t * NSLOT, L::LIDX_B, &bar[s]);
+    if constexpr (J2) bulk_g2s(stage_tan(s), tan + t * (NG * 8 * MF_TILE), L::TAN_B, &bar[s]);
+  };
+  if constexpr (TMA) {
+    if (tid == 0) {
+      mbar_init(&bar[0], 1);
+      mbar_init(&bar[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0 && (int64_t)blockIdx.x < ntile) issue(blockIdx.x, 0);
+  }
+  int it = 0;
+  for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x, ++it) {
+    const int s = it & 1;
+    if constexpr (TMA) {
+      const int64_t tn = t + gridDim.x;
+      if (tid == 0 && tn < ntile) issue(tn, s ^ 1);
+    }
+    // distinct nodes of the tile: gather masked v, clear the accumulators
+    const int64_t u0 = tptr[t];
+    const int nu = tptr[t + 1] - (int32_t)u0;
+    for (int j = tid; j < 3 * nu; j += MF_TILE) {
+      const int k = j / 3, c = j - 3 * k;
+      const int64_t n = tnodes[u0 + k];
+      const uint8_t bits = nfix ? nfix[n] : (uint8_t)0;
+      xs[c * maxu + k] = ((bits >> c) & 1) ? T(0) : v[3 * n + c];
+      ys[c * maxu + k] = T(0);
+    }
+    const T* g;
+    const uint16_t* li;
+    const T* tnp;
+    if constexpr (TMA) {
+      const bool ok = mbar_wait_bounded(&bar[s], (uint32_t)((it >> 1) & 1), err);
+      if (__syncthreads_or(!ok)) return;
+      g = stage_geo(s);
+      li = stage_lidx(s);
+      tnp = J2 ? stage_tan(s) : nullptr;
+    } else {
+      __syncthreads();
+      g = geo + t * (GS * MF_TILE);
+      li = lidx + t * NSLOT;
+      tnp = J2 ? tan + t * (NG * 8 * MF_TILE) : nullptr;
+    }
+    const int64_t e = t * MF_TILE + lt;
+    if (e < ne) {
+      int l[NN];
+      T va[NN][3];
 #pragma unroll
-  for (int a = 0; a < NN; ++a)
+      for (int a = 0; a < NN; ++a) {
+        l[a] = li[a * MF_TILE + lt];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
-      if (!((fx[a] >> c) & 1)) atomicAdd(y + 3 * (int64_t)nod[a] + c, f[a][c]);
+        for (int c = 0; c < 3; ++c) va[a][c] = xs[c * maxu + l[a]];
+      }
+      T f[NN][3];
+      element_product<T, ET, J2>(g + lt, J2 ? tnp + lt : nullptr, va, lam, mu, Kb, f);
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(&ys[c * maxu + l[a]], f[a][c]);
+    }
+    __syncthreads();
+    // one reduction per distinct node into y
+    for (int k = tid; k < nu; k += MF_TILE) {
+      const int64_t n = tnodes[u0 + k];
+      const uint8_t bits = nfix ? nfix[n] : (uint8_t)0;
+      red_node(y, n, ys[k], ys[maxu + k], ys[2 * maxu + k], bits);
+    }
+    __syncthreads();
+  }
 }
 
 // y = fixed ? v : 0 before the scatter
@@ -183,10 +332,50 @@ __global__ void mf_init_kernel(int64_t ndof, const uint8_t* __restrict__ fixed, 
     y[i] = (fixed && fixed[i]) ? v[i] : T(0);
 }
 
+// ---------------------------------------------------------------- launch
+template <class T, int ET, bool J2>
+static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const uint8_t* nf, const T* v, T* y,
+                 const int* skip, cudaStream_t s) {
+  constexpr bool TMA = sizeof(T) == 4;
+  using L = TileLayout<T, ET, J2>;
+  auto kern = mf_tile_kernel<T, ET, J2, TMA>;
+  const size_t smem = (TMA ? 2 * (size_t)L::STAGE_B : 0) + 2 * 3 * (size_t)b->maxu * sizeof(T);
+  // per (kernel, shared-memory size): opt in above 48 KB and size the persistent grid
+  static thread_local size_t opted = 0;
+  static thread_local int per_sm = 0, nsm = 0, dev = -1;
+  int cur;
+  EX_CUDA(cudaGetDevice(&cur));
+  if (smem > opted || cur != dev) {
+    EX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+    EX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cur));
+    EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MF_TILE, smem));
+    opted = smem;
+    dev = cur;
+  }
+  if (per_sm < 1) {
+    set_error("matrix-free tile kernel does not fit on an SM (%zu bytes of shared memory)", smem);
+    return EXFEM_ERR_UNSUPPORTED;
+  }
+  const int64_t grid = std::min<int64_t>(b->ntile, (int64_t)nsm * per_sm);
+  kern<<<(unsigned)grid, MF_TILE, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p,
+                                             b->tile_nodes.p, nf, v, y, (T)b->mat.lam, (T)b->mat.mu, (T)b->mat.K,
+                                             b->maxu, skip, b->dev_err.p);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
 template <class T>
 int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaStream_t s, bool bc) {
   const int64_t ndof = b->ndof();
   if (ndof == 0) return EXFEM_OK;
+  if ((reinterpret_cast<uintptr_t>(y) & 7) != 0) {
+    set_error("matrix-free product: y must be 8-byte aligned");
+    return EXFEM_ERR_ARG;
+  }
+  if (b->etype == EXFEM_C3D10 && !b->affine) {
+    set_error("matrix-free C3D10 needs straight-edged elements (mid-nodes at edge midpoints)");
+    return EXFEM_ERR_UNSUPPORTED;
+  }
   mf_init_kernel<T><<<grid_for(ndof, 256), 256, 0, s>>>(ndof, bc ? b->fixed.p : nullptr, v, y, skip);
   EX_LAUNCH_CHECK();
   if (b->ne == 0) return EXFEM_OK;
@@ -200,23 +389,12 @@ int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaSt
     tan = (const T*)b->tan32.p;
   }
   const bool j2 = b->mat.kind == EXFEM_J2;
-  const T lam = (T)b->mat.lam, mu = (T)b->mat.mu, Kb = (T)b->mat.K;
-  const int threads = 128;
-  const unsigned grid = (unsigned)((b->ne + threads - 1) / threads);
   const uint8_t* nf = bc ? b->node_fixed.p : nullptr;
-  if (b->etype == EXFEM_C3D8) {
-    if (j2) mf_matvec_kernel<T, EXFEM_C3D8, true><<<grid, threads, 0, s>>>(b->ne, geo, b->conn.p, tan, nf, v, y, lam, mu, Kb, skip);
-    else mf_matvec_kernel<T, EXFEM_C3D8, false><<<grid, threads, 0, s>>>(b->ne, geo, b->conn.p, tan, nf, v, y, lam, mu, Kb, skip);
-  } else {
-    if (!b->affine) {
-      set_error("matrix-free C3D10 needs straight-edged elements (mid-nodes at edge midpoints)");
-      return EXFEM_ERR_UNSUPPORTED;
-    }
-    if (j2) mf_matvec_kernel<T, EXFEM_C3D10, true><<<grid, threads, 0, s>>>(b->ne, geo, b->conn.p, tan, nf, v, y, lam, mu, Kb, skip);
-    else mf_matvec_kernel<T, EXFEM_C3D10, false><<<grid, threads, 0, s>>>(b->ne, geo, b->conn.p, tan, nf, v, y, lam, mu, Kb, skip);
-  }
-  EX_LAUNCH_CHECK();
-  return EXFEM_OK;
+  if (b->etype == EXFEM_C3D8)
+    return j2 ? mf_go<T, EXFEM_C3D8, true>(b, geo, tan, nf, v, y, skip, s)
+              : mf_go<T, EXFEM_C3D8, false>(b, geo, tan, nf, v, y, skip, s);
+  return j2 ? mf_go<T, EXFEM_C3D10, true>(b, geo, tan, nf, v, y, skip, s)
+            : mf_go<T, EXFEM_C3D10, false>(b, geo, tan, nf, v, y, skip, s);
 }
 
 template int launch_mf_matvec<float>(exfem_block_s*, const float*, float*, const int*, cudaStream_t, bool);

@@ -82,6 +82,18 @@ class Block:
         check(lib.exfem_block_colours(self._h, out.ctypes.data))
         return out
 
+    def tile_maps(self):
+        """(ptr, nodes, nend, perm) element-tile maps of the matrix-free operator."""
+        nt, nl, mu = C.c_int64(), C.c_int64(), C.c_int()
+        check(lib.exfem_block_tile_info(self._h, C.byref(nt), C.byref(nl), C.byref(mu)))
+        ptr_ = np.empty(nt.value + 1, np.int32)
+        nodes = np.empty(max(nl.value, 1), np.int32)
+        nend = np.empty(max(nl.value, 1), np.uint16)
+        perm = np.empty((nt.value, self.etype.nnode * 128), np.uint16)
+        check(lib.exfem_block_tile_maps(self._h, ptr_.ctypes.data, nodes.ctypes.data, nend.ctypes.data,
+                                        perm.ctypes.data))
+        return ptr_, nodes[:nl.value], nend[:nl.value], perm
+
     def init_state(self):                                              # model.py:154-155
         return torch.zeros((self.ne, self.etype.ngp, self.material.nstate), dtype=torch.float64, device="cuda")
 

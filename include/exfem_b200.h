@@ -94,6 +94,16 @@ int exfem_block_query(exfem_block b, int64_t* ne, int64_t* nn, int* nnode, int* 
  * (gfem/model.py:241-261); element colours (ne,) */
 int exfem_block_gather_plan(exfem_block b, int32_t* plan_host);
 int exfem_block_colours(exfem_block b, int32_t* colour_host);
+/* element-tile maps of the matrix-free operator (tiles of 128 consecutive
+ * elements; slot s = a*128 + l is local node a of the tile's element l): tile
+ * count, total length of the node lists and the longest list; then, copied to
+ * host, ptr (ntile+1), the sorted distinct nodes of every tile, for each listed
+ * node the end of its run of slots (uint16), and per tile the slots grouped by
+ * node in node order, increasing within a node (ntile, nnode*128, zero padded).
+ * No counterpart in the reference. */
+int exfem_block_tile_info(exfem_block b, int64_t* ntile, int64_t* nlist, int* maxu);
+int exfem_block_tile_maps(exfem_block b, int32_t* ptr_host, int32_t* nodes_host, uint16_t* nend_host,
+                          uint16_t* perm_host);
 /* per-element stiffness scale (gfem/model.py:449-463, fields["scale"]); NULL = 1 */
 int exfem_block_set_scale(exfem_block b, const double* scale_host);
 /* prescribed-DOF mask (ndof bytes, 1 = fixed): operators apply the reference's

@@ -408,21 +408,30 @@ def greedy_colouring(conn, nn):
 
 
 def tile_maps(conn, tile):
-    """Element-tile node maps used by the matrix-free matvec (no counterpart in the
-    reference).  Elements [t*tile, (t+1)*tile) form tile t; its node list is the
-    sorted set of distinct nodes they touch, and every element slot stores the
-    position of its node in that list.  Returns (ptr (ntile+1,), nodes, local (ne, nnode))."""
+    """Element-tile maps used by the matrix-free product (no counterpart in the
+    reference).  Elements [t*tile, (t+1)*tile) form tile t and slot s = a*tile + l
+    is local node a of its element l.  Per tile: the sorted distinct nodes; for each
+    node (in that order) its slots in increasing order, concatenated into perm
+    (padded with zeros to nnode*tile per tile); nend = end of each node's run.
+    Returns (ptr (ntile+1,), nodes, nend, perm (ntile, nnode*tile))."""
     conn = np.asarray(conn, dtype=np.int64)
-    ne = len(conn)
-    ptr, nodes, local = [0], [], np.empty(conn.shape, np.int32)
-    for t0 in range(0, ne, tile):
-        blk = conn[t0:t0 + tile]
+    ne, nnode = conn.shape
+    ntile = -(-ne // tile)
+    ptr, nodes, nend = [0], [], []
+    perm = np.zeros((ntile, nnode * tile), np.uint16)
+    for t in range(ntile):
+        blk = conn[t * tile:(t + 1) * tile]
         u = np.unique(blk)
+        slot_node = np.searchsorted(u, blk.T.reshape(-1))        # slot order a*tile + l (valid l only)
+        la = np.arange(blk.shape[0])
+        slots = (np.arange(nnode)[:, None] * tile + la[None, :]).reshape(-1)
+        order = np.argsort(slot_node, kind="stable")
+        perm[t, :len(order)] = slots[order]
+        nend.append(np.cumsum(np.bincount(slot_node, minlength=len(u))))
         nodes.append(u)
-        local[t0:t0 + tile] = np.searchsorted(u, blk)
         ptr.append(ptr[-1] + len(u))
-    return (np.asarray(ptr, np.int32), np.concatenate(nodes).astype(np.int32) if nodes else
-            np.zeros(0, np.int32), local)
+    cat = (lambda xs, dt: np.concatenate(xs).astype(dt) if xs else np.zeros(0, dt))
+    return np.asarray(ptr, np.int32), cat(nodes, np.int32), cat(nend, np.uint16), perm
 
 
 # ---------------------------------------------------------------- model
