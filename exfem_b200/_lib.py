@@ -70,6 +70,7 @@ _SIGS = {
     "exfem_amg_add_level": ([VP, I64, I64, P, P, P, P, P, P, P, P, P, P, D], C.c_int),
     "exfem_amg_set_coarse": ([VP, I64, P], C.c_int),
     "exfem_amg_vcycle": ([VP, C.c_int, P, P, VP, P, VP], C.c_int),
+    "exfem_amg_vcycle_noalloc": ([VP, C.c_int, P, P, VP, P, VP], C.c_int),
     "exfem_solver_create": ([VP, C.c_int, C.c_int, VP, C.POINTER(VP)], C.c_int),
     "exfem_solver_destroy": ([VP], C.c_int),
     "exfem_solver_set_ke": ([VP, P], C.c_int),

@@ -13,6 +13,9 @@
 // Level 0 can instead be smoothed with the current matrix-free tangent
 // (gfem/solvers.py:311-314), in which case the products go through the
 // element kernel and the vector updates through small elementwise kernels.
+#include <array>
+#include <mutex>
+
 #include "internal.h"
 #include "solver.h"
 
@@ -322,3 +325,180 @@ int amg_add_level(exfem_amg_s* h, int64_t n, int64_t nc, const int64_t* Ap, cons
 }
 
 }  // namespace exfem
+
+// ================================================================= allocation-free V-cycle
+// exfem_amg_vcycle_noalloc: the same V-cycle as exfem_amg_vcycle, for callers
+// that must not allocate device memory during the call — code recording a CUDA
+// graph by stream capture (cudaMalloc is not permitted while a capture is open)
+// and hosts whose device memory is owned by another allocator.  The per-level
+// work vectors (6 per level plus 2 coarse vectors) are carved from one
+// file-scope device array of EXFEM_VCYCLE_NOALLOC_BYTES (8 MiB), which every GPU
+// that loads the library holds until the process exits.  Hierarchies whose work
+// vectors do not fit are rejected with EXFEM_ERR_ARG.  All calls share the
+// array: calls whose work overlaps on the GPU (other streams, other host
+// threads) race with each other and must be serialised by the caller.  Nothing
+// in the array needs to start at zero: each call writes every work entry before
+// reading it, so contents left by the previous call are never read.
+namespace exfem {
+
+static __device__ __align__(256) unsigned char g_vcycle_scratch[EXFEM_VCYCLE_NOALLOC_BYTES];
+
+// device address of the scratch array, resolved once per device with that device
+// current (the host-side name of the array is not a device address)
+static std::mutex g_scratch_mu;
+static void* g_scratch_dev[64] = {nullptr};
+
+static int vcycle_scratch_address(void** out) {
+  int dev = 0;
+  EX_CUDA(cudaGetDevice(&dev));
+  EX_ARG(dev >= 0 && dev < 64, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_dev[dev]) {
+    void* p = nullptr;
+    EX_CUDA(cudaGetSymbolAddress(&p, g_vcycle_scratch));
+    g_scratch_dev[dev] = p;
+  }
+  *out = g_scratch_dev[dev];
+  return EXFEM_OK;
+}
+
+template <class T>
+struct NoallocWork {
+  std::vector<std::array<T*, AmgLevel::NW>> lv;
+  T* cb = nullptr;
+  T* cx = nullptr;
+};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+template <class T>
+static int noalloc_carve(exfem_amg_s* h, unsigned char* base, NoallocWork<T>& w) {
+  size_t off = 0;
+  w.lv.resize(h->levels.size());
+  for (size_t l = 0; l < h->levels.size(); ++l)
+    for (int k = 0; k < AmgLevel::NW; ++k) {
+      w.lv[l][k] = reinterpret_cast<T*>(base + off);
+      off += align256(sizeof(T) * (size_t)std::max<int64_t>(h->levels[l]->n, 1));
+    }
+  w.cb = reinterpret_cast<T*>(base + off);
+  off += align256(sizeof(T) * (size_t)std::max<int64_t>(h->nc, 1));
+  w.cx = reinterpret_cast<T*>(base + off);
+  off += align256(sizeof(T) * (size_t)std::max<int64_t>(h->nc, 1));
+  if (off > (size_t)EXFEM_VCYCLE_NOALLOC_BYTES) {
+    set_error("allocation-free V-cycle: the hierarchy needs %zu bytes of work vectors, the static scratch holds %zu",
+              off, (size_t)EXFEM_VCYCLE_NOALLOC_BYTES);
+    return EXFEM_ERR_ARG;
+  }
+  return EXFEM_OK;
+}
+
+template <class T>
+static int vcycle_level_noalloc(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0Op<T>* op0,
+                                NoallocWork<T>& w, cudaStream_t s) {
+  if (l == h->levels.size()) return coarse_solve<T>(h, b, x, nullptr, s);
+  AmgLevel& L = *h->levels[l];
+  const bool mf = (l == 0 && op0 && op0->apply);
+  const T* dinv = (l == 0 && op0 && op0->dinv) ? op0->dinv : lvdinv<T>(L);
+  const int64_t n = L.n;
+  T* r = w.lv[l][AmgLevel::WR];
+  T* d = w.lv[l][AmgLevel::WD];
+  T* d2 = w.lv[l][AmgLevel::WD2];
+  T* t = w.lv[l][AmgLevel::WTMP];
+  const double lmax = L.rho, lmin = L.rho / 30.0;
+  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  const double sigma = theta / delta;
+  double ca[8], cb[8];
+  {
+    double rh = 1.0 / sigma;
+    for (int j = 0; j < h->degree; ++j) {
+      const double rn = 1.0 / (2.0 * sigma - rh);
+      ca[j] = rn * rh;
+      cb[j] = 2.0 * rn / delta;
+      rh = rn;
+    }
+  }
+  const T ith = (T)(1.0 / theta);
+  const unsigned eg = grid_for(n, 256);
+  const T* vals = csr_vals<T>(L.A);
+  int st;
+  auto smooth_steps = [&]() -> int {
+    for (int j = 0; j < h->degree; ++j) {
+      if (mf) {
+        if ((st = op0->apply(op0->ctx, d, t, nullptr, s))) return st;
+        cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], nullptr);
+        EX_LAUNCH_CHECK();
+      } else {
+        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], nullptr, s)))
+          return st;
+      }
+      std::swap(d, d2);
+    }
+    add_kernel<T><<<eg, 256, 0, s>>>(n, d, x, nullptr);
+    EX_LAUNCH_CHECK();
+    return EXFEM_OK;
+  };
+  cheb_init0_kernel<T><<<eg, 256, 0, s>>>(n, b, dinv, x, r, d, ith, nullptr);
+  EX_LAUNCH_CHECK();
+  if ((st = smooth_steps())) return st;
+  if (mf) {
+    if ((st = op0->apply(op0->ctx, x, t, nullptr, s))) return st;
+    sub_kernel<T><<<eg, 256, 0, s>>>(n, b, t, nullptr);
+    EX_LAUNCH_CHECK();
+  } else {
+    if ((st = spmv_lanes<T, SP_RES>(L.A, vals, x, t, b, nullptr, nullptr, nullptr, T(0), T(0), nullptr, s))) return st;
+  }
+  T* bc = (l + 1 < h->levels.size()) ? w.lv[l + 1][AmgLevel::WB] : w.cb;
+  T* xc = (l + 1 < h->levels.size()) ? w.lv[l + 1][AmgLevel::WX] : w.cx;
+  if ((st = spmv_lanes<T, SP_SET>(L.R, csr_vals<T>(L.R), t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0), nullptr, s)))
+    return st;
+  if ((st = vcycle_level_noalloc<T>(h, l + 1, bc, xc, nullptr, w, s))) return st;
+  if ((st = spmv_lanes<T, SP_ADD>(L.P, csr_vals<T>(L.P), xc, x, nullptr, nullptr, nullptr, nullptr, T(0), T(0), nullptr, s)))
+    return st;
+  if (mf) {
+    if ((st = op0->apply(op0->ctx, x, t, nullptr, s))) return st;
+    resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, nullptr);
+    EX_LAUNCH_CHECK();
+  } else {
+    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), nullptr, s))) return st;
+  }
+  return smooth_steps();
+}
+
+template <class T>
+static int mf_apply_noalloc(void* ctx, const T* x, T* y, const int* skip, cudaStream_t s) {
+  return launch_mf_matvec<T>((exfem_block_s*)ctx, x, y, skip, s);
+}
+
+template <class T>
+static int vcycle_noalloc(exfem_amg_s* h, const T* r, T* z, exfem_block_s* level0, const T* dinv0, cudaStream_t s) {
+  EX_ARG(!h->levels.empty() || h->nc > 0, "empty AMG hierarchy");
+  void* base = nullptr;
+  int st;
+  if ((st = vcycle_scratch_address(&base))) return st;
+  NoallocWork<T> w;
+  if ((st = noalloc_carve<T>(h, static_cast<unsigned char*>(base), w))) return st;
+  if (h->levels.empty()) return coarse_solve<T>(h, r, z, nullptr, s);
+  Level0Op<T> op;
+  if (level0) {
+    op.apply = &mf_apply_noalloc<T>;
+    op.ctx = level0;
+    op.dinv = dinv0;
+  }
+  return vcycle_level_noalloc<T>(h, 0, r, z, level0 ? &op : nullptr, w, s);
+}
+
+}  // namespace exfem
+
+extern "C" int exfem_amg_vcycle_noalloc(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0,
+                                        const void* dinv0, void* stream) {
+  using namespace exfem;
+  EX_ARG(h && r && z, "NULL argument");
+  EX_ARG(!level0 || dinv0, "a level-0 block needs dinv0");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (dtype == EXFEM_F64)
+    return vcycle_noalloc<double>(h, (const double*)r, (double*)z, level0, (const double*)dinv0, s);
+  if (dtype == EXFEM_F32)
+    return vcycle_noalloc<float>(h, (const float*)r, (float*)z, level0, (const float*)dinv0, s);
+  set_error("V-cycle supports F64 and F32, got %d", dtype);
+  return EXFEM_ERR_ARG;
+}

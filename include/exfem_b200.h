@@ -169,6 +169,22 @@ int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv_dense);
  * matrix (gfem/solvers.py:311-314). */
 int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0,
                      const void* dinv0, void* stream);
+/* Allocation-free V-cycle (no counterpart in the reference).  Same result and
+ * arguments as exfem_amg_vcycle, for callers that must not allocate device
+ * memory during a call: code recording a CUDA graph by stream capture, where
+ * cudaMalloc is not permitted, and hosts whose device memory belongs to another
+ * allocator.  exfem_amg_vcycle allocates its per-level work vectors on first use;
+ * this variant takes them from one static device array of
+ * EXFEM_VCYCLE_NOALLOC_BYTES that every GPU loading the library holds until exit,
+ * and calls no cudaMalloc, cudaFree or allocating routine.  A hierarchy whose
+ * work vectors (6 per level and 2 coarse, each rounded up to 256 bytes) exceed
+ * the array is rejected with EXFEM_ERR_ARG.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race, so the caller must serialise them. */
+#define EXFEM_VCYCLE_NOALLOC_BYTES (8u << 20)
+int exfem_amg_vcycle_noalloc(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0,
+                             const void* dinv0, void* stream);
 
 /* ------------------------------------------------------------ solvers
  * A solver binds an operator (EXFEM_OP_*) of a block, a preconditioner
