@@ -1,0 +1,145 @@
+"""CPU: mesh fixtures, host index builders through the C ABI, exported symbols,
+host smoothed-aggregation set-up, and the world-size-2 replicas path (gloo)."""
+import ctypes as C
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from exfem_b200 import _lib, linalg, mesh
+from helpers import tet10_box
+from oracle import fem
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden", "mesh_fixtures.npz")
+
+
+def test_mesh_generators_match_reference_fixtures():
+    """Fixtures produced by the reference's gfem/mesh.py (tests/golden/make_golden.py)."""
+    g = np.load(GOLDEN)
+    cases = {"c1": (100.0, 20.0, 20.0, 20, 4, 4), "small": (1.0, 1.0, 1.0, 2, 3, 4), "cant": (10.0, 1.0, 1.0, 20, 2, 2)}
+    for name, args in cases.items():
+        X, c = mesh.box_hex(*args)
+        np.testing.assert_array_equal(X, g[f"{name}_hex_X"])
+        np.testing.assert_array_equal(c, g[f"{name}_hex_conn"])
+    for name in ("t", "tj"):
+        Xh = g[f"{name}_hexX"]
+        _, c = mesh.box_hex(1.0, 1.0, 1.0, 3, 3, 3)
+        X4, c4 = mesh.hex_to_tet4(Xh, c)
+        np.testing.assert_array_equal(c4, g[f"{name}_tet4"])
+        X10, c10 = mesh.tet4_to_tet10(X4, c4)
+        np.testing.assert_array_equal(c10, g[f"{name}_tet10"])
+        np.testing.assert_array_equal(X10, g[f"{name}_X10"])
+
+
+def test_library_exports_every_declared_symbol():
+    header = open(os.path.join(ROOT, "include", "exfem_b200.h")).read()
+    header = re.sub(r"/\*.*?\*/", "", header, flags=re.S)
+    names = set(re.findall(r"\bint\s+(exfem_\w+)\s*\(", header)) | set(re.findall(r"\bconst char\*\s+(exfem_\w+)\s*\(", header))
+    assert len(names) > 30
+    lib = C.CDLL(_lib.LIB_PATH)
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.EXPORTED) <= names
+
+
+def _host_plan(c, nn):
+    c32 = np.ascontiguousarray(c, dtype=np.int32)
+    vmax = C.c_int()
+    assert _lib.lib.exfem_host_gather_plan(nn, len(c), c.shape[1], c32.ctypes.data, None, C.byref(vmax)) == 0
+    plan = np.empty((nn, vmax.value), np.int32)
+    assert _lib.lib.exfem_host_gather_plan(nn, len(c), c.shape[1], c32.ctypes.data, plan.ctypes.data, C.byref(vmax)) == 0
+    return plan
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_host_gather_plan_and_colouring_bit_exact(kind):
+    if kind == "hex":
+        X, c = mesh.box_hex(1, 1, 1, 5, 4, 3)
+    else:
+        X, c = tet10_box(1, 1, 1, 3, 3, 2)
+    np.testing.assert_array_equal(_host_plan(c, len(X)), fem.gather_plan([c], len(X)))
+    col = np.empty(len(c), np.int32)
+    nc = C.c_int()
+    c32 = np.ascontiguousarray(c, dtype=np.int32)
+    assert _lib.lib.exfem_host_colouring(len(X), len(c), c.shape[1], c32.ctypes.data, col.ctypes.data, C.byref(nc)) == 0
+    np.testing.assert_array_equal(col, fem.greedy_colouring(c, len(X)))
+    assert nc.value == col.max() + 1
+
+
+def test_host_gather_plan_rejects_bad_connectivity():
+    c = np.array([[0, 1, 2, 3, 4, 5, 6, 99]], np.int32)
+    vmax = C.c_int()
+    assert _lib.lib.exfem_host_gather_plan(8, 1, 8, c.ctypes.data, None, C.byref(vmax)) == _lib.ERR_ARG
+    assert "outside" in _lib.last_error()
+
+
+def test_standard_aggregation_partitions_the_graph():
+    X, c = mesh.box_hex(1, 1, 1, 6, 5, 4)
+    rows = np.repeat(c, 8, axis=1).ravel()
+    cols = np.tile(c, (1, 8)).ravel()
+    S = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(len(X), len(X)))
+    S.sum_duplicates()
+    agg, nagg = linalg._aggregate(S)
+    assert agg.min() >= 0 and agg.max() == nagg - 1
+    assert np.bincount(agg).min() >= 1
+    # every aggregate is connected through the graph (a root and its neighbours)
+    for a in range(nagg):
+        members = np.nonzero(agg == a)[0]
+        sub = S[members][:, members]
+        ncomp, _ = sp.csgraph.connected_components(sub, directed=False)
+        assert ncomp == 1
+
+
+def test_sa_hierarchy_properties():
+    """Host set-up: P interpolates the rigid-body modes at the tentative stage,
+    coarse operators are symmetric Galerkin products, sizes shrink to <= 300."""
+    import torch
+    X, c = mesh.box_hex(10.0, 2.0, 2.0, 12, 3, 3)
+    m = fem.Model(X)
+    m.add_block(c, fem.HEX8, fem.LinearElastic(200e3, 0.3))
+    ops = [(d, K.numpy()) for d, K in m.stiffness_ops(torch.zeros(m.ndof, dtype=torch.float64), m.init_state())]
+    free = np.ones(m.ndof)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    for d in range(3):
+        free[fix * 3 + d] = 0
+    A = linalg.bc_matrix(fem.ops_assemble(ops, m.ndof), free)
+    B = linalg.rigid_body_modes(X)
+    levels, Ac = linalg.sa_hierarchy(A, B, 3, 300)
+    assert len(levels) >= 1 and Ac.shape[0] <= 300
+    for Al, P in levels:
+        assert abs(Al - Al.T).max() <= 1e-9 * abs(Al).max()
+    S = linalg._strength_graph(A, 3)
+    agg, nagg = linalg._aggregate(S)
+    T, Bc = linalg._fit_candidates(agg, nagg, B, 3)
+    free_nodes = np.nonzero(agg[np.arange(m.ndof) // 3] >= 0)[0]
+    np.testing.assert_allclose((T @ Bc)[free_nodes], B[free_nodes], atol=1e-9 * np.abs(B).max())
+
+
+def test_bench_replicas_world_size_two_gloo(tmp_path):
+    """The multi-GPU path is replicas: max-over-ranks timing and rank-0 output.
+    Exercised with two gloo ranks on the CPU."""
+    code = r'''
+import os, torch, torch.distributed as dist
+dist.init_process_group("gloo")
+r, w = dist.get_rank(), dist.get_world_size()
+t = torch.tensor([1.0 + r])
+dist.all_reduce(t, op=dist.ReduceOp.MAX)
+assert float(t) == float(w)
+units = torch.tensor([100.0])
+dist.all_reduce(units)
+if r == 0:
+    print("OK", float(units) / float(t))
+dist.destroy_process_group()
+'''
+    f = tmp_path / "rep.py"
+    f.write_text(code)
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT="29571")
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+                        "--master-addr", "127.0.0.1", "--master-port", "29571", str(f)],
+                       capture_output=True, text=True, env=env, timeout=300)
+    assert "OK 100.0" in r.stdout, r.stderr[-2000:]
