@@ -128,7 +128,7 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
   EX_ARG(nn >= 0 && ne >= 0, "negative sizes");
   EX_ARG(nn == 0 || X_host, "X is NULL");
   EX_ARG(ne == 0 || conn_host, "conn is NULL");
-  EX_ARG(3 * nn < (int64_t)INT32_MAX, "too many nodes for int32 DOF indices");
+  EX_ARG(3 * nn < (int64_t)INT32_MAX && nn < (int64_t(1) << 29), "too many nodes for int32 DOF indices");
   auto b = std::make_unique<exfem_block_s>();
   cudaGetDevice(&b->device);
   b->etype = etype;
@@ -180,6 +180,8 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
     b->ntile = (int64_t)tp.size() - 1;
     if ((s = b->tile_ptr.upload(tp.data(), tp.size()))) return s;
     if ((s = b->tile_nodes.upload(tn.data(), std::max<size_t>(tn.size(), 1)))) return s;
+    if ((s = b->tile_nodes_bc.upload(tn.data(), std::max<size_t>(tn.size(), 1)))) return s;
+    b->tile_nodes_host = tn;
     if ((s = b->tile_nend.upload(te.data(), std::max<size_t>(te.size(), 1)))) return s;
     if ((s = b->tile_perm.upload(tq.data(), std::max<size_t>(tq.size(), 1)))) return s;
     {  // forward map of the slot lists: list position of every slot's node
@@ -191,6 +193,16 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
           for (; q < te[tp[t] + k]; ++q) li[t * NS + tq[t * NS + q]] = (uint16_t)k;
       }
       if ((s = b->lidx.upload(li.data(), std::max<size_t>(li.size(), 1)))) return s;
+    }
+    {  // node -> entry map of the tile node lists (counting sort, entries increasing)
+      std::vector<int32_t> np(nn + 1, 0), dest(tn.size());
+      for (int32_t n : tn) ++np[n + 1];
+      for (int64_t n = 0; n < nn; ++n) np[n + 1] += np[n];
+      std::vector<int32_t> cur(np.begin(), np.end() - 1);
+      for (size_t q = 0; q < tn.size(); ++q) dest[q] = cur[tn[q]]++;   // tile order within a node
+      if ((s = b->node_ptr.upload(np.data(), np.size()))) return s;
+      if ((s = b->tile_dest.upload(dest.data(), std::max<size_t>(dest.size(), 1)))) return s;
+      if ((s = b->partial.alloc(std::max<size_t>(3 * tn.size(), 1)))) return s;
     }
     if ((s = b->dev_err.alloc(1))) return s;
     EX_CUDA(cudaMemset(b->dev_err.p, 0, sizeof(int)));
@@ -290,6 +302,9 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
   if (!fixed_host) {
     b->fixed.release();
     b->node_fixed.release();
+    if (!b->tile_nodes_host.empty())
+      EX_CUDA(cudaMemcpy(b->tile_nodes_bc.p, b->tile_nodes_host.data(), b->tile_nodes_host.size() * sizeof(int32_t),
+                         cudaMemcpyHostToDevice));
     return EXFEM_OK;
   }
   std::vector<uint8_t> f(fixed_host, fixed_host + b->ndof()), nf(b->nn, 0);
@@ -298,6 +313,11 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
       f[3 * n + c] = f[3 * n + c] ? 1 : 0;
       nf[n] |= (uint8_t)(f[3 * n + c] << c);
     }
+  if (!b->tile_nodes_host.empty()) {  // fixed-DOF bits packed above the node id
+    std::vector<int32_t> packed(b->tile_nodes_host);
+    for (auto& q : packed) q = (int32_t)((uint32_t)q | ((uint32_t)nf[q] << 29));
+    EX_CUDA(cudaMemcpy(b->tile_nodes_bc.p, packed.data(), packed.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   if (b->fixed.n == (size_t)b->ndof()) {
     EX_CUDA(cudaMemcpy(b->fixed.p, f.data(), f.size(), cudaMemcpyHostToDevice));
     EX_CUDA(cudaMemcpy(b->node_fixed.p, nf.data(), nf.size(), cudaMemcpyHostToDevice));

@@ -121,6 +121,15 @@ __host__ __device__ constexpr int tet_edge(int k, int end) {  // gfem/elements.p
   return end == 0 ? (k == 0 ? 0 : k == 1 ? 1 : k == 2 ? 2 : k == 3 ? 0 : k == 4 ? 1 : 2)
                   : (k == 0 ? 1 : k == 1 ? 2 : k == 2 ? 0 : 3);
 }
+// mid-edge node (4..9) between corners j != k (edge order of gfem/elements.py:167)
+__host__ __device__ constexpr int tet_edge_node(int j, int k) {
+  return (j == 0 && k == 1) || (j == 1 && k == 0)   ? 4
+       : (j == 1 && k == 2) || (j == 2 && k == 1) ? 5
+       : (j == 0 && k == 2) || (j == 2 && k == 0) ? 6
+       : (j == 0 && k == 3) || (j == 3 && k == 0) ? 7
+       : (j == 1 && k == 3) || (j == 3 && k == 1) ? 8
+                                                  : 9;
+}
 // dN_a / d xi_i at Gauss point g (corner: L(2L-1); edge: 4 L_p L_q)
 __host__ __device__ constexpr double tet10_dN(int g, int a, int i) {
   return a < 4 ? (4.0 * tet_L(g, a) - 1.0) * tet_dL(a, i)

@@ -34,9 +34,14 @@ struct exfem_block_s {
   int maxu = 0;                       // largest distinct-node count of a tile
   exfem::DevBuf<int32_t> tile_ptr;    // (ntile+1)
   exfem::DevBuf<int32_t> tile_nodes;  // concatenated sorted node lists
+  exfem::DevBuf<int32_t> tile_nodes_bc;  // same, node | fixed-DOF bits << 29
+  std::vector<int32_t> tile_nodes_host;
   exfem::DevBuf<uint16_t> lidx;       // tile-major (ntile, nnode*MF_TILE): list position of each slot's node
   exfem::DevBuf<uint16_t> tile_nend;  // per listed node: end of its slot run in tile_perm
   exfem::DevBuf<uint16_t> tile_perm;  // tile-major (ntile, nnode*MF_TILE) slots grouped by node
+  exfem::DevBuf<int32_t> node_ptr;    // (nn+1) node -> its run of tile entries in node-major order
+  exfem::DevBuf<int32_t> tile_dest;   // per tile-list entry: its node-major position
+  exfem::DevBuf<double> partial;      // per-entry tile sums, 3 per entry (FP64 or FP32 view)
   exfem::DevBuf<int> dev_err;         // set by bounded waits that give up
   exfem::DevBuf<double> geo64;        // (ne, geo_stride)
   exfem::DevBuf<float> geo32;

@@ -11,16 +11,21 @@
 //      single thread moves them into shared memory with bulk TMA copies
 //      (cp.async.bulk, mbarrier completion), double buffered so that the copy of
 //      the next tile overlaps the work on this one;
-//   2. v is gathered once per distinct node of the tile (masked by the fixed-DOF
-//      bits) into shared memory — ~3 distinct nodes per element instead of 8/10
-//      node slots;
+//   2. v is gathered once per distinct node of the tile into shared memory —
+//      ~3 distinct nodes per element instead of 8/10 node slots — with
+//      asynchronous cp.async copies issued one tile ahead (fixed DOFs, whose bits
+//      sit above the node id in the tile list, are zero filled), so the gather
+//      of the next tile overlaps the arithmetic of this one;
 //   3. one thread per element evaluates the element product from shared memory
 //      (C3D8: modal B-bar form; C3D10: constant inverse Jacobian of the
 //      straight-edged element) and accumulates it into per-node shared-memory
 //      sums;
-//   4. one global reduction per distinct node (an 8-byte vector reduction plus a
-//      scalar one) adds the tile's sums into y (initialised to fixed*v by a
-//      separate pass).
+//   4. the tile's per-node sums are stored (plain stores, no atomics) at their
+//      precomputed positions in a node-major partials buffer;
+// and a second, node-centric pass forms y[n] = fixed ? v : the sum of node n's
+// contiguous run of tile entries, in tile order (the reference's atomic-free
+// gather-plan assembly, gfem/model.py:241-267, at tile granularity).  The
+// product is deterministic.
 // Geometry: C3D8 stores the 7 modal coordinate vectors (coordinates with the
 // centroid removed) and the stiffness scale; C3D10 stores the inverse Jacobian
 // and scaled volume, formed in FP64 from the nodal coordinates and rounded once.
@@ -61,6 +66,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   if (err) atomicExch(err, 1);
   return false;
 }
+
+// 4- or 8-byte asynchronous global->shared copy; src_bytes = 0 writes zeros
+template <int N>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(dst)), "l"(src), "n"(N), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <class T>
 __device__ __forceinline__ void matmul3t(const T (&A)[9], const T (&B)[9], T (&C)[9]) {
@@ -145,26 +160,45 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       for (int i = 0; i < 3; ++i) Fm[i][c] += tacc * iJ0[3 * i + c];
     hex_from_modal(Fm, f);
   } else {
+    // C3D10 with a constant Jacobian, in barycentric form: with L the
+    // barycentric coordinates, w_j = du/dL_j = base_j + D * (g == j ? v_j : v_e(j,g))
+    // at Gauss point g (L_g = A, others B), base_j = (4B-1) v_j + 4B sum of the
+    // edge nodes at corner j, D = 4(A-B); the reference gradient is
+    // G_i = w_{i+1} - w_0.  The force is the adjoint of the same steps.
+    constexpr T A = T(TET_A), B = T(TET_B);
+    constexpr T D = T(4.0 * (TET_A - TET_B)), C0 = T(4.0 * TET_B - 1.0), C1 = T(4.0 * TET_B);
     T iJ[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) iJ[k] = g[k * MF_TILE];
     const T vol = g[9 * MF_TILE];
+    (void)A;
+    (void)B;
+    T base[4][3], vbar[10][3], bbar[4][3];
 #pragma unroll
-    for (int a = 0; a < 10; ++a) f[a][0] = f[a][1] = f[a][2] = T(0);
+    for (int c = 0; c < 3; ++c) {
+      base[0][c] = C0 * va[0][c] + C1 * (va[4][c] + va[6][c] + va[7][c]);
+      base[1][c] = C0 * va[1][c] + C1 * (va[4][c] + va[5][c] + va[8][c]);
+      base[2][c] = C0 * va[2][c] + C1 * (va[5][c] + va[6][c] + va[9][c]);
+      base[3][c] = C0 * va[3][c] + C1 * (va[7][c] + va[8][c] + va[9][c]);
+    }
+#pragma unroll
+    for (int a = 0; a < 10; ++a) vbar[a][0] = vbar[a][1] = vbar[a][2] = T(0);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bbar[j][0] = bbar[j][1] = bbar[j][2] = T(0);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
+      T w[4][3];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int src = jj == q ? jj : tet_edge_node(jj, q);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) w[jj][c] = base[jj][c] + D * va[src][c];
+      }
       T G[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) G[k] = T(0);
+      for (int c = 0; c < 3; ++c)
 #pragma unroll
-      for (int a = 0; a < 10; ++a)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const T dn = T(tet10_dN(q, a, i));
-          if (dn != T(0))
-#pragma unroll
-            for (int c = 0; c < 3; ++c) G[3 * c + i] += va[a][c] * dn;
-        }
+        for (int i = 0; i < 3; ++i) G[3 * c + i] = w[i + 1][c] - w[0][c];
       T H[9];
       matmul3t(G, iJ, H);
       T ee[6], s[6];
@@ -178,16 +212,40 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int k = 0; k < 3; ++k) Q[3 * i + k] = r[i][0] * iJ[3 * k] + r[i][1] * iJ[3 * k + 1] + r[i][2] * iJ[3 * k + 2];
+      // adjoint: wbar_{i+1} = Q[:, i], wbar_0 = -sum_i Q[:, i]
 #pragma unroll
-      for (int a = 0; a < 10; ++a)
+      for (int c = 0; c < 3; ++c) {
+        T wb[4];
+        wb[1] = Q[3 * c + 0];
+        wb[2] = Q[3 * c + 1];
+        wb[3] = Q[3 * c + 2];
+        wb[0] = -(wb[1] + wb[2] + wb[3]);
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          const T dn = T(tet10_dN(q, a, i));
-          if (dn != T(0))
-#pragma unroll
-            for (int c = 0; c < 3; ++c) f[a][c] += Q[3 * c + i] * dn;
+        for (int jj = 0; jj < 4; ++jj) {
+          bbar[jj][c] += wb[jj];
+          const int src = jj == q ? jj : tet_edge_node(jj, q);
+          vbar[src][c] += D * wb[jj];
         }
+      }
     }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      vbar[0][c] += C0 * bbar[0][c];
+      vbar[1][c] += C0 * bbar[1][c];
+      vbar[2][c] += C0 * bbar[2][c];
+      vbar[3][c] += C0 * bbar[3][c];
+      const T e0 = C1 * bbar[0][c], e1 = C1 * bbar[1][c], e2 = C1 * bbar[2][c], e3 = C1 * bbar[3][c];
+      vbar[4][c] += e0 + e1;   // edge (0,1)
+      vbar[5][c] += e1 + e2;   // edge (1,2)
+      vbar[6][c] += e0 + e2;   // edge (2,0)
+      vbar[7][c] += e0 + e3;   // edge (0,3)
+      vbar[8][c] += e1 + e3;   // edge (1,3)
+      vbar[9][c] += e2 + e3;   // edge (2,3)
+    }
+#pragma unroll
+    for (int a = 0; a < 10; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) f[a][c] = vbar[a][c];
   }
 }
 
@@ -202,35 +260,12 @@ struct TileLayout {
   static_assert(GEO_B % 16 == 0 && LIDX_B % 16 == 0 && TAN_B % 16 == 0, "bulk copies need 16-byte multiples");
 };
 
-// add a node's three components into y (12-byte stride): one 8-byte vector
-// reduction for the aligned pair and one scalar reduction
-__device__ __forceinline__ void red_node(float* y, int64_t n, float a, float b, float c, uint8_t bits) {
-  float* p = y + 3 * n;
-  if (bits) {
-    if (!(bits & 1)) atomicAdd(p, a);
-    if (!(bits & 2)) atomicAdd(p + 1, b);
-    if (!(bits & 4)) atomicAdd(p + 2, c);
-  } else if ((n & 1) == 0) {
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(a), "f"(b) : "memory");
-    atomicAdd(p + 2, c);
-  } else {
-    atomicAdd(p, a);
-    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p + 1), "f"(b), "f"(c) : "memory");
-  }
-}
-__device__ __forceinline__ void red_node(double* y, int64_t n, double a, double b, double c, uint8_t bits) {
-  double* p = y + 3 * n;
-  if (!(bits & 1)) atomicAdd(p, a);
-  if (!(bits & 2)) atomicAdd(p + 1, b);
-  if (!(bits & 4)) atomicAdd(p + 2, c);
-}
-
 template <class T, int ET, bool J2, bool TMA>
 __global__ void __launch_bounds__(MF_TILE)
 mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint16_t* __restrict__ lidx,
-               const T* __restrict__ tan, const int32_t* __restrict__ tptr, const int32_t* __restrict__ tnodes,
-               const uint8_t* __restrict__ nfix, const T* __restrict__ v, T* __restrict__ y, T lam, T mu, T Kb,
-               int maxu, const int* __restrict__ skip, int* __restrict__ err) {
+               const T* __restrict__ tan, const int32_t* __restrict__ tptr, const int32_t* __restrict__ tpack,
+               const int32_t* __restrict__ tdest, const T* __restrict__ v, T* __restrict__ part, T lam, T mu,
+               T Kb, int maxu, const int* __restrict__ skip, int* __restrict__ err) {
   using L = TileLayout<T, ET, J2>;
   constexpr int NN = L::NN, NG = L::NG, GS = L::GS, NSLOT = L::NSLOT;
   if (skip && *skip) return;
@@ -242,8 +277,10 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
   // order) fall into different warps and their shared-memory additions to the
   // same node rarely collide inside one warp instruction
   const int lt = 4 * (tid & 31) + (tid >> 5);
-  T* xs = reinterpret_cast<T*>(smem + (TMA ? 2 * L::STAGE_B : 0));  // gathered v, node-major per component
-  T* ys = xs + 3 * maxu;                                              // accumulated products
+  T* xsb[2];                                                          // gathered v, double buffered
+  xsb[0] = reinterpret_cast<T*>(smem + (TMA ? 2 * L::STAGE_B : 0));
+  xsb[1] = xsb[0] + 3 * maxu;
+  T* ys = xsb[1] + 3 * maxu;                                          // accumulated products
   auto stage_geo = [&](int s) { return reinterpret_cast<T*>(smem + s * L::STAGE_B); };
   auto stage_lidx = [&](int s) { return reinterpret_cast<uint16_t*>(smem + s * L::STAGE_B + L::GEO_B); };
   auto stage_tan = [&](int s) { return reinterpret_cast<T*>(smem + s * L::STAGE_B + L::GEO_B + L::LIDX_B); };
@@ -254,6 +291,21 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     bulk_g2s(stage_lidx(s), lidx + t * NSLOT, L::LIDX_B, &bar[s]);
     if constexpr (J2) bulk_g2s(stage_tan(s), tan + t * (NG * 8 * MF_TILE), L::TAN_B, &bar[s]);
   };
+  // asynchronous gather of the tile's distinct nodes (fixed DOFs zero filled)
+  auto gather = [&](int64_t t, T* xs) {
+    const int64_t u0 = tptr[t];
+    const int nu = tptr[t + 1] - (int32_t)u0;
+    for (int k = tid; k < nu; k += MF_TILE) {
+      const uint32_t pk = (uint32_t)tpack[u0 + k];
+      const int64_t n = pk & 0x1FFFFFFFu;
+      const uint32_t bits = pk >> 29;
+      const T* vp = v + 3 * n;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) cp_async<sizeof(T)>(xs + c * maxu + k, vp + c, ((bits >> c) & 1) ? 0 : (int)sizeof(T));
+    }
+    cp_async_commit();
+  };
+  for (int k = tid; k < 3 * maxu; k += MF_TILE) ys[k] = T(0);
   if constexpr (TMA) {
     if (tid == 0) {
       mbar_init(&bar[0], 1);
@@ -263,29 +315,27 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     __syncthreads();
     if (tid == 0 && (int64_t)blockIdx.x < ntile) issue(blockIdx.x, 0);
   }
+  if ((int64_t)blockIdx.x < ntile) gather(blockIdx.x, xsb[0]);
+  __syncthreads();
   int it = 0;
   for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x, ++it) {
     const int s = it & 1;
+    const int64_t tn = t + gridDim.x;
     if constexpr (TMA) {
-      const int64_t tn = t + gridDim.x;
       if (tid == 0 && tn < ntile) issue(tn, s ^ 1);
     }
-    // distinct nodes of the tile: gather masked v, clear the accumulators
-    const int64_t u0 = tptr[t];
-    const int nu = tptr[t + 1] - (int32_t)u0;
-    for (int j = tid; j < 3 * nu; j += MF_TILE) {
-      const int k = j / 3, c = j - 3 * k;
-      const int64_t n = tnodes[u0 + k];
-      const uint8_t bits = nfix ? nfix[n] : (uint8_t)0;
-      xs[c * maxu + k] = ((bits >> c) & 1) ? T(0) : v[3 * n + c];
-      ys[c * maxu + k] = T(0);
-    }
+    if (tn < ntile) gather(tn, xsb[s ^ 1]);
+    else cp_async_commit();                                            // keep one group per iteration
+    cp_async_wait<1>();                                                // this tile's gather has landed
     const T* g;
     const uint16_t* li;
     const T* tnp;
     if constexpr (TMA) {
       const bool ok = mbar_wait_bounded(&bar[s], (uint32_t)((it >> 1) & 1), err);
-      if (__syncthreads_or(!ok)) return;
+      if (__syncthreads_or(!ok)) {
+        cp_async_wait<0>();
+        return;
+      }
       g = stage_geo(s);
       li = stage_lidx(s);
       tnp = J2 ? stage_tan(s) : nullptr;
@@ -295,6 +345,7 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
       li = lidx + t * NSLOT;
       tnp = J2 ? tan + t * (NG * 8 * MF_TILE) : nullptr;
     }
+    const T* xs = xsb[s];
     const int64_t e = t * MF_TILE + lt;
     if (e < ne) {
       int l[NN];
@@ -313,33 +364,63 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
         for (int c = 0; c < 3; ++c) atomicAdd(&ys[c * maxu + l[a]], f[a][c]);
     }
     __syncthreads();
-    // one reduction per distinct node into y
+    // the tile's per-node sums, stored (not added) at their node-major positions
+    const int64_t u0 = tptr[t];
+    const int nu = tptr[t + 1] - (int32_t)u0;
     for (int k = tid; k < nu; k += MF_TILE) {
-      const int64_t n = tnodes[u0 + k];
-      const uint8_t bits = nfix ? nfix[n] : (uint8_t)0;
-      red_node(y, n, ys[k], ys[maxu + k], ys[2 * maxu + k], bits);
+      T* p = part + 3 * (int64_t)tdest[u0 + k];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        p[c] = ys[c * maxu + k];
+        ys[c * maxu + k] = T(0);
+      }
     }
     __syncthreads();
   }
+  cp_async_wait<0>();
 }
 
-// y = fixed ? v : 0 before the scatter
+// pass 2: y[3n+c] = fixed ? v : sum of node n's tile entries (a contiguous run
+// in node-major order, tile order inside the run)
 template <class T>
-__global__ void mf_init_kernel(int64_t ndof, const uint8_t* __restrict__ fixed, const T* __restrict__ v,
-                               T* __restrict__ y, const int* __restrict__ skip) {
+__global__ void mf_gather_kernel(int64_t nn, const int32_t* __restrict__ node_ptr, const T* __restrict__ part,
+                                 const uint8_t* __restrict__ fixed, const T* __restrict__ v, T* __restrict__ y,
+                                 const int* __restrict__ skip) {
   if (skip && *skip) return;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ndof; i += (int64_t)gridDim.x * blockDim.x)
-    y[i] = (fixed && fixed[i]) ? v[i] : T(0);
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    T s0 = T(0), s1 = T(0), s2 = T(0);
+    const int32_t q1 = node_ptr[n + 1];
+    for (int32_t q = node_ptr[n]; q < q1; q += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (q + u < q1) {
+          const T* p = part + 3 * (int64_t)(q + u);
+          s0 += p[0];
+          s1 += p[1];
+          s2 += p[2];
+        }
+    }
+    const int64_t d = 3 * n;
+    if (fixed) {
+      y[d] = fixed[d] ? v[d] : s0;
+      y[d + 1] = fixed[d + 1] ? v[d + 1] : s1;
+      y[d + 2] = fixed[d + 2] ? v[d + 2] : s2;
+    } else {
+      y[d] = s0;
+      y[d + 1] = s1;
+      y[d + 2] = s2;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- launch
 template <class T, int ET, bool J2>
-static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const uint8_t* nf, const T* v, T* y,
+static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* part,
                  const int* skip, cudaStream_t s) {
   constexpr bool TMA = sizeof(T) == 4;
   using L = TileLayout<T, ET, J2>;
   auto kern = mf_tile_kernel<T, ET, J2, TMA>;
-  const size_t smem = (TMA ? 2 * (size_t)L::STAGE_B : 0) + 2 * 3 * (size_t)b->maxu * sizeof(T);
+  const size_t smem = (TMA ? 2 * (size_t)L::STAGE_B : 0) + 3 * 3 * (size_t)b->maxu * sizeof(T);
   // per (kernel, shared-memory size): opt in above 48 KB and size the persistent grid
   static thread_local size_t opted = 0;
   static thread_local int per_sm = 0, nsm = 0, dev = -1;
@@ -357,8 +438,8 @@ static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const uint8_t* nf
     return EXFEM_ERR_UNSUPPORTED;
   }
   const int64_t grid = std::min<int64_t>(b->ntile, (int64_t)nsm * per_sm);
-  kern<<<(unsigned)grid, MF_TILE, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p,
-                                             b->tile_nodes.p, nf, v, y, (T)b->mat.lam, (T)b->mat.mu, (T)b->mat.K,
+  kern<<<(unsigned)grid, MF_TILE, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p, tpack,
+                                             b->tile_dest.p, v, part, (T)b->mat.lam, (T)b->mat.mu, (T)b->mat.K,
                                              b->maxu, skip, b->dev_err.p);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
@@ -368,33 +449,36 @@ template <class T>
 int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaStream_t s, bool bc) {
   const int64_t ndof = b->ndof();
   if (ndof == 0) return EXFEM_OK;
-  if ((reinterpret_cast<uintptr_t>(y) & 7) != 0) {
-    set_error("matrix-free product: y must be 8-byte aligned");
-    return EXFEM_ERR_ARG;
-  }
   if (b->etype == EXFEM_C3D10 && !b->affine) {
     set_error("matrix-free C3D10 needs straight-edged elements (mid-nodes at edge midpoints)");
     return EXFEM_ERR_UNSUPPORTED;
   }
-  mf_init_kernel<T><<<grid_for(ndof, 256), 256, 0, s>>>(ndof, bc ? b->fixed.p : nullptr, v, y, skip);
-  EX_LAUNCH_CHECK();
-  if (b->ne == 0) return EXFEM_OK;
-  const T* geo;
-  const T* tan;
-  if constexpr (sizeof(T) == 8) {
-    geo = (const T*)b->geo64.p;
-    tan = (const T*)b->tan64.p;
-  } else {
-    geo = (const T*)b->geo32.p;
-    tan = (const T*)b->tan32.p;
+  T* part = reinterpret_cast<T*>(b->partial.p);
+  if (b->ne) {
+    const T* geo;
+    const T* tan;
+    if constexpr (sizeof(T) == 8) {
+      geo = (const T*)b->geo64.p;
+      tan = (const T*)b->tan64.p;
+    } else {
+      geo = (const T*)b->geo32.p;
+      tan = (const T*)b->tan32.p;
+    }
+    const bool j2 = b->mat.kind == EXFEM_J2;
+    const int32_t* nf = (bc && b->fixed.p) ? b->tile_nodes_bc.p : b->tile_nodes.p;
+    int st;
+    if (b->etype == EXFEM_C3D8)
+      st = j2 ? mf_go<T, EXFEM_C3D8, true>(b, geo, tan, nf, v, part, skip, s)
+              : mf_go<T, EXFEM_C3D8, false>(b, geo, tan, nf, v, part, skip, s);
+    else
+      st = j2 ? mf_go<T, EXFEM_C3D10, true>(b, geo, tan, nf, v, part, skip, s)
+              : mf_go<T, EXFEM_C3D10, false>(b, geo, tan, nf, v, part, skip, s);
+    if (st) return st;
   }
-  const bool j2 = b->mat.kind == EXFEM_J2;
-  const uint8_t* nf = bc ? b->node_fixed.p : nullptr;
-  if (b->etype == EXFEM_C3D8)
-    return j2 ? mf_go<T, EXFEM_C3D8, true>(b, geo, tan, nf, v, y, skip, s)
-              : mf_go<T, EXFEM_C3D8, false>(b, geo, tan, nf, v, y, skip, s);
-  return j2 ? mf_go<T, EXFEM_C3D10, true>(b, geo, tan, nf, v, y, skip, s)
-            : mf_go<T, EXFEM_C3D10, false>(b, geo, tan, nf, v, y, skip, s);
+  mf_gather_kernel<T><<<grid_for(b->nn, 256), 256, 0, s>>>(b->nn, b->node_ptr.p, part, bc ? b->fixed.p : nullptr,
+                                                           v, y, skip);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
 }
 
 template int launch_mf_matvec<float>(exfem_block_s*, const float*, float*, const int*, cudaStream_t, bool);
