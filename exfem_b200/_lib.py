@@ -57,6 +57,7 @@ _SIGS = {
     "exfem_block_tile_maps": ([VP, P, P, P, P], C.c_int),
     "exfem_block_set_scale": ([VP, P], C.c_int),
     "exfem_block_set_fixed": ([VP, P], C.c_int),
+    "exfem_block_set_lame": ([VP, P, P], C.c_int),
     "exfem_internal_force": ([VP, P, P, P, P, P, C.c_int, VP], C.c_int),
     "exfem_element_stiffness": ([VP, P, P, C.c_int, P, VP], C.c_int),
     "exfem_tangent_update": ([VP, P, P, VP], C.c_int),
@@ -69,6 +70,8 @@ _SIGS = {
     "exfem_amg_destroy": ([VP], C.c_int),
     "exfem_amg_add_level": ([VP, I64, I64, P, P, P, P, P, P, P, P, P, P, D], C.c_int),
     "exfem_amg_set_coarse": ([VP, I64, P], C.c_int),
+    "exfem_amg_set_level_rows": ([VP, C.c_int, P], C.c_int),
+    "exfem_amg_set_coarse_blocks": ([VP, I64, P, P], C.c_int),
     "exfem_amg_vcycle": ([VP, C.c_int, P, P, VP, P, VP], C.c_int),
     "exfem_amg_vcycle_noalloc": ([VP, C.c_int, P, P, VP, P, VP], C.c_int),
     "exfem_solver_create": ([VP, C.c_int, C.c_int, VP, C.POINTER(VP)], C.c_int),
@@ -79,6 +82,10 @@ _SIGS = {
     "exfem_solver_pcg": ([VP, P, P, D, C.c_int, C.POINTER(I32), C.POINTER(D), VP], C.c_int),
     "exfem_solver_mixed": ([VP, P, P, D, D, C.c_int, C.c_int, C.POINTER(I32), C.POINTER(I32), C.POINTER(D), VP],
                            C.c_int),
+    "exfem_amg_replicate": ([VP, C.c_int, P, C.c_int, P], C.c_int),
+    "exfem_batch_create": ([VP, VP, C.c_int, P, C.POINTER(VP)], C.c_int),
+    "exfem_batch_destroy": ([VP], C.c_int),
+    "exfem_batch_solve": ([VP, P, P, D, D, C.c_int, C.c_int, P, C.POINTER(I32), P, VP], C.c_int),
     "exfem_host_gather_plan": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_colouring": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_standard_aggregation": ([I64, P, P, P, C.POINTER(I64)], C.c_int),

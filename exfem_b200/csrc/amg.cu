@@ -28,7 +28,8 @@ __global__ void __launch_bounds__(256)
 spmv_kernel(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx,
             const T* __restrict__ val, const T* __restrict__ x, T* __restrict__ y,
             const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ d2,
-            T* __restrict__ xo, T c1, T c2, const int* __restrict__ skip) {
+            T* __restrict__ xo, T c1, T c2, const T* __restrict__ rc1, const T* __restrict__ rc2,
+            const int64_t* __restrict__ rmap, const int64_t* __restrict__ cshift, const int* __restrict__ skip) {
   if (skip && *skip) return;
   constexpr int GPW = 32 / LANES;  // row groups per warp
   const int lane = threadIdx.x & (LANES - 1);
@@ -39,8 +40,10 @@ spmv_kernel(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restric
     const int64_t row = base + grp;
     T s = T(0);
     if (row < n) {
-      const int64_t k1 = ptr[row + 1];
-      for (int64_t k = ptr[row] + lane; k < k1; k += LANES) s += val[k] * x[idx[k]];
+      const int64_t sr = rmap ? rmap[row] : row;
+      const int64_t cs = rmap ? cshift[row] : 0;
+      const int64_t k1 = ptr[sr + 1];
+      for (int64_t k = ptr[sr] + lane; k < k1; k += LANES) s += val[k] * x[idx[k] + cs];
     }
 #pragma unroll
     for (int o = LANES / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LANES);
@@ -54,13 +57,13 @@ spmv_kernel(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restric
       } else if (MODE == SP_RESINIT) {
         const T r = dinv[row] * (b[row] - s);
         y[row] = r;
-        d2[row] = r * c1;
+        d2[row] = r * (rc1 ? rc1[5 * row] : c1);
       } else {  // SP_CHEB: x is the direction d
         const T d = x[row];
         xo[row] += d;
         const T r = y[row] - dinv[row] * s;
         y[row] = r;
-        d2[row] = c1 * d + c2 * r;
+        d2[row] = (rc1 ? rc1[5 * row] : c1) * d + (rc2 ? rc2[5 * row] : c2) * r;
       }
     }
   }
@@ -68,13 +71,15 @@ spmv_kernel(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restric
 
 template <class T, int MODE>
 static int spmv_lanes(const Csr64& A, const T* val, const T* x, T* y, const T* b, const T* dinv, T* d2,
-                      T* xo, T c1, T c2, const int* skip, cudaStream_t s) {
+                      T* xo, T c1, T c2, const int* skip, cudaStream_t s, const T* rc1 = nullptr,
+                      const T* rc2 = nullptr) {
   if (A.n == 0) return EXFEM_OK;
-  const double avg = A.n ? (double)A.nnz / (double)A.n : 0.0;
+  const int64_t nsrc = A.ptr.n ? (int64_t)A.ptr.n - 1 : A.n;  // stored rows (fewer when blocks are replicated)
+  const double avg = nsrc ? (double)A.nnz / (double)nsrc : 0.0;
   const int threads = 256;
   const int64_t warps_needed = (A.n + 7) / 8;
   const unsigned grid = grid_for((size_t)warps_needed * 32, threads, 148u * 24u);
-#define EXF_SP(L) spmv_kernel<T, L, MODE><<<grid, threads, 0, s>>>(A.n, A.ptr.p, A.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, skip)
+#define EXF_SP(L) spmv_kernel<T, L, MODE><<<grid, threads, 0, s>>>(A.n, A.ptr.p, A.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, rc1, rc2, A.rmap.p, A.cshift.p, skip)
   if (avg <= 8) EXF_SP(4);
   else if (avg <= 24) EXF_SP(8);
   else if (avg <= 64) EXF_SP(16);
@@ -93,39 +98,40 @@ template <> const float* csr_vals<float>(const Csr64& A) { return A.v32.p; }
 template <class T>
 __global__ void cheb_init0_kernel(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv,
                                   T* __restrict__ x, T* __restrict__ r, T* __restrict__ d, T ith,
-                                  const int* __restrict__ skip) {
+                                  const int* __restrict__ skip, const T* __restrict__ rith = nullptr) {
   if (skip && *skip) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T ri = dinv[i] * b[i];
     x[i] = T(0);
     r[i] = ri;
-    d[i] = ri * ith;
+    d[i] = ri * (rith ? rith[5 * i] : ith);
   }
 }
 
 template <class T>
 __global__ void cheb_update_kernel(int64_t n, T* __restrict__ x, const T* __restrict__ d, T* __restrict__ r,
                                    const T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ d2,
-                                   T c1, T c2, const int* __restrict__ skip) {
+                                   T c1, T c2, const int* __restrict__ skip, const T* __restrict__ rc1 = nullptr,
+                                   const T* __restrict__ rc2 = nullptr) {
   if (skip && *skip) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T di = d[i];
     x[i] += di;
     const T ri = r[i] - dinv[i] * Ad[i];
     r[i] = ri;
-    d2[i] = c1 * di + c2 * ri;
+    d2[i] = (rc1 ? rc1[5 * i] : c1) * di + (rc2 ? rc2[5 * i] : c2) * ri;
   }
 }
 
 template <class T>
 __global__ void resinit_kernel(int64_t n, const T* __restrict__ b, const T* __restrict__ Ax,
                                const T* __restrict__ dinv, T* __restrict__ r, T* __restrict__ d, T ith,
-                               const int* __restrict__ skip) {
+                               const int* __restrict__ skip, const T* __restrict__ rith = nullptr) {
   if (skip && *skip) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T ri = dinv[i] * (b[i] - Ax[i]);
     r[i] = ri;
-    d[i] = ri * ith;
+    d[i] = ri * (rith ? rith[5 * i] : ith);
   }
 }
 
@@ -158,11 +164,32 @@ __global__ void coarse_kernel(int64_t nc, const double* __restrict__ Ainv, const
   if (lane == 0) x[row] = (T)s;
 }
 
+// block-diagonal coarse solve: row r lies in block [s, s+m) whose inverse starts at a
+template <class T>
+__global__ void coarse_blocks_kernel(int64_t nc, const double* __restrict__ Ainv, const int64_t* __restrict__ rs,
+                                     const int64_t* __restrict__ rm, const int64_t* __restrict__ ra,
+                                     const T* __restrict__ b, T* __restrict__ x, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  const int64_t row = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (row >= nc) return;
+  const int64_t s0 = rs[row], m = rm[row], a = ra[row] + (row - s0) * m;
+  double s = 0.0;
+  for (int64_t j = lane; j < m; j += 32) s += Ainv[a + j] * (double)b[s0 + j];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) x[row] = (T)s;
+}
+
 // ---------------------------------------------------------------- V-cycle driver
 template <class T>
 static T* lvbuf(AmgLevel& L, int k);
 template <> double* lvbuf<double>(AmgLevel& L, int k) { return L.w64[k].p; }
 template <> float* lvbuf<float>(AmgLevel& L, int k) { return L.w32[k].p; }
+template <class T>
+static const T* lvcoef(AmgLevel& L);
+template <> const double* lvcoef<double>(AmgLevel& L) { return L.coef64.p; }
+template <> const float* lvcoef<float>(AmgLevel& L) { return L.coef32.p; }
 template <class T>
 static const T* lvdinv(AmgLevel& L);
 template <> const double* lvdinv<double>(AmgLevel& L) { return L.dinv64.p; }
@@ -193,6 +220,12 @@ template <class T>
 static int coarse_solve(exfem_amg_s* h, const T* b, T* x, const int* skip, cudaStream_t s) {
   if (h->nc == 0) return EXFEM_OK;
   const int threads = 128;
+  if (h->crow_s.p) {
+    coarse_blocks_kernel<T><<<(unsigned)((h->nc * 32 + threads - 1) / threads), threads, 0, s>>>(
+        h->nc, h->Ainv.p, h->crow_s.p, h->crow_m.p, h->crow_a.p, b, x, skip);
+    EX_LAUNCH_CHECK();
+    return EXFEM_OK;
+  }
   coarse_kernel<T><<<(unsigned)((h->nc * 32 + threads - 1) / threads), threads, 0, s>>>(h->nc, h->Ainv.p, b, x, skip);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
@@ -204,7 +237,12 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
   if (l == h->levels.size()) return coarse_solve<T>(h, b, x, skip, s);
   AmgLevel& L = *h->levels[l];
   const bool mf = (l == 0 && op0 && op0->apply);
+  if (!mf && L.A.nnz == 0) {
+    set_error("AMG level %zu holds no stored matrix: smooth it with a level-0 block", l);
+    return EXFEM_ERR_ARG;
+  }
   const T* dinv = (l == 0 && op0 && op0->dinv) ? op0->dinv : lvdinv<T>(L);
+  const T* rc = lvcoef<T>(L);  // per-row Chebyshev coefficients (union of independent hierarchies)
   const int64_t n = L.n;
   T* r = lvbuf<T>(L, AmgLevel::WR);
   T* d = lvbuf<T>(L, AmgLevel::WD);
@@ -231,10 +269,13 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
     for (int j = 0; j < h->degree; ++j) {
       if (mf) {
         if ((st = op0->apply(op0->ctx, d, t, skip, s))) return st;
-        cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], skip);
+        cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], skip,
+                                                 rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr);
         EX_LAUNCH_CHECK();
       } else {
-        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s))) return st;
+        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s,
+                                         rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr)))
+          return st;
       }
       std::swap(d, d2);
     }
@@ -243,7 +284,7 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
     return EXFEM_OK;
   };
   // pre-smoothing from x = 0
-  cheb_init0_kernel<T><<<eg, 256, 0, s>>>(n, b, dinv, x, r, d, ith, skip);
+  cheb_init0_kernel<T><<<eg, 256, 0, s>>>(n, b, dinv, x, r, d, ith, skip, rc ? rc + 4 : nullptr);
   EX_LAUNCH_CHECK();
   if ((st = smooth_steps())) return st;
   // residual and restriction
@@ -270,10 +311,12 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
   // post-smoothing from the corrected x
   if (mf) {
     if ((st = op0->apply(op0->ctx, x, t, skip, s))) return st;
-    resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, skip);
+    resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, skip, rc ? rc + 4 : nullptr);
     EX_LAUNCH_CHECK();
   } else {
-    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), skip, s))) return st;
+    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), skip, s,
+                                        rc ? rc + 4 : nullptr)))
+      return st;
   }
   return smooth_steps();
 }
@@ -306,6 +349,39 @@ static int upload_csr(Csr64& M, int64_t n, int64_t ncols, const int64_t* ptr, co
   return M.v32.upload(v32.data(), M.nnz);
 }
 
+// per-row Chebyshev coefficients (degree 2) from per-row spectral bounds (0 marks a
+// pass-through row whose smoother is switched off): for each
+// row [ca0, cb0, ca1, cb1, 1/theta] of the reference's recurrence (linalg.py:161-175)
+int amg_set_level_rows(exfem_amg_s* h, size_t l, const double* rho_rows) {
+  EX_ARG(l < h->levels.size(), "level %zu out of range", l);
+  EX_ARG(h->degree == 2, "per-row Chebyshev coefficients cover degree 2");
+  AmgLevel& L = *h->levels[l];
+  std::vector<double> c((size_t)L.n * 5);
+  std::vector<float> c32((size_t)L.n * 5);
+  for (int64_t i = 0; i < L.n; ++i) {
+    const double rho = rho_rows[i];
+    EX_ARG(rho >= 0 && std::isfinite(rho), "invalid spectral bound %g at row %lld", rho, (long long)i);
+    if (rho == 0.0) {  // pass-through row: no smoothing, the level only relays to the next
+      for (int k = 0; k < 5; ++k) c[5 * i + k] = 0.0;
+      continue;
+    }
+    const double lmax = rho, lmin = rho / 30.0;
+    const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin), sigma = theta / delta;
+    double rh = 1.0 / sigma;
+    for (int j = 0; j < 2; ++j) {
+      const double rn = 1.0 / (2.0 * sigma - rh);
+      c[5 * i + 2 * j] = rn * rh;
+      c[5 * i + 2 * j + 1] = 2.0 * rn / delta;
+      rh = rn;
+    }
+    c[5 * i + 4] = 1.0 / theta;
+  }
+  for (size_t k = 0; k < c.size(); ++k) c32[k] = (float)c[k];
+  int st;
+  if ((st = L.coef64.upload(c.data(), c.size()))) return st;
+  return L.coef32.upload(c32.data(), c32.size());
+}
+
 int amg_add_level(exfem_amg_s* h, int64_t n, int64_t nc, const int64_t* Ap, const int32_t* Ai, const double* Av,
                   const int64_t* Pp, const int32_t* Pi, const double* Pv, const int64_t* Rp, const int32_t* Ri,
                   const double* Rv, const double* dinv, double rho) {
@@ -321,6 +397,113 @@ int amg_add_level(exfem_amg_s* h, int64_t n, int64_t nc, const int64_t* Ap, cons
   std::vector<float> d32(dinv, dinv + n);
   if ((st = L->dinv32.upload(d32.data(), n))) return st;
   h->levels.push_back(std::move(L));
+  return EXFEM_OK;
+}
+
+// Replicate a hierarchy of nmesh independent blocks into ninst copies (instance i
+// copies block inst_mesh[i]).  Matrices keep one stored copy per block; the copies
+// address it through per-row maps.  Vectors (inverse diagonals, per-row Chebyshev
+// coefficients) and the block-diagonal coarse solve are expanded.
+template <class T>
+static int download(std::vector<T>& h, const DevBuf<T>& d) {
+  h.resize(d.n);
+  if (d.n) EX_CUDA(cudaMemcpy(h.data(), d.p, d.bytes(), cudaMemcpyDeviceToHost));
+  return EXFEM_OK;
+}
+
+template <class T>
+static int expand_rows(DevBuf<T>& d, const std::vector<int64_t>& rmap, int per_row) {
+  if (!d.p) return EXFEM_OK;
+  std::vector<T> h, out(rmap.size() * per_row);
+  int st;
+  if ((st = download(h, d))) return st;
+  for (size_t r = 0; r < rmap.size(); ++r)
+    for (int k = 0; k < per_row; ++k) out[r * per_row + k] = h[(size_t)rmap[r] * per_row + k];
+  return d.upload(out.data(), out.size());
+}
+
+int amg_replicate(exfem_amg_s* h, int nmesh, const int64_t* level_offsets, int ninst, const int32_t* inst_mesh) {
+  const size_t nl = h->levels.size();
+  const int64_t* off = level_offsets;  // (nl + 1) rows of nmesh + 1 offsets
+  EX_ARG(h->nc > 0, "set the coarse solve before replicating");
+  for (size_t l = 0; l <= nl; ++l) {
+    const int64_t* o = off + l * (nmesh + 1);
+    const int64_t want = l < nl ? h->levels[l]->n : h->nc;
+    EX_ARG(o[0] == 0 && o[nmesh] == want, "level %zu offsets do not cover its %lld rows", l, (long long)want);
+    for (int m = 0; m < nmesh; ++m) EX_ARG(o[m + 1] > o[m], "block %d is empty at level %zu", m, l);
+  }
+  for (int i = 0; i < ninst; ++i) EX_ARG(inst_mesh[i] >= 0 && inst_mesh[i] < nmesh, "instance %d: bad block", i);
+  if (h->crow_s.p) {  // an existing block-diagonal coarse solve must use the same blocks
+    std::vector<int64_t> rs;
+    int st;
+    if ((st = download(rs, h->crow_s))) return st;
+    const int64_t* o = off + nl * (nmesh + 1);
+    for (int m = 0; m < nmesh; ++m)
+      EX_ARG(rs[o[m]] == o[m] && rs[o[m + 1] - 1] == o[m], "coarse blocks differ from the level offsets");
+  } else {
+    EX_ARG(nmesh == 1, "a dense coarse solve replicates a single block only");
+  }
+  // per level: stored row of each union row and the instance of each union row
+  std::vector<std::vector<int64_t>> rmap(nl + 1), shift(nl + 1), ishift(nl + 1);
+  for (size_t l = 0; l <= nl; ++l) {
+    const int64_t* o = off + l * (nmesh + 1);
+    int64_t u = 0;
+    ishift[l].resize(ninst);
+    for (int i = 0; i < ninst; ++i) {
+      const int m = inst_mesh[i];
+      ishift[l][i] = u - o[m];
+      for (int64_t k = o[m]; k < o[m + 1]; ++k, ++u) {
+        rmap[l].push_back(k);
+        shift[l].push_back(u - k);  // constant over the instance's rows
+      }
+    }
+  }
+  auto inst_of_rows = [&](size_t l) {  // instance index per union row
+    std::vector<int> w;
+    w.reserve(rmap[l].size());
+    const int64_t* o = off + l * (nmesh + 1);
+    for (int i = 0; i < ninst; ++i)
+      for (int64_t k = o[inst_mesh[i]]; k < o[inst_mesh[i] + 1]; ++k) w.push_back(i);
+    return w;
+  };
+  int st;
+  for (size_t l = 0; l < nl; ++l) {
+    AmgLevel& L = *h->levels[l];
+    const std::vector<int> wi = inst_of_rows(l), wc = inst_of_rows(l + 1);
+    std::vector<int64_t> cs_p(wi.size()), cs_r(wc.size());
+    for (size_t r = 0; r < wi.size(); ++r) cs_p[r] = ishift[l + 1][wi[r]];
+    for (size_t r = 0; r < wc.size(); ++r) cs_r[r] = ishift[l][wc[r]];
+    const int64_t n = (int64_t)rmap[l].size(), nc = (int64_t)rmap[l + 1].size();
+    if ((st = L.A.rmap.upload(rmap[l].data(), n)) || (st = L.A.cshift.upload(shift[l].data(), n))) return st;
+    if ((st = L.P.rmap.upload(rmap[l].data(), n)) || (st = L.P.cshift.upload(cs_p.data(), n))) return st;
+    if ((st = L.R.rmap.upload(rmap[l + 1].data(), nc)) || (st = L.R.cshift.upload(cs_r.data(), nc))) return st;
+    if ((st = expand_rows(L.dinv64, rmap[l], 1)) || (st = expand_rows(L.dinv32, rmap[l], 1))) return st;
+    if ((st = expand_rows(L.coef64, rmap[l], 5)) || (st = expand_rows(L.coef32, rmap[l], 5))) return st;
+    L.n = L.A.n = L.A.ncols = L.P.n = L.R.ncols = n;
+    L.nc = L.P.ncols = L.R.n = nc;
+  }
+  // block-diagonal coarse solve over the instances
+  const std::vector<int64_t>& rc = rmap[nl];
+  const int64_t nu = (int64_t)rc.size();
+  std::vector<int64_t> s0(nu), sm(nu), sa(nu), us(nu), um(nu), ua(nu);
+  if (h->crow_s.p) {
+    if ((st = download(s0, h->crow_s)) || (st = download(sm, h->crow_m)) || (st = download(sa, h->crow_a))) return st;
+  } else {
+    s0.assign(h->nc, 0);
+    sm.assign(h->nc, h->nc);
+    sa.assign(h->nc, 0);
+  }
+  for (int64_t r = 0; r < nu; ++r) {
+    const int64_t k = rc[r];
+    us[r] = s0[k] + shift[nl][r];
+    um[r] = sm[k];
+    ua[r] = sa[k];
+  }
+  if ((st = h->crow_s.upload(us.data(), nu)) || (st = h->crow_m.upload(um.data(), nu)) ||
+      (st = h->crow_a.upload(ua.data(), nu)))
+    return st;
+  h->nc = nu;
+  h->replicated = true;
   return EXFEM_OK;
 }
 
@@ -399,6 +582,7 @@ static int vcycle_level_noalloc(exfem_amg_s* h, size_t l, const T* b, T* x, cons
   AmgLevel& L = *h->levels[l];
   const bool mf = (l == 0 && op0 && op0->apply);
   const T* dinv = (l == 0 && op0 && op0->dinv) ? op0->dinv : lvdinv<T>(L);
+  const T* rc = lvcoef<T>(L);  // per-row Chebyshev coefficients (union of independent hierarchies)
   const int64_t n = L.n;
   T* r = w.lv[l][AmgLevel::WR];
   T* d = w.lv[l][AmgLevel::WD];
@@ -425,10 +609,12 @@ static int vcycle_level_noalloc(exfem_amg_s* h, size_t l, const T* b, T* x, cons
     for (int j = 0; j < h->degree; ++j) {
       if (mf) {
         if ((st = op0->apply(op0->ctx, d, t, nullptr, s))) return st;
-        cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], nullptr);
+        cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], nullptr,
+                                                 rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr);
         EX_LAUNCH_CHECK();
       } else {
-        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], nullptr, s)))
+        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], nullptr, s,
+                                         rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr)))
           return st;
       }
       std::swap(d, d2);
@@ -437,7 +623,7 @@ static int vcycle_level_noalloc(exfem_amg_s* h, size_t l, const T* b, T* x, cons
     EX_LAUNCH_CHECK();
     return EXFEM_OK;
   };
-  cheb_init0_kernel<T><<<eg, 256, 0, s>>>(n, b, dinv, x, r, d, ith, nullptr);
+  cheb_init0_kernel<T><<<eg, 256, 0, s>>>(n, b, dinv, x, r, d, ith, nullptr, rc ? rc + 4 : nullptr);
   EX_LAUNCH_CHECK();
   if ((st = smooth_steps())) return st;
   if (mf) {
@@ -456,10 +642,12 @@ static int vcycle_level_noalloc(exfem_amg_s* h, size_t l, const T* b, T* x, cons
     return st;
   if (mf) {
     if ((st = op0->apply(op0->ctx, x, t, nullptr, s))) return st;
-    resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, nullptr);
+    resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, nullptr, rc ? rc + 4 : nullptr);
     EX_LAUNCH_CHECK();
   } else {
-    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), nullptr, s))) return st;
+    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), nullptr, s,
+                                        rc ? rc + 4 : nullptr)))
+      return st;
   }
   return smooth_steps();
 }

@@ -295,6 +295,25 @@ int exfem_block_set_scale(exfem_block b, const double* scale_host) {
   return build_geometry(b);
 }
 
+int exfem_block_set_lame(exfem_block b, const double* lam_host, const double* mu_host) {
+  EX_ARG(b, "block is NULL");
+  EX_ARG((lam_host == nullptr) == (mu_host == nullptr), "give both Lame arrays or neither");
+  EX_ARG(b->mat.kind == EXFEM_LINEAR_ELASTIC || !lam_host, "per-element Lame parameters apply to linear elasticity");
+  int s;
+  if (lam_host) {
+    for (int64_t e = 0; e < b->ne; ++e)
+      EX_ARG(mu_host[e] > 0 && lam_host[e] > -2.0 / 3.0 * mu_host[e], "invalid Lame parameters at element %lld",
+             (long long)e);
+    if ((s = b->lam_e.upload(lam_host, b->ne))) return s;
+    if ((s = b->mu_e.upload(mu_host, b->ne))) return s;
+  } else {
+    b->lam_e.release();
+    b->mu_e.release();
+  }
+  ++b->bc_gen;
+  return build_geometry(b);
+}
+
 int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
   EX_ARG(b, "block is NULL");
   int s;
@@ -410,14 +429,55 @@ int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc, const int64_t* A_ptr
   EX_ARG(h->levels.empty() || h->levels.back()->nc == n, "level size %lld does not match the previous coarse size",
          (long long)n);
   EX_ARG(rho > 0 && std::isfinite(rho), "invalid spectral bound %g", rho);
+  EX_ARG(!h->replicated, "hierarchy already replicated");
   return amg_add_level(h, n, nc, A_ptr, A_idx, A_val, P_ptr, P_idx, P_val, R_ptr, R_idx, R_val, dinv, rho);
 }
 
 int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv) {
   EX_ARG(h && Ainv, "NULL argument");
+  EX_ARG(!h->replicated, "hierarchy already replicated");
   EX_ARG(h->levels.empty() || h->levels.back()->nc == nc, "coarse size mismatch");
   h->nc = nc;
+  h->crow_s.release();
+  h->crow_m.release();
+  h->crow_a.release();
   return h->Ainv.upload(Ainv, (size_t)(nc * nc));
+}
+
+int exfem_amg_set_level_rows(exfem_amg h, int level, const double* rho_rows) {
+  EX_ARG(h && rho_rows, "NULL argument");
+  EX_ARG(!h->replicated, "hierarchy already replicated");
+  EX_ARG(level >= 0, "negative level");
+  return amg_set_level_rows(h, (size_t)level, rho_rows);
+}
+
+int exfem_amg_set_coarse_blocks(exfem_amg h, int64_t nblk, const int64_t* offsets, const double* Ainv_blocks) {
+  EX_ARG(h && offsets && Ainv_blocks && nblk > 0, "NULL argument or no blocks");
+  EX_ARG(!h->replicated, "hierarchy already replicated");
+  const int64_t nc = offsets[nblk];
+  EX_ARG(offsets[0] == 0 && nc > 0, "block offsets must start at 0 and cover at least one row");
+  EX_ARG(h->levels.empty() || h->levels.back()->nc == nc, "coarse size mismatch");
+  std::vector<int64_t> rs(nc), rm(nc), ra(nc);
+  int64_t a = 0;
+  for (int64_t b = 0; b < nblk; ++b) {
+    const int64_t s0 = offsets[b], m = offsets[b + 1] - s0;
+    EX_ARG(m > 0, "empty coarse block %lld", (long long)b);
+    for (int64_t r = s0; r < s0 + m; ++r) { rs[r] = s0; rm[r] = m; ra[r] = a; }
+    a += m * m;
+  }
+  int st;
+  h->nc = nc;
+  if ((st = h->Ainv.upload(Ainv_blocks, (size_t)a))) return st;
+  if ((st = h->crow_s.upload(rs.data(), nc))) return st;
+  if ((st = h->crow_m.upload(rm.data(), nc))) return st;
+  return h->crow_a.upload(ra.data(), nc);
+}
+
+int exfem_amg_replicate(exfem_amg h, int nblk, const int64_t* level_offsets, int ninst, const int32_t* inst_block) {
+  EX_ARG(h && level_offsets && inst_block, "NULL argument");
+  EX_ARG(nblk >= 1 && ninst >= 1, "need at least one block and one instance");
+  EX_ARG(!h->replicated, "hierarchy already replicated");
+  return amg_replicate(h, nblk, level_offsets, ninst, inst_block);
 }
 
 int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0, const void* dinv0,

@@ -152,11 +152,11 @@ __host__ __device__ __forceinline__ int64_t tile_index(int64_t e, int k, int wid
 template <int ET> struct ElemTraits;
 template <> struct ElemTraits<EXFEM_C3D8> {
   static constexpr int nnode = 8, ngp = 8, nd = 24;
-  static constexpr int geo_stride = 24;  // modal c1..c7 (21), scale, 2 pad
+  static constexpr int geo_stride = 24;  // modal c1..c7 (21), scale, lambda, mu
 };
 template <> struct ElemTraits<EXFEM_C3D10> {
   static constexpr int nnode = 10, ngp = 4, nd = 30;
-  static constexpr int geo_stride = 12;  // inverse Jacobian (9), vol*scale, 2 pad
+  static constexpr int geo_stride = 12;  // inverse Jacobian (9), vol*scale, lambda, mu
 };
 
 // ---------------------------------------------------------------- materials
@@ -287,8 +287,9 @@ __device__ __forceinline__ void j2_return(const MatDev& m, const double (&eps)[6
   }
 }
 
-// stress at a Gauss point for the FP64 residual; writes the state and the tangent data
-__device__ __forceinline__ void material_stress(const MatDev& m, const double (&H)[9],
+// stress at a Gauss point for the FP64 residual; writes the state and the tangent data.
+// lam, mu: the element's Lame parameters (linear elasticity; J2 uses the material's)
+__device__ __forceinline__ void material_stress(const MatDev& m, double lam, double mu, const double (&H)[9],
                                                 const double* st, double* sn, double (&sig)[6],
                                                 double (&tn)[8]) {
   double e[6];
@@ -296,7 +297,7 @@ __device__ __forceinline__ void material_stress(const MatDev& m, const double (&
   if (m.kind == EXFEM_J2) {
     j2_return(m, e, st, sn, sig, tn);
   } else {
-    elastic_stress(m.lam, m.mu, e, sig);
+    elastic_stress(lam, mu, e, sig);
     if (sn) sn[0] = st ? st[0] : 0.0;
 #pragma unroll
     for (int k = 0; k < 6; ++k) tn[k] = 0.0;

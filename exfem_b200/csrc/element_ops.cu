@@ -46,11 +46,14 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
              const double* __restrict__ u, const double* __restrict__ scale,
              const double* __restrict__ st_old, double* __restrict__ st_new, double* __restrict__ fe,
              double* __restrict__ tan64, float* __restrict__ tan32, double* __restrict__ S,
-             double* __restrict__ mises, double* __restrict__ peeq, const MatDev mat) {
+             double* __restrict__ mises, double* __restrict__ peeq, const MatDev mat,
+             const double* __restrict__ lam_e, const double* __restrict__ mu_e) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, NG = Tr::ngp;
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= ne) return;
+  // per-element Lame parameters (linear elasticity) override the material's
+  const double lam_k = lam_e ? lam_e[e] : mat.lam, mu_k = lam_e ? mu_e[e] : mat.mu;
   const int ns = mat.kind == EXFEM_J2 ? 19 : 1;
   const double sc = (MODE != FORCE_STRESS && scale) ? scale[e] : 1.0;
   int nod[NN];
@@ -103,7 +106,7 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
       H[8] += bb;
       double sig[6], tn[8];
       const double* st = st_e ? st_e + g * ns : zero_state;
-      material_stress(mat, H, st, sn_e ? sn_e + g * ns : nullptr, sig, tn);
+      material_stress(mat, lam_k, mu_k, H, st, sn_e ? sn_e + g * ns : nullptr, sig, tn);
       if (MODE != FORCE_STRESS) {
         if (tan64)
 #pragma unroll
@@ -123,7 +126,7 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
         hex_modal_grad_adj(Q, x, y, z, Fm);
       } else if (MODE == FORCE_STRESS) {
         double snew[19];
-        material_stress(mat, H, st, snew, sig, tn);
+        material_stress(mat, lam_k, mu_k, H, st, snew, sig, tn);
 #pragma unroll
         for (int k = 0; k < 6; ++k) Sacc[k] += detJ * sig[k];
         vsum += detJ;
@@ -173,7 +176,7 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
       matmul3(G, iJ, H);
       double sig[6], tn[8];
       const double* st = st_e ? st_e + g * ns : zero_state;
-      material_stress(mat, H, st, sn_e ? sn_e + g * ns : nullptr, sig, tn);
+      material_stress(mat, lam_k, mu_k, H, st, sn_e ? sn_e + g * ns : nullptr, sig, tn);
       if (MODE != FORCE_STRESS) {
         if (tan64)
 #pragma unroll
@@ -202,7 +205,7 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
           }
       } else if (MODE == FORCE_STRESS) {
         double snew[19];
-        material_stress(mat, H, st, snew, sig, tn);
+        material_stress(mat, lam_k, mu_k, H, st, snew, sig, tn);
         const double w = detJ / 24.0;
 #pragma unroll
         for (int k = 0; k < 6; ++k) Sacc[k] += w * sig[k];
@@ -244,7 +247,8 @@ static int force_dispatch(exfem_block_s* b, const double* u, const double* st_ol
   double* t64 = (MODE != FORCE_STRESS && j2) ? b->tan64.p : nullptr;
   float* t32 = (MODE != FORCE_STRESS && j2) ? b->tan32.p : nullptr;
   force_kernel<ET, MODE><<<grid, threads, 0, s>>>(b->ne, b->X.p, b->conn.p, u, b->scale.p, st_old,
-                                                  st_new, fe, t64, t32, S, mises, peeq, b->mat);
+                                                  st_new, fe, t64, t32, S, mises, peeq, b->mat, b->lam_e.p,
+                                                  b->mu_e.p);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
 }
@@ -330,7 +334,8 @@ int launch_colour_assemble(exfem_block_s* b, const double* fe, double* f, cudaSt
 // ---------------------------------------------------------------- geometry streams
 template <int ET>
 __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn,
-                                const double* __restrict__ scale, double* __restrict__ g64,
+                                const double* __restrict__ scale, const double* __restrict__ lam_e,
+                                const double* __restrict__ mu_e, double lam0, double mu0, double* __restrict__ g64,
                                 float* __restrict__ g32) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, GS = Tr::geo_stride;
@@ -352,6 +357,8 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
 #pragma unroll
       for (int c = 0; c < 3; ++c) out[3 * k + c] = cm[k][c];
     out[21] = sc;
+    out[22] = lam_e ? lam_e[e] : lam0;
+    out[23] = mu_e ? mu_e[e] : mu0;
   } else {
     double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
 #pragma unroll
@@ -366,6 +373,8 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[k] = iJ[k];
     out[9] = det / 24.0 * sc;
+    out[10] = lam_e ? lam_e[e] : lam0;
+    out[11] = mu_e ? mu_e[e] : mu0;
   }
 #pragma unroll
   for (int k = 0; k < GS; ++k) {
@@ -388,9 +397,11 @@ int build_geometry(exfem_block_s* b) {
   const int threads = 128;
   const unsigned grid = (unsigned)((b->ne + threads - 1) / threads);
   if (b->etype == EXFEM_C3D8)
-    geometry_kernel<EXFEM_C3D8><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->geo64.p, b->geo32.p);
+    geometry_kernel<EXFEM_C3D8><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
+                                                   b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p);
   else
-    geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->geo64.p, b->geo32.p);
+    geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
+                                                    b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p);
   EX_LAUNCH_CHECK();
   EX_CUDA(cudaDeviceSynchronize());
   return EXFEM_OK;
@@ -424,7 +435,8 @@ __global__ void __launch_bounds__(64)
 stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn,
                  const double* __restrict__ u, const double* __restrict__ scale,
                  const double* __restrict__ st_old, const double* __restrict__ tan_in,
-                 const MatDev mat, OutT* __restrict__ Ke, double* __restrict__ ediag) {
+                 const MatDev mat, const double* __restrict__ lam_e, const double* __restrict__ mu_e,
+                 OutT* __restrict__ Ke, double* __restrict__ ediag) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, NG = Tr::ngp, ND = 3 * NN, EPB = 64 / NN;
   constexpr bool BBAR = ET == EXFEM_C3D8;
@@ -435,6 +447,8 @@ stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __rest
   const int le = threadIdx.x / NN, a = threadIdx.x % NN;
   const int64_t e = (int64_t)blockIdx.x * EPB + le;
   const bool valid = le < EPB && e < ne;
+  const bool own = valid && lam_e;  // per-element Lame parameters override the material's
+  const double lam_k = own ? lam_e[e] : mat.lam, mu_k = own ? mu_e[e] : mat.mu;
   const int ns = mat.kind == EXFEM_J2 ? 19 : 1;
   if (valid && a < NG) {
     const int g = a;
@@ -478,7 +492,7 @@ stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __rest
     if (tan_in) {
       for (int k = 0; k < 8; ++k) tn[k] = tan_in[tile_index(e, g * 8 + k, NG * 8)];
     } else {
-      material_stress(mat, H, st, nullptr, sig, tn);
+      material_stress(mat, lam_k, mu_k, H, st, nullptr, sig, tn);
     }
     for (int k = 0; k < 9; ++k) s_iJ[le][g][k] = iJ[k];
     s_vol[le][g] = (ET == EXFEM_C3D8 ? 1.0 : 1.0 / 24.0) * detJ * sc;
@@ -504,7 +518,7 @@ stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __rest
       for (int i = 0; i < 3; ++i) s += 0.125 * hex_sign(a, i) * s_iJ0[le][3 * i + j];
       dN0a[j] = s;
     }
-  const double Kb = mat.K, mu = mat.mu;
+  const double Kb = own ? lam_k + 2.0 * mu_k / 3.0 : mat.K, mu = mu_k;
   for (int b = (MODE == 1 ? a : 0); b < (MODE == 1 ? a + 1 : NN); ++b) {
     double dNb[NG][3], dN0b[3] = {0, 0, 0};
 #pragma unroll
@@ -569,10 +583,10 @@ static void stiffness_go(exfem_block_s* b, const double* u, const double* st_old
   const unsigned grid = (unsigned)((b->ne + EPB - 1) / EPB);
   if (ediag)
     stiffness_kernel<ET, 1, OutT><<<grid, 64, 0, s>>>(b->ne, b->X.p, b->conn.p, u, b->scale.p, st_old,
-                                                      tan_in, b->mat, Ke, ediag);
+                                                      tan_in, b->mat, b->lam_e.p, b->mu_e.p, Ke, ediag);
   else
     stiffness_kernel<ET, 0, OutT><<<grid, 64, 0, s>>>(b->ne, b->X.p, b->conn.p, u, b->scale.p, st_old,
-                                                      tan_in, b->mat, Ke, ediag);
+                                                      tan_in, b->mat, b->lam_e.p, b->mu_e.p, Ke, ediag);
 }
 
 int launch_stiffness(exfem_block_s* b, const double* u, const double* st_old, int dtype, void* Ke,

@@ -16,6 +16,7 @@ struct exfem_block_s {
   exfem::DevBuf<double> X;            // (nn, 3)
   exfem::DevBuf<int32_t> conn;        // (ne, nnode)
   exfem::DevBuf<double> scale;        // (ne), empty = 1
+  exfem::DevBuf<double> lam_e, mu_e;  // (ne) per-element Lame parameters, empty = material's
   // index maps
   int vmax = 0;
   exfem::DevBuf<int32_t> plan;        // (nn, vmax), sentinel ne*nnode
@@ -63,6 +64,9 @@ struct Csr64 {  // device CSR, FP64 values and an FP32 copy
   DevBuf<int32_t> idx;
   DevBuf<double> v64;
   DevBuf<float> v32;
+  // replicated blocks (optional): row r reads stored row rmap[r] and shifts its
+  // column indices by cshift[r], so copies of a block share one set of entries
+  DevBuf<int64_t> rmap, cshift;
 };
 
 // element kernels (element_ops.cu)

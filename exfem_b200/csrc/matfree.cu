@@ -110,6 +110,7 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
 #pragma unroll
       for (int c = 0; c < 3; ++c) cm[k][c] = g[(3 * k + c) * MF_TILE];
     const T sc = g[21 * MF_TILE];
+    const T le = g[22 * MF_TILE], me = J2 ? mu : g[23 * MF_TILE];
     hex_to_modal(va, um);
     T J0[9], iJ0[9], G0[9], H0[9];
 #pragma unroll
@@ -140,7 +141,7 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       H[8] += bb;
       T ee[6], s[6];
       sym_from_grad(H, ee);
-      mf_stress<T, J2>(tn + q * 8 * MF_TILE, lam, mu, Kb, ee, s);
+      mf_stress<T, J2>(tn + q * 8 * MF_TILE, le, me, Kb, ee, s);
       const T vol = detJ * sc;
       const T t = vol * (s[0] + s[1] + s[2]) * T(1.0 / 3.0);
       tacc += t;
@@ -171,6 +172,7 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
 #pragma unroll
     for (int k = 0; k < 9; ++k) iJ[k] = g[k * MF_TILE];
     const T vol = g[9 * MF_TILE];
+    const T le = g[10 * MF_TILE], me = J2 ? mu : g[11 * MF_TILE];
     (void)A;
     (void)B;
     T base[4][3], vbar[10][3], bbar[4][3];
@@ -203,7 +205,7 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       matmul3t(G, iJ, H);
       T ee[6], s[6];
       sym_from_grad(H, ee);
-      mf_stress<T, J2>(tn + q * 8 * MF_TILE, lam, mu, Kb, ee, s);
+      mf_stress<T, J2>(tn + q * 8 * MF_TILE, le, me, Kb, ee, s);
       const T r[3][3] = {{vol * s[0], vol * s[3], vol * s[5]},
                          {vol * s[3], vol * s[1], vol * s[4]},
                          {vol * s[5], vol * s[4], vol * s[2]}};

@@ -15,6 +15,8 @@ struct AmgLevel {
   Csr64 A, P, R;
   DevBuf<double> dinv64;
   DevBuf<float> dinv32;
+  DevBuf<double> coef64;  // optional per-row Chebyshev coefficients (5 per row)
+  DevBuf<float> coef32;
   DevBuf<double> w64[NW];
   DevBuf<float> w32[NW];
 };
@@ -30,6 +32,8 @@ struct Level0Op {
 template <class T>
 int amg_vcycle(exfem_amg_s* h, const T* b, T* x, const Level0Op<T>* op0, const int* skip, cudaStream_t s);
 int amg_prepare(exfem_amg_s* h, int dtype);
+int amg_set_level_rows(exfem_amg_s* h, size_t l, const double* rho_rows);
+int amg_replicate(exfem_amg_s* h, int nmesh, const int64_t* level_offsets, int ninst, const int32_t* inst_mesh);
 int amg_add_level(exfem_amg_s* h, int64_t n, int64_t nc, const int64_t* Ap, const int32_t* Ai, const double* Av,
                   const int64_t* Pp, const int32_t* Pi, const double* Pv, const int64_t* Rp, const int32_t* Ri,
                   const double* Rv, const double* dinv, double rho);
@@ -47,6 +51,8 @@ struct exfem_amg_s {
   std::vector<std::unique_ptr<exfem::AmgLevel>> levels;
   int64_t nc = 0;
   exfem::DevBuf<double> Ainv;
+  exfem::DevBuf<int64_t> crow_s, crow_m, crow_a;  // block-diagonal coarse solve: per-row block start, size, offset
+  bool replicated = false;                          // levels address shared blocks through row maps
   exfem::DevBuf<double> cb64, cx64;
   exfem::DevBuf<float> cb32, cx32;
 };

@@ -241,37 +241,46 @@ def _csr_parts(M):
             np.ascontiguousarray(M.data.astype(np.float64)))
 
 
+def amg_setup(A, X=None, max_coarse=300, rot_mask=None):
+    """Host part of :class:`AMG`: dict with ``levels`` (list of dicts A, P, R, dinv,
+    rho, n, nc), ``coarse`` (regularised Cholesky factor of the coarsest matrix),
+    ``coarse_inv`` (its dense inverse product) and ``nnz`` per level
+    (gfem/linalg.py:102-146).
+    Needs no GPU, so many independent set-ups can run in worker processes."""
+    A = A.tocsr()
+    n = A.shape[0]
+    if X is not None and n == 3 * len(X):
+        B, bs = rigid_body_modes(X, rot_mask), 3
+    else:
+        B, bs = np.ones((n, 1)), 1
+    sa_levels, Ac = sa_hierarchy(A, B, bs, max_coarse)
+    levels = []
+    for Al, P in sa_levels:
+        d = Al.diagonal()
+        dinv = np.where(np.abs(d) > 0, 1.0 / np.where(d == 0, 1, d), 0.0)
+        levels.append(dict(A=Al, P=P, R=P.T.tocsr(), dinv=dinv, rho=float(_rho(Al, dinv)),
+                           n=Al.shape[0], nc=P.shape[1]))
+    Acd = Ac.toarray()
+    Acd = 0.5 * (Acd + Acd.T)
+    try:
+        Lc = np.linalg.cholesky(Acd + 1e-13 * np.abs(Acd).max() * np.eye(len(Acd)))
+    except np.linalg.LinAlgError:
+        w, V = np.linalg.eigh(Acd)
+        Lc = np.linalg.cholesky(V @ np.diag(np.maximum(w, 1e-12 * w.max())) @ V.T)
+    Linv = np.linalg.inv(Lc)
+    nnz = [lv["A"].nnz for lv in levels] + [int(np.count_nonzero(Acd))]
+    return dict(levels=levels, coarse=Lc, coarse_inv=np.ascontiguousarray(Linv.T @ Linv), nnz=nnz)
+
+
 class AMG:
     """Smoothed-aggregation AMG: host set-up, device V-cycle (gfem/linalg.py:102-195)."""
 
     def __init__(self, A, X=None, max_coarse=300, degree=2, presmooth=1, rot_mask=None):
         t0 = time.time()
-        A = A.tocsr()
-        n = A.shape[0]
-        if X is not None and n == 3 * len(X):
-            B, bs = rigid_body_modes(X, rot_mask), 3
-        else:
-            B, bs = np.ones((n, 1)), 1
-        sa_levels, Ac = sa_hierarchy(A, B, bs, max_coarse)
-        self.levels = []
-        for Al, P in sa_levels:
-            d = Al.diagonal()
-            dinv = np.where(np.abs(d) > 0, 1.0 / np.where(d == 0, 1, d), 0.0)
-            self.levels.append(dict(A=Al, P=P, R=P.T.tocsr(), dinv=dinv, rho=float(_rho(Al, dinv)),
-                                    n=Al.shape[0], nc=P.shape[1]))
-        Acd = Ac.toarray()
-        Acd = 0.5 * (Acd + Acd.T)
-        try:
-            Lc = np.linalg.cholesky(Acd + 1e-13 * np.abs(Acd).max() * np.eye(len(Acd)))
-        except np.linalg.LinAlgError:
-            w, V = np.linalg.eigh(Acd)
-            Lc = np.linalg.cholesky(V @ np.diag(np.maximum(w, 1e-12 * w.max())) @ V.T)
-        self.coarse = Lc
-        Linv = np.linalg.inv(Lc)
-        self.coarse_inv = np.ascontiguousarray(Linv.T @ Linv)
+        h = amg_setup(A, X, max_coarse, rot_mask)
+        self.levels, self.coarse, self.coarse_inv, nnz = h["levels"], h["coarse"], h["coarse_inv"], h["nnz"]
         self.degree, self.presmooth = degree, presmooth
-        nnz = [lv["A"].nnz for lv in self.levels] + [int(np.count_nonzero(Acd))]
-        self.sizes = [lv["n"] for lv in self.levels] + [Acd.shape[0]]
+        self.sizes = [lv["n"] for lv in self.levels] + [self.coarse_inv.shape[0]]
         self.complexity = float(sum(nnz) / max(nnz[0], 1))
         self.nlevels = len(self.sizes)
         self.setup_time = time.time() - t0

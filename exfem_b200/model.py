@@ -115,6 +115,19 @@ class Block:
             check(lib.exfem_block_set_scale(self._h, s.ctypes.data))
             self._scale_key = key
 
+    def set_lame(self, lam, mu):
+        """Per-element Lame parameters of the matrix-free operator (a block holding
+        many linear-elastic instances with their own E and nu); None, None = the
+        block material's."""
+        if lam is None and mu is None:
+            check(lib.exfem_block_set_lame(self._h, None, None))
+            return
+        lam = np.ascontiguousarray(np.asarray(lam, dtype=np.float64).reshape(-1))
+        mu = np.ascontiguousarray(np.asarray(mu, dtype=np.float64).reshape(-1))
+        if lam.size != self.ne or mu.size != self.ne:
+            raise ValueError(f"need {self.ne} Lame pairs, got {lam.size} and {mu.size}")
+        check(lib.exfem_block_set_lame(self._h, lam.ctypes.data, mu.ctypes.data))
+
     def set_fixed(self, fixed):
         """Prescribed-DOF mask (ndof of this block's node set) used by opA."""
         if fixed is None:

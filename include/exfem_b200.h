@@ -72,6 +72,7 @@ typedef struct {
 typedef struct exfem_block_s* exfem_block;
 typedef struct exfem_amg_s* exfem_amg;
 typedef struct exfem_solver_s* exfem_solver;
+typedef struct exfem_batch_s* exfem_batch;
 
 /* ------------------------------------------------------------ library */
 int exfem_version(void);
@@ -106,6 +107,12 @@ int exfem_block_tile_maps(exfem_block b, int32_t* ptr_host, int32_t* nodes_host,
                           uint16_t* perm_host);
 /* per-element stiffness scale (gfem/model.py:449-463, fields["scale"]); NULL = 1 */
 int exfem_block_set_scale(exfem_block b, const double* scale_host);
+/* per-element Lame parameters (ne each) of a linear-elastic block, used by every
+ * element kernel (forces, stresses, Ke, the matrix-free operator and its
+ * diagonal) in place of the material's; lets one block hold many
+ * independent instances with different E and nu.  NULL, NULL = the material's.
+ * No counterpart in the reference (one material per block, gfem/model.py:21-26). */
+int exfem_block_set_lame(exfem_block b, const double* lam_host, const double* mu_host);
 /* prescribed-DOF mask (ndof bytes, 1 = fixed): operators apply the reference's
  * opA, y = free*K(free*v) + fixed*v (gfem/solvers.py:257-267); NULL = all free */
 int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host);
@@ -162,6 +169,23 @@ int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc,
                         const int64_t* R_ptr, const int32_t* R_idx, const double* R_val,
                         const double* dinv, double rho);
 int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv_dense);
+/* Union of independent hierarchies (batched solves, no counterpart in the
+ * reference): per-row spectral bounds of level `level` (n doubles; each row
+ * smoothed with its own instance's Chebyshev coefficients, degree 2; a bound of 0
+ * marks a pass-through row with smoothing switched off, used where an instance
+ * has fewer levels than the union and identity levels relay it), and a
+ * block-diagonal coarsest solve: nblk blocks at row offsets (nblk+1, int64) whose
+ * inverses are concatenated row-major in Ainv_blocks. */
+int exfem_amg_set_level_rows(exfem_amg h, int level, const double* rho_rows);
+int exfem_amg_set_coarse_blocks(exfem_amg h, int64_t nblk, const int64_t* offsets, const double* Ainv_blocks);
+/* Replicate a block-diagonal hierarchy of nblk independent blocks into ninst
+ * instances, instance i a copy of block inst_block[i], laid out one after the
+ * other at every level (batched solves of several right-hand sides per mesh; no
+ * counterpart in the reference).  level_offsets holds (levels + 1) rows of
+ * nblk + 1 row offsets of the blocks, the last row for the coarsest level.  The
+ * stored matrices are shared by the copies; call after every level and the
+ * coarse solve are set, once. */
+int exfem_amg_replicate(exfem_amg h, int nblk, const int64_t* level_offsets, int ninst, const int32_t* inst_block);
 /* One V-cycle z = M(r) (gfem/linalg.py:156-195, Chebyshev degree 2 over
  * [rho/30, rho]) in dtype F64 or F32; the coarse solve is FP64 in both.  When
  * level0 is a block, level 0 is smoothed with that block's matrix-free tangent
@@ -212,6 +236,22 @@ int exfem_solver_pcg(exfem_solver s, const double* b, double* x, double tol, int
 int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, double inner_tol,
                        int max_pass, int maxiter, int* iters, int* passes, double* relres,
                        void* stream);
+
+/* ------------------------------------------------------------ batched solves
+ * Many independent linear-elastic systems in one set of launches (no counterpart
+ * in the reference, which solves one Model at a time; nearest is the vmapped
+ * multi-RHS PCG of gfem/optimize.py:116-143).  `blk` is the union of the
+ * instances' meshes (per-element Lame parameters, prescribed-DOF mask), `amg` the
+ * block-diagonal union of their hierarchies (exfem_amg_set_level_rows,
+ * exfem_amg_set_coarse_blocks), dof_offsets (ninst+1) the instances' contiguous
+ * DOF ranges.  The solve runs FP32 matrix-free AMG-PCG per instance inside FP64
+ * iterative refinement with per-instance scaling, scalars and stopping rule
+ * ||b_i - A x_i|| <= tol ||b_i||; iters (ninst) and relres (ninst) are per
+ * instance.  Synchronises the stream. */
+int exfem_batch_create(exfem_block blk, exfem_amg amg, int ninst, const int64_t* dof_offsets, exfem_batch* out);
+int exfem_batch_destroy(exfem_batch b);
+int exfem_batch_solve(exfem_batch b, const double* rhs, double* x, double tol, double inner_tol, int max_pass,
+                      int maxiter, int* iters, int* passes, double* relres, void* stream);
 
 /* ------------------------------------------------------------ host index builders
  * Host-side, no device work.  Gather plan of one connectivity exactly as

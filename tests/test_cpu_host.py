@@ -143,3 +143,41 @@ dist.destroy_process_group()
                         "--master-addr", "127.0.0.1", "--master-port", "29571", str(f)],
                        capture_output=True, text=True, env=env, timeout=300)
     assert "OK 100.0" in r.stdout, r.stderr[-2000:]
+
+
+def test_batch_host_setups_in_spawned_workers():
+    """Per-problem host hierarchies of a batch (element stiffness from the oracle):
+    spawned worker processes give the same hierarchy as the in-process set-up, and
+    a problem below the coarse size has no level (it is relayed in the union)."""
+    import torch
+    from exfem_b200 import batch
+    from exfem_b200.materials import LinearElastic
+    probs = [batch.cantilever(14, 3, 3, 5.0, LinearElastic(150e3, 0.3), [[0, 0, -100.0]]),
+             batch.cantilever(2, 1, 1, 5.0, LinearElastic(80e3, 0.3), [[0, 0, -100.0]])]
+    stiff = []
+    for p in probs:
+        m = fem.Model(p.X)
+        m.add_block(p.conn, fem.HEX8, fem.LinearElastic(p.material.E, p.material.nu))
+        (d, K), = m.stiffness_ops(torch.zeros(m.ndof, dtype=torch.float64), m.init_state())
+        stiff.append((np.asarray(d), K.numpy()))
+    a = batch.host_setups(probs, workers=0, stiffness=stiff)
+    b = batch.host_setups(probs, workers=2, stiffness=stiff)
+    assert len(a[0]["levels"]) >= 1 and len(a[1]["levels"]) == 0
+    for ha, hb in zip(a, b):
+        np.testing.assert_array_equal(ha["coarse_inv"], hb["coarse_inv"])
+        for la, lb in zip(ha["levels"], hb["levels"]):
+            assert (la["P"] != lb["P"]).nnz == 0 and la["rho"] == lb["rho"]
+
+
+def test_random_cantilevers_follow_the_stated_ranges():
+    from exfem_b200 import batch
+    probs = batch.random_cantilevers(40, seed=3)
+    for p in probs:
+        ne = len(p.conn)
+        assert 4 * 2 * 2 <= ne <= 64 * 16 * 16
+        assert 70e3 <= p.material.E <= 210e3 and 0.25 <= p.material.nu <= 0.35
+        assert p.rhs.shape == (4, p.ndof)
+        tot = p.rhs.reshape(4, -1, 3).sum(1)
+        mags = np.abs(tot).max(1)
+        assert np.all((mags >= 100.0) & (mags <= 1000.0))
+        np.testing.assert_allclose(np.sign(tot).astype(int), [[1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, -1]])

@@ -1,0 +1,91 @@
+"""Batched solves of uneven problems: each instance against its own single solve
+(the FP32/FP64 mixed path with its own hierarchy) and against a sparse direct
+FP64 solve; the same instance alone and inside a larger batch."""
+import numpy as np
+import pytest
+import torch
+
+from exfem_b200 import batch, linalg
+from exfem_b200.materials import LinearElastic
+
+pytestmark = pytest.mark.gpu
+
+# displacement tolerance: residual stopping rule 1e-8 times the conditioning of
+# slender cantilevers leaves errors of a few 1e-8 against the direct solution
+TOL_DIRECT = 1e-6
+TOL_PAIR = 1e-6
+
+
+def _problems():
+    dirs = np.array([[1.0, 0, 0], [0, 0, -1.0]])
+    return [
+        batch.cantilever(12, 3, 2, 5.0, LinearElastic(210e3, 0.3), dirs * 500.0),
+        batch.cantilever(2, 1, 1, 5.0, LinearElastic(70e3, 0.33), dirs * 200.0),     # 36 DOF: no SA level
+        batch.cantilever(20, 4, 5, 5.0, LinearElastic(120e3, 0.27), dirs * 800.0),
+        batch.cantilever(7, 2, 2, 5.0, LinearElastic(95e3, 0.35), dirs[::-1] * 300.0),
+    ]
+
+
+def _direct(p, r):
+    dofs, Ke = batch._element_stiffness(p)
+    A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke)], p.ndof), (~p.fixed).astype(float))
+    return linalg.Direct(A).solve(p.rhs[r])
+
+
+def _rel(a, b):
+    a = np.asarray(a.detach().cpu() if hasattr(a, "detach") else a)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_batch_matches_direct_and_single_solves(cuda):
+    probs = _problems()
+    S = batch.BatchSolver(probs, workers=0)
+    x, info = S.solve(tol=1e-10)
+    assert info["converged"], info
+    assert np.all(info["relres"] <= 1e-10)
+    xs = S.split(x)
+    from exfem_b200.model import Block
+    for i, (k, r) in enumerate(S.inst):
+        p = probs[k]
+        xd = _direct(p, r)
+        assert _rel(xs[i], xd) <= TOL_DIRECT, (i, _rel(xs[i], xd))
+        # the single-solve mixed path with the problem's own hierarchy
+        blk = Block(p.conn, p.etype, p.material, p.X)
+        blk.set_fixed(p.fixed)
+        dofs, Ke = batch._element_stiffness(p)
+        A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke)], p.ndof), (~p.fixed).astype(float))
+        ns = linalg.NativeSolver(blk, "mf32", "amg", linalg.AMG(A, p.X))
+        x1, k1, p1, rel1 = ns.mixed(torch.as_tensor(p.rhs[r], device="cuda"), tol=1e-10)
+        assert _rel(xs[i], x1.cpu().numpy()) <= TOL_PAIR
+        # same hierarchy and stopping rule: inner iteration counts agree closely
+        assert abs(int(info["iters"][i]) - k1) <= max(2, k1 // 10), (i, info["iters"][i], k1)
+
+
+def test_batch_instance_same_alone_and_in_mix(cuda):
+    probs = _problems()
+    setups = batch.host_setups(probs, workers=0)
+    mix = batch.BatchSolver(probs, setups=setups)
+    xm, im = mix.solve()
+    alone = batch.BatchSolver([probs[2]], setups=[setups[2]])
+    xa, ia = alone.solve()
+    assert im["converged"] and ia["converged"]
+    k0 = [i for i, (k, _) in enumerate(mix.inst) if k == 2]
+    xm_s, xa_s = mix.split(xm), alone.split(xa)
+    for j, i in enumerate(k0):
+        assert _rel(xm_s[i], xa_s[j].cpu().numpy()) <= 1e-8, (i, _rel(xm_s[i], xa_s[j].cpu().numpy()))
+        assert abs(int(im["iters"][i]) - int(ia["iters"][j])) <= 2
+    # repeat solves of the same batch give the same iteration counts
+    xm2, im2 = mix.solve()
+    np.testing.assert_array_equal(im["iters"], im2["iters"])
+    assert _rel(xm2, xm.cpu().numpy()) <= 1e-12
+
+
+def test_batch_rejects_mixed_element_types_and_plastic_materials(cuda):
+    from exfem_b200 import elements
+    from exfem_b200.materials import J2Plasticity
+    a = batch.cantilever(3, 1, 1, 5.0, LinearElastic(210e3, 0.3), [[0, 0, -100.0]])
+    b = batch.cantilever(3, 1, 1, 5.0, LinearElastic(210e3, 0.3), [[0, 0, -100.0]], etype=elements.TET10)
+    with pytest.raises(ValueError):
+        batch.BatchSolver([a, b], workers=0)
+    with pytest.raises(TypeError):
+        batch.Problem(a.X, a.conn, a.etype, J2Plasticity(210e3, 0.3, [[250.0, 0.0], [1250.0, 1.0]]), a.fixed, a.rhs)
