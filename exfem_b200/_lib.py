@@ -55,6 +55,9 @@ _SIGS = {
     "exfem_block_colours": ([VP, P], C.c_int),
     "exfem_block_tile_info": ([VP, C.POINTER(I64), C.POINTER(I64), C.POINTER(I32)], C.c_int),
     "exfem_block_tile_maps": ([VP, P, P, P, P], C.c_int),
+    "exfem_block_tile_order": ([VP, C.POINTER(I32), P], C.c_int),
+    "exfem_set_tile": ([I32, I32], C.c_int),
+    "exfem_get_tile": ([I32, C.POINTER(I32)], C.c_int),
     "exfem_block_set_scale": ([VP, P], C.c_int),
     "exfem_block_set_fixed": ([VP, P], C.c_int),
     "exfem_block_set_lame": ([VP, P, P], C.c_int),
@@ -89,6 +92,7 @@ _SIGS = {
     "exfem_host_gather_plan": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_colouring": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_standard_aggregation": ([I64, P, P, P, C.POINTER(I64)], C.c_int),
+    "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     _f = getattr(lib, _name)

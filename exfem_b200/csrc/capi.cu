@@ -8,6 +8,8 @@
 namespace exfem {
 
 static thread_local std::string g_err;
+// elements per matrix-free tile for blocks created from now on: C3D8, C3D10
+static int g_tile[2] = {128, 128};
 
 void set_error(const char* fmt, ...) {
   char buf[1024];
@@ -26,6 +28,8 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line) {
 int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan, int& vmax);
 int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& colour, int& ncolour);
 int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg);
+int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
+                    std::vector<int32_t>& order);
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
                    int& maxu);
@@ -64,13 +68,13 @@ static int init_tangent(exfem_block_s* b) {
   if (b->mat.kind != EXFEM_J2) return EXFEM_OK;
   // elastic tangent data (c1 = 1) in the tile-major layout, padding included
   const int W = b->ngp * 8;
-  const size_t n = (size_t)b->ntile * MF_TILE * W;
+  const size_t n = (size_t)b->ntile * b->tile * W;
   std::vector<double> t(n, 0.0);
   std::vector<float> t32(n, 0.0f);
-  for (int64_t e = 0; e < b->ntile * MF_TILE; ++e)
+  for (int64_t p = 0; p < b->ntile * b->tile; ++p)
     for (int g = 0; g < b->ngp; ++g) {
-      t[tile_index(e, g * 8 + 6, W)] = 1.0;
-      t32[tile_index(e, g * 8 + 6, W)] = 1.0f;
+      t[tile_index(p, g * 8 + 6, W, b->tile)] = 1.0;
+      t32[tile_index(p, g * 8 + 6, W, b->tile)] = 1.0f;
     }
   int s;
   if ((s = b->tan64.upload(t.data(), n))) return s;
@@ -174,9 +178,20 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
     }
   }
   {
+    // tile order: elements by mesh component, then along a Morton curve
+    b->tile = g_tile[etype == EXFEM_C3D8 ? 0 : 1];
+    if ((s = host_tile_order(nn, ne, b->nnode, etype == EXFEM_C3D8 ? 8 : 4, X_host, conn_host, b->order_host)))
+      return s;
+    std::vector<int32_t> conn_ord((size_t)ne * b->nnode), tpos(ne);
+    for (int64_t p = 0; p < ne; ++p) {
+      const int64_t e = b->order_host[p];
+      tpos[e] = (int32_t)p;
+      memcpy(&conn_ord[p * b->nnode], conn_host + e * b->nnode, b->nnode * sizeof(int32_t));
+    }
+    if ((s = b->tpos.upload(tpos.data(), std::max<size_t>(tpos.size(), 1)))) return s;
     std::vector<int32_t> tp, tn;
     std::vector<uint16_t> te, tq;
-    if ((s = host_tile_maps(nn, ne, b->nnode, conn_host, MF_TILE, tp, tn, te, tq, b->maxu))) return s;
+    if ((s = host_tile_maps(nn, ne, b->nnode, conn_ord.data(), b->tile, tp, tn, te, tq, b->maxu))) return s;
     b->ntile = (int64_t)tp.size() - 1;
     if ((s = b->tile_ptr.upload(tp.data(), tp.size()))) return s;
     if ((s = b->tile_nodes.upload(tn.data(), std::max<size_t>(tn.size(), 1)))) return s;
@@ -186,13 +201,24 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
     if ((s = b->tile_perm.upload(tq.data(), std::max<size_t>(tq.size(), 1)))) return s;
     {  // forward map of the slot lists: list position of every slot's node
       std::vector<uint16_t> li(tq.size(), 0);
-      const int NS = b->nnode * MF_TILE;
+      const int NS = b->nnode * b->tile;
       for (int64_t t = 0; t < b->ntile; ++t) {
         int q = 0;
         for (int k = 0; k < tp[t + 1] - tp[t]; ++k)
           for (; q < te[tp[t] + k]; ++q) li[t * NS + tq[t * NS + q]] = (uint16_t)k;
       }
       if ((s = b->lidx.upload(li.data(), std::max<size_t>(li.size(), 1)))) return s;
+    }
+    {  // run ends per tile, each tile's run padded to a multiple of 8 entries (16 bytes)
+      std::vector<int32_t> off(std::max<int64_t>(b->ntile, 1), 0);
+      std::vector<uint16_t> pad;
+      for (int64_t t = 0; t < b->ntile; ++t) {
+        off[t] = (int32_t)pad.size();
+        pad.insert(pad.end(), te.begin() + tp[t], te.begin() + tp[t + 1]);
+        pad.resize((pad.size() + 7) & ~size_t(7), 0);
+      }
+      if ((s = b->nend_off.upload(off.data(), off.size()))) return s;
+      if ((s = b->tile_nend_pad.upload(pad.data(), std::max<size_t>(pad.size(), 8)))) return s;
     }
     {  // node -> entry map of the tile node lists (counting sort, entries increasing)
       std::vector<int32_t> np(nn + 1, 0), dest(tn.size());
@@ -278,8 +304,29 @@ int exfem_block_tile_maps(exfem_block b, int32_t* ptr_host, int32_t* nodes_host,
   if (nodes_host && nl) EX_CUDA(cudaMemcpy(nodes_host, b->tile_nodes.p, nl * sizeof(int32_t), cudaMemcpyDeviceToHost));
   if (nend_host && nl) EX_CUDA(cudaMemcpy(nend_host, b->tile_nend.p, nl * sizeof(uint16_t), cudaMemcpyDeviceToHost));
   if (perm_host && b->ntile)
-    EX_CUDA(cudaMemcpy(perm_host, b->tile_perm.p, (size_t)b->ntile * b->nnode * MF_TILE * sizeof(uint16_t),
+    EX_CUDA(cudaMemcpy(perm_host, b->tile_perm.p, (size_t)b->ntile * b->nnode * b->tile * sizeof(uint16_t),
                        cudaMemcpyDeviceToHost));
+  return EXFEM_OK;
+}
+
+int exfem_block_tile_order(exfem_block b, int* tile, int32_t* order_host) {
+  EX_ARG(b, "block is NULL");
+  if (tile) *tile = b->tile;
+  if (order_host && b->ne) memcpy(order_host, b->order_host.data(), b->ne * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_set_tile(int etype, int tile) {
+  EX_ARG(etype == EXFEM_C3D8 || etype == EXFEM_C3D10, "unknown element type %d", etype);
+  EX_ARG(tile == 128 || tile == 256, "tile size must be 128 or 256, got %d", tile);
+  g_tile[etype == EXFEM_C3D8 ? 0 : 1] = tile;
+  return EXFEM_OK;
+}
+
+int exfem_get_tile(int etype, int* tile) {
+  EX_ARG(etype == EXFEM_C3D8 || etype == EXFEM_C3D10, "unknown element type %d", etype);
+  EX_ARG(tile, "tile is NULL");
+  *tile = g_tile[etype == EXFEM_C3D8 ? 0 : 1];
   return EXFEM_OK;
 }
 
@@ -590,6 +637,20 @@ int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn,
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
   EX_ARG(ptr && idx && agg && nagg, "NULL argument");
   return host_standard_aggregation(n, ptr, idx, agg, *nagg);
+}
+
+int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
+                          int32_t* order) {
+  EX_ARG(nn >= 0 && ne >= 0 && nnode > 0 && ncorner > 0 && ncorner <= nnode, "invalid sizes");
+  EX_ARG((X || nn == 0) && (conn || ne == 0) && (order || ne == 0), "NULL argument");
+  for (int64_t k = 0; k < ne * nnode; ++k)
+    EX_ARG(conn[k] >= 0 && conn[k] < nn, "connectivity entry %d at slot %lld is outside [0, %lld)", conn[k],
+           (long long)k, (long long)nn);
+  std::vector<int32_t> o;
+  int s;
+  if ((s = host_tile_order(nn, ne, nnode, ncorner, X, conn, o))) return s;
+  if (ne) memcpy(order, o.data(), ne * sizeof(int32_t));
+  return EXFEM_OK;
 }
 
 }  // extern "C"

@@ -138,14 +138,14 @@ __host__ __device__ constexpr double tet10_dN(int g, int a, int i) {
 }
 
 // ---------------------------------------------------------------- tile-major streams
-// Per-element streams of the matrix-free operator (geometry, J2 tangent data,
-// tile-local node indices) are stored tile-major ("AoSoA"): tiles of MF_TILE
-// consecutive elements, and inside a tile component k of element l at
-// k*MF_TILE + l.  A tile's stream is one contiguous block (one bulk copy), and a
-// warp reading component k of its 32 elements touches 128 contiguous bytes.
-constexpr int MF_TILE = 128;
-__host__ __device__ __forceinline__ int64_t tile_index(int64_t e, int k, int width) {
-  return ((e / MF_TILE) * width + k) * MF_TILE + (e % MF_TILE);
+// Per-element streams of the matrix-free operator (geometry, J2 tangent data) are
+// stored tile-major ("AoSoA") over the block's tile order: tiles of `tile`
+// consecutive positions, and inside a tile component k of the element at
+// position p at k*tile + p.  A tile's stream is one contiguous block (one bulk
+// copy), and the thread that evaluates positions 2j and 2j+1 reads component k of
+// both with one 8- (FP32) or 16-byte (FP64) load.
+__host__ __device__ __forceinline__ int64_t tile_index(int64_t pos, int k, int width, int tile) {
+  return ((pos / tile) * width + k) * tile + (pos % tile);
 }
 
 // ---------------------------------------------------------------- element traits

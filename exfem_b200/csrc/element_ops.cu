@@ -47,7 +47,8 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
              const double* __restrict__ st_old, double* __restrict__ st_new, double* __restrict__ fe,
              double* __restrict__ tan64, float* __restrict__ tan32, double* __restrict__ S,
              double* __restrict__ mises, double* __restrict__ peeq, const MatDev mat,
-             const double* __restrict__ lam_e, const double* __restrict__ mu_e) {
+             const double* __restrict__ lam_e, const double* __restrict__ mu_e,
+             const int32_t* __restrict__ tpos, int tile) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, NG = Tr::ngp;
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -110,10 +111,10 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
       if (MODE != FORCE_STRESS) {
         if (tan64)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan64[tile_index(e, g * 8 + k, NG * 8)] = tn[k];
+          for (int k = 0; k < 8; ++k) tan64[tile_index(tpos[e], g * 8 + k, NG * 8, tile)] = tn[k];
         if (tan32)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan32[tile_index(e, g * 8 + k, NG * 8)] = (float)tn[k];
+          for (int k = 0; k < 8; ++k) tan32[tile_index(tpos[e], g * 8 + k, NG * 8, tile)] = (float)tn[k];
       }
       if (MODE == FORCE_FULL) {
         const double vol = detJ * sc;
@@ -180,10 +181,10 @@ force_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict
       if (MODE != FORCE_STRESS) {
         if (tan64)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan64[tile_index(e, g * 8 + k, NG * 8)] = tn[k];
+          for (int k = 0; k < 8; ++k) tan64[tile_index(tpos[e], g * 8 + k, NG * 8, tile)] = tn[k];
         if (tan32)
 #pragma unroll
-          for (int k = 0; k < 8; ++k) tan32[tile_index(e, g * 8 + k, NG * 8)] = (float)tn[k];
+          for (int k = 0; k < 8; ++k) tan32[tile_index(tpos[e], g * 8 + k, NG * 8, tile)] = (float)tn[k];
       }
       if (MODE == FORCE_FULL) {
         const double vol = detJ / 24.0 * sc;
@@ -248,7 +249,7 @@ static int force_dispatch(exfem_block_s* b, const double* u, const double* st_ol
   float* t32 = (MODE != FORCE_STRESS && j2) ? b->tan32.p : nullptr;
   force_kernel<ET, MODE><<<grid, threads, 0, s>>>(b->ne, b->X.p, b->conn.p, u, b->scale.p, st_old,
                                                   st_new, fe, t64, t32, S, mises, peeq, b->mat, b->lam_e.p,
-                                                  b->mu_e.p);
+                                                  b->mu_e.p, b->tpos.p, b->tile);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
 }
@@ -336,7 +337,7 @@ template <int ET>
 __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn,
                                 const double* __restrict__ scale, const double* __restrict__ lam_e,
                                 const double* __restrict__ mu_e, double lam0, double mu0, double* __restrict__ g64,
-                                float* __restrict__ g32) {
+                                float* __restrict__ g32, const int32_t* __restrict__ tpos, int tile) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, GS = Tr::geo_stride;
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -378,15 +379,15 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
   }
 #pragma unroll
   for (int k = 0; k < GS; ++k) {
-    g64[tile_index(e, k, GS)] = out[k];
-    g32[tile_index(e, k, GS)] = (float)out[k];
+    g64[tile_index(tpos[e], k, GS, tile)] = out[k];
+    g32[tile_index(tpos[e], k, GS, tile)] = (float)out[k];
   }
 }
 
 int build_geometry(exfem_block_s* b) {
   const int GS = b->etype == EXFEM_C3D8 ? ElemTraits<EXFEM_C3D8>::geo_stride : ElemTraits<EXFEM_C3D10>::geo_stride;
   int st;
-  const int64_t padded = b->ntile * MF_TILE * GS;
+  const int64_t padded = b->ntile * b->tile * GS;
   if (b->geo64.n != (size_t)padded) {
     if ((st = b->geo64.alloc(padded))) return st;
     if ((st = b->geo32.alloc(padded))) return st;
@@ -398,10 +399,12 @@ int build_geometry(exfem_block_s* b) {
   const unsigned grid = (unsigned)((b->ne + threads - 1) / threads);
   if (b->etype == EXFEM_C3D8)
     geometry_kernel<EXFEM_C3D8><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
-                                                   b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p);
+                                                   b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p,
+                                                   b->tpos.p, b->tile);
   else
     geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
-                                                    b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p);
+                                                    b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p,
+                                                   b->tpos.p, b->tile);
   EX_LAUNCH_CHECK();
   EX_CUDA(cudaDeviceSynchronize());
   return EXFEM_OK;
@@ -436,7 +439,7 @@ stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __rest
                  const double* __restrict__ u, const double* __restrict__ scale,
                  const double* __restrict__ st_old, const double* __restrict__ tan_in,
                  const MatDev mat, const double* __restrict__ lam_e, const double* __restrict__ mu_e,
-                 OutT* __restrict__ Ke, double* __restrict__ ediag) {
+                 OutT* __restrict__ Ke, double* __restrict__ ediag, const int32_t* __restrict__ tpos, int tile) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, NG = Tr::ngp, ND = 3 * NN, EPB = 64 / NN;
   constexpr bool BBAR = ET == EXFEM_C3D8;
@@ -490,7 +493,7 @@ stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __rest
     const double* st = st_old ? st_old + (e * NG + g) * ns : zero_state;
     double sig[6], tn[8];
     if (tan_in) {
-      for (int k = 0; k < 8; ++k) tn[k] = tan_in[tile_index(e, g * 8 + k, NG * 8)];
+      for (int k = 0; k < 8; ++k) tn[k] = tan_in[tile_index(tpos[e], g * 8 + k, NG * 8, tile)];
     } else {
       material_stress(mat, lam_k, mu_k, H, st, nullptr, sig, tn);
     }
@@ -583,10 +586,12 @@ static void stiffness_go(exfem_block_s* b, const double* u, const double* st_old
   const unsigned grid = (unsigned)((b->ne + EPB - 1) / EPB);
   if (ediag)
     stiffness_kernel<ET, 1, OutT><<<grid, 64, 0, s>>>(b->ne, b->X.p, b->conn.p, u, b->scale.p, st_old,
-                                                      tan_in, b->mat, b->lam_e.p, b->mu_e.p, Ke, ediag);
+                                                      tan_in, b->mat, b->lam_e.p, b->mu_e.p, Ke, ediag,
+                                                      b->tpos.p, b->tile);
   else
     stiffness_kernel<ET, 0, OutT><<<grid, 64, 0, s>>>(b->ne, b->X.p, b->conn.p, u, b->scale.p, st_old,
-                                                      tan_in, b->mat, b->lam_e.p, b->mu_e.p, Ke, ediag);
+                                                      tan_in, b->mat, b->lam_e.p, b->mu_e.p, Ke, ediag,
+                                                      b->tpos.p, b->tile);
 }
 
 int launch_stiffness(exfem_block_s* b, const double* u, const double* st_old, int dtype, void* Ke,

@@ -17,6 +17,7 @@
 //      pass 3: still-unaggregated nodes seed new aggregates with their
 //              unaggregated neighbours.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -81,17 +82,95 @@ int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::
   return EXFEM_OK;
 }
 
+// Tile order of the matrix-free operator (no counterpart in the reference):
+// elements are grouped by connected component (components in the order of their
+// first element) and, inside a component, sorted along a Morton (Z-order) curve
+// of their corner-node coordinate sums, ties by element index.  Consecutive
+// positions are then spatially compact, so a tile of consecutive positions
+// touches few distinct nodes, and the tiles of one mesh never mix with another
+// mesh of the same union block.  The key:
+//   s_e   = x_{c0} + x_{c1} + ... (corner nodes in local order, summed in order)
+//   q_e,d = min(floor((s_e,d - lo_d) / (hi_d - lo_d) * 2^21), 2^21 - 1)
+//           (0 when hi_d == lo_d), lo/hi the extent of s over all elements
+//   key   = bits of q_x, q_y, q_z interleaved (x lowest).
+int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
+                    std::vector<int32_t>& order) {
+  order.resize(ne);
+  if (ne == 0) return EXFEM_OK;
+  // components: union-find over the nodes of each element
+  std::vector<int32_t> parent(nn);
+  for (int64_t n = 0; n < nn; ++n) parent[n] = (int32_t)n;
+  auto find = [&](int32_t a) {
+    while (parent[a] != a) {
+      parent[a] = parent[parent[a]];
+      a = parent[a];
+    }
+    return a;
+  };
+  for (int64_t e = 0; e < ne; ++e) {
+    int32_t r0 = find(conn[e * nnode]);
+    for (int a = 1; a < nnode; ++a) {
+      const int32_t r = find(conn[e * nnode + a]);
+      if (r < r0) {
+        parent[r0] = r;
+        r0 = r;
+      } else if (r > r0) {
+        parent[r] = r0;
+      }
+    }
+  }
+  std::vector<int64_t> first(nn, -1), comp(ne);
+  for (int64_t e = 0; e < ne; ++e) {
+    const int32_t r = find(conn[e * nnode]);
+    if (first[r] < 0) first[r] = e;
+    comp[e] = first[r];
+  }
+  std::vector<double> s((size_t)ne * 3);
+  double lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+  for (int64_t e = 0; e < ne; ++e)
+    for (int d = 0; d < 3; ++d) {
+      double v = X[3 * (int64_t)conn[e * nnode] + d];
+      for (int a = 1; a < ncorner; ++a) v += X[3 * (int64_t)conn[e * nnode + a] + d];
+      s[3 * e + d] = v;
+      if (e == 0 || v < lo[d]) lo[d] = v;
+      if (e == 0 || v > hi[d]) hi[d] = v;
+    }
+  std::vector<uint64_t> key(ne);
+  for (int64_t e = 0; e < ne; ++e) {
+    uint64_t k = 0;
+    for (int d = 0; d < 3; ++d) {
+      uint64_t q = 0;
+      if (hi[d] > lo[d]) {
+        const double f = std::floor((s[3 * e + d] - lo[d]) / (hi[d] - lo[d]) * 2097152.0);
+        q = f >= 2097151.0 ? 2097151u : (f > 0.0 ? (uint64_t)f : 0u);
+      }
+      for (int b = 0; b < 21; ++b) k |= ((q >> b) & 1ull) << (3 * b + d);
+    }
+    key[e] = k;
+  }
+  for (int64_t e = 0; e < ne; ++e) order[e] = (int32_t)e;
+  std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+    if (comp[a] != comp[b]) return comp[a] < comp[b];
+    if (key[a] != key[b]) return key[a] < key[b];
+    return a < b;
+  });
+  return EXFEM_OK;
+}
+
 // Element-tile maps of the matrix-free operator.  Tiles are `tile` consecutive
-// elements; a slot of a tile is s = a*tile + l (local node a of the tile's
-// element l).  Per tile: the sorted distinct nodes it touches; for each of them,
-// in node order, its slots in increasing slot order, concatenated into `perm`
-// (tile-major, padded to nnode*tile entries per tile); and `nend`, the end of
-// each node's run in perm (aligned with the node list).
+// positions of the tile order (conn is given in that order).  Each thread of the
+// product evaluates the pair of elements at positions 2j and 2j+1 of its tile, so
+// slots are numbered s = a*tile + (p % 2)*(tile/2) + p/2 for local node a of the
+// element at tile position p: thread j's slots are a*tile + j and
+// a*tile + tile/2 + j.  Per tile: the sorted distinct nodes it touches; for each
+// of them, in node order, its slots in increasing slot order, concatenated into
+// `perm` (tile-major, padded to nnode*tile entries per tile); and `nend`, the end
+// of each node's run in perm (aligned with the node list).
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
                    int& maxu) {
   const int64_t ntile = (ne + tile - 1) / tile;
-  const int nslot = nnode * tile;
+  const int nslot = nnode * tile, half = tile / 2;
   ptr.assign(ntile + 1, 0);
   nodes.clear();
   nend.clear();
@@ -103,6 +182,7 @@ int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int t
   for (int64_t t = 0; t < ntile; ++t) {
     list.clear();
     const int64_t e0 = t * tile, e1 = std::min<int64_t>(ne, e0 + tile);
+    const int cntl = (int)(e1 - e0);
     for (int64_t k = e0 * nnode; k < e1 * nnode; ++k) {
       const int32_t n = conn[k];
       if (stamp[n] != t) { stamp[n] = t; list.push_back(n); }
@@ -112,13 +192,18 @@ int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int t
     for (int i = 0; i < nu; ++i) pos[list[i]] = i;
     cnt.assign(nu, 0);
     for (int a = 0; a < nnode; ++a)
-      for (int64_t e = e0; e < e1; ++e) ++cnt[pos[conn[e * nnode + a]]];
+      for (int p = 0; p < cntl; ++p) ++cnt[pos[conn[(e0 + p) * nnode + a]]];
     start.assign(nu + 1, 0);
     for (int i = 0; i < nu; ++i) start[i + 1] = start[i] + cnt[i];
     uint16_t* pm = perm.data() + (size_t)t * nslot;
     for (int i = 0; i < nu; ++i) cnt[i] = start[i];
     for (int a = 0; a < nnode; ++a)                      // increasing slot order
-      for (int64_t e = e0; e < e1; ++e) pm[cnt[pos[conn[e * nnode + a]]]++] = (uint16_t)(a * tile + (e - e0));
+      for (int h = 0; h < 2; ++h)
+        for (int j = 0; j < half; ++j) {
+          const int p = 2 * j + h;
+          if (p >= cntl) continue;
+          pm[cnt[pos[conn[(e0 + p) * nnode + a]]]++] = (uint16_t)(a * tile + h * half + j);
+        }
     nodes.insert(nodes.end(), list.begin(), list.end());
     for (int i = 0; i < nu; ++i) nend.push_back((uint16_t)start[i + 1]);
     ptr[t + 1] = (int32_t)nodes.size();

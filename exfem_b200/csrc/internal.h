@@ -28,18 +28,24 @@ struct exfem_block_s {
   // boundary conditions
   exfem::DevBuf<uint8_t> fixed;       // (ndof) 1 = prescribed; empty = all free
   exfem::DevBuf<uint8_t> node_fixed;  // (nn) bit c set = dof c prescribed
-  // matrix-free operator data: tiles of MF_TILE consecutive elements, each with
-  // the sorted list of distinct nodes it touches and per-slot local indices
+  // matrix-free operator data: tiles of `tile` consecutive positions of the tile
+  // order (elements by mesh component, then along a Morton curve), each with the
+  // sorted list of distinct nodes it touches and per-slot local indices
   int affine = 1;
+  int tile = 128;                     // elements per tile (128 or 256)
   int64_t ntile = 0;
   int maxu = 0;                       // largest distinct-node count of a tile
+  std::vector<int32_t> order_host;    // (ne) tile position -> element
+  exfem::DevBuf<int32_t> tpos;        // (ne) element -> tile position
   exfem::DevBuf<int32_t> tile_ptr;    // (ntile+1)
   exfem::DevBuf<int32_t> tile_nodes;  // concatenated sorted node lists
   exfem::DevBuf<int32_t> tile_nodes_bc;  // same, node | fixed-DOF bits << 29
   std::vector<int32_t> tile_nodes_host;
-  exfem::DevBuf<uint16_t> lidx;       // tile-major (ntile, nnode*MF_TILE): list position of each slot's node
+  exfem::DevBuf<uint16_t> lidx;       // tile-major (ntile, nnode*tile): list position of each slot's node
   exfem::DevBuf<uint16_t> tile_nend;  // per listed node: end of its slot run in tile_perm
-  exfem::DevBuf<uint16_t> tile_perm;  // tile-major (ntile, nnode*MF_TILE) slots grouped by node
+  exfem::DevBuf<uint16_t> tile_nend_pad;  // the same per tile, each tile's run padded to 8 entries
+  exfem::DevBuf<int32_t> nend_off;    // (ntile) start of each tile's run in tile_nend_pad
+  exfem::DevBuf<uint16_t> tile_perm;  // tile-major (ntile, nnode*tile) slots grouped by node
   exfem::DevBuf<int32_t> node_ptr;    // (nn+1) node -> its run of tile entries in node-major order
   exfem::DevBuf<int32_t> tile_dest;   // per tile-list entry: its node-major position
   exfem::DevBuf<double> partial;      // per-entry tile sums, 3 per entry (FP64 or FP32 view)
@@ -47,7 +53,7 @@ struct exfem_block_s {
   exfem::DevBuf<double> geo64;        // (ne, geo_stride)
   exfem::DevBuf<float> geo32;
   int plastic_tangent = 0;            // 1 once tangent data differs from elastic
-  exfem::DevBuf<double> tan64;        // (ne, ngp, 8)
+  exfem::DevBuf<double> tan64;        // tile-major (ntile, ngp*8, tile)
   exfem::DevBuf<float> tan32;
   // generations: tangent data and boundary-condition buffers (solvers compare)
   uint64_t tan_gen = 0, bc_gen = 0;

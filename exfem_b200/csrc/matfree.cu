@@ -4,32 +4,37 @@
 // Model.tangent_jvp) and its stored-Ke product (gfem/model.py:264-267) inside
 // opA (gfem/solvers.py:257-267):  y = free * K (free * v) + fixed * v.
 //
-// Work unit: a tile of MF_TILE = 128 consecutive elements, one CTA of 128 threads
-// per tile, persistent over tiles.  Per tile:
-//   1. element streams (geometry, tile-local node indices, J2 tangent data) are
-//      one contiguous block each in the tile-major layout; in the FP32 kernel a
-//      single thread moves them into shared memory with bulk TMA copies
-//      (cp.async.bulk, mbarrier completion), double buffered so that the copy of
-//      the next tile overlaps the work on this one;
-//   2. v is gathered once per distinct node of the tile into shared memory —
-//      ~3 distinct nodes per element instead of 8/10 node slots — with
+// Work unit: a tile of TT consecutive positions of the block's tile order
+// (elements grouped by mesh component and sorted along a Morton curve, so that a
+// tile is a compact patch), one CTA of TT/2 threads per tile, persistent over
+// tiles.  Per tile:
+//   1. the tile's streams (geometry, slot -> node-list position, the slots
+//      grouped by node and the end of each node's run) are one contiguous block
+//      each; in the FP32 kernel one thread moves them into shared memory with
+//      bulk TMA copies (cp.async.bulk, mbarrier completion), double buffered so
+//      that the copy of the next tile overlaps the work on this one;
+//   2. v is gathered once per distinct node of the tile into shared memory with
 //      asynchronous cp.async copies issued one tile ahead (fixed DOFs, whose bits
-//      sit above the node id in the tile list, are zero filled), so the gather
-//      of the next tile overlaps the arithmetic of this one;
-//   3. one thread per element evaluates the element product from shared memory
-//      (C3D8: modal B-bar form; C3D10: constant inverse Jacobian of the
-//      straight-edged element) and accumulates it into per-node shared-memory
-//      sums;
-//   4. the tile's per-node sums are stored (plain stores, no atomics) at their
-//      precomputed positions in a node-major partials buffer;
+//      sit above the node id in the tile list, are zero filled);
+//   3. thread j evaluates the products of the elements at tile positions 2j and
+//      2j+1 together, every arithmetic operation on a lane pair (in FP32 one
+//      packed FFMA2/FADD2/FMUL2 instruction for both elements), and writes the 2 x
+//      nnode nodal force vectors into its own slots;
+//   4. each distinct node of the tile sums its slots in increasing slot order
+//      (no atomics, a fixed order) and stores the sum at its precomputed position
+//      in a node-major partials buffer;
 // and a second, node-centric pass forms y[n] = fixed ? v : the sum of node n's
 // contiguous run of tile entries, in tile order (the reference's atomic-free
 // gather-plan assembly, gfem/model.py:241-267, at tile granularity).  The
-// product is deterministic.
+// product is deterministic: every sum has a fixed order.
 // Geometry: C3D8 stores the 7 modal coordinate vectors (coordinates with the
 // centroid removed) and the stiffness scale; C3D10 stores the inverse Jacobian
 // and scaled volume, formed in FP64 from the nodal coordinates and rounded once.
+#include <limits>
+#include <type_traits>
+
 #include "internal.h"
+#include "pair_math.cuh"
 
 namespace exfem {
 
@@ -86,33 +91,34 @@ __device__ __forceinline__ void matmul3t(const T (&A)[9], const T (&B)[9], T (&C
 }
 
 // stress at a Gauss point from the strain: elastic or the stored J2 tangent
-// (tn points to component 0 of this element/point, stride MF_TILE)
-template <class T, bool J2>
-__device__ __forceinline__ void mf_stress(const T* tn, T lam, T mu, T Kb, const T (&e)[6], T (&s)[6]) {
+// (tn points to component 0 of this element pair and point, stride S pairs)
+template <class P, int S, bool J2>
+__device__ __forceinline__ void mf_stress(const P* tn, P lam, P mu, P Kb, const P (&e)[6], P (&s)[6]) {
   if constexpr (J2) {
-    T t[8];
+    P t[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) t[k] = tn[k * MF_TILE];
+    for (int k = 0; k < 8; ++k) t[k] = tn[k * S];
     tangent_stress(Kb, mu, t, e, s);
   } else {
     elastic_stress(lam, mu, e, s);
   }
 }
 
-// element product f = Ke v_e from the element's streams (strided by MF_TILE)
-template <class T, int ET, bool J2>
-__device__ __forceinline__ void element_product(const T* g, const T* tn, const T (&va)[ElemTraits<ET>::nnode][3],
-                                                T lam, T mu, T Kb, T (&f)[ElemTraits<ET>::nnode][3]) {
+// products f = Ke v_e of an element pair from its streams (g, tn: component 0 of
+// the pair, stride S pairs); P is a lane pair (F2 or D2)
+template <class P, int ET, bool J2, int S>
+__device__ __forceinline__ void element_product(const P* g, const P* tn, const P (&va)[ElemTraits<ET>::nnode][3],
+                                                P mu, P Kb, P (&f)[ElemTraits<ET>::nnode][3]) {
   if constexpr (ET == EXFEM_C3D8) {
-    T cm[7][3], um[7][3];
+    P cm[7][3], um[7][3];
 #pragma unroll
     for (int k = 0; k < 7; ++k)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) cm[k][c] = g[(3 * k + c) * MF_TILE];
-    const T sc = g[21 * MF_TILE];
-    const T le = g[22 * MF_TILE], me = J2 ? mu : g[23 * MF_TILE];
+      for (int c = 0; c < 3; ++c) cm[k][c] = g[(3 * k + c) * S];
+    const P sc = g[21 * S];
+    const P le = g[22 * S], me = J2 ? mu : g[23 * S];
     hex_to_modal(va, um);
-    T J0[9], iJ0[9], G0[9], H0[9];
+    P J0[9], iJ0[9], G0[9], H0[9];
 #pragma unroll
     for (int n = 0; n < 3; ++n)
 #pragma unroll
@@ -122,33 +128,33 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       }
     inv3(J0, iJ0);
     matmul3t(G0, iJ0, H0);
-    const T tr0 = H0[0] + H0[4] + H0[8];
-    T Fm[7][3];
+    const P tr0 = H0[0] + H0[4] + H0[8];
+    P Fm[7][3];
 #pragma unroll
-    for (int k = 0; k < 7; ++k) Fm[k][0] = Fm[k][1] = Fm[k][2] = T(0);
-    T tacc = T(0);
+    for (int k = 0; k < 7; ++k) Fm[k][0] = Fm[k][1] = Fm[k][2] = P(0.0);
+    P tacc = P(0.0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const T x = T(HEX_GQ * hex_sign(q, 0)), yy = T(HEX_GQ * hex_sign(q, 1)), z = T(HEX_GQ * hex_sign(q, 2));
-      T J[9], iJ[9], G[9], H[9];
+      const P x = P(HEX_GQ * hex_sign(q, 0)), yy = P(HEX_GQ * hex_sign(q, 1)), z = P(HEX_GQ * hex_sign(q, 2));
+      P J[9], iJ[9], G[9], H[9];
       hex_modal_grad(cm, x, yy, z, J);
-      const T detJ = inv3(J, iJ);
+      const P detJ = inv3(J, iJ);
       hex_modal_grad(um, x, yy, z, G);
       matmul3t(G, iJ, H);
-      const T bb = (tr0 - (H[0] + H[4] + H[8])) * T(1.0 / 3.0);
+      const P bb = P((tr0 - (H[0] + H[4] + H[8])) * P(1.0 / 3.0));
       H[0] += bb;
       H[4] += bb;
       H[8] += bb;
-      T ee[6], s[6];
+      P ee[6], s[6];
       sym_from_grad(H, ee);
-      mf_stress<T, J2>(tn + q * 8 * MF_TILE, le, me, Kb, ee, s);
-      const T vol = detJ * sc;
-      const T t = vol * (s[0] + s[1] + s[2]) * T(1.0 / 3.0);
+      mf_stress<P, S, J2>(tn + q * 8 * S, le, me, Kb, ee, s);
+      const P vol = P(detJ * sc);
+      const P t = P(vol * (s[0] + s[1] + s[2]) * P(1.0 / 3.0));
       tacc += t;
-      const T r[3][3] = {{vol * s[0] - t, vol * s[3], vol * s[5]},
-                         {vol * s[3], vol * s[1] - t, vol * s[4]},
-                         {vol * s[5], vol * s[4], vol * s[2] - t}};
-      T Q[9];
+      const P r[3][3] = {{vol * s[0] - t, P(vol * s[3]), P(vol * s[5])},
+                         {P(vol * s[3]), vol * s[1] - t, P(vol * s[4])},
+                         {P(vol * s[5]), P(vol * s[4]), vol * s[2] - t}};
+      P Q[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -160,22 +166,101 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
 #pragma unroll
       for (int i = 0; i < 3; ++i) Fm[i][c] += tacc * iJ0[3 * i + c];
     hex_from_modal(Fm, f);
+  } else if constexpr (!J2) {
+    // linear-elastic C3D10 with a constant Jacobian (straight edges): the
+    // displacement gradient is linear in the barycentric coordinates L, so the
+    // stress is too, and the 4-point rule integrates the degree-2 integrand
+    // exactly.  With sigma_k the stress at corner k, g_i = grad L_i (rows of the
+    // inverse Jacobian, g_0 = -(g_1 + g_2 + g_3)), V = 4 vol the element volume
+    // and s_k = (V/20) sigma_k, S = sum_k s_k, the exact integrals
+    //   f_i  = (4 s_i - S) g_i                     (corner i)
+    //   f_ij = 4 ((S + s_j) g_i + (S + s_i) g_j)   (mid-node of edge ij)
+    // equal the quadrature sums of the reference.  The corner gradients follow
+    // from du/dL_i at corner k: 3 u_k for i = k, 4 u_ik - u_i otherwise.
+    P iJ[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) iJ[k] = g[k * S];
+    const P vol = g[9 * S];
+    const P lt = P(P(0.2) * vol * g[10 * S]), mt = P(P(0.2) * vol * g[11 * S]), m2 = P(P(2.0) * mt);
+    P sv[4][6];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      P nw[3];                                          // -du/dL_0 at corner k
+#pragma unroll
+      for (int c = 0; c < 3; ++c) nw[c] = k == 0 ? P(P(-3.0) * va[0][c]) : P(-4.0) * va[tet_edge_node(0, k)][c] + va[0][c];
+      P G[9];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int m = 1; m < 4; ++m)
+          G[3 * c + m - 1] = m == k ? P(3.0) * va[k][c] + nw[c] : P(4.0) * va[tet_edge_node(m, k)][c] + (nw[c] - va[m][c]);
+      P Hk[9];
+      matmul3t(G, iJ, Hk);
+      const P tr = Hk[0] + Hk[4] + Hk[8];
+      const P ltr = P(lt * tr);
+      sv[k][0] = m2 * Hk[0] + ltr;
+      sv[k][1] = m2 * Hk[4] + ltr;
+      sv[k][2] = m2 * Hk[8] + ltr;
+      sv[k][3] = P(mt * (Hk[1] + Hk[3]));
+      sv[k][4] = P(mt * (Hk[5] + Hk[7]));
+      sv[k][5] = P(mt * (Hk[2] + Hk[6]));
+    }
+    P NSs[6], S4[6];                                    // -S, 4 S
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      const P Ss = sv[0][j] + sv[1][j] + sv[2][j] + sv[3][j];
+      NSs[j] = -Ss;
+      S4[j] = P(P(4.0) * Ss);
+    }
+    P gr[4][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      gr[1][j] = iJ[j];
+      gr[2][j] = iJ[3 + j];
+      gr[3][j] = iJ[6 + j];
+      gr[0][j] = -(gr[1][j] + gr[2][j] + gr[3][j]);
+    }
+    // symmetric (xx yy zz xy yz xz) times vector
+    auto smv = [](const P (&m)[6], const P (&x)[3], P (&y)[3]) {
+      y[0] = m[0] * x[0] + m[3] * x[1] + m[5] * x[2];
+      y[1] = m[3] * x[0] + m[1] * x[1] + m[4] * x[2];
+      y[2] = m[5] * x[0] + m[4] * x[1] + m[2] * x[2];
+    };
+    auto smv_acc = [](const P (&m)[6], const P (&x)[3], P (&y)[3]) {
+      y[0] += m[0] * x[0] + m[3] * x[1] + m[5] * x[2];
+      y[1] += m[3] * x[0] + m[1] * x[1] + m[4] * x[2];
+      y[2] += m[5] * x[0] + m[4] * x[1] + m[2] * x[2];
+    };
+    P U[4][6];                                          // 4 (S + s_k)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      P Z[6];                                           // 4 s_k - S
+#pragma unroll
+      for (int j = 0; j < 6; ++j) {
+        Z[j] = P(4.0) * sv[k][j] + NSs[j];
+        U[k][j] = P(4.0) * sv[k][j] + S4[j];
+      }
+      smv(Z, gr[k], f[k]);
+    }
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      const int i = tet_edge(e, 0), j = tet_edge(e, 1);
+      smv(U[j], gr[i], f[4 + e]);
+      smv_acc(U[i], gr[j], f[4 + e]);
+    }
   } else {
     // C3D10 with a constant Jacobian, in barycentric form: with L the
     // barycentric coordinates, w_j = du/dL_j = base_j + D * (g == j ? v_j : v_e(j,g))
     // at Gauss point g (L_g = A, others B), base_j = (4B-1) v_j + 4B sum of the
     // edge nodes at corner j, D = 4(A-B); the reference gradient is
     // G_i = w_{i+1} - w_0.  The force is the adjoint of the same steps.
-    constexpr T A = T(TET_A), B = T(TET_B);
-    constexpr T D = T(4.0 * (TET_A - TET_B)), C0 = T(4.0 * TET_B - 1.0), C1 = T(4.0 * TET_B);
-    T iJ[9];
+    const P D = P(4.0 * (TET_A - TET_B)), C0 = P(4.0 * TET_B - 1.0), C1 = P(4.0 * TET_B);
+    P iJ[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) iJ[k] = g[k * MF_TILE];
-    const T vol = g[9 * MF_TILE];
-    const T le = g[10 * MF_TILE], me = J2 ? mu : g[11 * MF_TILE];
-    (void)A;
-    (void)B;
-    T base[4][3], vbar[10][3], bbar[4][3];
+    for (int k = 0; k < 9; ++k) iJ[k] = g[k * S];
+    const P vol = g[9 * S];
+    const P le = g[10 * S], me = J2 ? mu : g[11 * S];
+    P base[4][3], vbar[10][3], bbar[4][3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       base[0][c] = C0 * va[0][c] + C1 * (va[4][c] + va[6][c] + va[7][c]);
@@ -184,32 +269,32 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       base[3][c] = C0 * va[3][c] + C1 * (va[7][c] + va[8][c] + va[9][c]);
     }
 #pragma unroll
-    for (int a = 0; a < 10; ++a) vbar[a][0] = vbar[a][1] = vbar[a][2] = T(0);
+    for (int a = 0; a < 10; ++a) vbar[a][0] = vbar[a][1] = vbar[a][2] = P(0.0);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) bbar[j][0] = bbar[j][1] = bbar[j][2] = T(0);
+    for (int j = 0; j < 4; ++j) bbar[j][0] = bbar[j][1] = bbar[j][2] = P(0.0);
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      T w[4][3];
+      P w[4][3];
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
         const int src = jj == q ? jj : tet_edge_node(jj, q);
 #pragma unroll
         for (int c = 0; c < 3; ++c) w[jj][c] = base[jj][c] + D * va[src][c];
       }
-      T G[9];
+      P G[9];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
 #pragma unroll
         for (int i = 0; i < 3; ++i) G[3 * c + i] = w[i + 1][c] - w[0][c];
-      T H[9];
+      P H[9];
       matmul3t(G, iJ, H);
-      T ee[6], s[6];
+      P ee[6], s[6];
       sym_from_grad(H, ee);
-      mf_stress<T, J2>(tn + q * 8 * MF_TILE, le, me, Kb, ee, s);
-      const T r[3][3] = {{vol * s[0], vol * s[3], vol * s[5]},
-                         {vol * s[3], vol * s[1], vol * s[4]},
-                         {vol * s[5], vol * s[4], vol * s[2]}};
-      T Q[9];
+      mf_stress<P, S, J2>(tn + q * 8 * S, le, me, Kb, ee, s);
+      const P r[3][3] = {{P(vol * s[0]), P(vol * s[3]), P(vol * s[5])},
+                         {P(vol * s[3]), P(vol * s[1]), P(vol * s[4])},
+                         {P(vol * s[5]), P(vol * s[4]), P(vol * s[2])}};
+      P Q[9];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -217,7 +302,7 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       // adjoint: wbar_{i+1} = Q[:, i], wbar_0 = -sum_i Q[:, i]
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        T wb[4];
+        P wb[4];
         wb[1] = Q[3 * c + 0];
         wb[2] = Q[3 * c + 1];
         wb[3] = Q[3 * c + 2];
@@ -236,7 +321,7 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
       vbar[1][c] += C0 * bbar[1][c];
       vbar[2][c] += C0 * bbar[2][c];
       vbar[3][c] += C0 * bbar[3][c];
-      const T e0 = C1 * bbar[0][c], e1 = C1 * bbar[1][c], e2 = C1 * bbar[2][c], e3 = C1 * bbar[3][c];
+      const P e0 = C1 * bbar[0][c], e1 = C1 * bbar[1][c], e2 = C1 * bbar[2][c], e3 = C1 * bbar[3][c];
       vbar[4][c] += e0 + e1;   // edge (0,1)
       vbar[5][c] += e1 + e2;   // edge (1,2)
       vbar[6][c] += e0 + e2;   // edge (2,0)
@@ -251,63 +336,99 @@ __device__ __forceinline__ void element_product(const T* g, const T* tn, const T
   }
 }
 
-template <class T, int ET, bool J2>
+// Fixed-point accumulation of the tile's node sums: every nodal force of the
+// tile is scaled by q = 2^(B - e), with 2^e > vmax * max|f| over the tile (vmax
+// the largest number of element slots at one node), rounded to an integer and
+// added with native shared-memory integer atomics; the sums are exact integers,
+// independent of the order of the additions, and |sum| < 2^B fits the integer.
+// Converted back they carry a rounding error of at most vmax / (2q) <
+// 2^-B vmax^2 max|f|, below the rounding of the FP32 / FP64 sums they replace.
+template <class T> struct FixedOf;
+template <> struct FixedOf<float> {
+  using type = int32_t;
+  static constexpr int B = 30;
+};
+template <> struct FixedOf<double> {
+  using type = unsigned long long;
+  static constexpr int B = 62;
+};
+__device__ __forceinline__ float max_nan(float a, float b) {
+  float r;
+  asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ double max_nan(double a, double b) { return (a != a || b != b) ? a + b : fmax(a, b); }
+__device__ __forceinline__ int32_t to_fixed(float x) { return __float2int_rn(x); }
+__device__ __forceinline__ unsigned long long to_fixed(double x) { return (unsigned long long)__double2ll_rn(x); }
+__device__ __forceinline__ float from_fixed(int32_t i, float) { return __int2float_rn(i); }
+__device__ __forceinline__ double from_fixed(unsigned long long i, double) { return __ll2double_rn((long long)i); }
+
+template <class T, int ET, int TT, int LANES>
 struct TileLayout {
   using Tr = ElemTraits<ET>;
-  static constexpr int NN = Tr::nnode, NG = Tr::ngp, GS = Tr::geo_stride, NSLOT = NN * MF_TILE;
-  static constexpr uint32_t GEO_B = GS * MF_TILE * sizeof(T);
+  using I = typename FixedOf<T>::type;
+  static constexpr int NN = Tr::nnode, NG = Tr::ngp, GS = Tr::geo_stride, NSLOT = NN * TT, NT = TT / LANES;
+  static constexpr uint32_t GEO_B = GS * TT * sizeof(T);
   static constexpr uint32_t LIDX_B = NSLOT * sizeof(uint16_t);
-  static constexpr uint32_t TAN_B = J2 ? NG * 8 * MF_TILE * sizeof(T) : 0;
-  static constexpr uint32_t STAGE_B = GEO_B + LIDX_B + TAN_B;
-  static_assert(GEO_B % 16 == 0 && LIDX_B % 16 == 0 && TAN_B % 16 == 0, "bulk copies need 16-byte multiples");
+  static constexpr uint32_t STAGE_B = GEO_B + LIDX_B;
+  static_assert(GEO_B % 16 == 0 && LIDX_B % 16 == 0, "bulk copies need 16-byte multiples");
+  // shared memory: [2 stages (TMA only): geometry | lidx] [gathered v: 2 x 3 x mu]
+  // [node-major destinations: 2 x mu] [fixed-point sums: mu x 4] with mu = maxu
+  // rounded up to 8
+  static size_t smem_bytes(bool tma, int mu) {
+    return (tma ? 2 * (size_t)STAGE_B : 0) + 6 * (size_t)mu * sizeof(T) + 2 * (size_t)mu * sizeof(int32_t) +
+           4 * (size_t)mu * sizeof(I);
+  }
 };
 
-template <class T, int ET, bool J2, bool TMA>
-__global__ void __launch_bounds__(MF_TILE)
+// LANES = 2: thread j evaluates the elements at tile positions 2j and 2j+1 as one
+// lane pair (slot columns j and TT/2 + j); LANES = 1: thread j evaluates the
+// element of slot column j alone (position 2 (j mod TT/2) + j div (TT/2)), for
+// element types and precisions whose pair arithmetic would not fit in registers.
+template <class T, int ET, bool J2, int TT, int LANES, bool TMA>
+__global__ void __launch_bounds__(TT / LANES)
 mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint16_t* __restrict__ lidx,
                const T* __restrict__ tan, const int32_t* __restrict__ tptr, const int32_t* __restrict__ tpack,
-               const int32_t* __restrict__ tdest, const T* __restrict__ v, T* __restrict__ part, T lam, T mu,
-               T Kb, int maxu, const int* __restrict__ skip, int* __restrict__ err) {
-  using L = TileLayout<T, ET, J2>;
-  constexpr int NN = L::NN, NG = L::NG, GS = L::GS, NSLOT = L::NSLOT;
+               const int32_t* __restrict__ tdest, const T* __restrict__ v, T* __restrict__ part, T mu_m, T K_m,
+               int mu, int vmax, const int* __restrict__ skip, int* __restrict__ err) {
+  using L = TileLayout<T, ET, TT, LANES>;
+  using I = typename L::I;
+  using P = std::conditional_t<LANES == 2, typename PairOf<T>::type, T>;
+  constexpr int NN = L::NN, NG = L::NG, GS = L::GS, NSLOT = L::NSLOT, NT = L::NT, H = TT / 2, NW = NT / 32;
+  constexpr int B = FixedOf<T>::B;
   if (skip && *skip) return;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
+  __shared__ T wmax[NW];
   const int tid = threadIdx.x;
-  // element of the tile handled by this thread: lanes of a warp take every 4th
-  // element, so the elements that share corner nodes (neighbours in the mesh
-  // order) fall into different warps and their shared-memory additions to the
-  // same node rarely collide inside one warp instruction
-  const int lt = 4 * (tid & 31) + (tid >> 5);
-  T* xsb[2];                                                          // gathered v, double buffered
-  xsb[0] = reinterpret_cast<T*>(smem + (TMA ? 2 * L::STAGE_B : 0));
-  xsb[1] = xsb[0] + 3 * maxu;
-  T* ys = xsb[1] + 3 * maxu;                                          // accumulated products
-  auto stage_geo = [&](int s) { return reinterpret_cast<T*>(smem + s * L::STAGE_B); };
-  auto stage_lidx = [&](int s) { return reinterpret_cast<uint16_t*>(smem + s * L::STAGE_B + L::GEO_B); };
-  auto stage_tan = [&](int s) { return reinterpret_cast<T*>(smem + s * L::STAGE_B + L::GEO_B + L::LIDX_B); };
+  unsigned char* base = smem + (TMA ? 2 * L::STAGE_B : 0);
+  T* xsb = reinterpret_cast<T*>(base);                                     // [2][3][mu]
+  int32_t* tdb = reinterpret_cast<int32_t*>(base + 6 * (size_t)mu * sizeof(T));   // [2][mu]
+  I* acc = reinterpret_cast<I*>(base + 6 * (size_t)mu * sizeof(T) + 2 * (size_t)mu * sizeof(int32_t));  // [mu][4]
+  auto stage = [&](int s) { return smem + s * L::STAGE_B; };
   auto issue = [&](int64_t t, int s) {
     fence_proxy_async();
     mbar_expect_tx(&bar[s], L::STAGE_B);
-    bulk_g2s(stage_geo(s), geo + t * (GS * MF_TILE), L::GEO_B, &bar[s]);
-    bulk_g2s(stage_lidx(s), lidx + t * NSLOT, L::LIDX_B, &bar[s]);
-    if constexpr (J2) bulk_g2s(stage_tan(s), tan + t * (NG * 8 * MF_TILE), L::TAN_B, &bar[s]);
+    bulk_g2s(stage(s), geo + t * (GS * TT), L::GEO_B, &bar[s]);
+    bulk_g2s(stage(s) + L::GEO_B, lidx + t * NSLOT, L::LIDX_B, &bar[s]);
   };
-  // asynchronous gather of the tile's distinct nodes (fixed DOFs zero filled)
-  auto gather = [&](int64_t t, T* xs) {
+  // asynchronous gather of the tile's distinct nodes (fixed DOFs zero filled) and
+  // of their node-major destinations
+  auto gather = [&](int64_t t, int buf) {
     const int64_t u0 = tptr[t];
     const int nu = tptr[t + 1] - (int32_t)u0;
-    for (int k = tid; k < nu; k += MF_TILE) {
+    T* xs = xsb + buf * 3 * mu;
+    for (int k = tid; k < nu; k += NT) {
       const uint32_t pk = (uint32_t)tpack[u0 + k];
-      const int64_t n = pk & 0x1FFFFFFFu;
+      const T* vp = v + 3 * (int64_t)(pk & 0x1FFFFFFFu);
       const uint32_t bits = pk >> 29;
-      const T* vp = v + 3 * n;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) cp_async<sizeof(T)>(xs + c * maxu + k, vp + c, ((bits >> c) & 1) ? 0 : (int)sizeof(T));
+      for (int c = 0; c < 3; ++c) cp_async<sizeof(T)>(xs + c * mu + k, vp + c, ((bits >> c) & 1) ? 0 : (int)sizeof(T));
+      cp_async<4>(tdb + buf * mu + k, tdest + u0 + k, 4);
     }
     cp_async_commit();
   };
-  for (int k = tid; k < 3 * maxu; k += MF_TILE) ys[k] = T(0);
+  for (int k = tid; k < 4 * mu; k += NT) acc[k] = I(0);
   if constexpr (TMA) {
     if (tid == 0) {
       mbar_init(&bar[0], 1);
@@ -317,8 +438,7 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     __syncthreads();
     if (tid == 0 && (int64_t)blockIdx.x < ntile) issue(blockIdx.x, 0);
   }
-  if ((int64_t)blockIdx.x < ntile) gather(blockIdx.x, xsb[0]);
-  __syncthreads();
+  if ((int64_t)blockIdx.x < ntile) gather(blockIdx.x, 0);
   int it = 0;
   for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -326,56 +446,118 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     if constexpr (TMA) {
       if (tid == 0 && tn < ntile) issue(tn, s ^ 1);
     }
-    if (tn < ntile) gather(tn, xsb[s ^ 1]);
+    if (tn < ntile) gather(tn, s ^ 1);
     else cp_async_commit();                                            // keep one group per iteration
     cp_async_wait<1>();                                                // this tile's gather has landed
     const T* g;
     const uint16_t* li;
-    const T* tnp;
     if constexpr (TMA) {
       const bool ok = mbar_wait_bounded(&bar[s], (uint32_t)((it >> 1) & 1), err);
       if (__syncthreads_or(!ok)) {
+        // let the copies into the other stage finish (bounded) before leaving
+        if (tid == 0 && tn < ntile) mbar_wait_bounded(&bar[s ^ 1], (uint32_t)(((it + 1) >> 1) & 1), nullptr);
         cp_async_wait<0>();
         return;
       }
-      g = stage_geo(s);
-      li = stage_lidx(s);
-      tnp = J2 ? stage_tan(s) : nullptr;
+      g = reinterpret_cast<const T*>(stage(s));
+      li = reinterpret_cast<const uint16_t*>(stage(s) + L::GEO_B);
     } else {
       __syncthreads();
-      g = geo + t * (GS * MF_TILE);
+      g = geo + t * (GS * TT);
       li = lidx + t * NSLOT;
-      tnp = J2 ? tan + t * (NG * 8 * MF_TILE) : nullptr;
     }
-    const T* xs = xsb[s];
-    const int64_t e = t * MF_TILE + lt;
-    if (e < ne) {
-      int l[NN];
-      T va[NN][3];
+    const T* xs = xsb + s * 3 * mu;
+    const int64_t rem = ne - t * TT;
+    const int cnt = rem < TT ? (int)rem : TT;                         // elements in this tile
+    // LANES = 2: the element pair at positions 2 tid, 2 tid + 1 (slot columns
+    // tid, H + tid); LANES = 1: the element of slot column tid
+    const int pos = LANES == 2 ? tid : 2 * (tid % H) + tid / H;        // stream offset in P units
+    int l0[NN], l1[NN];
+    P f[NN][3];
+    {
+      P va[NN][3];
 #pragma unroll
       for (int a = 0; a < NN; ++a) {
-        l[a] = li[a * MF_TILE + lt];
+        l0[a] = li[a * TT + tid];
+        if constexpr (LANES == 2) {
+          l1[a] = li[a * TT + H + tid];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) va[a][c] = xs[c * maxu + l[a]];
+          for (int c = 0; c < 3; ++c) va[a][c] = P(xs[c * mu + l0[a]], xs[c * mu + l1[a]]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) va[a][c] = xs[c * mu + l0[a]];
+        }
       }
-      T f[NN][3];
-      element_product<T, ET, J2>(g + lt, J2 ? tnp + lt : nullptr, va, lam, mu, Kb, f);
-#pragma unroll
-      for (int a = 0; a < NN; ++a)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) atomicAdd(&ys[c * maxu + l[a]], f[a][c]);
+      const P* gp = reinterpret_cast<const P*>(g) + pos;
+      const P* tp = J2 ? reinterpret_cast<const P*>(tan + t * (NG * 8 * TT)) + pos : nullptr;
+      element_product<P, ET, J2, NT>(gp, tp, va, P(mu_m), P(K_m), f);
     }
-    __syncthreads();
-    // the tile's per-node sums, stored (not added) at their node-major positions
-    const int64_t u0 = tptr[t];
-    const int nu = tptr[t + 1] - (int32_t)u0;
-    for (int k = tid; k < nu; k += MF_TILE) {
-      T* p = part + 3 * (int64_t)tdest[u0 + k];
+    // lanes past the end of the mesh (zero geometry) contribute nothing
+    bool ok0, ok1;
+    if constexpr (LANES == 2) {
+      ok0 = 2 * tid < cnt;
+      ok1 = 2 * tid + 1 < cnt;
+    } else {
+      ok0 = pos < cnt;
+      ok1 = false;
+    }
+    // tile-wide max |f| (NaN and infinity propagate)
+    T m = T(0);
+#pragma unroll
+    for (int a = 0; a < NN; ++a)
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        p[c] = ys[c * maxu + k];
-        ys[c * maxu + k] = T(0);
+        if constexpr (LANES == 2) {
+          m = max_nan(m, ok0 ? fabs(f[a][c].lo()) : T(0));
+          m = max_nan(m, ok1 ? fabs(f[a][c].hi()) : T(0));
+        } else {
+          m = max_nan(m, ok0 ? fabs(f[a][c]) : T(0));
+        }
       }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = max_nan(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0) wmax[tid >> 5] = m;
+    __syncthreads();
+    T M = wmax[0];
+#pragma unroll
+    for (int w = 1; w < NW; ++w) M = max_nan(M, wmax[w]);
+    const bool bad = !(M <= std::numeric_limits<T>::max());            // NaN or infinity in the tile
+    int e = 0;
+    if (!bad && M > T(0)) {
+      frexp(M * T(vmax), &e);                                          // vmax * M < 2^e
+      e = max(e, B + std::numeric_limits<T>::min_exponent);          // keep q finite
+    }
+    const T q = bad ? T(1) : scalbn(T(1), B - e), iq = scalbn(T(1), e - B);
+#pragma unroll
+    for (int a = 0; a < NN; ++a) {
+      I* d0 = acc + 4 * l0[a];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        if constexpr (LANES == 2) {
+          const P fq = P(f[a][c] * P(q));
+          if (ok0) atomicAdd(d0 + c, to_fixed(fq.lo()));
+          if (ok1) atomicAdd(acc + 4 * l1[a] + c, to_fixed(fq.hi()));
+        } else {
+          if (ok0) atomicAdd(d0 + c, to_fixed(f[a][c] * q));
+        }
+      }
+    }
+    __syncthreads();
+    // node sums back to T, stored (not added) at their node-major positions;
+    // the accumulators are cleared for the next tile
+    const int nu = tptr[t + 1] - tptr[t];
+    const int32_t* td = tdb + s * mu;
+    for (int k = tid; k < nu; k += NT) {
+      I* w = acc + 4 * k;
+      const I w0 = w[0], w1 = w[1], w2 = w[2];
+      w[0] = I(0);
+      w[1] = I(0);
+      w[2] = I(0);
+      T* p = part + 3 * (int64_t)td[k];
+      const T nan = std::numeric_limits<T>::quiet_NaN();
+      p[0] = bad ? nan : from_fixed(w0, T(0)) * iq;
+      p[1] = bad ? nan : from_fixed(w1, T(0)) * iq;
+      p[2] = bad ? nan : from_fixed(w2, T(0)) * iq;
     }
     __syncthreads();
   }
@@ -416,22 +598,27 @@ __global__ void mf_gather_kernel(int64_t nn, const int32_t* __restrict__ node_pt
 }
 
 // ---------------------------------------------------------------- launch
-template <class T, int ET, bool J2>
+template <class T, int ET, bool J2, int TT>
 static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* part,
                  const int* skip, cudaStream_t s) {
   constexpr bool TMA = sizeof(T) == 4;
-  using L = TileLayout<T, ET, J2>;
-  auto kern = mf_tile_kernel<T, ET, J2, TMA>;
-  const size_t smem = (TMA ? 2 * (size_t)L::STAGE_B : 0) + 3 * 3 * (size_t)b->maxu * sizeof(T);
-  // per (kernel, shared-memory size): opt in above 48 KB and size the persistent grid
+  // lane pairs for the FP32 C3D10 product; one element per thread where pair
+  // arithmetic would spill (C3D8's modal form, FP64)
+  constexpr int LANES = (sizeof(T) == 4 && ET == EXFEM_C3D10) ? 2 : 1;
+  using L = TileLayout<T, ET, TT, LANES>;
+  auto kern = mf_tile_kernel<T, ET, J2, TT, LANES, TMA>;
+  const int mu = (b->maxu + 7) & ~7;
+  const size_t smem = L::smem_bytes(TMA, mu);
+  // per (kernel, shared-memory size, device): opt in above 48 KB and size the
+  // persistent grid
   static thread_local size_t opted = 0;
   static thread_local int per_sm = 0, nsm = 0, dev = -1;
   int cur;
   EX_CUDA(cudaGetDevice(&cur));
-  if (smem > opted || cur != dev) {
+  if (smem != opted || cur != dev) {
     EX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
     EX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cur));
-    EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MF_TILE, smem));
+    EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NT, smem));
     opted = smem;
     dev = cur;
   }
@@ -440,11 +627,23 @@ static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tp
     return EXFEM_ERR_UNSUPPORTED;
   }
   const int64_t grid = std::min<int64_t>(b->ntile, (int64_t)nsm * per_sm);
-  kern<<<(unsigned)grid, MF_TILE, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p, tpack,
-                                             b->tile_dest.p, v, part, (T)b->mat.lam, (T)b->mat.mu, (T)b->mat.K,
-                                             b->maxu, skip, b->dev_err.p);
+  kern<<<(unsigned)grid, L::NT, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p, tpack,
+                                           b->tile_dest.p, v, part, (T)b->mat.mu, (T)b->mat.K, mu, b->vmax, skip,
+                                           b->dev_err.p);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
+}
+
+template <class T, int ET, bool J2>
+static int mf_tile(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* part,
+                   const int* skip, cudaStream_t s) {
+  switch (b->tile) {
+    case 128: return mf_go<T, ET, J2, 128>(b, geo, tan, tpack, v, part, skip, s);
+    case 256: return mf_go<T, ET, J2, 256>(b, geo, tan, tpack, v, part, skip, s);
+    default:
+      set_error("unsupported matrix-free tile size %d", b->tile);
+      return EXFEM_ERR_UNSUPPORTED;
+  }
 }
 
 template <class T>
@@ -470,11 +669,11 @@ int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaSt
     const int32_t* nf = (bc && b->fixed.p) ? b->tile_nodes_bc.p : b->tile_nodes.p;
     int st;
     if (b->etype == EXFEM_C3D8)
-      st = j2 ? mf_go<T, EXFEM_C3D8, true>(b, geo, tan, nf, v, part, skip, s)
-              : mf_go<T, EXFEM_C3D8, false>(b, geo, tan, nf, v, part, skip, s);
+      st = j2 ? mf_tile<T, EXFEM_C3D8, true>(b, geo, tan, nf, v, part, skip, s)
+              : mf_tile<T, EXFEM_C3D8, false>(b, geo, tan, nf, v, part, skip, s);
     else
-      st = j2 ? mf_go<T, EXFEM_C3D10, true>(b, geo, tan, nf, v, part, skip, s)
-              : mf_go<T, EXFEM_C3D10, false>(b, geo, tan, nf, v, part, skip, s);
+      st = j2 ? mf_tile<T, EXFEM_C3D10, true>(b, geo, tan, nf, v, part, skip, s)
+              : mf_tile<T, EXFEM_C3D10, false>(b, geo, tan, nf, v, part, skip, s);
     if (st) return st;
   }
   mf_gather_kernel<T><<<grid_for(b->nn, 256), 256, 0, s>>>(b->nn, b->node_ptr.p, part, bc ? b->fixed.p : nullptr,

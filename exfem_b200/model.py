@@ -86,13 +86,21 @@ class Block:
         """(ptr, nodes, nend, perm) element-tile maps of the matrix-free operator."""
         nt, nl, mu = C.c_int64(), C.c_int64(), C.c_int()
         check(lib.exfem_block_tile_info(self._h, C.byref(nt), C.byref(nl), C.byref(mu)))
+        tile, _ = self.tile_order()
         ptr_ = np.empty(nt.value + 1, np.int32)
         nodes = np.empty(max(nl.value, 1), np.int32)
         nend = np.empty(max(nl.value, 1), np.uint16)
-        perm = np.empty((nt.value, self.etype.nnode * 128), np.uint16)
+        perm = np.empty((nt.value, self.etype.nnode * tile), np.uint16)
         check(lib.exfem_block_tile_maps(self._h, ptr_.ctypes.data, nodes.ctypes.data, nend.ctypes.data,
                                         perm.ctypes.data))
         return ptr_, nodes[:nl.value], nend[:nl.value], perm
+
+    def tile_order(self):
+        """(tile, order): elements per tile and the tile order (position -> element)."""
+        tile = C.c_int()
+        order = np.empty(max(self.ne, 1), np.int32)
+        check(lib.exfem_block_tile_order(self._h, C.byref(tile), order.ctypes.data))
+        return tile.value, order[:self.ne]
 
     def init_state(self):                                              # model.py:154-155
         return torch.zeros((self.ne, self.etype.ngp, self.material.nstate), dtype=torch.float64, device="cuda")

@@ -95,16 +95,26 @@ int exfem_block_query(exfem_block b, int64_t* ne, int64_t* nn, int* nnode, int* 
  * (gfem/model.py:241-261); element colours (ne,) */
 int exfem_block_gather_plan(exfem_block b, int32_t* plan_host);
 int exfem_block_colours(exfem_block b, int32_t* colour_host);
-/* element-tile maps of the matrix-free operator (tiles of 128 consecutive
- * elements; slot s = a*128 + l is local node a of the tile's element l): tile
- * count, total length of the node lists and the longest list; then, copied to
- * host, ptr (ntile+1), the sorted distinct nodes of every tile, for each listed
- * node the end of its run of slots (uint16), and per tile the slots grouped by
- * node in node order, increasing within a node (ntile, nnode*128, zero padded).
- * No counterpart in the reference. */
+/* element-tile maps of the matrix-free operator.  The block's elements are put
+ * in a tile order (grouped by mesh component, in the order of each component's
+ * first element, then along a Morton curve of the corner-coordinate sums, ties by
+ * element index); a tile is `tile` consecutive positions of that order, and slot
+ * s = a*tile + (p % 2)*(tile/2) + p/2 is local node a of the element at tile
+ * position p.  tile_info: tile count, total length of the node lists and the
+ * longest list; tile_maps, copied to host: ptr (ntile+1), the sorted distinct
+ * nodes of every tile, for each listed node the end of its run of slots
+ * (uint16), and per tile the slots grouped by node in node order, increasing
+ * within a node (ntile, nnode*tile, zero padded); tile_order: the tile size and
+ * the order (ne,) as position -> element.  No counterpart in the reference. */
 int exfem_block_tile_info(exfem_block b, int64_t* ntile, int64_t* nlist, int* maxu);
 int exfem_block_tile_maps(exfem_block b, int32_t* ptr_host, int32_t* nodes_host, uint16_t* nend_host,
                           uint16_t* perm_host);
+int exfem_block_tile_order(exfem_block b, int* tile, int32_t* order_host);
+/* elements per matrix-free tile (128 or 256) for blocks of element type etype
+ * created after the call, process-wide; chosen by the autotuner
+ * (exfem_b200.tuning).  No counterpart in the reference. */
+int exfem_set_tile(int etype, int tile);
+int exfem_get_tile(int etype, int* tile);
 /* per-element stiffness scale (gfem/model.py:449-463, fields["scale"]); NULL = 1 */
 int exfem_block_set_scale(exfem_block b, const double* scale_host);
 /* per-element Lame parameters (ne each) of a linear-elastic block, used by every
@@ -264,6 +274,11 @@ int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn,
                          int* ncolour);
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx,
                                     int32_t* agg, int64_t* nagg);
+/* tile order of the matrix-free operator (see exfem_block_tile_order) for a mesh
+ * of ne elements with nnode nodes each, the first ncorner of them corners:
+ * order (ne,) position -> element.  No counterpart in the reference. */
+int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X,
+                          const int32_t* conn, int32_t* order);
 
 #ifdef __cplusplus
 }

@@ -407,12 +407,51 @@ def greedy_colouring(conn, nn):
     return col
 
 
+def tile_order(X, conn, ncorner):
+    """Tile order of the matrix-free product (no counterpart in the reference),
+    position -> element.  Elements are grouped by connected component (elements
+    sharing nodes), components in the order of their first element; inside a
+    component they follow a Morton curve of the corner-coordinate sums s_e (corner
+    nodes summed in local order), quantised per axis as
+    min(floor((s - lo) / (hi - lo) * 2^21), 2^21 - 1) over the extent [lo, hi] of
+    all sums, bits interleaved x lowest; ties by element index."""
+    X = np.asarray(X, dtype=np.float64)
+    conn = np.asarray(conn, dtype=np.int64)
+    ne, nnode = conn.shape
+    if ne == 0:
+        return np.zeros(0, np.int32)
+    import scipy.sparse as sps
+    from scipy.sparse.csgraph import connected_components
+    nn = len(X)
+    rows = np.repeat(np.arange(ne), nnode)
+    G = sps.csr_matrix((np.ones(ne * nnode), (rows, ne + conn.reshape(-1))), shape=(ne + nn, ne + nn))
+    _, lab = connected_components(G, directed=False)
+    first = np.full(lab.max() + 1, ne, np.int64)
+    np.minimum.at(first, lab[:ne], np.arange(ne))
+    comp = first[lab[:ne]]
+    s = X[conn[:, 0]].copy()
+    for a in range(1, ncorner):
+        s = s + X[conn[:, a]]
+    lo, hi = s.min(0), s.max(0)
+    key = np.zeros(ne, np.uint64)
+    for d in range(3):
+        if hi[d] > lo[d]:
+            f = np.floor((s[:, d] - lo[d]) / (hi[d] - lo[d]) * 2097152.0)
+            q = np.minimum(np.maximum(f, 0.0), 2097151.0).astype(np.uint64)
+        else:
+            q = np.zeros(ne, np.uint64)
+        for b in range(21):
+            key |= ((q >> np.uint64(b)) & np.uint64(1)) << np.uint64(3 * b + d)
+    return np.lexsort((np.arange(ne), key, comp)).astype(np.int32)
+
+
 def tile_maps(conn, tile):
     """Element-tile maps used by the matrix-free product (no counterpart in the
-    reference).  Elements [t*tile, (t+1)*tile) form tile t and slot s = a*tile + l
-    is local node a of its element l.  Per tile: the sorted distinct nodes; for each
-    node (in that order) its slots in increasing order, concatenated into perm
-    (padded with zeros to nnode*tile per tile); nend = end of each node's run.
+    reference), for conn given in tile order.  Positions [t*tile, (t+1)*tile) form
+    tile t; slot s = a*tile + (p % 2)*(tile/2) + p//2 is local node a of the
+    element at tile position p.  Per tile: the sorted distinct nodes; for each node
+    (in that order) its slots in increasing order, concatenated into perm (padded
+    with zeros to nnode*tile per tile); nend = end of each node's run.
     Returns (ptr (ntile+1,), nodes, nend, perm (ntile, nnode*tile))."""
     conn = np.asarray(conn, dtype=np.int64)
     ne, nnode = conn.shape
@@ -422,9 +461,11 @@ def tile_maps(conn, tile):
     for t in range(ntile):
         blk = conn[t * tile:(t + 1) * tile]
         u = np.unique(blk)
-        slot_node = np.searchsorted(u, blk.T.reshape(-1))        # slot order a*tile + l (valid l only)
-        la = np.arange(blk.shape[0])
-        slots = (np.arange(nnode)[:, None] * tile + la[None, :]).reshape(-1)
+        pos = np.arange(blk.shape[0])
+        slots = (np.arange(nnode)[:, None] * tile + (pos % 2)[None, :] * (tile // 2) + (pos // 2)[None, :]).reshape(-1)
+        slot_node = np.searchsorted(u, blk.T.reshape(-1))
+        inc = np.argsort(slots, kind="stable")                  # increasing slot order
+        slots, slot_node = slots[inc], slot_node[inc]
         order = np.argsort(slot_node, kind="stable")
         perm[t, :len(order)] = slots[order]
         nend.append(np.cumsum(np.bincount(slot_node, minlength=len(u))))

@@ -71,6 +71,41 @@ def test_host_gather_plan_and_colouring_bit_exact(kind):
     assert nc.value == col.max() + 1
 
 
+def _host_order(X, c, ncorner):
+    order = np.empty(len(c), np.int32)
+    c32 = np.ascontiguousarray(c, dtype=np.int32)
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    assert _lib.lib.exfem_host_tile_order(len(X), len(c), c.shape[1], ncorner, X.ctypes.data, c32.ctypes.data,
+                                          order.ctypes.data) == 0
+    return order
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet", "union"])
+def test_host_tile_order_bit_exact(kind):
+    """The native Morton tile order equals the oracle's restatement; components
+    (here several meshes in one block) stay contiguous."""
+    if kind == "hex":
+        X, c = mesh.box_hex(1, 1, 1, 9, 5, 4)
+        X = mesh.jitter_interior(X, 1.0 / 9, 0.1, 2)
+        nc = 8
+    elif kind == "tet":
+        X, c = tet10_box(1, 1, 1, 4, 3, 3)
+        nc = 4
+    else:
+        X1, c1 = mesh.box_hex(1, 1, 1, 6, 2, 2)
+        X2, c2 = mesh.box_hex(2, 1, 1, 3, 3, 1)
+        X = np.concatenate([X1, X2, X1])
+        c = np.concatenate([c1, c2 + len(X1), c1 + len(X1) + len(X2)])
+        nc = 8
+    order = _host_order(X, c, nc)
+    np.testing.assert_array_equal(order, fem.tile_order(X, c, nc))
+    np.testing.assert_array_equal(np.sort(order), np.arange(len(c)))
+    if kind == "union":
+        n1, n2 = len(c1), len(c2)
+        np.testing.assert_array_equal(np.sort(order[:n1]), np.arange(n1))
+        np.testing.assert_array_equal(np.sort(order[n1:n1 + n2]), np.arange(n1, n1 + n2))
+
+
 def test_host_gather_plan_rejects_bad_connectivity():
     c = np.array([[0, 1, 2, 3, 4, 5, 6, 99]], np.int32)
     vmax = C.c_int()

@@ -139,7 +139,9 @@ def test_index_maps_bit_exact(cuda, kind):
     X, c, pmod, omod = _pair(kind, "el", n=(5, 4, 3))
     np.testing.assert_array_equal(pmod.gather(), ofem.gather_plan([c], len(X)))
     np.testing.assert_array_equal(pmod.blocks[0].colours(), ofem.greedy_colouring(c, len(X)))
-    for got, want in zip(pmod.blocks[0].tile_maps(), ofem.tile_maps(c, 128)):
+    tile, order = pmod.blocks[0].tile_order()
+    np.testing.assert_array_equal(order, ofem.tile_order(X, c, 8 if kind == "hex" else 4))
+    for got, want in zip(pmod.blocks[0].tile_maps(), ofem.tile_maps(np.asarray(c)[order], tile)):
         np.testing.assert_array_equal(got, want)
 
 
