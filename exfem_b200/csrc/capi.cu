@@ -132,7 +132,7 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
   EX_ARG(nn >= 0 && ne >= 0, "negative sizes");
   EX_ARG(nn == 0 || X_host, "X is NULL");
   EX_ARG(ne == 0 || conn_host, "conn is NULL");
-  EX_ARG(3 * nn < (int64_t)INT32_MAX && nn < (int64_t(1) << 29), "too many nodes for int32 DOF indices");
+  EX_ARG(3 * nn < (int64_t)INT32_MAX && nn < (int64_t(1) << 28), "too many nodes for int32 DOF indices");
   auto b = std::make_unique<exfem_block_s>();
   cudaGetDevice(&b->device);
   b->etype = etype;
@@ -209,26 +209,35 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
       }
       if ((s = b->lidx.upload(li.data(), std::max<size_t>(li.size(), 1)))) return s;
     }
-    {  // run ends per tile, each tile's run padded to a multiple of 8 entries (16 bytes)
-      std::vector<int32_t> off(std::max<int64_t>(b->ntile, 1), 0);
-      std::vector<uint16_t> pad;
-      for (int64_t t = 0; t < b->ntile; ++t) {
-        off[t] = (int32_t)pad.size();
-        pad.insert(pad.end(), te.begin() + tp[t], te.begin() + tp[t + 1]);
-        pad.resize((pad.size() + 7) & ~size_t(7), 0);
+    {
+      // destinations of the tile sums: a node listed by one tile only is written
+      // to y directly by that tile (0x80000000 | node); the others' tile sums go
+      // to a compact node-major partials array (node runs in node order, tile
+      // order inside a run) that the node pass adds up; that pass covers every
+      // node not listed exactly once (multi-tile and unreferenced nodes)
+      std::vector<int32_t> occ(nn, 0);
+      for (int32_t n : tn) ++occ[n];
+      std::vector<int32_t> mlist, mptr(1, 0), start(nn, -1);
+      for (int64_t n = 0; n < nn; ++n)
+        if (occ[n] != 1) {
+          start[n] = mptr.back();
+          mlist.push_back((int32_t)n);
+          mptr.push_back(mptr.back() + occ[n]);
+        }
+      std::vector<int32_t> dest(tn.size());
+      for (size_t q = 0; q < tn.size(); ++q) {                 // entries in tile order
+        const int32_t n = tn[q];
+        dest[q] = occ[n] == 1 ? (int32_t)(0x80000000u | (uint32_t)n) : start[n]++;
       }
-      if ((s = b->nend_off.upload(off.data(), off.size()))) return s;
-      if ((s = b->tile_nend_pad.upload(pad.data(), std::max<size_t>(pad.size(), 8)))) return s;
-    }
-    {  // node -> entry map of the tile node lists (counting sort, entries increasing)
-      std::vector<int32_t> np(nn + 1, 0), dest(tn.size());
-      for (int32_t n : tn) ++np[n + 1];
-      for (int64_t n = 0; n < nn; ++n) np[n + 1] += np[n];
-      std::vector<int32_t> cur(np.begin(), np.end() - 1);
-      for (size_t q = 0; q < tn.size(); ++q) dest[q] = cur[tn[q]]++;   // tile order within a node
-      if ((s = b->node_ptr.upload(np.data(), np.size()))) return s;
-      if ((s = b->tile_dest.upload(dest.data(), std::max<size_t>(dest.size(), 1)))) return s;
-      if ((s = b->partial.alloc(std::max<size_t>(3 * tn.size(), 1)))) return s;
+      b->tile_dest_host = dest;
+      b->nmulti = (int64_t)mlist.size();
+      if (mlist.empty()) mlist.push_back(0);                   // keep the buffers non-empty
+      if (dest.empty()) dest.push_back(0);
+      if ((s = b->multi_nodes.upload(mlist.data(), mlist.size()))) return s;
+      if ((s = b->multi_ptr.upload(mptr.data(), mptr.size()))) return s;
+      if ((s = b->tile_dest.upload(dest.data(), dest.size()))) return s;
+      if ((s = b->tile_dest_bc.upload(dest.data(), dest.size()))) return s;
+      if ((s = b->partial.alloc(std::max<size_t>(3 * (size_t)mptr.back(), 1)))) return s;
     }
     if ((s = b->dev_err.alloc(1))) return s;
     EX_CUDA(cudaMemset(b->dev_err.p, 0, sizeof(int)));
@@ -368,6 +377,9 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
   if (!fixed_host) {
     b->fixed.release();
     b->node_fixed.release();
+    if (!b->tile_dest_host.empty())
+      EX_CUDA(cudaMemcpy(b->tile_dest_bc.p, b->tile_dest_host.data(), b->tile_dest_host.size() * sizeof(int32_t),
+                         cudaMemcpyHostToDevice));
     if (!b->tile_nodes_host.empty())
       EX_CUDA(cudaMemcpy(b->tile_nodes_bc.p, b->tile_nodes_host.data(), b->tile_nodes_host.size() * sizeof(int32_t),
                          cudaMemcpyHostToDevice));
@@ -379,6 +391,12 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
       f[3 * n + c] = f[3 * n + c] ? 1 : 0;
       nf[n] |= (uint8_t)(f[3 * n + c] << c);
     }
+  if (!b->tile_dest_host.empty()) {   // fixed-DOF bits of nodes written directly, at bits 28-30
+    std::vector<int32_t> packed(b->tile_dest_host);
+    for (auto& q : packed)
+      if (q < 0) q = (int32_t)((uint32_t)q | ((uint32_t)nf[q & 0x0FFFFFFF] << 28));
+    EX_CUDA(cudaMemcpy(b->tile_dest_bc.p, packed.data(), packed.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   if (!b->tile_nodes_host.empty()) {  // fixed-DOF bits packed above the node id
     std::vector<int32_t> packed(b->tile_nodes_host);
     for (auto& q : packed) q = (int32_t)((uint32_t)q | ((uint32_t)nf[q] << 29));

@@ -74,7 +74,8 @@ struct DevBuf {
   int upload(const T* host, size_t count) {
     int s = alloc(count);
     if (s) return s;
-    if (count) EX_CUDA(cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    if (count && host) EX_CUDA(cudaMemcpy(p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    else if (count) EX_CUDA(cudaMemset(p, 0, count * sizeof(T)));   // nothing to copy: zero filled
     return EXFEM_OK;
   }
   size_t bytes() const { return n * sizeof(T); }

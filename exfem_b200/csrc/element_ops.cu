@@ -333,19 +333,23 @@ int launch_colour_assemble(exfem_block_s* b, const double* fe, double* f, cudaSt
 }
 
 // ---------------------------------------------------------------- geometry streams
+// Per element: C3D8 the 7 modal coordinate vectors (21) and the stiffness scale;
+// C3D10 the inverse Jacobian (9) and vol * scale; then, only for blocks with
+// per-element Lame parameters, lambda and mu (the matrix-free kernels otherwise
+// take the material's from their arguments).
 template <int ET>
 __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn,
                                 const double* __restrict__ scale, const double* __restrict__ lam_e,
-                                const double* __restrict__ mu_e, double lam0, double mu0, double* __restrict__ g64,
+                                const double* __restrict__ mu_e, int GS, double* __restrict__ g64,
                                 float* __restrict__ g32, const int32_t* __restrict__ tpos, int tile) {
   using Tr = ElemTraits<ET>;
-  constexpr int NN = Tr::nnode, GS = Tr::geo_stride;
+  constexpr int NN = Tr::nnode, GF = Tr::geo_stride;
   const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (e >= ne) return;
   const double sc = scale ? scale[e] : 1.0;
-  double out[GS];
+  double out[GF];
 #pragma unroll
-  for (int k = 0; k < GS; ++k) out[k] = 0.0;
+  for (int k = 0; k < GF; ++k) out[k] = 0.0;
   if constexpr (ET == EXFEM_C3D8) {
     double xa[8][3], cm[7][3];
 #pragma unroll
@@ -358,8 +362,6 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
 #pragma unroll
       for (int c = 0; c < 3; ++c) out[3 * k + c] = cm[k][c];
     out[21] = sc;
-    out[22] = lam_e ? lam_e[e] : lam0;
-    out[23] = mu_e ? mu_e[e] : mu0;
   } else {
     double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
 #pragma unroll
@@ -374,10 +376,11 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
 #pragma unroll
     for (int k = 0; k < 9; ++k) out[k] = iJ[k];
     out[9] = det / 24.0 * sc;
-    out[10] = lam_e ? lam_e[e] : lam0;
-    out[11] = mu_e ? mu_e[e] : mu0;
   }
-#pragma unroll
+  if (lam_e) {
+    out[GF - 2] = lam_e[e];
+    out[GF - 1] = mu_e[e];
+  }
   for (int k = 0; k < GS; ++k) {
     g64[tile_index(tpos[e], k, GS, tile)] = out[k];
     g32[tile_index(tpos[e], k, GS, tile)] = (float)out[k];
@@ -385,26 +388,26 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
 }
 
 int build_geometry(exfem_block_s* b) {
-  const int GS = b->etype == EXFEM_C3D8 ? ElemTraits<EXFEM_C3D8>::geo_stride : ElemTraits<EXFEM_C3D10>::geo_stride;
+  const int GF = b->etype == EXFEM_C3D8 ? ElemTraits<EXFEM_C3D8>::geo_stride : ElemTraits<EXFEM_C3D10>::geo_stride;
+  const int GS = b->lam_e.p ? GF : GF - 2;
   int st;
   const int64_t padded = b->ntile * b->tile * GS;
-  if (b->geo64.n != (size_t)padded) {
+  if (b->geo64.n != (size_t)padded || b->geo_stride != GS) {
     if ((st = b->geo64.alloc(padded))) return st;
     if ((st = b->geo32.alloc(padded))) return st;
     EX_CUDA(cudaMemset(b->geo64.p, 0, b->geo64.bytes()));
     EX_CUDA(cudaMemset(b->geo32.p, 0, b->geo32.bytes()));
   }
+  b->geo_stride = GS;
   if (b->ne == 0) return EXFEM_OK;
   const int threads = 128;
   const unsigned grid = (unsigned)((b->ne + threads - 1) / threads);
   if (b->etype == EXFEM_C3D8)
     geometry_kernel<EXFEM_C3D8><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
-                                                   b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p,
-                                                   b->tpos.p, b->tile);
+                                                   GS, b->geo64.p, b->geo32.p, b->tpos.p, b->tile);
   else
     geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
-                                                    b->mat.lam, b->mat.mu, b->geo64.p, b->geo32.p,
-                                                   b->tpos.p, b->tile);
+                                                    GS, b->geo64.p, b->geo32.p, b->tpos.p, b->tile);
   EX_LAUNCH_CHECK();
   EX_CUDA(cudaDeviceSynchronize());
   return EXFEM_OK;

@@ -158,19 +158,17 @@ int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double
 }
 
 // Element-tile maps of the matrix-free operator.  Tiles are `tile` consecutive
-// positions of the tile order (conn is given in that order).  Each thread of the
-// product evaluates the pair of elements at positions 2j and 2j+1 of its tile, so
-// slots are numbered s = a*tile + (p % 2)*(tile/2) + p/2 for local node a of the
-// element at tile position p: thread j's slots are a*tile + j and
-// a*tile + tile/2 + j.  Per tile: the sorted distinct nodes it touches; for each
-// of them, in node order, its slots in increasing slot order, concatenated into
-// `perm` (tile-major, padded to nnode*tile entries per tile); and `nend`, the end
-// of each node's run in perm (aligned with the node list).
+// positions of the tile order (conn is given in that order), and slot
+// s = a*tile + p is local node a of the element at tile position p.  Per tile:
+// the sorted distinct nodes it touches; for each of them, in node order, its
+// slots in increasing slot order, concatenated into `perm` (tile-major, padded
+// to nnode*tile entries per tile); and `nend`, the end of each node's run in
+// perm (aligned with the node list).
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
                    int& maxu) {
   const int64_t ntile = (ne + tile - 1) / tile;
-  const int nslot = nnode * tile, half = tile / 2;
+  const int nslot = nnode * tile;
   ptr.assign(ntile + 1, 0);
   nodes.clear();
   nend.clear();
@@ -182,7 +180,6 @@ int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int t
   for (int64_t t = 0; t < ntile; ++t) {
     list.clear();
     const int64_t e0 = t * tile, e1 = std::min<int64_t>(ne, e0 + tile);
-    const int cntl = (int)(e1 - e0);
     for (int64_t k = e0 * nnode; k < e1 * nnode; ++k) {
       const int32_t n = conn[k];
       if (stamp[n] != t) { stamp[n] = t; list.push_back(n); }
@@ -192,18 +189,13 @@ int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int t
     for (int i = 0; i < nu; ++i) pos[list[i]] = i;
     cnt.assign(nu, 0);
     for (int a = 0; a < nnode; ++a)
-      for (int p = 0; p < cntl; ++p) ++cnt[pos[conn[(e0 + p) * nnode + a]]];
+      for (int64_t e = e0; e < e1; ++e) ++cnt[pos[conn[e * nnode + a]]];
     start.assign(nu + 1, 0);
     for (int i = 0; i < nu; ++i) start[i + 1] = start[i] + cnt[i];
     uint16_t* pm = perm.data() + (size_t)t * nslot;
     for (int i = 0; i < nu; ++i) cnt[i] = start[i];
     for (int a = 0; a < nnode; ++a)                      // increasing slot order
-      for (int h = 0; h < 2; ++h)
-        for (int j = 0; j < half; ++j) {
-          const int p = 2 * j + h;
-          if (p >= cntl) continue;
-          pm[cnt[pos[conn[(e0 + p) * nnode + a]]]++] = (uint16_t)(a * tile + h * half + j);
-        }
+      for (int64_t e = e0; e < e1; ++e) pm[cnt[pos[conn[e * nnode + a]]]++] = (uint16_t)(a * tile + (e - e0));
     nodes.insert(nodes.end(), list.begin(), list.end());
     for (int i = 0; i < nu; ++i) nend.push_back((uint16_t)start[i + 1]);
     ptr[t + 1] = (int32_t)nodes.size();

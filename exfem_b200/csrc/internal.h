@@ -43,14 +43,17 @@ struct exfem_block_s {
   std::vector<int32_t> tile_nodes_host;
   exfem::DevBuf<uint16_t> lidx;       // tile-major (ntile, nnode*tile): list position of each slot's node
   exfem::DevBuf<uint16_t> tile_nend;  // per listed node: end of its slot run in tile_perm
-  exfem::DevBuf<uint16_t> tile_nend_pad;  // the same per tile, each tile's run padded to 8 entries
-  exfem::DevBuf<int32_t> nend_off;    // (ntile) start of each tile's run in tile_nend_pad
   exfem::DevBuf<uint16_t> tile_perm;  // tile-major (ntile, nnode*tile) slots grouped by node
-  exfem::DevBuf<int32_t> node_ptr;    // (nn+1) node -> its run of tile entries in node-major order
-  exfem::DevBuf<int32_t> tile_dest;   // per tile-list entry: its node-major position
+  exfem::DevBuf<int32_t> tile_dest;   // per tile-list entry: 0x80000000|node (only tile of the node) or its partials position
+  exfem::DevBuf<int32_t> tile_dest_bc;  // same, fixed-DOF bits of directly written nodes at bits 28-30
+  std::vector<int32_t> tile_dest_host;
+  int64_t nmulti = 0;                 // nodes not listed by exactly one tile
+  exfem::DevBuf<int32_t> multi_nodes; // (nmulti) those nodes, ascending
+  exfem::DevBuf<int32_t> multi_ptr;   // (nmulti+1) their runs of partials
   exfem::DevBuf<double> partial;      // per-entry tile sums, 3 per entry (FP64 or FP32 view)
   exfem::DevBuf<int> dev_err;         // set by bounded waits that give up
-  exfem::DevBuf<double> geo64;        // (ne, geo_stride)
+  int geo_stride = 0;                 // per-element geometry entries (without the Lame pair when uniform)
+  exfem::DevBuf<double> geo64;        // tile-major (ntile, geo_stride, tile)
   exfem::DevBuf<float> geo32;
   int plastic_tangent = 0;            // 1 once tangent data differs from elastic
   exfem::DevBuf<double> tan64;        // tile-major (ntile, ngp*8, tile)

@@ -104,11 +104,13 @@ __device__ __forceinline__ void mf_stress(const P* tn, P lam, P mu, P Kb, const 
   }
 }
 
-// products f = Ke v_e of an element pair from its streams (g, tn: component 0 of
-// the pair, stride S pairs); P is a lane pair (F2 or D2)
-template <class P, int ET, bool J2, int S>
+// products f = Ke v_e of an element (pair) from its streams (g, tn: component 0
+// of the element (pair), stride S); P is a lane pair (F2, D2) or a scalar.  With
+// ELAME the Lame parameters follow the geometry, otherwise lam and mu are the
+// material's (J2 uses mu and the bulk modulus Kb).
+template <class P, int ET, bool J2, bool ELAME, int S>
 __device__ __forceinline__ void element_product(const P* g, const P* tn, const P (&va)[ElemTraits<ET>::nnode][3],
-                                                P mu, P Kb, P (&f)[ElemTraits<ET>::nnode][3]) {
+                                                P lam, P mu, P Kb, P (&f)[ElemTraits<ET>::nnode][3]) {
   if constexpr (ET == EXFEM_C3D8) {
     P cm[7][3], um[7][3];
 #pragma unroll
@@ -116,7 +118,7 @@ __device__ __forceinline__ void element_product(const P* g, const P* tn, const P
 #pragma unroll
       for (int c = 0; c < 3; ++c) cm[k][c] = g[(3 * k + c) * S];
     const P sc = g[21 * S];
-    const P le = g[22 * S], me = J2 ? mu : g[23 * S];
+    const P le = ELAME ? g[22 * S] : lam, me = (J2 || !ELAME) ? mu : g[23 * S];
     hex_to_modal(va, um);
     P J0[9], iJ0[9], G0[9], H0[9];
 #pragma unroll
@@ -181,7 +183,8 @@ __device__ __forceinline__ void element_product(const P* g, const P* tn, const P
 #pragma unroll
     for (int k = 0; k < 9; ++k) iJ[k] = g[k * S];
     const P vol = g[9 * S];
-    const P lt = P(P(0.2) * vol * g[10 * S]), mt = P(P(0.2) * vol * g[11 * S]), m2 = P(P(2.0) * mt);
+    const P lt = P(P(0.2) * vol * (ELAME ? g[10 * S] : lam)), mt = P(P(0.2) * vol * (ELAME ? g[11 * S] : mu));
+    const P m2 = P(P(2.0) * mt);
     P sv[4][6];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -259,7 +262,7 @@ __device__ __forceinline__ void element_product(const P* g, const P* tn, const P
 #pragma unroll
     for (int k = 0; k < 9; ++k) iJ[k] = g[k * S];
     const P vol = g[9 * S];
-    const P le = g[10 * S], me = J2 ? mu : g[11 * S];
+    const P le = ELAME ? g[10 * S] : lam, me = (J2 || !ELAME) ? mu : g[11 * S];
     P base[4][3], vbar[10][3], bbar[4][3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -363,48 +366,57 @@ __device__ __forceinline__ unsigned long long to_fixed(double x) { return (unsig
 __device__ __forceinline__ float from_fixed(int32_t i, float) { return __int2float_rn(i); }
 __device__ __forceinline__ double from_fixed(unsigned long long i, double) { return __ll2double_rn((long long)i); }
 
-template <class T, int ET, int TT, int LANES>
+template <class T, int ET, int TT, int LANES, bool ELAME>
 struct TileLayout {
   using Tr = ElemTraits<ET>;
   using I = typename FixedOf<T>::type;
-  static constexpr int NN = Tr::nnode, NG = Tr::ngp, GS = Tr::geo_stride, NSLOT = NN * TT, NT = TT / LANES;
+  static constexpr int NN = Tr::nnode, NG = Tr::ngp, NSLOT = NN * TT, NT = TT / LANES;
+  static constexpr int GS = ELAME ? Tr::geo_stride : Tr::geo_stride - 2;
   static constexpr uint32_t GEO_B = GS * TT * sizeof(T);
   static constexpr uint32_t LIDX_B = NSLOT * sizeof(uint16_t);
   static constexpr uint32_t STAGE_B = GEO_B + LIDX_B;
   static_assert(GEO_B % 16 == 0 && LIDX_B % 16 == 0, "bulk copies need 16-byte multiples");
-  // shared memory: [2 stages (TMA only): geometry | lidx] [gathered v: 2 x 3 x mu]
-  // [node-major destinations: 2 x mu] [fixed-point sums: mu x 4] with mu = maxu
-  // rounded up to 8
+  // one shared-memory record per distinct node of the tile: v (3) and the
+  // fixed-point sums (3), padded to an odd number of elements (FP32: 7 words;
+  // FP64: 7 eight-byte words, which keeps every double 8-byte aligned) so that a
+  // warp's scattered record accesses spread over all banks; one address serves a
+  // node's loads and its atomic additions
+  static constexpr int RW = sizeof(T) == 4 ? 7 : 14;                  // record size in 4-byte words
+  static_assert((RW * 4) % sizeof(T) == 0 && (RW * 4) % sizeof(I) == 0, "records keep their members aligned");
+  static constexpr int ROFF = 3 * sizeof(T);                          // byte offset of the sums
+  // shared memory: [2 stages (TMA only): geometry | lidx] [records: mu]
+  // [destinations: 2 x mu], mu = maxu rounded up to 8
   static size_t smem_bytes(bool tma, int mu) {
-    return (tma ? 2 * (size_t)STAGE_B : 0) + 6 * (size_t)mu * sizeof(T) + 2 * (size_t)mu * sizeof(int32_t) +
-           4 * (size_t)mu * sizeof(I);
+    return (tma ? 2 * (size_t)STAGE_B : 0) + (size_t)mu * RW * 4 + 2 * (size_t)mu * sizeof(int32_t);
   }
+  // lane pairs: registers capped so that 3 CTAs of 128 (6 of 64) threads fit an SM
+  static constexpr int MINB = (LANES == 2) ? 384 / NT : 1;
 };
 
 // LANES = 2: thread j evaluates the elements at tile positions 2j and 2j+1 as one
-// lane pair (slot columns j and TT/2 + j); LANES = 1: thread j evaluates the
-// element of slot column j alone (position 2 (j mod TT/2) + j div (TT/2)), for
+// lane pair; LANES = 1: thread j evaluates the element at position j alone, for
 // element types and precisions whose pair arithmetic would not fit in registers.
-template <class T, int ET, bool J2, int TT, int LANES, bool TMA>
-__global__ void __launch_bounds__(TT / LANES)
+template <class T, int ET, bool J2, bool ELAME, int TT, int LANES, bool TMA>
+__global__ void __launch_bounds__(TT / LANES, TileLayout<T, ET, TT, LANES, ELAME>::MINB)
 mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint16_t* __restrict__ lidx,
                const T* __restrict__ tan, const int32_t* __restrict__ tptr, const int32_t* __restrict__ tpack,
-               const int32_t* __restrict__ tdest, const T* __restrict__ v, T* __restrict__ part, T mu_m, T K_m,
-               int mu, int vmax, const int* __restrict__ skip, int* __restrict__ err) {
-  using L = TileLayout<T, ET, TT, LANES>;
+               const int32_t* __restrict__ tdest, const T* __restrict__ v, T* __restrict__ y, T* __restrict__ part,
+               T lam_m, T mu_m, T K_m, int mu, int vmax, const int* __restrict__ skip, int* __restrict__ err) {
+  using L = TileLayout<T, ET, TT, LANES, ELAME>;
   using I = typename L::I;
   using P = std::conditional_t<LANES == 2, typename PairOf<T>::type, T>;
-  constexpr int NN = L::NN, NG = L::NG, GS = L::GS, NSLOT = L::NSLOT, NT = L::NT, H = TT / 2, NW = NT / 32;
-  constexpr int B = FixedOf<T>::B;
+  constexpr int NN = L::NN, NG = L::NG, GS = L::GS, NSLOT = L::NSLOT, NT = L::NT, NW = NT / 32;
+  constexpr int B = FixedOf<T>::B, GK = 8;
   if (skip && *skip) return;
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ T wmax[NW];
   const int tid = threadIdx.x;
   unsigned char* base = smem + (TMA ? 2 * L::STAGE_B : 0);
-  T* xsb = reinterpret_cast<T*>(base);                                     // [2][3][mu]
-  int32_t* tdb = reinterpret_cast<int32_t*>(base + 6 * (size_t)mu * sizeof(T));   // [2][mu]
-  I* acc = reinterpret_cast<I*>(base + 6 * (size_t)mu * sizeof(T) + 2 * (size_t)mu * sizeof(int32_t));  // [mu][4]
+  unsigned char* rec = base;                                                        // [mu] records
+  int32_t* tdb = reinterpret_cast<int32_t*>(base + (size_t)mu * L::RW * 4);         // [2][mu]
+  auto vval = [&](int k) { return reinterpret_cast<T*>(rec + k * (L::RW * 4)); };
+  auto sums = [&](int k) { return reinterpret_cast<I*>(rec + k * (L::RW * 4) + L::ROFF); };
   auto stage = [&](int s) { return smem + s * L::STAGE_B; };
   auto issue = [&](int64_t t, int s) {
     fence_proxy_async();
@@ -412,23 +424,43 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     bulk_g2s(stage(s), geo + t * (GS * TT), L::GEO_B, &bar[s]);
     bulk_g2s(stage(s) + L::GEO_B, lidx + t * NSLOT, L::LIDX_B, &bar[s]);
   };
-  // asynchronous gather of the tile's distinct nodes (fixed DOFs zero filled) and
-  // of their node-major destinations
-  auto gather = [&](int64_t t, int buf) {
-    const int64_t u0 = tptr[t];
-    const int nu = tptr[t + 1] - (int32_t)u0;
-    T* xs = xsb + buf * 3 * mu;
-    for (int k = tid; k < nu; k += NT) {
-      const uint32_t pk = (uint32_t)tpack[u0 + k];
+  // node lists run ahead: the packed ids of tile t+2 are loaded into registers
+  // while tile t is processed, and the asynchronous copies of tile t+1's node
+  // values and destinations (fixed DOFs zero filled) are issued, from the ids
+  // loaded one tile earlier, as soon as tile t's elements have read theirs
+  struct Ids {
+    int32_t u0, nu;
+    uint32_t pk[GK];
+  };
+  auto load_ids = [&](int64_t t, Ids& d) {
+    d.u0 = tptr[t];
+    d.nu = tptr[t + 1] - d.u0;
+#pragma unroll
+    for (int i = 0; i < GK; ++i) {
+      const int k = tid + i * NT;
+      d.pk[i] = k < d.nu ? (uint32_t)tpack[d.u0 + k] : 0u;
+    }
+  };
+  auto copies = [&](const Ids& d, int buf) {
+    auto one = [&](int k, uint32_t pk) {
       const T* vp = v + 3 * (int64_t)(pk & 0x1FFFFFFFu);
       const uint32_t bits = pk >> 29;
+      T* xk = vval(k);
 #pragma unroll
-      for (int c = 0; c < 3; ++c) cp_async<sizeof(T)>(xs + c * mu + k, vp + c, ((bits >> c) & 1) ? 0 : (int)sizeof(T));
-      cp_async<4>(tdb + buf * mu + k, tdest + u0 + k, 4);
+      for (int c = 0; c < 3; ++c) cp_async<sizeof(T)>(xk + c, vp + c, ((bits >> c) & 1) ? 0 : (int)sizeof(T));
+      cp_async<4>(tdb + buf * mu + k, tdest + d.u0 + k, 4);
+    };
+#pragma unroll
+    for (int i = 0; i < GK; ++i) {
+      const int k = tid + i * NT;
+      if (k < d.nu) one(k, d.pk[i]);
     }
-    cp_async_commit();
+    for (int k = tid + GK * NT; k < d.nu; k += NT) one(k, (uint32_t)tpack[d.u0 + k]);
   };
-  for (int k = tid; k < 4 * mu; k += NT) acc[k] = I(0);
+  for (int k = tid; k < mu; k += NT) {
+    I* a = sums(k);
+    a[0] = a[1] = a[2] = I(0);
+  }
   if constexpr (TMA) {
     if (tid == 0) {
       mbar_init(&bar[0], 1);
@@ -438,7 +470,14 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     __syncthreads();
     if (tid == 0 && (int64_t)blockIdx.x < ntile) issue(blockIdx.x, 0);
   }
-  if ((int64_t)blockIdx.x < ntile) gather(blockIdx.x, 0);
+  Ids cur, nxt;
+  cur.nu = nxt.nu = 0;
+  if ((int64_t)blockIdx.x < ntile) {
+    load_ids(blockIdx.x, cur);
+    copies(cur, 0);
+  }
+  cp_async_commit();
+  if ((int64_t)blockIdx.x + gridDim.x < ntile) load_ids(blockIdx.x + gridDim.x, nxt);
   int it = 0;
   for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -446,9 +485,8 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     if constexpr (TMA) {
       if (tid == 0 && tn < ntile) issue(tn, s ^ 1);
     }
-    if (tn < ntile) gather(tn, s ^ 1);
-    else cp_async_commit();                                            // keep one group per iteration
-    cp_async_wait<1>();                                                // this tile's gather has landed
+    const int nu = cur.nu;
+    cp_async_wait<0>();                                                // this tile's copies have landed
     const T* g;
     const uint16_t* li;
     if constexpr (TMA) {
@@ -466,40 +504,46 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
       g = geo + t * (GS * TT);
       li = lidx + t * NSLOT;
     }
-    const T* xs = xsb + s * 3 * mu;
     const int64_t rem = ne - t * TT;
     const int cnt = rem < TT ? (int)rem : TT;                         // elements in this tile
-    // LANES = 2: the element pair at positions 2 tid, 2 tid + 1 (slot columns
-    // tid, H + tid); LANES = 1: the element of slot column tid
-    const int pos = LANES == 2 ? tid : 2 * (tid % H) + tid / H;        // stream offset in P units
-    int l0[NN], l1[NN];
+    // LANES = 2: the element pair at positions 2 tid, 2 tid + 1; LANES = 1: the
+    // element at position tid (slots a*TT + position)
+    uint32_t r0[NN], r1[NN];                                           // record byte offsets
     P f[NN][3];
     {
       P va[NN][3];
 #pragma unroll
       for (int a = 0; a < NN; ++a) {
-        l0[a] = li[a * TT + tid];
         if constexpr (LANES == 2) {
-          l1[a] = li[a * TT + H + tid];
+          const uint32_t lp = reinterpret_cast<const uint32_t*>(li + a * TT)[tid];   // both slots in one load
+          r0[a] = (lp & 0xFFFFu) * (L::RW * 4);
+          r1[a] = (lp >> 16) * (L::RW * 4);
+          const T* x0 = reinterpret_cast<const T*>(rec + r0[a]);
+          const T* x1 = reinterpret_cast<const T*>(rec + r1[a]);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) va[a][c] = P(xs[c * mu + l0[a]], xs[c * mu + l1[a]]);
+          for (int c = 0; c < 3; ++c) va[a][c] = P(x0[c], x1[c]);
         } else {
+          r0[a] = li[a * TT + tid] * (L::RW * 4);
+          const T* x0 = reinterpret_cast<const T*>(rec + r0[a]);
 #pragma unroll
-          for (int c = 0; c < 3; ++c) va[a][c] = xs[c * mu + l0[a]];
+          for (int c = 0; c < 3; ++c) va[a][c] = x0[c];
         }
       }
-      const P* gp = reinterpret_cast<const P*>(g) + pos;
-      const P* tp = J2 ? reinterpret_cast<const P*>(tan + t * (NG * 8 * TT)) + pos : nullptr;
-      element_product<P, ET, J2, NT>(gp, tp, va, P(mu_m), P(K_m), f);
+      const P* gp = reinterpret_cast<const P*>(g) + tid;
+      const P* tp = J2 ? reinterpret_cast<const P*>(tan + t * (NG * 8 * TT)) + tid : nullptr;
+      element_product<P, ET, J2, ELAME, NT>(gp, tp, va, P(lam_m), P(mu_m), P(K_m), f);
     }
-    // lanes past the end of the mesh (zero geometry) contribute nothing
-    bool ok0, ok1;
-    if constexpr (LANES == 2) {
-      ok0 = 2 * tid < cnt;
-      ok1 = 2 * tid + 1 < cnt;
-    } else {
-      ok0 = pos < cnt;
-      ok1 = false;
+    // positions past the end of the mesh (zero geometry, last tile only)
+    // contribute nothing
+    if (cnt < TT) {
+      const bool ok0 = LANES * tid < cnt, ok1 = LANES * tid + 1 < cnt;
+#pragma unroll
+      for (int a = 0; a < NN; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          if constexpr (LANES == 2) f[a][c] = P(ok0 ? f[a][c].lo() : T(0), ok1 ? f[a][c].hi() : T(0));
+          else f[a][c] = ok0 ? f[a][c] : T(0);
+        }
     }
     // tile-wide max |f| (NaN and infinity propagate)
     T m = T(0);
@@ -508,10 +552,10 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if constexpr (LANES == 2) {
-          m = max_nan(m, ok0 ? fabs(f[a][c].lo()) : T(0));
-          m = max_nan(m, ok1 ? fabs(f[a][c].hi()) : T(0));
+          m = max_nan(m, fabs(f[a][c].lo()));
+          m = max_nan(m, fabs(f[a][c].hi()));
         } else {
-          m = max_nan(m, ok0 ? fabs(f[a][c]) : T(0));
+          m = max_nan(m, fabs(f[a][c]));
         }
       }
 #pragma unroll
@@ -521,6 +565,11 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     T M = wmax[0];
 #pragma unroll
     for (int w = 1; w < NW; ++w) M = max_nan(M, wmax[w]);
+    // every element has read its node values: the next tile's may come in
+    if (tn < ntile) copies(nxt, s ^ 1);
+    cp_async_commit();
+    cur = nxt;
+    if (tn + gridDim.x < ntile) load_ids(tn + gridDim.x, nxt);
     const bool bad = !(M <= std::numeric_limits<T>::max());            // NaN or infinity in the tile
     int e = 0;
     if (!bad && M > T(0)) {
@@ -530,51 +579,54 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     const T q = bad ? T(1) : scalbn(T(1), B - e), iq = scalbn(T(1), e - B);
 #pragma unroll
     for (int a = 0; a < NN; ++a) {
-      I* d0 = acc + 4 * l0[a];
+      I* a0 = reinterpret_cast<I*>(rec + r0[a] + L::ROFF);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         if constexpr (LANES == 2) {
           const P fq = P(f[a][c] * P(q));
-          if (ok0) atomicAdd(d0 + c, to_fixed(fq.lo()));
-          if (ok1) atomicAdd(acc + 4 * l1[a] + c, to_fixed(fq.hi()));
+          atomicAdd(a0 + c, to_fixed(fq.lo()));
+          atomicAdd(reinterpret_cast<I*>(rec + r1[a] + L::ROFF) + c, to_fixed(fq.hi()));
         } else {
-          if (ok0) atomicAdd(d0 + c, to_fixed(f[a][c] * q));
+          atomicAdd(a0 + c, to_fixed(f[a][c] * q));
         }
       }
     }
     __syncthreads();
-    // node sums back to T, stored (not added) at their node-major positions;
-    // the accumulators are cleared for the next tile
-    const int nu = tptr[t + 1] - tptr[t];
+    // node sums back to T: a node listed by this tile only goes to y directly
+    // (prescribed DOFs take v), the others' sums are stored (not added) at their
+    // partials positions; the accumulators are cleared for the next tile
     const int32_t* td = tdb + s * mu;
+    const T nan = std::numeric_limits<T>::quiet_NaN();
     for (int k = tid; k < nu; k += NT) {
-      I* w = acc + 4 * k;
-      const I w0 = w[0], w1 = w[1], w2 = w[2];
-      w[0] = I(0);
-      w[1] = I(0);
-      w[2] = I(0);
-      T* p = part + 3 * (int64_t)td[k];
-      const T nan = std::numeric_limits<T>::quiet_NaN();
-      p[0] = bad ? nan : from_fixed(w0, T(0)) * iq;
-      p[1] = bad ? nan : from_fixed(w1, T(0)) * iq;
-      p[2] = bad ? nan : from_fixed(w2, T(0)) * iq;
+      I* a = sums(k);
+      const int32_t d = td[k];
+      const bool direct = d < 0;
+      const int64_t n3 = 3 * (int64_t)(d & 0x0FFFFFFF);
+      T* p = direct ? y + n3 : part + 3 * (int64_t)d;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const T r = bad ? nan : from_fixed(a[c], T(0)) * iq;
+        a[c] = I(0);
+        p[c] = (direct && (((uint32_t)d >> (28 + c)) & 1u)) ? v[n3 + c] : r;
+      }
     }
     __syncthreads();
   }
   cp_async_wait<0>();
 }
 
-// pass 2: y[3n+c] = fixed ? v : sum of node n's tile entries (a contiguous run
-// in node-major order, tile order inside the run)
+// pass 2 over the nodes not listed by exactly one tile:
+// y[3n+c] = fixed ? v : sum of node n's partials (a contiguous run, tile order)
 template <class T>
-__global__ void mf_gather_kernel(int64_t nn, const int32_t* __restrict__ node_ptr, const T* __restrict__ part,
-                                 const uint8_t* __restrict__ fixed, const T* __restrict__ v, T* __restrict__ y,
-                                 const int* __restrict__ skip) {
+__global__ void mf_gather_kernel(int64_t nm, const int32_t* __restrict__ mnodes, const int32_t* __restrict__ mptr,
+                                 const T* __restrict__ part, const uint8_t* __restrict__ fixed,
+                                 const T* __restrict__ v, T* __restrict__ y, const int* __restrict__ skip) {
   if (skip && *skip) return;
-  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t n = mnodes[i];
     T s0 = T(0), s1 = T(0), s2 = T(0);
-    const int32_t q1 = node_ptr[n + 1];
-    for (int32_t q = node_ptr[n]; q < q1; q += 4) {
+    const int32_t q1 = mptr[i + 1];
+    for (int32_t q = mptr[i]; q < q1; q += 4) {
 #pragma unroll
       for (int u = 0; u < 4; ++u)
         if (q + u < q1) {
@@ -598,15 +650,19 @@ __global__ void mf_gather_kernel(int64_t nn, const int32_t* __restrict__ node_pt
 }
 
 // ---------------------------------------------------------------- launch
-template <class T, int ET, bool J2, int TT>
-static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* part,
+template <class T, int ET, bool J2, bool ELAME, int TT>
+static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* y, T* part,
                  const int* skip, cudaStream_t s) {
   constexpr bool TMA = sizeof(T) == 4;
   // lane pairs for the FP32 C3D10 product; one element per thread where pair
   // arithmetic would spill (C3D8's modal form, FP64)
   constexpr int LANES = (sizeof(T) == 4 && ET == EXFEM_C3D10) ? 2 : 1;
-  using L = TileLayout<T, ET, TT, LANES>;
-  auto kern = mf_tile_kernel<T, ET, J2, TT, LANES, TMA>;
+  using L = TileLayout<T, ET, TT, LANES, ELAME>;
+  auto kern = mf_tile_kernel<T, ET, J2, ELAME, TT, LANES, TMA>;
+  if (b->geo_stride != L::GS) {
+    set_error("geometry stream stride %d does not match the kernel's %d", b->geo_stride, L::GS);
+    return EXFEM_ERR_ARG;
+  }
   const int mu = (b->maxu + 7) & ~7;
   const size_t smem = L::smem_bytes(TMA, mu);
   // per (kernel, shared-memory size, device): opt in above 48 KB and size the
@@ -627,23 +683,32 @@ static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tp
     return EXFEM_ERR_UNSUPPORTED;
   }
   const int64_t grid = std::min<int64_t>(b->ntile, (int64_t)nsm * per_sm);
-  kern<<<(unsigned)grid, L::NT, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p, tpack,
-                                           b->tile_dest.p, v, part, (T)b->mat.mu, (T)b->mat.K, mu, b->vmax, skip,
+  const int32_t* tdest = tpack == b->tile_nodes_bc.p ? b->tile_dest_bc.p : b->tile_dest.p;
+  kern<<<(unsigned)grid, L::NT, smem, s>>>(b->ne, b->ntile, geo, b->lidx.p, tan, b->tile_ptr.p, tpack, tdest, v,
+                                           y, part, (T)b->mat.lam, (T)b->mat.mu, (T)b->mat.K, mu, b->vmax, skip,
                                            b->dev_err.p);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
 }
 
-template <class T, int ET, bool J2>
-static int mf_tile(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* part,
+template <class T, int ET, bool J2, bool ELAME>
+static int mf_tile(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* y, T* part,
                    const int* skip, cudaStream_t s) {
   switch (b->tile) {
-    case 128: return mf_go<T, ET, J2, 128>(b, geo, tan, tpack, v, part, skip, s);
-    case 256: return mf_go<T, ET, J2, 256>(b, geo, tan, tpack, v, part, skip, s);
+    case 128: return mf_go<T, ET, J2, ELAME, 128>(b, geo, tan, tpack, v, y, part, skip, s);
+    case 256: return mf_go<T, ET, J2, ELAME, 256>(b, geo, tan, tpack, v, y, part, skip, s);
     default:
       set_error("unsupported matrix-free tile size %d", b->tile);
       return EXFEM_ERR_UNSUPPORTED;
   }
+}
+
+template <class T, int ET>
+static int mf_dispatch(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tpack, const T* v, T* y,
+                       T* part, const int* skip, cudaStream_t s) {
+  if (b->mat.kind == EXFEM_J2) return mf_tile<T, ET, true, false>(b, geo, tan, tpack, v, y, part, skip, s);
+  if (b->lam_e.p) return mf_tile<T, ET, false, true>(b, geo, tan, tpack, v, y, part, skip, s);
+  return mf_tile<T, ET, false, false>(b, geo, tan, tpack, v, y, part, skip, s);
 }
 
 template <class T>
@@ -665,19 +730,14 @@ int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaSt
       geo = (const T*)b->geo32.p;
       tan = (const T*)b->tan32.p;
     }
-    const bool j2 = b->mat.kind == EXFEM_J2;
     const int32_t* nf = (bc && b->fixed.p) ? b->tile_nodes_bc.p : b->tile_nodes.p;
-    int st;
-    if (b->etype == EXFEM_C3D8)
-      st = j2 ? mf_tile<T, EXFEM_C3D8, true>(b, geo, tan, nf, v, part, skip, s)
-              : mf_tile<T, EXFEM_C3D8, false>(b, geo, tan, nf, v, part, skip, s);
-    else
-      st = j2 ? mf_tile<T, EXFEM_C3D10, true>(b, geo, tan, nf, v, part, skip, s)
-              : mf_tile<T, EXFEM_C3D10, false>(b, geo, tan, nf, v, part, skip, s);
+    const int st = b->etype == EXFEM_C3D8 ? mf_dispatch<T, EXFEM_C3D8>(b, geo, tan, nf, v, y, part, skip, s)
+                                          : mf_dispatch<T, EXFEM_C3D10>(b, geo, tan, nf, v, y, part, skip, s);
     if (st) return st;
   }
-  mf_gather_kernel<T><<<grid_for(b->nn, 256), 256, 0, s>>>(b->nn, b->node_ptr.p, part, bc ? b->fixed.p : nullptr,
-                                                           v, y, skip);
+  if (b->nmulti)
+    mf_gather_kernel<T><<<grid_for(b->nmulti, 256), 256, 0, s>>>(b->nmulti, b->multi_nodes.p, b->multi_ptr.p, part,
+                                                                 bc ? b->fixed.p : nullptr, v, y, skip);
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
 }

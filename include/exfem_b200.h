@@ -99,8 +99,7 @@ int exfem_block_colours(exfem_block b, int32_t* colour_host);
  * in a tile order (grouped by mesh component, in the order of each component's
  * first element, then along a Morton curve of the corner-coordinate sums, ties by
  * element index); a tile is `tile` consecutive positions of that order, and slot
- * s = a*tile + (p % 2)*(tile/2) + p/2 is local node a of the element at tile
- * position p.  tile_info: tile count, total length of the node lists and the
+ * s = a*tile + p is local node a of the element at tile position p.  tile_info: tile count, total length of the node lists and the
  * longest list; tile_maps, copied to host: ptr (ntile+1), the sorted distinct
  * nodes of every tile, for each listed node the end of its run of slots
  * (uint16), and per tile the slots grouped by node in node order, increasing

@@ -448,10 +448,10 @@ def tile_order(X, conn, ncorner):
 def tile_maps(conn, tile):
     """Element-tile maps used by the matrix-free product (no counterpart in the
     reference), for conn given in tile order.  Positions [t*tile, (t+1)*tile) form
-    tile t; slot s = a*tile + (p % 2)*(tile/2) + p//2 is local node a of the
-    element at tile position p.  Per tile: the sorted distinct nodes; for each node
-    (in that order) its slots in increasing order, concatenated into perm (padded
-    with zeros to nnode*tile per tile); nend = end of each node's run.
+    tile t; slot s = a*tile + p is local node a of the element at tile position p.
+    Per tile: the sorted distinct nodes; for each node (in that order) its slots in
+    increasing order, concatenated into perm (padded with zeros to nnode*tile per
+    tile); nend = end of each node's run.
     Returns (ptr (ntile+1,), nodes, nend, perm (ntile, nnode*tile))."""
     conn = np.asarray(conn, dtype=np.int64)
     ne, nnode = conn.shape
@@ -461,11 +461,9 @@ def tile_maps(conn, tile):
     for t in range(ntile):
         blk = conn[t * tile:(t + 1) * tile]
         u = np.unique(blk)
-        pos = np.arange(blk.shape[0])
-        slots = (np.arange(nnode)[:, None] * tile + (pos % 2)[None, :] * (tile // 2) + (pos // 2)[None, :]).reshape(-1)
-        slot_node = np.searchsorted(u, blk.T.reshape(-1))
-        inc = np.argsort(slots, kind="stable")                  # increasing slot order
-        slots, slot_node = slots[inc], slot_node[inc]
+        slot_node = np.searchsorted(u, blk.T.reshape(-1))        # slot order a*tile + p (valid p only)
+        la = np.arange(blk.shape[0])
+        slots = (np.arange(nnode)[:, None] * tile + la[None, :]).reshape(-1)
         order = np.argsort(slot_node, kind="stable")
         perm[t, :len(order)] = slots[order]
         nend.append(np.cumsum(np.bincount(slot_node, minlength=len(u))))
