@@ -9,7 +9,7 @@ namespace exfem {
 
 static thread_local std::string g_err;
 // elements per matrix-free tile for blocks created from now on: C3D8, C3D10
-static int g_tile[2] = {128, 128};
+static int g_tile[2] = {128, 256};
 
 void set_error(const char* fmt, ...) {
   char buf[1024];
@@ -234,6 +234,8 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
       if (mlist.empty()) mlist.push_back(0);                   // keep the buffers non-empty
       if (dest.empty()) dest.push_back(0);
       if ((s = b->multi_nodes.upload(mlist.data(), mlist.size()))) return s;
+      if ((s = b->multi_nodes_bc.upload(mlist.data(), mlist.size()))) return s;
+      b->multi_nodes_host = mlist;
       if ((s = b->multi_ptr.upload(mptr.data(), mptr.size()))) return s;
       if ((s = b->tile_dest.upload(dest.data(), dest.size()))) return s;
       if ((s = b->tile_dest_bc.upload(dest.data(), dest.size()))) return s;
@@ -380,6 +382,9 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
     if (!b->tile_dest_host.empty())
       EX_CUDA(cudaMemcpy(b->tile_dest_bc.p, b->tile_dest_host.data(), b->tile_dest_host.size() * sizeof(int32_t),
                          cudaMemcpyHostToDevice));
+    if (!b->multi_nodes_host.empty())
+      EX_CUDA(cudaMemcpy(b->multi_nodes_bc.p, b->multi_nodes_host.data(),
+                         b->multi_nodes_host.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
     if (!b->tile_nodes_host.empty())
       EX_CUDA(cudaMemcpy(b->tile_nodes_bc.p, b->tile_nodes_host.data(), b->tile_nodes_host.size() * sizeof(int32_t),
                          cudaMemcpyHostToDevice));
@@ -391,6 +396,11 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
       f[3 * n + c] = f[3 * n + c] ? 1 : 0;
       nf[n] |= (uint8_t)(f[3 * n + c] << c);
     }
+  if (!b->multi_nodes_host.empty()) {  // fixed-DOF bits of the node pass's nodes, at bits 28-30
+    std::vector<int32_t> packed(b->multi_nodes_host);
+    for (auto& q : packed) q = (int32_t)((uint32_t)q | ((uint32_t)nf[q] << 28));
+    EX_CUDA(cudaMemcpy(b->multi_nodes_bc.p, packed.data(), packed.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  }
   if (!b->tile_dest_host.empty()) {   // fixed-DOF bits of nodes written directly, at bits 28-30
     std::vector<int32_t> packed(b->tile_dest_host);
     for (auto& q : packed)

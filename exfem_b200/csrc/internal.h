@@ -49,6 +49,8 @@ struct exfem_block_s {
   std::vector<int32_t> tile_dest_host;
   int64_t nmulti = 0;                 // nodes not listed by exactly one tile
   exfem::DevBuf<int32_t> multi_nodes; // (nmulti) those nodes, ascending
+  exfem::DevBuf<int32_t> multi_nodes_bc;  // same, fixed-DOF bits at 28-30
+  std::vector<int32_t> multi_nodes_host;
   exfem::DevBuf<int32_t> multi_ptr;   // (nmulti+1) their runs of partials
   exfem::DevBuf<double> partial;      // per-entry tile sums, 3 per entry (FP64 or FP32 view)
   exfem::DevBuf<int> dev_err;         // set by bounded waits that give up

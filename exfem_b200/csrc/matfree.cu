@@ -615,36 +615,42 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
   cp_async_wait<0>();
 }
 
-// pass 2 over the nodes not listed by exactly one tile:
-// y[3n+c] = fixed ? v : sum of node n's partials (a contiguous run, tile order)
+// pass 2 over the nodes not listed by exactly one tile (ids with fixed-DOF bits
+// at 28-30): y[3n+c] = fixed ? v : sum of node n's partials (a contiguous run, tile
+// order).  Each thread takes U nodes a grid stride apart, so that their loads are
+// in flight together.
 template <class T>
 __global__ void mf_gather_kernel(int64_t nm, const int32_t* __restrict__ mnodes, const int32_t* __restrict__ mptr,
-                                 const T* __restrict__ part, const uint8_t* __restrict__ fixed,
-                                 const T* __restrict__ v, T* __restrict__ y, const int* __restrict__ skip) {
+                                 const T* __restrict__ part, const T* __restrict__ v, T* __restrict__ y,
+                                 const int* __restrict__ skip) {
+  constexpr int U = 4;
   if (skip && *skip) return;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t n = mnodes[i];
-    T s0 = T(0), s1 = T(0), s2 = T(0);
-    const int32_t q1 = mptr[i + 1];
-    for (int32_t q = mptr[i]; q < q1; q += 4) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < nm; i0 += U * stride) {
+    uint32_t id[U];
+    int32_t q0[U], q1[U];
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (q + u < q1) {
-          const T* p = part + 3 * (int64_t)(q + u);
-          s0 += p[0];
-          s1 += p[1];
-          s2 += p[2];
-        }
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = i0 + u * stride;
+      id[u] = i < nm ? (uint32_t)mnodes[i] : 0u;
+      q0[u] = i < nm ? mptr[i] : 0;
+      q1[u] = i < nm ? mptr[i + 1] : 0;
     }
-    const int64_t d = 3 * n;
-    if (fixed) {
-      y[d] = fixed[d] ? v[d] : s0;
-      y[d + 1] = fixed[d + 1] ? v[d + 1] : s1;
-      y[d + 2] = fixed[d + 2] ? v[d + 2] : s2;
-    } else {
-      y[d] = s0;
-      y[d + 1] = s1;
-      y[d + 2] = s2;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (i0 + u * stride >= nm) break;
+      T s0 = T(0), s1 = T(0), s2 = T(0);
+      for (int32_t q = q0[u]; q < q1[u]; ++q) {
+        const T* p = part + 3 * (int64_t)q;
+        s0 += p[0];
+        s1 += p[1];
+        s2 += p[2];
+      }
+      const int64_t d = 3 * (int64_t)(id[u] & 0x0FFFFFFFu);
+      const uint32_t bits = id[u] >> 28;
+      y[d] = (bits & 1u) ? v[d] : s0;
+      y[d + 1] = (bits & 2u) ? v[d + 1] : s1;
+      y[d + 2] = (bits & 4u) ? v[d + 2] : s2;
     }
   }
 }
@@ -735,9 +741,11 @@ int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaSt
                                           : mf_dispatch<T, EXFEM_C3D10>(b, geo, tan, nf, v, y, part, skip, s);
     if (st) return st;
   }
-  if (b->nmulti)
-    mf_gather_kernel<T><<<grid_for(b->nmulti, 256), 256, 0, s>>>(b->nmulti, b->multi_nodes.p, b->multi_ptr.p, part,
-                                                                 bc ? b->fixed.p : nullptr, v, y, skip);
+  if (b->nmulti) {
+    const int32_t* mn = (bc && b->fixed.p) ? b->multi_nodes_bc.p : b->multi_nodes.p;
+    mf_gather_kernel<T><<<grid_for((b->nmulti + 3) / 4, 256), 256, 0, s>>>(b->nmulti, mn, b->multi_ptr.p, part, v, y,
+                                                                           skip);
+  }
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
 }
