@@ -275,9 +275,9 @@ def amg_setup(A, X=None, max_coarse=300, rot_mask=None):
 class AMG:
     """Smoothed-aggregation AMG: host set-up, device V-cycle (gfem/linalg.py:102-195)."""
 
-    def __init__(self, A, X=None, max_coarse=300, degree=2, presmooth=1, rot_mask=None):
+    def __init__(self, A, X=None, max_coarse=300, degree=2, presmooth=1, rot_mask=None, setup=None):
         t0 = time.time()
-        h = amg_setup(A, X, max_coarse, rot_mask)
+        h = setup if setup is not None else amg_setup(A, X, max_coarse, rot_mask)
         self.levels, self.coarse, self.coarse_inv, nnz = h["levels"], h["coarse"], h["coarse_inv"], h["nnz"]
         self.degree, self.presmooth = degree, presmooth
         self.sizes = [lv["n"] for lv in self.levels] + [self.coarse_inv.shape[0]]
@@ -286,13 +286,21 @@ class AMG:
         self.setup_time = time.time() - t0
         self._upload()
 
+    @classmethod
+    def from_setup(cls, setup, degree=2, presmooth=1):
+        """Upload a hierarchy made by :func:`amg_setup` (for instance in a worker
+        process).  A level whose ``A`` is None stores no matrix: it is smoothed
+        with the solver's level-0 operator (the matrix-free product)."""
+        return cls(None, setup=setup, degree=degree, presmooth=presmooth)
+
     def _upload(self):
         _lib.require_cuda()
         h = C.c_void_p()
         check(lib.exfem_amg_create(C.byref(h)))
         self._h = h
         for lv in self.levels:
-            Ap, Ai, Av = _csr_parts(lv["A"])
+            Al = lv["A"] if lv["A"] is not None else sp.csr_matrix((lv["n"], lv["n"]))
+            Ap, Ai, Av = _csr_parts(Al)
             Pp, Pi, Pv = _csr_parts(lv["P"])
             Rp, Ri, Rv = _csr_parts(lv["R"])
             dinv = np.ascontiguousarray(lv["dinv"], dtype=np.float64)

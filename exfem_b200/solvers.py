@@ -140,6 +140,7 @@ class _LinearSystem:                                                    # solver
         self.cg_tol, self.cg_maxiter = cg_tol, cg_maxiter
         self.mon = monitor or Monitor(False)
         self.graph = graph
+        self.pinned_amg = None                # a hierarchy every step starts from (served solves)
         self.amg = None
         self.amg_iters0 = None
         self.last_iters = 0
@@ -147,7 +148,7 @@ class _LinearSystem:                                                    # solver
         self._solvers = {}
 
     def reset(self):
-        self.amg = None
+        self.amg = self.pinned_amg
         self.amg_iters0 = None
         self._solvers = {}
 
@@ -219,11 +220,15 @@ class _LinearSystem:                                                    # solver
 
 class StaticSolver:                                                     # solvers.py:481-683
     def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
-                 cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True):
+                 cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None):
+        """``amg``: a prebuilt :class:`linalg.AMG` that every step starts from instead
+        of assembling and setting up its own (the serving path keeps one resident
+        per mesh); the rebuild rule still applies."""
         self.m, self.rtol, self.max_iter = model, rtol, max_iter
         self.mon = monitor or Monitor(verbose)
         self.line_search = line_search
         self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph)
+        self.lin.pinned_amg = amg
         self.newton_iterations = 0
 
     def _fields(self, scale=None):

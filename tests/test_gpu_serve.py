@@ -1,0 +1,74 @@
+"""Served request stream on the device: every result against a sparse direct
+FP64 solve, and the same request alone and inside a mix of concurrent requests on
+other meshes (bit-identical: every reduction of the path has a fixed order)."""
+import numpy as np
+import pytest
+import torch
+
+from exfem_b200 import batch, elements, linalg, mesh, serve
+from exfem_b200.materials import J2Plasticity, LinearElastic
+from exfem_b200.solvers import Step
+
+pytestmark = pytest.mark.gpu
+
+
+def _linear_spec(key, n, etype, E, nu):
+    p = batch.cantilever(*n, 5.0, LinearElastic(E, nu), [[0.0, 0.0, -500.0]], etype=etype)
+    return serve.MeshSpec(key, p.X, p.conn, etype, p.material, p.fixed), p.rhs[0]
+
+
+def _j2_spec(key):
+    X, c = mesh.box_hex(40.0, 10.0, 10.0, 8, 2, 2)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > 40.0 - 1e-9)
+    fixed = np.zeros(3 * len(X), bool)
+    for d in range(3):
+        fixed[3 * fix + d] = True
+    mat = J2Plasticity(210e3, 0.3, [[250.0, 0.0], [1250.0, 1.0]])
+    step = Step(bcs=[(fix, d, 0.0) for d in range(3)] + [(tip, 2, -0.6)], dt_init=0.2, dt_max=0.2)
+    return serve.MeshSpec(key, X, c, elements.HEX8, mat, fixed), step
+
+
+def _direct(spec, rhs):
+    blk = batch.Problem(spec.X, spec.conn, spec.etype, spec.material, spec.fixed, rhs[None])
+    dofs, Ke = batch._element_stiffness(blk)
+    A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke)], spec.ndof), (~spec.fixed).astype(float))
+    return linalg.Direct(A).solve(rhs)
+
+
+def _mix():
+    reqs = []
+    for i, (n, et, E, nu) in enumerate([((10, 3, 2), elements.HEX8, 210e3, 0.3),
+                                        ((3, 2, 2), elements.TET10, 70e3, 0.33),
+                                        ((16, 4, 3), elements.HEX8, 120e3, 0.27),
+                                        ((6, 2, 2), elements.TET10, 95e3, 0.35)]):
+        spec, rhs = _linear_spec(f"lin{i}", n, et, E, nu)
+        for s in (1.0, -0.5, 2.0):
+            reqs.append((spec, rhs * s))
+    return reqs
+
+
+def test_served_results_match_direct_and_alone(cuda):
+    reqs = _mix()
+    j2spec, step = _j2_spec("j2")
+    with serve.SolveServer(slots=4, setup_workers=0) as srv:
+        futs = [srv.submit(serve.SolveRequest(sp, rhs=r)) for sp, r in reqs]
+        futs.append(srv.submit(serve.SolveRequest(j2spec, step=step)))
+        out = [f.result(timeout=600) for f in futs]
+        st = serve.latency_stats(srv.completed)
+        assert st["n"] == len(reqs) + 1
+        # requests ran concurrently on several slots
+        assert len({r.info["slot"] for r in srv.completed}) > 1
+    for (sp, r), (x, info) in zip(reqs, out[:-1]):
+        xd = _direct(sp, r)
+        assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-6, info
+    assert out[-1][1]["increments"] >= 3
+    # the same requests alone (one slot, nothing else on the server)
+    for k in (0, 7, 11):
+        sp, r = reqs[k]
+        with serve.SolveServer(slots=1, setup_workers=0) as srv:
+            xa, _ = srv.submit(serve.SolveRequest(sp, rhs=r)).result(timeout=600)
+        np.testing.assert_array_equal(xa, out[k][0])
+    with serve.SolveServer(slots=1, setup_workers=0) as srv:
+        ua, _ = srv.submit(serve.SolveRequest(j2spec, step=step)).result(timeout=600)
+    np.testing.assert_array_equal(ua, out[-1][0])
