@@ -218,6 +218,210 @@ def solve_section(reps=10):
     return out
 
 
+def batch_section(count=512, nplain=24, seed=0, workers=None):
+    """Batched uneven solves (512 C3D8 cantilevers x 4 right-hand sides, FP32
+    matrix-free AMG-PCG inside FP64 refinement to 1e-8) against the plain FP64
+    single-solve path (FP64 matrix-free AMG-PCG to 1e-8, one solve at a time, no
+    graphs, hierarchy prebuilt) on a seeded sample of the same instances."""
+    import torch
+    from exfem_b200 import batch, linalg
+    from exfem_b200.model import Block
+    t0 = time.time()
+    probs = batch.random_cantilevers(count, seed=seed)
+    stiff = [batch._element_stiffness(p) for p in probs]
+    setups = batch.host_setups(probs, workers=workers, stiffness=stiff)
+    S = batch.BatchSolver(probs, setups=setups)
+    t_setup = time.time() - t0
+    x, info = S.solve()
+    torch.cuda.synchronize()
+    reps = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        x, info = S.solve()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    xs = S.split(x)
+    rng = np.random.default_rng(seed + 1)
+    sample = rng.choice(S.ninst, size=min(nplain, S.ninst), replace=False)
+    tp, errs = [], []
+    for i in sample:
+        k, r = S.inst[i]
+        p = probs[k]
+        blk = Block(p.conn, p.etype, p.material, p.X)
+        blk.set_fixed(p.fixed)
+        dofs, Ke = stiff[k]
+        A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke)], p.ndof), (~p.fixed).astype(float))
+        h = dict(setups[k], levels=[dict(lv) for lv in setups[k]["levels"]])
+        if h["levels"]:
+            h["levels"][0]["A"] = A                        # the plain path smooths level 0 with the stored matrix
+        ns = linalg.NativeSolver(blk, "mf64", "amg", linalg.AMG.from_setup(h), graph=False)
+        b = torch.as_tensor(p.rhs[r], device="cuda")
+        ns.pcg(b, tol=1e-8)
+        torch.cuda.synchronize()
+        c0 = time.perf_counter()
+        xp, kk, rr = ns.pcg(b, tol=1e-8)
+        torch.cuda.synchronize()
+        tp.append(time.perf_counter() - c0)
+        errs.append(float((xs[i] - xp).norm() / xp.norm()))
+    plain = 1.0 / float(np.mean(tp))
+    batched = S.ninst / (ms * 1e-3)
+    return dict(workload=f"{count} seeded C3D8 cantilevers (nx 4-64, ny/nz 2-16, h 5 mm), 4 RHS each",
+                instances=S.ninst, dof_total=int(sum(p.ndof for p in probs)), solves_per_s=batched,
+                ms_per_batch=ms, refinement_passes=info["passes"], pcg_iters_max=int(info["iters"].max()),
+                pcg_iters_mean=float(info["iters"].mean()), plain_fp64_solves_per_s=plain,
+                plain_sample=len(sample), speedup_vs_plain=batched / plain,
+                max_rel_err_vs_plain_fp64=max(errs), host_setup_s=t_setup)
+
+
+def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e5), j2_frac=0.2, slots=8, seed=0,
+                  nplain=32):
+    """Served request stream: a catalogue of seeded C3D8 / C3D10 jittered
+    cantilever meshes (DOF log-uniform in `dof`), a fraction `j2_frac` of them J2
+    (5 displacement increments), Poisson arrivals at each rate for `duration`
+    seconds; p50/p99 latency and solves/s, against serial plain FP64 solves of a
+    sample of the same requests on the same GPU."""
+    import threading
+    import torch
+    from exfem_b200 import elements, linalg, mesh, serve
+    from exfem_b200.materials import J2Plasticity, LinearElastic
+    from exfem_b200.model import Block, Model
+    from exfem_b200.solvers import StaticSolver, Step
+    rng = np.random.default_rng(seed)
+    specs, extra = [], []
+    for i in range(nmesh):
+        target = float(np.exp(rng.uniform(np.log(dof[0]), np.log(dof[1]))))
+        tet = bool(rng.integers(0, 2))
+        per_node = 3.0
+        nodes = target / per_node
+        # aspect 4:1:1 boxes; a C3D10 mesh of n hexes per edge has (2n+1)^3-like node counts
+        k = (nodes / 4.0) ** (1.0 / 3.0)
+        if tet:
+            k = max(1, int(round((k - 1) / 2)))
+            n = (4 * k, k, k)
+        else:
+            k = max(1, int(round(k - 1)))
+            n = (4 * k, k, k)
+        h = 5.0
+        X, c = mesh.box_hex(n[0] * h, n[1] * h, n[2] * h, *n)
+        X = mesh.jitter_interior(X, h, 0.1, seed + i)
+        et = elements.HEX8
+        if tet:
+            X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+            et = elements.TET10
+        L = n[0] * h
+        fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9 * L)
+        tip = mesh.nodes_where(X, lambda x, y, z: x > L * (1 - 1e-9))
+        fixed = np.zeros(3 * len(X), bool)
+        for d in range(3):
+            fixed[3 * fix + d] = True
+        E, nu = rng.uniform(70e3, 210e3), rng.uniform(0.25, 0.35)
+        j2 = rng.uniform() < j2_frac
+        mat = J2Plasticity(E, nu, [[250.0, 0.0], [1250.0, 1.0]]) if j2 else LinearElastic(E, nu)
+        specs.append(serve.MeshSpec(f"m{i}", X, c, et, mat, fixed))
+        extra.append(dict(fix=fix, tip=tip, L=L))
+
+    def make_request(r):
+        i = int(r.integers(0, nmesh))
+        sp, ex = specs[i], extra[i]
+        if sp.j2:
+            d = -L_over(ex) * r.uniform(0.5, 1.0)
+            step = Step(bcs=[(ex["fix"], k, 0.0) for k in range(3)] + [(ex["tip"], 2, d)], dt_init=0.2, dt_max=0.2)
+            return serve.SolveRequest(sp, step=step)
+        f = r.standard_normal(3)
+        f *= r.uniform(100.0, 1000.0) / np.linalg.norm(f)
+        rhs = np.zeros(sp.ndof)
+        for k in range(3):
+            rhs[3 * ex["tip"] + k] = f[k] / len(ex["tip"])
+        return serve.SolveRequest(sp, rhs=rhs)
+
+    def L_over(ex):
+        return ex["L"] / 400.0
+
+    out = dict(workload=f"{nmesh} seeded C3D8/C3D10 jittered cantilevers, DOF log-uniform in "
+                        f"[{dof[0]:.0e}, {dof[1]:.0e}], {int(100 * j2_frac)}% of meshes J2 (5 increments)",
+               slots=slots, rates={})
+    srv = serve.SolveServer(slots=slots, hbm_budget=150e9, setup_workers=8)
+    try:
+        t0 = time.time()
+        srv.warm(specs)
+        out["catalogue_setup_s"] = time.time() - t0
+        out["dof"] = [int(s.ndof) for s in specs]
+        # warm the graphs of every entry once
+        for f in [srv.submit(make_request(np.random.default_rng(1000 + i))) for i in range(2 * nmesh)]:
+            f.result()
+        for rate in rates:
+            r = np.random.default_rng(seed + int(rate))
+            arrivals = np.cumsum(r.exponential(1.0 / rate, size=int(rate * duration * 1.2) + 10))
+            arrivals = arrivals[arrivals < duration]
+            reqs = [make_request(r) for _ in arrivals]
+            srv.completed.clear()
+            futs = []
+            tstart = time.perf_counter()
+            for a, q in zip(arrivals, reqs):
+                dt = tstart + a - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                futs.append(srv.submit(q))
+            for f in futs:
+                f.result()
+            st = serve.latency_stats(list(srv.completed))
+            st["offered_per_s"] = float(len(arrivals) / duration)
+            st["j2_requests"] = int(sum(q.spec.j2 for q in reqs))
+            out["rates"][str(int(rate))] = st
+        # serial plain FP64 solves of a sample of requests (hierarchies prebuilt)
+        r = np.random.default_rng(seed + 7)
+        sample = [make_request(r) for _ in range(nplain)]
+        times, errs = [], []
+        plain_cache = {}
+        for q in sample:
+            sp = q.spec
+            ent = srv.entry(sp.key)
+            served_x, _ = srv.submit(q).result()
+            if sp.key not in plain_cache:
+                blk0 = Block(sp.conn, sp.etype, LinearElastic(sp.material.E, sp.material.nu), sp.X)
+                Ke = blk0.stiffness(torch.zeros(sp.ndof, dtype=torch.float64, device="cuda"), blk0.init_state())
+                dofs = (sp.conn.astype(np.int64)[:, :, None] * 3 + np.arange(3)).reshape(len(sp.conn), -1)
+                A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke.cpu().numpy())], sp.ndof),
+                                     (~sp.fixed).astype(float))
+                h = dict(levels=[dict(lv) for lv in ent.amg.levels], coarse=ent.amg.coarse,
+                         coarse_inv=ent.amg.coarse_inv, nnz=[1])
+                if h["levels"]:
+                    h["levels"][0]["A"] = A
+                amg = linalg.AMG.from_setup(h)
+                if sp.j2:
+                    m = Model(sp.X)
+                    m.add_block(sp.conn, sp.etype, sp.material)
+                    plain_cache[sp.key] = ("j2", m, amg)
+                else:
+                    blk = Block(sp.conn, sp.etype, sp.material, sp.X)
+                    blk.set_fixed(sp.fixed)
+                    plain_cache[sp.key] = ("lin", linalg.NativeSolver(blk, "mf64", "amg", amg, graph=False), amg)
+            kind, obj, amg = plain_cache[sp.key]
+            torch.cuda.synchronize()
+            c0 = time.perf_counter()
+            if kind == "lin":
+                xp, _, _ = obj.pcg(torch.as_tensor(q.rhs, device="cuda"), tol=1e-8)
+            else:
+                s = StaticSolver(obj, rtol=1e-6, linear_solver="amg", tangent="mf", cg_tol=1e-6, verbose=False,
+                                 graph=False, amg=amg)
+                xp, _, _ = s.solve(q.step)
+            xp = xp.cpu().numpy()
+            times.append(time.perf_counter() - c0)
+            if kind == "lin":
+                errs.append(float(np.linalg.norm(served_x - xp) / np.linalg.norm(xp)))
+        out["plain_fp64_serial_solves_per_s"] = float(len(times) / np.sum(times))
+        out["plain_sample"] = len(times)
+        out["max_rel_err_vs_plain_fp64_linear"] = max(errs) if errs else None
+        best = max(v["solves_per_s"] for v in out["rates"].values())
+        out["speedup_vs_plain_serial"] = best / out["plain_fp64_serial_solves_per_s"]
+        out["evictions"] = srv.evictions
+    finally:
+        srv.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -227,9 +431,22 @@ def main():
     ap.add_argument("--n", type=int, default=80, help="hexahedra per cube edge (80 = the scale case)")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", default="product", choices=["product", "batch", "serve"],
+                    help="product: the C3D10 matrix-free product line (default); batch: batched uneven "
+                         "solves; serve: served request stream")
+    ap.add_argument("--count", type=int, default=512, help="cantilevers of the batch mode")
+    ap.add_argument("--rates", default="50,200", help="arrival rates (solves/s) of the serve mode")
+    ap.add_argument("--duration", type=float, default=15.0, help="seconds per arrival rate (serve mode)")
+    ap.add_argument("--max-dof", type=float, default=2e5, help="largest catalogue mesh (serve mode)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode != "product":
+        sec = (batch_section(args.count) if args.mode == "batch" else
+               serve_section(rates=tuple(float(r) for r in args.rates.split(",")), duration=args.duration,
+                             dof=(1e3, args.max_dof)))
+        print(json.dumps(dict(mode=args.mode, **sec)), flush=True)
+        return
 
     import ctypes as C
     import torch

@@ -31,6 +31,7 @@
 // centroid removed) and the stiffness scale; C3D10 stores the inverse Jacobian
 // and scaled volume, formed in FP64 from the nodal coordinates and rounded once.
 #include <limits>
+#include <mutex>
 #include <type_traits>
 
 #include "internal.h"
@@ -671,18 +672,33 @@ static int mf_go(exfem_block_s* b, const T* geo, const T* tan, const int32_t* tp
   }
   const int mu = (b->maxu + 7) & ~7;
   const size_t smem = L::smem_bytes(TMA, mu);
-  // per (kernel, shared-memory size, device): opt in above 48 KB and size the
-  // persistent grid
-  static thread_local size_t opted = 0;
-  static thread_local int per_sm = 0, nsm = 0, dev = -1;
+  // The kernel's dynamic shared-memory limit is a process-wide attribute (per
+  // device): it only ever grows, under a lock, so that a launch on one host thread
+  // never finds it lowered by another thread's smaller mesh.  The persistent grid
+  // is sized per (shared-memory size, device) from the occupancy query.
+  static std::mutex attr_mu;
+  static size_t opted_dev[64] = {0};
+  static thread_local size_t q_smem = 0;
+  static thread_local int per_sm = 0, nsm = 0, q_dev = -1;
   int cur;
   EX_CUDA(cudaGetDevice(&cur));
-  if (smem != opted || cur != dev) {
-    EX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024)));
+  if (cur < 0 || cur >= 64) {
+    set_error("device ordinal %d out of range", cur);
+    return EXFEM_ERR_UNSUPPORTED;
+  }
+  {
+    std::lock_guard<std::mutex> lock(attr_mu);
+    if (smem > opted_dev[cur]) {
+      const size_t want = std::max<size_t>(smem, 48 * 1024);
+      EX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want));
+      opted_dev[cur] = want;
+    }
+  }
+  if (smem != q_smem || cur != q_dev) {
     EX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, cur));
     EX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, L::NT, smem));
-    opted = smem;
-    dev = cur;
+    q_smem = smem;
+    q_dev = cur;
   }
   if (per_sm < 1) {
     set_error("matrix-free tile kernel does not fit on an SM (%zu bytes of shared memory)", smem);
