@@ -431,6 +431,7 @@ def main():
     ap.add_argument("--n", type=int, default=80, help="hexahedra per cube edge (80 = the scale case)")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default tile size (no autotuning)")
     ap.add_argument("--mode", default="product", choices=["product", "batch", "serve"],
                     help="product: the C3D10 matrix-free product line (default); batch: batched uneven "
                          "solves; serve: served request stream")
@@ -455,6 +456,11 @@ def main():
     from exfem_b200.model import Model
 
     rank, world, dist = dist_setup(args.gpus)
+    tuned = None
+    if not args.no_tune:
+        from exfem_b200 import tuning
+        tuned = {k: dict(tile=t, ms={str(a): b for a, b in ms.items()})
+                 for k, (t, ms) in tuning.autotune((xf.TET10,)).items()}
     X, c, scale = build_config3(args.n)
     m = Model(X)
     blk = m.add_block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3))
@@ -545,7 +551,8 @@ def main():
         ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
         data="synthetic",
         config=dict(workload=WORKLOAD, ne=ne, nodes=nn, ndof=ndof, parallelism=f"replicas x{world}",
-                    l2="per-step stream 600 MB > 126 MB L2, no flush", seed=0),
+                    l2="per-step stream 600 MB > 126 MB L2, no flush", seed=0, tile=blk.tile_order()[0],
+                    autotune=tuned),
         e2e=dict(value=world * ndof / (e_ms * 1e-3), unit=UNIT, h2d_bytes_per_step=4 * ndof,
                  d2h_bytes_per_step=4 * ndof, ms_per_step=e_ms),
         roofline=dict(bound="hbm", achieved=achieved, peak=pk, unit="GB/s", frac=achieved / pk,

@@ -172,3 +172,26 @@ def test_scale_field(cuda):
     yo = omod.tangent_jvp(torch.as_tensor(u), omod.init_state(), v, scale=[sc])
     yp = pmod.tangent_jvp(torch.as_tensor(u, device="cuda"), pmod.init_state(), v.cuda(), dict(scale=[sc]))
     assert rel_err(yp, yo) < 1e-12
+
+
+def test_autotuner_picks_a_tile_and_both_tiles_agree(cuda):
+    import exfem_b200 as xf
+    from exfem_b200 import tuning
+    from exfem_b200.model import Block
+    res = tuning.autotune((xf.TET10,), n=12, reps=3)
+    tile, times = res["C3D10"]
+    assert tile in tuning.CANDIDATES and set(times) == set(tuning.CANDIDATES)
+    assert tuning.current(xf.TET10) == tile
+    X, c = tet10_box(1, 1, 1, 4, 3, 3)
+    rng = np.random.default_rng(5)
+    v = torch.as_tensor(rng.standard_normal(3 * len(X)), device="cuda")
+    ys = {}
+    for t in tuning.CANDIDATES:
+        tuning.apply(xf.TET10, t)
+        blk = Block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3), X)
+        assert blk.tile_order()[0] == t
+        ys[t] = blk.tangent_matvec(v.float()).double()
+        y64 = blk.tangent_matvec(v)
+    tuning.apply(xf.TET10, tile)
+    for t in tuning.CANDIDATES:
+        assert rel_err(ys[t], y64) < 2e-6
