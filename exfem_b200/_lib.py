@@ -67,6 +67,7 @@ _SIGS = {
     "exfem_tangent_matvec": ([VP, C.c_int, P, P, C.c_int, VP], C.c_int),
     "exfem_tangent_diagonal": ([VP, P, VP], C.c_int),
     "exfem_ebe_matvec": ([VP, P, P, P, C.c_int, VP], C.c_int),
+    "exfem_ebe_matvec_bf16_multi": ([VP, P, I32, P, P, I32, VP], C.c_int),
     "exfem_ebe_diagonal": ([VP, P, P, VP], C.c_int),
     "exfem_stresses": ([VP, P, P, P, P, P, VP], C.c_int),
     "exfem_amg_create": ([C.POINTER(VP)], C.c_int),

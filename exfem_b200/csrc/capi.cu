@@ -466,6 +466,15 @@ int exfem_tangent_diagonal(exfem_block b, double* diag, void* stream) {
   return launch_mf_diagonal(b, diag, as_stream(stream));
 }
 
+int exfem_ebe_matvec_bf16_multi(exfem_block b, const void* Ke_bf16, int nrhs, const float* V, float* Y,
+                                int apply_bc, void* stream) {
+  EX_ARG(b && (b->ne == 0 || Ke_bf16) && V && Y, "NULL argument");
+  StreamGuard g;
+  int s;
+  if ((s = g.init(stream))) return s;
+  return launch_ebe_matvec_tc(b, (const __nv_bfloat16*)Ke_bf16, nrhs, V, Y, g.work, apply_bc != 0);
+}
+
 int exfem_ebe_matvec(exfem_block b, const double* Ke, const double* v, double* y, int apply_bc, void* stream) {
   EX_ARG(b && Ke && v && y, "NULL argument");
   return launch_ebe_matvec(b, Ke, v, y, nullptr, as_stream(stream), apply_bc != 0);

@@ -1,5 +1,7 @@
 // Internal handle layouts and cross-file launchers of the exfem_b200 library.
 #pragma once
+#include <cuda_bf16.h>
+
 #include <memory>
 #include <vector>
 
@@ -64,6 +66,7 @@ struct exfem_block_s {
   uint64_t tan_gen = 0, bc_gen = 0;
   // scratch
   exfem::DevBuf<double> ys;           // (ne*nnode*3) element vectors for gather assembly
+  exfem::DevBuf<float> ys_tc;         // (ne*nnode*3*nrhs) element rows of the tensor-core stored-Ke product
   int64_t ndof() const { return 3 * nn; }
 };
 
@@ -96,6 +99,9 @@ int launch_ebe_diagonal(exfem_block_s* b, const double* Ke, double* diag, cudaSt
 template <class T>
 int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaStream_t s, bool bc = true);
 int launch_mf_diagonal(exfem_block_s* b, double* diag, cudaStream_t s);
+// stored-Ke product for several right-hand sides on the tensor cores (ebe_tc.cu)
+int launch_ebe_matvec_tc(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, const float* V, float* Y,
+                         cudaStream_t s, bool bc);
 
 // reductions and vector kernels (krylov.cu)
 enum ModeForce { FORCE_FULL = 0, FORCE_TANGENT = 1, FORCE_STRESS = 2 };

@@ -185,6 +185,16 @@ class Block:
         check(lib.exfem_tangent_diagonal(self._h, ptr(d), stream_ptr()))
         return d
 
+    def ebe_matvec_multi(self, Ke_bf16, V, apply_bc=True):
+        """Stored-Ke product of several right-hand sides on the tensor cores: Ke
+        (ne, nd, nd) BF16, V (ndof, nrhs <= 16) FP32 -> (ndof, nrhs) FP32 (V rounded
+        to BF16, FP32 accumulation)."""
+        V = V.to(torch.float32).contiguous()
+        Y = torch.empty_like(V)
+        check(lib.exfem_ebe_matvec_bf16_multi(self._h, ptr(Ke_bf16.contiguous()), V.shape[1], ptr(V), ptr(Y),
+                                              1 if apply_bc else 0, stream_ptr()))
+        return Y
+
     def ebe_matvec(self, Ke, v, apply_bc=True):
         v = _dev(v)
         y = torch.empty_like(v)

@@ -195,3 +195,32 @@ def test_autotuner_picks_a_tile_and_both_tiles_agree(cuda):
     tuning.apply(xf.TET10, tile)
     for t in tuning.CANDIDATES:
         assert rel_err(ys[t], y64) < 2e-6
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+@pytest.mark.parametrize("nrhs", [1, 4, 16])
+def test_tensor_core_stored_ke_multi_rhs(cuda, kind, nrhs):
+    """BF16 Ke x BF16 right-hand sides with FP32 accumulation (tcgen05): equal to
+    the same BF16-rounded operands multiplied in FP64 up to FP32 accumulation
+    (1e-5), and to the FP64 stored-Ke product within BF16 rounding (2e-2)."""
+    from exfem_b200.model import Block
+    X, c, pmod, omod = _pair(kind, "el", n=(5, 4, 3))
+    blk = pmod.blocks[0]
+    fixed = np.zeros(pmod.ndof, bool)
+    fixed[::7] = True
+    blk.set_fixed(fixed)
+    zero = torch.zeros(pmod.ndof, dtype=torch.float64, device="cuda")
+    Kb = blk.stiffness(zero, blk.init_state(), dtype=torch.bfloat16)
+    K64 = blk.stiffness(zero, blk.init_state())
+    rng = np.random.default_rng(nrhs)
+    V = torch.as_tensor(rng.standard_normal((pmod.ndof, nrhs)), dtype=torch.float32, device="cuda")
+    Y = blk.ebe_matvec_multi(Kb, V)
+    Vb = V.to(torch.bfloat16).double()
+    for r in range(nrhs):
+        yb = blk.ebe_matvec(Kb.double(), Vb[:, r].contiguous())
+        y64 = blk.ebe_matvec(K64, V[:, r].double().contiguous())
+        # prescribed rows take v itself (FP32 V, not its BF16 rounding)
+        yb[torch.as_tensor(fixed, device="cuda")] = V[torch.as_tensor(fixed, device="cuda"), r].double()
+        assert rel_err(Y[:, r].double(), yb) < 1e-5
+        assert rel_err(Y[:, r].double(), y64) < 2e-2
+    blk.set_fixed(None)
