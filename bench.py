@@ -422,6 +422,51 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e5), 
     return out
 
 
+def stored_ke_section(n=(160, 40, 40), reps=20):
+    """Multi-right-hand-side products on one C3D8 mesh (n hexahedra, jittered,
+    linear elastic, x = 0 clamped): the BF16 stored-Ke tensor-core product for 4
+    and 16 right-hand sides against the FP32 matrix-free product applied to each
+    right-hand side.  Reported as DOF x right-hand sides x products / s."""
+    import torch
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = mesh.box_hex(5.0 * n[0], 5.0 * n[1], 5.0 * n[2], *n)
+    X = mesh.jitter_interior(X, 5.0, 0.1, 0)
+    m = xf.Model(X)
+    blk = m.add_block(c, xf.HEX8, xf.LinearElastic(210e3, 0.3))
+    fixed = np.zeros(m.ndof, bool)
+    fixed[: 3 * (n[1] + 1) * (n[2] + 1)] = True
+    blk.set_fixed(fixed)
+    zero = torch.zeros(m.ndof, dtype=torch.float64, device="cuda")
+    Kb = blk.stiffness(zero, blk.init_state(), dtype=torch.bfloat16)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(reps):
+            fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        return ev0.elapsed_time(ev1) / reps
+
+    out = dict(workload=f"C3D8 {n[0]}x{n[1]}x{n[2]} jittered cantilever ({len(c)} el, {m.ndof} DOF), BF16 Ke "
+                        f"{Kb.numel() * 2 / 1e6:.0f} MB")
+    v = torch.randn(m.ndof, dtype=torch.float32, device="cuda")
+    ms_mf = timed(lambda: blk.tangent_matvec(v))
+    out["mf_fp32_ms_per_rhs"] = ms_mf
+    for nr in (4, 16):
+        V = torch.randn(m.ndof, nr, dtype=torch.float32, device="cuda")
+        ms = timed(lambda: blk.ebe_matvec_multi(Kb, V))
+        out[f"tc_bf16_{nr}rhs"] = dict(ms=ms, dof_rhs_per_s=m.ndof * nr / (ms * 1e-3),
+                                       mf_fp32_dof_rhs_per_s=m.ndof / (ms_mf * 1e-3),
+                                       speedup_vs_mf=ms_mf * nr / ms,
+                                       ke_gbs=Kb.numel() * 2 / (ms * 1e-3) / 1e9)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -432,7 +477,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default tile size (no autotuning)")
-    ap.add_argument("--mode", default="product", choices=["product", "batch", "serve"],
+    ap.add_argument("--mode", default="product", choices=["product", "batch", "serve", "stored_ke"],
                     help="product: the C3D10 matrix-free product line (default); batch: batched uneven "
                          "solves; serve: served request stream")
     ap.add_argument("--count", type=int, default=512, help="cantilevers of the batch mode")
@@ -443,9 +488,13 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     if args.mode != "product":
-        sec = (batch_section(args.count) if args.mode == "batch" else
-               serve_section(rates=tuple(float(r) for r in args.rates.split(",")), duration=args.duration,
-                             dof=(1e3, args.max_dof)))
+        if args.mode == "batch":
+            sec = batch_section(args.count)
+        elif args.mode == "stored_ke":
+            sec = stored_ke_section()
+        else:
+            sec = serve_section(rates=tuple(float(r) for r in args.rates.split(",")), duration=args.duration,
+                                dof=(1e3, args.max_dof))
         print(json.dumps(dict(mode=args.mode, **sec)), flush=True)
         return
 
