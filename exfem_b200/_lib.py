@@ -94,6 +94,8 @@ _SIGS = {
     "exfem_host_colouring": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_standard_aggregation": ([I64, P, P, P, C.POINTER(I64)], C.c_int),
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
+    "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
+    "exfem_block_tile_conn": ([VP, P], C.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     _f = getattr(lib, _name)

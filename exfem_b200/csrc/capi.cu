@@ -30,6 +30,7 @@ int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::
 int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg);
 int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
                     std::vector<int32_t>& order);
+int host_tile_pairs(int64_t ne, const int32_t* conn, std::vector<int32_t>& order, std::vector<int32_t>& conn_tile);
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
                    int& maxu);
@@ -183,12 +184,17 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
     if ((s = host_tile_order(nn, ne, b->nnode, etype == EXFEM_C3D8 ? 8 : 4, X_host, conn_host, b->order_host)))
       return s;
     std::vector<int32_t> conn_ord((size_t)ne * b->nnode), tpos(ne);
-    for (int64_t p = 0; p < ne; ++p) {
-      const int64_t e = b->order_host[p];
-      tpos[e] = (int32_t)p;
-      memcpy(&conn_ord[p * b->nnode], conn_host + e * b->nnode, b->nnode * sizeof(int32_t));
+    if (etype == EXFEM_C3D10 && b->mat.kind == EXFEM_LINEAR_ELASTIC) {
+      // face-sharing pairs side by side, in the local numbering the pairs share
+      if ((s = host_tile_pairs(ne, conn_host, b->order_host, conn_ord))) return s;
+    } else {
+      for (int64_t p = 0; p < ne; ++p)
+        memcpy(&conn_ord[p * b->nnode], conn_host + (int64_t)b->order_host[p] * b->nnode, b->nnode * sizeof(int32_t));
     }
+    for (int64_t p = 0; p < ne; ++p) tpos[b->order_host[p]] = (int32_t)p;
     if ((s = b->tpos.upload(tpos.data(), std::max<size_t>(tpos.size(), 1)))) return s;
+    if ((s = b->order_dev.upload(b->order_host.data(), std::max<size_t>(b->order_host.size(), 1)))) return s;
+    if ((s = b->conn_tile.upload(conn_ord.data(), std::max<size_t>(conn_ord.size(), 1)))) return s;
     std::vector<int32_t> tp, tn;
     std::vector<uint16_t> te, tq;
     if ((s = host_tile_maps(nn, ne, b->nnode, conn_ord.data(), b->tile, tp, tn, te, tq, b->maxu))) return s;
@@ -324,6 +330,14 @@ int exfem_block_tile_order(exfem_block b, int* tile, int32_t* order_host) {
   EX_ARG(b, "block is NULL");
   if (tile) *tile = b->tile;
   if (order_host && b->ne) memcpy(order_host, b->order_host.data(), b->ne * sizeof(int32_t));
+  return EXFEM_OK;
+}
+
+int exfem_block_tile_conn(exfem_block b, int32_t* conn_tile_host) {
+  EX_ARG(b && conn_tile_host, "NULL argument");
+  if (b->ne)
+    EX_CUDA(cudaMemcpy(conn_tile_host, b->conn_tile.p, (size_t)b->ne * b->nnode * sizeof(int32_t),
+                       cudaMemcpyDeviceToHost));
   return EXFEM_OK;
 }
 
@@ -674,6 +688,18 @@ int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn,
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
   EX_ARG(ptr && idx && agg && nagg, "NULL argument");
   return host_standard_aggregation(n, ptr, idx, agg, *nagg);
+}
+
+int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile) {
+  EX_ARG(ne >= 0 && (conn || ne == 0) && (order || ne == 0) && (conn_tile || ne == 0), "NULL argument");
+  std::vector<int32_t> o(order, order + ne), ct;
+  int s;
+  if ((s = host_tile_pairs(ne, conn, o, ct))) return s;
+  if (ne) {
+    memcpy(order, o.data(), ne * sizeof(int32_t));
+    memcpy(conn_tile, ct.data(), ct.size() * sizeof(int32_t));
+  }
+  return EXFEM_OK;
 }
 
 int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,

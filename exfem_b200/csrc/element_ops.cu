@@ -338,14 +338,16 @@ int launch_colour_assemble(exfem_block_s* b, const double* fe, double* f, cudaSt
 // per-element Lame parameters, lambda and mu (the matrix-free kernels otherwise
 // take the material's from their arguments).
 template <int ET>
-__global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn,
-                                const double* __restrict__ scale, const double* __restrict__ lam_e,
-                                const double* __restrict__ mu_e, int GS, double* __restrict__ g64,
-                                float* __restrict__ g32, const int32_t* __restrict__ tpos, int tile) {
+__global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn_tile,
+                                const int32_t* __restrict__ order, const double* __restrict__ scale,
+                                const double* __restrict__ lam_e, const double* __restrict__ mu_e, int GS,
+                                double* __restrict__ g64, float* __restrict__ g32, int tile) {
   using Tr = ElemTraits<ET>;
   constexpr int NN = Tr::nnode, GF = Tr::geo_stride;
-  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (e >= ne) return;
+  const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;   // tile position
+  if (p >= ne) return;
+  const int64_t e = order[p];
+  const int32_t* cn = conn_tile + p * NN;                              // this position's nodes
   const double sc = scale ? scale[e] : 1.0;
   double out[GF];
 #pragma unroll
@@ -355,7 +357,7 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
 #pragma unroll
     for (int a = 0; a < 8; ++a)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) xa[a][c] = X[3 * (int64_t)conn[e * NN + a] + c];
+      for (int c = 0; c < 3; ++c) xa[a][c] = X[3 * (int64_t)cn[a] + c];
     hex_to_modal(xa, cm);
 #pragma unroll
     for (int k = 0; k < 7; ++k)
@@ -366,7 +368,7 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
     double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
 #pragma unroll
     for (int a = 0; a < 10; ++a) {
-      const int64_t n3 = 3 * (int64_t)conn[e * NN + a];
+      const int64_t n3 = 3 * (int64_t)cn[a];
 #pragma unroll
       for (int i = 0; i < 3; ++i)
 #pragma unroll
@@ -382,8 +384,8 @@ __global__ void geometry_kernel(int64_t ne, const double* __restrict__ X, const 
     out[GF - 1] = mu_e[e];
   }
   for (int k = 0; k < GS; ++k) {
-    g64[tile_index(tpos[e], k, GS, tile)] = out[k];
-    g32[tile_index(tpos[e], k, GS, tile)] = (float)out[k];
+    g64[tile_index(p, k, GS, tile)] = out[k];
+    g32[tile_index(p, k, GS, tile)] = (float)out[k];
   }
 }
 
@@ -403,11 +405,11 @@ int build_geometry(exfem_block_s* b) {
   const int threads = 128;
   const unsigned grid = (unsigned)((b->ne + threads - 1) / threads);
   if (b->etype == EXFEM_C3D8)
-    geometry_kernel<EXFEM_C3D8><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
-                                                   GS, b->geo64.p, b->geo32.p, b->tpos.p, b->tile);
+    geometry_kernel<EXFEM_C3D8><<<grid, threads>>>(b->ne, b->X.p, b->conn_tile.p, b->order_dev.p, b->scale.p,
+                                                   b->lam_e.p, b->mu_e.p, GS, b->geo64.p, b->geo32.p, b->tile);
   else
-    geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn.p, b->scale.p, b->lam_e.p, b->mu_e.p,
-                                                    GS, b->geo64.p, b->geo32.p, b->tpos.p, b->tile);
+    geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn_tile.p, b->order_dev.p, b->scale.p,
+                                                    b->lam_e.p, b->mu_e.p, GS, b->geo64.p, b->geo32.p, b->tile);
   EX_LAUNCH_CHECK();
   EX_CUDA(cudaDeviceSynchronize());
   return EXFEM_OK;

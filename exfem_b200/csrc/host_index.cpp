@@ -157,6 +157,125 @@ int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double
   return EXFEM_OK;
 }
 
+// Face pairs of the C3D10 tile order (no counterpart in the reference).  The
+// FP32 product evaluates the elements at positions 2j and 2j+1 in one thread; when
+// the two share a face, their three shared corners and three shared edge nodes are
+// loaded and accumulated once if they sit at fixed local positions: corners
+// (p, q, r) of the face at local 0, 1, 2 of the first element and at 1, 0, 2 of the
+// second (so local 0<->1, 1<->0, 2<->2 and edge nodes 4<->4, 5<->6, 6<->5), the
+// other corner last.  Both stay positively oriented: the first element is an even
+// permutation of its corners with the non-shared corner last, the second is
+// (q, p, r, t), which is even for a valid mesh (t lies on the other side of the
+// face); if it is not, the pair keeps its elements' own numbering.
+//   pairing: walking the tile order, every element not yet placed takes the first
+//   unplaced element sharing three corners with it among the next 16 positions;
+//   the pairs and the remaining single elements keep the order of their first
+//   element, and consecutive singles are put side by side.
+// Returns the new order and the connectivity of every position in the local
+// numbering used by the tiles (mid-edge nodes follow their corners).
+static const int TET_EDGES[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+
+static int tet_edge_of(int a, int b) {
+  for (int k = 0; k < 6; ++k)
+    if ((TET_EDGES[k][0] == a && TET_EDGES[k][1] == b) || (TET_EDGES[k][0] == b && TET_EDGES[k][1] == a)) return k;
+  return -1;
+}
+
+static bool even_perm(const int* p) {
+  int inv = 0;
+  for (int i = 0; i < 4; ++i)
+    for (int j = i + 1; j < 4; ++j) inv += p[i] > p[j];
+  return (inv & 1) == 0;
+}
+
+// new local corner i = old local corner pi[i]; writes the element's 10 nodes
+static void tet10_permuted(const int32_t* c, const int* pi, int32_t* out) {
+  for (int i = 0; i < 4; ++i) out[i] = c[pi[i]];
+  for (int k = 0; k < 6; ++k) out[4 + k] = c[4 + tet_edge_of(pi[TET_EDGES[k][0]], pi[TET_EDGES[k][1]])];
+}
+
+int host_tile_pairs(int64_t ne, const int32_t* conn, std::vector<int32_t>& order, std::vector<int32_t>& conn_tile) {
+  constexpr int W = 16;
+  std::vector<char> used(ne, 0);
+  std::vector<std::pair<int32_t, int32_t>> units;
+  units.reserve(ne);
+  auto shared = [&](int32_t e, int32_t f) {
+    int n = 0;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j) n += conn[e * 10 + i] == conn[f * 10 + j];
+    return n;
+  };
+  for (int64_t k = 0; k < ne; ++k) {
+    const int32_t e = order[k];
+    if (used[e]) continue;
+    used[e] = 1;
+    int32_t mate = -1;
+    for (int64_t m = k + 1; m < ne && m <= k + W; ++m) {
+      const int32_t f = order[m];
+      if (!used[f] && shared(e, f) == 3) {
+        mate = f;
+        break;
+      }
+    }
+    if (mate >= 0) used[mate] = 1;
+    units.push_back({e, mate});
+  }
+  order.clear();
+  conn_tile.assign((size_t)ne * 10, 0);
+  auto emit = [&](int32_t e, const int* pi) {
+    const int64_t p = (int64_t)order.size();
+    order.push_back(e);
+    if (pi) tet10_permuted(conn + (int64_t)e * 10, pi, conn_tile.data() + p * 10);
+    else memcpy(conn_tile.data() + p * 10, conn + (int64_t)e * 10, 10 * sizeof(int32_t));
+  };
+  int32_t pending = -1;
+  for (const auto& u : units) {
+    if (u.second < 0) {
+      if (pending < 0) {
+        pending = u.first;
+      } else {
+        emit(pending, nullptr);
+        emit(u.first, nullptr);
+        pending = -1;
+      }
+      continue;
+    }
+    const int32_t* ce = conn + (int64_t)u.first * 10;
+    const int32_t* cf = conn + (int64_t)u.second * 10;
+    int se = -1, tf = -1;                       // local index of the corner off the shared face
+    for (int i = 0; i < 4; ++i) {
+      bool in_f = false, in_e = false;
+      for (int j = 0; j < 4; ++j) {
+        in_f |= ce[i] == cf[j];
+        in_e |= cf[i] == ce[j];
+      }
+      if (!in_f) se = i;
+      if (!in_e) tf = i;
+    }
+    int pe[4] = {0, 1, 2, 3}, pf[4];
+    bool ok = false;
+    do {                                          // first even permutation (lexicographic) with se last
+      if (pe[3] == se && even_perm(pe)) { ok = true; break; }
+    } while (std::next_permutation(pe, pe + 4));
+    if (ok) {
+      const int32_t want[4] = {ce[pe[1]], ce[pe[0]], ce[pe[2]], cf[tf]};   // (q, p, r, t)
+      for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+          if (cf[j] == want[i]) pf[i] = j;
+      ok = even_perm(pf);
+    }
+    if (ok) {
+      emit(u.first, pe);
+      emit(u.second, pf);
+    } else {
+      emit(u.first, nullptr);
+      emit(u.second, nullptr);
+    }
+  }
+  if (pending >= 0) emit(pending, nullptr);
+  return EXFEM_OK;
+}
+
 // Element-tile maps of the matrix-free operator.  Tiles are `tile` consecutive
 // positions of the tile order (conn is given in that order), and slot
 // s = a*tile + p is local node a of the element at tile position p.  Per tile:

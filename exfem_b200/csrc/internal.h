@@ -39,6 +39,8 @@ struct exfem_block_s {
   int maxu = 0;                       // largest distinct-node count of a tile
   std::vector<int32_t> order_host;    // (ne) tile position -> element
   exfem::DevBuf<int32_t> tpos;        // (ne) element -> tile position
+  exfem::DevBuf<int32_t> order_dev;   // (ne) tile position -> element
+  exfem::DevBuf<int32_t> conn_tile;   // (ne, nnode) connectivity per position, in the tiles' local numbering
   exfem::DevBuf<int32_t> tile_ptr;    // (ntile+1)
   exfem::DevBuf<int32_t> tile_nodes;  // concatenated sorted node lists
   exfem::DevBuf<int32_t> tile_nodes_bc;  // same, node | fixed-DOF bits << 29

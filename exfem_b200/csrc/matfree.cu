@@ -367,6 +367,19 @@ __device__ __forceinline__ unsigned long long to_fixed(double x) { return (unsig
 __device__ __forceinline__ float from_fixed(int32_t i, float) { return __int2float_rn(i); }
 __device__ __forceinline__ double from_fixed(unsigned long long i, double) { return __ll2double_rn((long long)i); }
 
+// local node of the second element of a face pair that may hold the same node as
+// local node a of the first (and conversely: the map is an involution), -1 if
+// none.  C3D10 face pairs put the shared face's corners at (0,1,2) and (1,0,2),
+// so the shared edge nodes are 4<->4 (edge 01), 5<->6 (edges 12 and 20); the
+// kernel compares the two nodes before sharing anything.
+template <int ET>
+__host__ __device__ constexpr int pair_partner(int a) {
+  if constexpr (ET == EXFEM_C3D10)
+    return a == 0 ? 1 : a == 1 ? 0 : a == 2 ? 2 : a == 4 ? 4 : a == 5 ? 6 : a == 6 ? 5 : -1;
+  else
+    return -1;
+}
+
 template <class T, int ET, int TT, int LANES, bool ELAME>
 struct TileLayout {
   using Tr = ElemTraits<ET>;
@@ -513,17 +526,32 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     P f[NN][3];
     {
       P va[NN][3];
+      if constexpr (LANES == 2) {
 #pragma unroll
-      for (int a = 0; a < NN; ++a) {
-        if constexpr (LANES == 2) {
+        for (int a = 0; a < NN; ++a) {
           const uint32_t lp = reinterpret_cast<const uint32_t*>(li + a * TT)[tid];   // both slots in one load
           r0[a] = (lp & 0xFFFFu) * (L::RW * 4);
           r1[a] = (lp >> 16) * (L::RW * 4);
-          const T* x0 = reinterpret_cast<const T*>(rec + r0[a]);
-          const T* x1 = reinterpret_cast<const T*>(rec + r1[a]);
+        }
+        T x0[NN][3];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) va[a][c] = P(x0[c], x1[c]);
-        } else {
+        for (int a = 0; a < NN; ++a)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) x0[a][c] = reinterpret_cast<const T*>(rec + r0[a])[c];
+#pragma unroll
+        for (int b = 0; b < NN; ++b) {
+          // a node the pair shares (face pairs: fixed local partner) is loaded once
+          const int sb = pair_partner<ET>(b);
+          const bool sh = sb >= 0 && r1[b] == r0[sb >= 0 ? sb : 0];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const T x1 = sh ? x0[sb >= 0 ? sb : 0][c] : reinterpret_cast<const T*>(rec + r1[b])[c];
+            va[b][c] = P(x0[b][c], x1);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < NN; ++a) {
           r0[a] = li[a * TT + tid] * (L::RW * 4);
           const T* x0 = reinterpret_cast<const T*>(rec + r0[a]);
 #pragma unroll
@@ -578,18 +606,40 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
       e = max(e, B + std::numeric_limits<T>::min_exponent);          // keep q finite
     }
     const T q = bad ? T(1) : scalbn(T(1), B - e), iq = scalbn(T(1), e - B);
+    if constexpr (LANES == 2) {
+      P fq[NN][3];
 #pragma unroll
-    for (int a = 0; a < NN; ++a) {
-      I* a0 = reinterpret_cast<I*>(rec + r0[a] + L::ROFF);
+      for (int a = 0; a < NN; ++a)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        if constexpr (LANES == 2) {
-          const P fq = P(f[a][c] * P(q));
-          atomicAdd(a0 + c, to_fixed(fq.lo()));
-          atomicAdd(reinterpret_cast<I*>(rec + r1[a] + L::ROFF) + c, to_fixed(fq.hi()));
-        } else {
-          atomicAdd(a0 + c, to_fixed(f[a][c] * q));
+        for (int c = 0; c < 3; ++c) fq[a][c] = P(f[a][c] * P(q));
+      // the pair's shared nodes take one addition of both forces
+#pragma unroll
+      for (int a = 0; a < NN; ++a) {
+        const int sa = pair_partner<ET>(a);
+        const bool sh = sa >= 0 && r0[a] == r1[sa >= 0 ? sa : 0];
+        I* d0 = reinterpret_cast<I*>(rec + r0[a] + L::ROFF);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T w = sh ? fq[a][c].lo() + fq[sa >= 0 ? sa : 0][c].hi() : fq[a][c].lo();
+          atomicAdd(d0 + c, to_fixed(w));
         }
+      }
+#pragma unroll
+      for (int b = 0; b < NN; ++b) {
+        const int sb = pair_partner<ET>(b);
+        const bool sh = sb >= 0 && r1[b] == r0[sb >= 0 ? sb : 0];
+        if (!sh) {
+          I* d1 = reinterpret_cast<I*>(rec + r1[b] + L::ROFF);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) atomicAdd(d1 + c, to_fixed(fq[b][c].hi()));
+        }
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < NN; ++a) {
+        I* a0 = reinterpret_cast<I*>(rec + r0[a] + L::ROFF);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) atomicAdd(a0 + c, to_fixed(f[a][c] * q));
       }
     }
     __syncthreads();

@@ -95,6 +95,12 @@ class Block:
                                         perm.ctypes.data))
         return ptr_, nodes[:nl.value], nend[:nl.value], perm
 
+    def tile_conn(self):
+        """(ne, nnode) connectivity of every tile position in the tiles' numbering."""
+        out = np.empty((max(self.ne, 1), self.etype.nnode), np.int32)
+        check(lib.exfem_block_tile_conn(self._h, out.ctypes.data))
+        return out[:self.ne]
+
     def tile_order(self):
         """(tile, order): elements per tile and the tile order (position -> element)."""
         tile = C.c_int()

@@ -109,6 +109,10 @@ int exfem_block_tile_info(exfem_block b, int64_t* ntile, int64_t* nlist, int* ma
 int exfem_block_tile_maps(exfem_block b, int32_t* ptr_host, int32_t* nodes_host, uint16_t* nend_host,
                           uint16_t* perm_host);
 int exfem_block_tile_order(exfem_block b, int* tile, int32_t* order_host);
+/* connectivity of every tile position (ne, nnode) in the local numbering the
+ * tiles use: linear-elastic C3D10 blocks renumber face-sharing pairs (see
+ * exfem_host_tile_pairs), other blocks keep each element's own numbering. */
+int exfem_block_tile_conn(exfem_block b, int32_t* conn_tile_host);
 /* elements per matrix-free tile (128 or 256) for blocks of element type etype
  * created after the call, process-wide; chosen by the autotuner
  * (exfem_b200.tuning).  No counterpart in the reference. */
@@ -286,6 +290,12 @@ int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t
  * order (ne,) position -> element.  No counterpart in the reference. */
 int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X,
                           const int32_t* conn, int32_t* order);
+/* face pairs of a C3D10 tile order (linear-elastic blocks): order (ne,) in/out,
+ * conn_tile (ne, 10) out.  Elements sharing a face are put at positions 2j, 2j+1
+ * with the face's corners (p, q, r) at local 0, 1, 2 of the first and 1, 0, 2 of
+ * the second (both positively oriented), so the product loads and adds their six
+ * shared nodes once.  No counterpart in the reference. */
+int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile);
 
 #ifdef __cplusplus
 }

@@ -445,6 +445,87 @@ def tile_order(X, conn, ncorner):
     return np.lexsort((np.arange(ne), key, comp)).astype(np.int32)
 
 
+_TET_EDGES = ((0, 1), (1, 2), (2, 0), (0, 3), (1, 3), (2, 3))
+
+
+def _even(p):
+    return sum(p[i] > p[j] for i in range(4) for j in range(i + 1, 4)) % 2 == 0
+
+
+def _tet10_permuted(c, pi):
+    out = [c[pi[i]] for i in range(4)]
+    for a, b in _TET_EDGES:
+        k = next(k for k, (x, y) in enumerate(_TET_EDGES) if {x, y} == {pi[a], pi[b]})
+        out.append(c[4 + k])
+    return out
+
+
+def tile_pairs(order, conn, window=16):
+    """Face pairs of a C3D10 tile order (no counterpart in the reference).  Walking
+    the order, each element not yet placed takes the first unplaced element among
+    the next `window` positions that shares three corners with it; pairs and the
+    remaining singles keep the order of their first element and consecutive singles
+    go side by side.  A pair (e, f) sharing face corners p, q, r gets local corners
+    (p, q, r, s) for e -- the first even permutation (lexicographic) of e's corners
+    with its off-face corner s last -- and (q, p, r, t) for f when that is an even
+    permutation of f's corners (else both keep their numbering); mid-edge nodes
+    follow their corners.  Returns (order, conn_tile)."""
+    import itertools
+    conn = np.asarray(conn, dtype=np.int64)
+    order = [int(e) for e in order]
+    ne = len(order)
+    used = np.zeros(conn.shape[0], bool)
+    units = []
+    for k, e in enumerate(order):
+        if used[e]:
+            continue
+        used[e] = True
+        mate = -1
+        for m in range(k + 1, min(ne, k + window + 1)):
+            f = order[m]
+            if not used[f] and len(set(conn[e, :4]) & set(conn[f, :4])) == 3:
+                mate = f
+                break
+        if mate >= 0:
+            used[mate] = True
+        units.append((e, mate))
+    out_o, out_c = [], []
+
+    def emit(e, pi=None):
+        out_o.append(e)
+        out_c.append(list(conn[e]) if pi is None else _tet10_permuted(list(conn[e]), pi))
+
+    pending = -1
+    for e, f in units:
+        if f < 0:
+            if pending < 0:
+                pending = e
+            else:
+                emit(pending)
+                emit(e)
+                pending = -1
+            continue
+        ce, cf = list(conn[e, :4]), list(conn[f, :4])
+        se = next(i for i in range(4) if ce[i] not in cf)
+        tf = next(i for i in range(4) if cf[i] not in ce)
+        pe = next((list(p) for p in itertools.permutations(range(4)) if p[3] == se and _even(p)), None)
+        pf = None
+        if pe is not None:
+            want = [ce[pe[1]], ce[pe[0]], ce[pe[2]], cf[tf]]
+            pf = [cf.index(w) for w in want]
+            if not _even(pf):
+                pf = None
+        if pf is not None:
+            emit(e, pe)
+            emit(f, pf)
+        else:
+            emit(e)
+            emit(f)
+    if pending >= 0:
+        emit(pending)
+    return np.asarray(out_o, np.int32), np.asarray(out_c, np.int32).reshape(-1, conn.shape[1])
+
+
 def tile_maps(conn, tile):
     """Element-tile maps used by the matrix-free product (no counterpart in the
     reference), for conn given in tile order.  Positions [t*tile, (t+1)*tile) form

@@ -106,6 +106,30 @@ def test_host_tile_order_bit_exact(kind):
         np.testing.assert_array_equal(np.sort(order[n1:n1 + n2]), np.arange(n1, n1 + n2))
 
 
+def test_host_tile_pairs_bit_exact_and_oriented():
+    """Face pairs of the C3D10 tile order equal the oracle's restatement; paired
+    elements share their face at local corners (0,1,2) <-> (1,0,2), every element
+    keeps its node set and stays positively oriented, and mid-nodes follow corners."""
+    X, c = tet10_box(1, 1, 1, 4, 3, 3)
+    order = _host_order(X, c, 4)
+    o, ct = order.copy(), np.empty_like(c, dtype=np.int32)
+    c32 = np.ascontiguousarray(c, dtype=np.int32)
+    assert _lib.lib.exfem_host_tile_pairs(len(c), c32.ctypes.data, o.ctypes.data, ct.ctypes.data) == 0
+    wo, wc = fem.tile_pairs(order, c)
+    np.testing.assert_array_equal(o, wo)
+    np.testing.assert_array_equal(ct, wc)
+    np.testing.assert_array_equal(np.sort(o), np.arange(len(c)))
+    for p, e in enumerate(o):
+        assert sorted(ct[p]) == sorted(c[e])
+        x = X[ct[p, :4]]
+        assert np.linalg.det(np.stack([x[1] - x[0], x[2] - x[0], x[3] - x[0]])) > 0
+        for k, (a, b) in enumerate([(0, 1), (1, 2), (2, 0), (0, 3), (1, 3), (2, 3)]):
+            np.testing.assert_allclose(X[ct[p, 4 + k]], 0.5 * (X[ct[p, a]] + X[ct[p, b]]), atol=1e-12)
+    paired = sum(ct[2 * j, 0] == ct[2 * j + 1, 1] and ct[2 * j, 1] == ct[2 * j + 1, 0] and ct[2 * j, 2] == ct[2 * j + 1, 2]
+                 for j in range(len(c) // 2))
+    assert paired >= 0.9 * (len(c) // 2)          # Kuhn tets pair up almost completely
+
+
 def test_host_gather_plan_rejects_bad_connectivity():
     c = np.array([[0, 1, 2, 3, 4, 5, 6, 99]], np.int32)
     vmax = C.c_int()

@@ -140,8 +140,13 @@ def test_index_maps_bit_exact(cuda, kind):
     np.testing.assert_array_equal(pmod.gather(), ofem.gather_plan([c], len(X)))
     np.testing.assert_array_equal(pmod.blocks[0].colours(), ofem.greedy_colouring(c, len(X)))
     tile, order = pmod.blocks[0].tile_order()
-    np.testing.assert_array_equal(order, ofem.tile_order(X, c, 8 if kind == "hex" else 4))
-    for got, want in zip(pmod.blocks[0].tile_maps(), ofem.tile_maps(np.asarray(c)[order], tile)):
+    want_order = ofem.tile_order(X, c, 8 if kind == "hex" else 4)
+    want_conn = np.asarray(c)[want_order]
+    if kind == "tet":                               # linear-elastic C3D10: face pairs
+        want_order, want_conn = ofem.tile_pairs(want_order, c)
+    np.testing.assert_array_equal(order, want_order)
+    np.testing.assert_array_equal(pmod.blocks[0].tile_conn(), want_conn)
+    for got, want in zip(pmod.blocks[0].tile_maps(), ofem.tile_maps(want_conn, tile)):
         np.testing.assert_array_equal(got, want)
 
 
