@@ -245,7 +245,7 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
       if ((s = b->multi_ptr.upload(mptr.data(), mptr.size()))) return s;
       if ((s = b->tile_dest.upload(dest.data(), dest.size()))) return s;
       if ((s = b->tile_dest_bc.upload(dest.data(), dest.size()))) return s;
-      if ((s = b->partial.alloc(std::max<size_t>(3 * (size_t)mptr.back(), 1)))) return s;
+      if ((s = b->partial.alloc(std::max<size_t>(4 * (size_t)mptr.back(), 4)))) return s;   // (x, y, z, 0) per entry
     }
     if ((s = b->dev_err.alloc(1))) return s;
     EX_CUDA(cudaMemset(b->dev_err.p, 0, sizeof(int)));

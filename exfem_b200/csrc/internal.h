@@ -56,7 +56,7 @@ struct exfem_block_s {
   exfem::DevBuf<int32_t> multi_nodes_bc;  // same, fixed-DOF bits at 28-30
   std::vector<int32_t> multi_nodes_host;
   exfem::DevBuf<int32_t> multi_ptr;   // (nmulti+1) their runs of partials
-  exfem::DevBuf<double> partial;      // per-entry tile sums, 3 per entry (FP64 or FP32 view)
+  exfem::DevBuf<double> partial;      // per-entry tile sums, (x, y, z, 0) per entry (FP64 or FP32 view)
   exfem::DevBuf<int> dev_err;         // set by bounded waits that give up
   int geo_stride = 0;                 // per-element geometry entries (without the Lame pair when uniform)
   exfem::DevBuf<double> geo64;        // tile-major (ntile, geo_stride, tile)

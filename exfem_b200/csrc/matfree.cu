@@ -650,15 +650,19 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     const T nan = std::numeric_limits<T>::quiet_NaN();
     for (int k = tid; k < nu; k += NT) {
       I* a = sums(k);
-      const int32_t d = td[k];
-      const bool direct = d < 0;
-      const int64_t n3 = 3 * (int64_t)(d & 0x0FFFFFFF);
-      T* p = direct ? y + n3 : part + 3 * (int64_t)d;
+      T r[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const T r = bad ? nan : from_fixed(a[c], T(0)) * iq;
+        r[c] = bad ? nan : from_fixed(a[c], T(0)) * iq;
         a[c] = I(0);
-        p[c] = (direct && (((uint32_t)d >> (28 + c)) & 1u)) ? v[n3 + c] : r;
+      }
+      const int32_t d = td[k];
+      if (d < 0) {
+        const int64_t n3 = 3 * (int64_t)(d & 0x0FFFFFFF);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[n3 + c] = (((uint32_t)d >> (28 + c)) & 1u) ? v[n3 + c] : r[c];
+      } else {
+        reinterpret_cast<Node4<T>*>(part)[d] = Node4<T>{r[0], r[1], r[2], T(0)};   // one 16-byte entry
       }
     }
     __syncthreads();
@@ -667,8 +671,8 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
 }
 
 // pass 2 over the nodes not listed by exactly one tile (ids with fixed-DOF bits
-// at 28-30): y[3n+c] = fixed ? v : sum of node n's partials (a contiguous run, tile
-// order).  Each thread takes U nodes a grid stride apart, so that their loads are
+// at 28-30): y[3n+c] = fixed ? v : sum of node n's partials (a contiguous run of
+// (x, y, z, 0) entries, tile order).  Each thread takes U nodes a grid stride apart, so that their loads are
 // in flight together.
 template <class T>
 __global__ void mf_gather_kernel(int64_t nm, const int32_t* __restrict__ mnodes, const int32_t* __restrict__ mptr,
@@ -692,10 +696,10 @@ __global__ void mf_gather_kernel(int64_t nm, const int32_t* __restrict__ mnodes,
       if (i0 + u * stride >= nm) break;
       T s0 = T(0), s1 = T(0), s2 = T(0);
       for (int32_t q = q0[u]; q < q1[u]; ++q) {
-        const T* p = part + 3 * (int64_t)q;
-        s0 += p[0];
-        s1 += p[1];
-        s2 += p[2];
+        const Node4<T> w = reinterpret_cast<const Node4<T>*>(part)[q];
+        s0 += w.x;
+        s1 += w.y;
+        s2 += w.z;
       }
       const int64_t d = 3 * (int64_t)(id[u] & 0x0FFFFFFFu);
       const uint32_t bits = id[u] >> 28;
