@@ -87,29 +87,36 @@ struct TcShape {
 }  // namespace
 
 // ys[(e*nd + i)*nrhs + r] = sum_j Ke[e, i, j] * bf16(free * V)[dof(e, j), r]
-template <int ET>
+//
+// Two-stage pipeline per CTA over its groups (stage s = group parity): while the
+// tensor cores run group i out of shared-memory stage s into tensor-memory columns
+// 16 s .. 16 s + 15, the CTA waits for group i-1's MMAs, starts the asynchronous
+// copies of group i+1's Ke into the other stage, loads group i+1's nodal values
+// into registers, and reads group i-1's products out of tensor memory.
+template <int ET, int NR>
 __global__ void __launch_bounds__(128)
 ebe_tc_kernel(int64_t ne, const int32_t* __restrict__ conn, const __nv_bfloat16* __restrict__ Ke,
-              const float* __restrict__ V, const uint8_t* __restrict__ fixed, int nrhs, float* __restrict__ ys,
+              const float* __restrict__ V, const uint8_t* __restrict__ fixed, float* __restrict__ ys,
               int* __restrict__ err) {
   using S = TcShape<ET>;
   constexpr int NN = S::NN, ND = S::ND, NDP = S::NDP, G = S::G;
+  constexpr int nrhs = NR;
+  constexpr int STAGE = A_BYTES + B_BYTES;
+  constexpr int VPT = (G * ND * NR + 127) / 128;      // prefetched nodal values per thread
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  // 1024-byte aligned operands
   unsigned char* base = smem_raw + ((1024 - (smem_addr(smem_raw) & 1023)) & 1023);
-  unsigned char* As = base;
-  unsigned char* Bs = base + A_BYTES;
-  __shared__ __align__(8) uint64_t mma_bar;
+  auto As = [&](int s) { return base + s * STAGE; };
+  auto Bs = [&](int s) { return base + s * STAGE + A_BYTES; };
+  __shared__ __align__(8) uint64_t mma_bar[2];
   __shared__ uint32_t tmem_base_s;
-  __shared__ int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int64_t ngroup = (ne + G - 1) / G;
 
-  for (int k = tid; k < (int)((A_BYTES + B_BYTES) / 16); k += 128) reinterpret_cast<uint4*>(base)[k] = make_uint4(0, 0, 0, 0);
+  for (int k = tid; k < 2 * STAGE / 16; k += 128) reinterpret_cast<uint4*>(base)[k] = make_uint4(0, 0, 0, 0);
   if (tid == 0) {
-    bar_init(&mma_bar, 1);
+    bar_init(&mma_bar[0], 1);
+    bar_init(&mma_bar[1], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_fail = 0;
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_base_s)),
@@ -120,84 +127,167 @@ ebe_tc_kernel(int64_t ne, const int32_t* __restrict__ conn, const __nv_bfloat16*
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_base_s;
+  bool failed = false;                                // CTA-uniform: a bounded wait gave up
 
-  uint32_t phase = 0;
-  for (int64_t grp = blockIdx.x; grp < ngroup; grp += gridDim.x) {
+  // Ke of a group into stage s: asynchronous 16-byte copies where the element rows
+  // allow (C3D8: 48-byte rows), 4-byte copies otherwise; rows past the mesh are zero
+  auto fill_a = [&](int64_t grp, int s) {
     const int64_t e0 = grp * G;
-    // A: the group's element matrices on the diagonal (pairs of BF16)
-    for (int q = tid; q < G * ND * (ND / 2); q += 128) {
-      const int g = q / (ND * (ND / 2));
-      const int rem = q - g * (ND * (ND / 2));
-      const int i = rem / (ND / 2), j = 2 * (rem - i * (ND / 2));
-      const int64_t e = e0 + g;
-      uint32_t w = 0;
-      if (e < ne) w = *reinterpret_cast<const uint32_t*>(Ke + (e * ND + i) * ND + j);
-      *reinterpret_cast<uint32_t*>(As + kmajor_off(g * NDP + i, g * NDP + j, TC_M)) = w;
-    }
-    // B: nodal values of the group (prescribed DOFs zero), BF16, right-hand sides as columns
-    for (int q = tid; q < G * ND * nrhs; q += 128) {
-      const int g = q / (ND * nrhs);
-      const int rem = q - g * (ND * nrhs);
-      const int i = rem / nrhs, r = rem - i * nrhs;
-      const int64_t e = e0 + g;
-      float x = 0.0f;
-      if (e < ne) {
-        const int64_t d = 3 * (int64_t)conn[e * NN + i / 3] + i % 3;
-        if (!(fixed && fixed[d])) x = V[d * nrhs + r];
+    unsigned char* A = As(s);
+    if constexpr ((ND * 2) % 16 == 0) {
+      constexpr int CH = ND * 2 / 16;                 // 16-byte chunks per row
+      for (int q = tid; q < G * ND * CH; q += 128) {
+        const int g = q / (ND * CH), rem = q - g * (ND * CH), i = rem / CH, j = 8 * (rem - i * CH);
+        const int64_t e = e0 + g;
+        const uint32_t dst = smem_addr(A + kmajor_off(g * NDP + i, g * NDP + j, TC_M));
+        const __nv_bfloat16* src = Ke + ((e < ne ? e : 0) * ND + i) * ND + j;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(e < ne ? 16 : 0)
+                     : "memory");
       }
-      *reinterpret_cast<__nv_bfloat16*>(Bs + kmajor_off(r, g * NDP + i, TC_N)) = __float2bfloat16_rn(x);
+    } else {
+      for (int q = tid; q < G * ND * (ND / 2); q += 128) {
+        const int g = q / (ND * (ND / 2)), rem = q - g * (ND * (ND / 2)), i = rem / (ND / 2);
+        const int j = 2 * (rem - i * (ND / 2));
+        const int64_t e = e0 + g;
+        const uint32_t dst = smem_addr(A + kmajor_off(g * NDP + i, g * NDP + j, TC_M));
+        const __nv_bfloat16* src = Ke + ((e < ne ? e : 0) * ND + i) * ND + j;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(e < ne ? 4 : 0)
+                     : "memory");
+      }
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");      // generic stores -> tensor-core reads
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_addr(As), b0 = smem_addr(Bs);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // nodal values of a group (prescribed DOFs zero) into registers
+  float vr[VPT];
+  // (all node ids first, then every value and mask load in flight together; the
+  // mask is applied with a select so that no load waits for another's result)
+  auto load_v = [&](int64_t grp) {
+    const int64_t e0 = grp * G;
+    int64_t dv[VPT];
 #pragma unroll
-      for (int s = 0; s < TC_K / 16; ++s) {
-        const uint64_t ad = smem_desc(a0 + s * 2 * A_LBO, A_LBO, A_SBO);
-        const uint64_t bd = smem_desc(b0 + s * 2 * B_LBO, B_LBO, B_SBO);
-        const uint32_t acc = s > 0 ? 1u : 0u;
-        asm volatile(
-            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(tmem),
-            "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u)
-            : "memory");
+    for (int u = 0; u < VPT; ++u) {
+      const int q = tid + 128 * u;
+      dv[u] = -1;
+      if (q < G * ND * nrhs) {
+        const int g = q / (ND * nrhs), rem = q - g * (ND * nrhs), i = rem / nrhs, r = rem - i * nrhs;
+        const int64_t e = e0 + g;
+        if (e < ne) dv[u] = (3 * (int64_t)__ldg(conn + e * NN + i / 3) + i % 3) * nrhs + r;
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_addr(&mma_bar))
-                   : "memory");
     }
-    const bool ok = bar_wait(&mma_bar, phase);
-    if (ok) phase ^= 1u;
-    else s_fail = 1;
-    __syncthreads();
-    if (s_fail) break;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // warp w reads lanes 32w .. 32w+31 (rows of D), 16 columns
+#pragma unroll
+    for (int u = 0; u < VPT; ++u) {
+      const int64_t k = dv[u] < 0 ? 0 : dv[u];
+      const float x = __ldg(V + k);
+      const bool off = dv[u] < 0 || (fixed && __ldg(fixed + k / nrhs));
+      vr[u] = off ? 0.0f : x;
+    }
+  };
+  auto store_b = [&](int s) {
+    unsigned char* B = Bs(s);
+#pragma unroll
+    for (int u = 0; u < VPT; ++u) {
+      const int q = tid + 128 * u;
+      if (q < G * ND * nrhs) {
+        const int g = q / (ND * nrhs), rem = q - g * (ND * nrhs), i = rem / nrhs, r = rem - i * nrhs;
+        *reinterpret_cast<__nv_bfloat16*>(B + kmajor_off(r, g * NDP + i, TC_N)) = __float2bfloat16_rn(vr[u]);
+      }
+    }
+  };
+  auto epilogue = [&](int64_t grp, int s) {
     uint32_t d[16];
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
         "%15}, [%16];"
         : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
           "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
-        : "r"(tmem + ((uint32_t)(32 * warp) << 16)));
+        : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(TC_N * s)));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     const int row = 32 * warp + lane;
     const int g = row / NDP, i = row - g * NDP;
-    const int64_t e = e0 + g;
+    const int64_t e = grp * G + g;
     if (g < G && i < ND && e < ne) {
       float* out = ys + (e * ND + i) * nrhs;
+      if ((nrhs & 3) == 0) {
 #pragma unroll
-      for (int r = 0; r < TC_N; ++r)
-        if (r < nrhs) out[r] = __uint_as_float(d[r]);
+        for (int r = 0; r < TC_N; r += 4)
+          if (r < nrhs)
+            *reinterpret_cast<float4*>(out + r) = make_float4(__uint_as_float(d[r]), __uint_as_float(d[r + 1]),
+                                                              __uint_as_float(d[r + 2]), __uint_as_float(d[r + 3]));
+      } else {
+#pragma unroll
+        for (int r = 0; r < TC_N; ++r)
+          if (r < nrhs) out[r] = __uint_as_float(d[r]);
+      }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();                                   // D read and operands consumed before the next group
+  };
+
+  const int64_t g0 = blockIdx.x, gs = gridDim.x;
+  if (g0 < ngroup) {
+    fill_a(g0, 0);
+    load_v(g0);
   }
-  if (s_fail && tid == 0) {
-    atomicExch(err, 1);
-    bar_wait(&mma_bar, phase);                          // let the MMAs in flight finish (bounded)
+  int it = 0;
+  for (int64_t grp = g0; grp < ngroup; grp += gs, ++it) {
+    const int s = it & 1;
+    // 1. this group's operands are in stage s
+    store_b(s);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic / async-copy stores -> tensor-core reads
+    __syncthreads();
+    // 2. its MMAs into tensor-memory columns 16 s ..
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_addr(As(s)), b0 = smem_addr(Bs(s));
+#pragma unroll
+      for (int k = 0; k < TC_K / 16; ++k) {
+        const uint64_t ad = smem_desc(a0 + k * 2 * A_LBO, A_LBO, A_SBO);
+        const uint64_t bd = smem_desc(b0 + k * 2 * B_LBO, B_LBO, B_SBO);
+        const uint32_t acc = k > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}\n" ::"r"(
+                tmem + (uint32_t)(TC_N * s)),
+            "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc), "r"(0u)
+            : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_addr(&mma_bar[s]))
+                   : "memory");
+    }
+    // 3. the previous group's MMAs have finished: its stage and columns are free
+    if (it > 0) {
+      const bool ok = bar_wait(&mma_bar[s ^ 1], (uint32_t)(((it - 1) >> 1) & 1));
+      if (__syncthreads_or(!ok)) {
+        failed = true;
+        ++it;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    // 4. the next group's Ke and nodal values start coming in
+    const int64_t nxt = grp + gs;
+    if (nxt < ngroup) {
+      fill_a(nxt, s ^ 1);
+      load_v(nxt);
+    }
+    // 5. the previous group's products out of tensor memory
+    if (it > 0) epilogue(grp - gs, s ^ 1);
   }
+  // the last group
+  if (it > 0 && !failed) {
+    const int s = (it - 1) & 1;
+    const bool ok = bar_wait(&mma_bar[s], (uint32_t)(((it - 1) >> 1) & 1));
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+    } else {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      epilogue(g0 + (int64_t)(it - 1) * gs, s);
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncthreads();
+  if (failed && tid == 0) atomicExch(err, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
@@ -206,15 +296,45 @@ ebe_tc_kernel(int64_t ne, const int32_t* __restrict__ conn, const __nv_bfloat16*
   }
 }
 
-// y[3n+c, r] = fixed ? v : sum over node n's gather-plan slots of the element rows
+// y[3n+c, r] = fixed ? v : sum over node n's gather-plan slots of the element rows;
+// one thread per node and group of four right-hand sides (16-byte loads and stores)
+// when nrhs is a multiple of 4, else per node and right-hand side
 __global__ void gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32_t* __restrict__ plan,
                                     int64_t sentinel, const float* __restrict__ ys, const uint8_t* __restrict__ fixed,
                                     const float* __restrict__ V, int nrhs, float* __restrict__ Y) {
+  const int nd = 3 * nnode;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if ((nrhs & 3) == 0) {
+    const int nq = nrhs >> 2;
+    if (t >= nn * nq) return;
+    const int64_t n = t / nq;
+    const int r4 = (int)(t - n * nq) * 4;
+    float4 s[3] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0)};
+    for (int k = 0; k < vmax; ++k) {
+      const int64_t slot = plan[n * vmax + k];
+      if (slot == sentinel) break;
+      const int64_t e = slot / nnode;
+      const int a = (int)(slot - e * nnode);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float4 w = *reinterpret_cast<const float4*>(ys + (e * nd + 3 * a + c) * nrhs + r4);
+        s[c].x += w.x;
+        s[c].y += w.y;
+        s[c].z += w.z;
+        s[c].w += w.w;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const int64_t d = 3 * n + c;
+      float4* out = reinterpret_cast<float4*>(Y + d * nrhs + r4);
+      *out = (fixed && fixed[d]) ? *reinterpret_cast<const float4*>(V + d * nrhs + r4) : s[c];
+    }
+    return;
+  }
   if (t >= nn * nrhs) return;
   const int64_t n = t / nrhs;
   const int r = (int)(t - n * nrhs);
-  const int nd = 3 * nnode;
   float s[3] = {0.f, 0.f, 0.f};
   for (int k = 0; k < vmax; ++k) {
     const int64_t slot = plan[n * vmax + k];
@@ -231,6 +351,34 @@ __global__ void gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32
   }
 }
 
+template <int ET>
+static int tc_launch(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, const float* V, const uint8_t* fx,
+                     cudaStream_t s) {
+  const size_t smem = 2 * (A_BYTES + B_BYTES) + 1024;
+  int dev, nsm;
+  EX_CUDA(cudaGetDevice(&dev));
+  EX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int64_t ng = (b->ne + TcShape<ET>::G - 1) / TcShape<ET>::G;
+  const unsigned grid = (unsigned)std::min<int64_t>(ng, (int64_t)nsm * 3);
+  auto go = [&](auto kern) -> int {
+    EX_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<grid, 128, smem, s>>>(b->ne, b->conn.p, Ke, V, fx, b->ys_tc.p, b->dev_err.p);
+    EX_LAUNCH_CHECK();
+    return EXFEM_OK;
+  };
+  switch (nrhs) {
+    case 1: return go(ebe_tc_kernel<ET, 1>);
+    case 2: return go(ebe_tc_kernel<ET, 2>);
+    case 3: return go(ebe_tc_kernel<ET, 3>);
+    case 4: return go(ebe_tc_kernel<ET, 4>);
+    case 8: return go(ebe_tc_kernel<ET, 8>);
+    case 16: return go(ebe_tc_kernel<ET, 16>);
+    default:
+      set_error("the tensor-core stored-Ke product takes 1, 2, 3, 4, 8 or 16 right-hand sides, got %d", nrhs);
+      return EXFEM_ERR_ARG;
+  }
+}
+
 int launch_ebe_matvec_tc(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, const float* V, float* Y,
                          cudaStream_t s, bool bc) {
   if (nrhs < 1 || nrhs > TC_N) {
@@ -241,25 +389,12 @@ int launch_ebe_matvec_tc(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, co
   const size_t need = (size_t)b->ne * b->nd * nrhs;
   if (b->ys_tc.n < need && (st = b->ys_tc.alloc(need))) return st;
   if (b->ne) {
-    const size_t smem = A_BYTES + B_BYTES + 1024;
-    int dev, nsm;
-    EX_CUDA(cudaGetDevice(&dev));
-    EX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const uint8_t* fx = bc ? b->fixed.p : nullptr;
-    if (b->etype == EXFEM_C3D8) {
-      EX_CUDA(cudaFuncSetAttribute(ebe_tc_kernel<EXFEM_C3D8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      const int64_t ng = (b->ne + TcShape<EXFEM_C3D8>::G - 1) / TcShape<EXFEM_C3D8>::G;
-      const unsigned grid = (unsigned)std::min<int64_t>(ng, (int64_t)nsm * 4);
-      ebe_tc_kernel<EXFEM_C3D8><<<grid, 128, smem, s>>>(b->ne, b->conn.p, Ke, V, fx, nrhs, b->ys_tc.p, b->dev_err.p);
-    } else {
-      EX_CUDA(cudaFuncSetAttribute(ebe_tc_kernel<EXFEM_C3D10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      const int64_t ng = (b->ne + TcShape<EXFEM_C3D10>::G - 1) / TcShape<EXFEM_C3D10>::G;
-      const unsigned grid = (unsigned)std::min<int64_t>(ng, (int64_t)nsm * 4);
-      ebe_tc_kernel<EXFEM_C3D10><<<grid, 128, smem, s>>>(b->ne, b->conn.p, Ke, V, fx, nrhs, b->ys_tc.p, b->dev_err.p);
-    }
-    EX_LAUNCH_CHECK();
+    const int st = b->etype == EXFEM_C3D8 ? tc_launch<EXFEM_C3D8>(b, Ke, nrhs, V, fx, s)
+                                          : tc_launch<EXFEM_C3D10>(b, Ke, nrhs, V, fx, s);
+    if (st) return st;
   }
-  const int64_t work = b->nn * nrhs;
+  const int64_t work = (nrhs & 3) == 0 ? b->nn * (nrhs / 4) : b->nn * nrhs;
   if (work) {
     gather_multi_kernel<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(
         b->nn, b->vmax, b->nnode, b->plan.p, b->ne * b->nnode, b->ys_tc.p, bc ? b->fixed.p : nullptr, V, nrhs, Y);

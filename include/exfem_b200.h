@@ -159,7 +159,7 @@ int exfem_tangent_diagonal(exfem_block b, double* diag, void* stream);
  * gather_matvec within opA, gfem/solvers.py:257-267), else y = K v
  * (gfem/model.py:162-166 ops_matvec). */
 int exfem_ebe_matvec(exfem_block b, const double* Ke, const double* v, double* y, int apply_bc, void* stream);
-/* stored-Ke product for nrhs (1..16) right-hand sides at once on the tensor cores:
+/* stored-Ke product for nrhs (1, 2, 3, 4, 8 or 16) right-hand sides at once on the tensor cores:
  * Ke (ne, nd, nd) BF16 as written by exfem_element_stiffness with EXFEM_BF16, V and
  * Y (ndof, nrhs) FP32 with the right-hand sides fastest; V is rounded to BF16 and
  * the products accumulate in FP32 (tcgen05.mma).  apply_bc as exfem_ebe_matvec.
