@@ -95,6 +95,8 @@ _SIGS = {
     "exfem_host_standard_aggregation": ([I64, P, P, P, C.POINTER(I64)], C.c_int),
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
     "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
+    "exfem_block_status": ([VP, VP], C.c_int),
+    "exfem_selftest_bounded_wait": ([I32, VP], C.c_int),
     "exfem_block_tile_conn": ([VP, P], C.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():

@@ -40,6 +40,20 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
 int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st);
 int solver_alloc(exfem_solver_s* S);
 
+// a bounded wait inside one of the block's kernels gave up (a copy or a tensor-core
+// operation that did not complete): report it once and clear the flag
+int block_wait_status(exfem_block_s* b, cudaStream_t s) {
+  if (!b->dev_err.p) return EXFEM_OK;
+  int h = 0;
+  EX_CUDA(cudaMemcpyAsync(&h, b->dev_err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  EX_CUDA(cudaStreamSynchronize(s));
+  if (!h) return EXFEM_OK;
+  EX_CUDA(cudaMemsetAsync(b->dev_err.p, 0, sizeof(int), s));
+  set_error("a bounded device wait gave up (an asynchronous copy or tensor-core operation did not complete); "
+            "the results of the call are invalid");
+  return EXFEM_ERR_TIMEOUT;
+}
+
 static int set_material(exfem_block_s* b, const exfem_material* m) {
   EX_ARG(m, "material is NULL");
   EX_ARG(m->kind == EXFEM_LINEAR_ELASTIC || m->kind == EXFEM_J2, "unknown material kind %d", m->kind);
@@ -652,7 +666,10 @@ int exfem_solver_pcg(exfem_solver s, const double* b, double* x, double tol, int
   StreamGuard g;
   int st;
   if ((st = g.init(stream))) return st;
-  return solver_pcg(s, b, x, tol, maxiter, iters, relres, g.work);
+  const int r = solver_pcg(s, b, x, tol, maxiter, iters, relres, g.work);
+  if (r < 0) return r;
+  const int w = block_wait_status(s->blk, g.work);
+  return w < 0 ? w : r;
 }
 
 int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, double inner_tol, int max_pass,
@@ -662,7 +679,37 @@ int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, d
   StreamGuard g;
   int st;
   if ((st = g.init(stream))) return st;
-  return solver_mixed(s, b, x, tol, inner_tol, max_pass, maxiter, iters, passes, relres, g.work);
+  const int r = solver_mixed(s, b, x, tol, inner_tol, max_pass, maxiter, iters, passes, relres, g.work);
+  if (r < 0) return r;
+  const int w = block_wait_status(s->blk, g.work);
+  return w < 0 ? w : r;
+}
+
+int exfem_block_status(exfem_block b, void* stream) {
+  EX_ARG(b, "block is NULL");
+  StreamGuard g;
+  int st;
+  if ((st = g.init(stream))) return st;
+  return block_wait_status(b, g.work);
+}
+
+int exfem_selftest_bounded_wait(int polls, void* stream) {
+  EX_ARG(polls > 0, "polls must be positive");
+  DevBuf<int> flag;
+  int s;
+  if ((s = flag.alloc(1))) return s;
+  StreamGuard g;
+  if ((s = g.init(stream))) return s;
+  EX_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), g.work));
+  if ((s = launch_wait_selftest(polls, flag.p, g.work))) return s;
+  int h = 0;
+  EX_CUDA(cudaMemcpyAsync(&h, flag.p, sizeof(int), cudaMemcpyDeviceToHost, g.work));
+  EX_CUDA(cudaStreamSynchronize(g.work));
+  if (h) {
+    set_error("bounded wait gave up after %d polls (expected: nothing arrives in the self-test)", polls);
+    return EXFEM_ERR_TIMEOUT;
+  }
+  return EXFEM_OK;
 }
 
 // ---------------------------------------------------------------- host builders

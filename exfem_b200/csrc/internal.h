@@ -101,6 +101,10 @@ int launch_ebe_diagonal(exfem_block_s* b, const double* Ke, double* diag, cudaSt
 template <class T>
 int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaStream_t s, bool bc = true);
 int launch_mf_diagonal(exfem_block_s* b, double* diag, cudaStream_t s);
+// bounded device waits: read and clear a block's wait-failure flag (capi.cu); a
+// kernel whose only wait can never complete (matfree.cu)
+int block_wait_status(exfem_block_s* b, cudaStream_t s);
+int launch_wait_selftest(int polls, int* err, cudaStream_t s);
 // stored-Ke product for several right-hand sides on the tensor cores (ebe_tc.cu)
 int launch_ebe_matvec_tc(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, const float* V, float* Y,
                          cudaStream_t s, bool bc);

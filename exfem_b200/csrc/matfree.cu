@@ -65,12 +65,32 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// bounded wait: gives up after ~2^24 polls, records the failure and returns false
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-  for (int i = 0; i < (1 << 24); ++i)
+// bounded wait: gives up after `polls` polls (default ~2^24, seconds at most),
+// records the failure in *err and returns false
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, int polls = 1 << 24) {
+  for (int i = 0; i < polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   if (err) atomicExch(err, 1);
   return false;
+}
+
+// Self-test of the bounded wait: nothing ever arrives on the barrier, so every
+// thread's wait must give up after `polls` polls and record it; the kernel then
+// returns normally and the context stays usable.
+__global__ void wait_selftest_kernel(int polls, int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  mbar_wait_bounded(&bar, 0, err, polls);
+}
+
+int launch_wait_selftest(int polls, int* err, cudaStream_t s) {
+  wait_selftest_kernel<<<1, 32, 0, s>>>(polls, err);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
 }
 
 // 4- or 8-byte asynchronous global->shared copy; src_bytes = 0 writes zeros

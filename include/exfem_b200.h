@@ -87,6 +87,16 @@ const char* exfem_last_error(void);
 int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const double* X_host,
                        int64_t ne, const int32_t* conn_host, exfem_block* out);
 int exfem_block_destroy(exfem_block b);
+/* the block's kernels wait on asynchronous copies and tensor-core operations with
+ * bounded waits; one that gives up sets a device flag instead of hanging.  Returns
+ * EXFEM_ERR_TIMEOUT (and clears the flag) if that happened since the last check,
+ * EXFEM_OK otherwise; the solver calls check it themselves.  No counterpart in the
+ * reference. */
+int exfem_block_status(exfem_block b, void* stream);
+/* failure detection self-test: a kernel waits, with a limit of `polls` polls, on a
+ * barrier nothing arrives on; returns EXFEM_ERR_TIMEOUT when the wait gave up and the
+ * kernel returned (the expected result; the context stays usable). */
+int exfem_selftest_bounded_wait(int polls, void* stream);
 /* sizes: ne, nn, nnode, ngp, nstate, gather-plan width vmax, colour count,
  * affine (1 if every C3D10 has straight edges), device bytes held */
 int exfem_block_query(exfem_block b, int64_t* ne, int64_t* nn, int* nnode, int* ngp, int* nstate,

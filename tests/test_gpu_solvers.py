@@ -226,3 +226,23 @@ def test_tet10_mixed_vs_direct(cuda):
     up, _, _ = xf.StaticSolver(pm, rtol=1e-6, linear_solver="mixed", cg_tol=1e-10, verbose=False).solve(
         xf.Step(bcs=bcs, loads=loads), scale=[sc])
     assert rel_err(up, uo) < 1e-8
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
+    """Failure detection without a GPU fault: a kernel whose barrier nothing arrives
+    on must give up after its poll limit and report EXFEM_ERR_TIMEOUT; the next
+    product still works and the block reports no failed wait."""
+    from exfem_b200 import _lib
+    from exfem_b200._lib import lib, stream_ptr
+    st = lib.exfem_selftest_bounded_wait(1 << 10, stream_ptr())
+    assert st == _lib.ERR_TIMEOUT
+    assert "gave up" in _lib.last_error()
+    X, c = tet10_box(1, 1, 1, 3, 2, 2)
+    import exfem_b200 as xf
+    m = xf.Model(X)
+    blk = m.add_block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3))
+    v = torch.randn(m.ndof, dtype=torch.float32, device="cuda")
+    y = blk.tangent_matvec(v)
+    torch.cuda.synchronize()
+    assert torch.isfinite(y).all()
+    assert lib.exfem_block_status(blk.handle, stream_ptr()) == _lib.OK
