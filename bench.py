@@ -46,11 +46,11 @@ METRIC = "DOF·matvec/s, solves/s, p50/p99 latency at 1e-8 rel err vs plain FP64
 UNIT = "DOF·matvec/s"
 WORKLOAD = "C3D10 80^3x6 unit cube (3,072,000 el, 12,519,843 DOF), FP32 matrix-free tangent product"
 # DRAM bytes per product (tile pass + node pass) from one ncu capture of the
-# 56^3-cube case (dram__bytes_read.sum + dram__bytes_write.sum: 125.7 MB over
-# 1,053,696 elements in the tile pass and 33.4 MB over 1,442,897 nodes in the node
+# 56^3-cube case (dram__bytes_read.sum + dram__bytes_write.sum: 128.0 MB over
+# 1,053,696 elements in the tile pass and 41.5 MB over 1,442,897 nodes in the node
 # pass), scaled to the 80^3 cube by elements and nodes; the traffic of both passes
 # grows in proportion to them.
-TRAFFIC_BYTES = int(3072000 * 119.3 + 4173281 * 23.2)
+TRAFFIC_BYTES = int(3072000 * 121.49 + 4173281 * 28.75)
 
 
 def peaks():

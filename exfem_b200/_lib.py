@@ -96,6 +96,8 @@ _SIGS = {
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
     "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
     "exfem_block_status": ([VP, VP], C.c_int),
+    "exfem_amg_setup_block": ([VP, VP, P, I32, I32, VP], C.c_int),
+    "exfem_amg_info": ([VP, I32, P, P, P], C.c_int),
     "exfem_selftest_bounded_wait": ([I32, VP], C.c_int),
     "exfem_block_tile_conn": ([VP, P], C.c_int),
 }

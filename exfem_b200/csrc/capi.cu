@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstring>
 
+#include "sa.h"
 #include "solver.h"
 
 namespace exfem {
@@ -691,6 +692,39 @@ int exfem_block_status(exfem_block b, void* stream) {
   int st;
   if ((st = g.init(stream))) return st;
   return block_wait_status(b, g.work);
+}
+
+int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_coarse, int keep_level0,
+                          void* stream) {
+  EX_ARG(h && b, "NULL handle");
+  StreamGuard g;
+  int st;
+  if ((st = g.init(stream))) return st;
+  st = amg_setup_block(h, b, Ke, max_coarse, keep_level0, g.work);
+  if (st) {  // leave the handle empty rather than half built
+    h->levels.clear();
+    h->nc = 0;
+    h->coarse_nnz = 0;
+    h->Ainv.release();
+  }
+  return st;
+}
+
+int exfem_amg_info(exfem_amg h, int cap, int* nlevels, int64_t* rows, int64_t* nnz) {
+  EX_ARG(h && nlevels, "NULL argument");
+  const int nl = (int)h->levels.size() + (h->nc > 0 ? 1 : 0);
+  *nlevels = nl;
+  for (int l = 0; l < nl && l < cap; ++l) {
+    if (l < (int)h->levels.size()) {
+      const auto& L = *h->levels[l];
+      if (rows) rows[l] = L.n;
+      if (nnz) nnz[l] = L.A.nnz ? L.A.nnz : L.op_nnz;
+    } else {
+      if (rows) rows[l] = h->nc;
+      if (nnz) nnz[l] = h->coarse_nnz ? h->coarse_nnz : h->nc * h->nc;
+    }
+  }
+  return EXFEM_OK;
 }
 
 int exfem_selftest_bounded_wait(int polls, void* stream) {

@@ -12,6 +12,7 @@ struct AmgLevel {
   enum { WB = 0, WX = 1, WR = 2, WD = 3, WD2 = 4, WTMP = 5, NW = 6 };
   int64_t n = 0, nc = 0;
   double rho = 1.0;
+  int64_t op_nnz = 0;     // nonzeros of the level operator when it is not stored (device set-up)
   Csr64 A, P, R;
   DevBuf<double> dinv64;
   DevBuf<float> dinv32;
@@ -50,6 +51,7 @@ struct exfem_amg_s {
   int degree = 2;
   std::vector<std::unique_ptr<exfem::AmgLevel>> levels;
   int64_t nc = 0;
+  int64_t coarse_nnz = 0;  // nonzeros of the coarsest operator (device set-up)
   exfem::DevBuf<double> Ainv;
   exfem::DevBuf<int64_t> crow_s, crow_m, crow_a;  // block-diagonal coarse solve: per-row block start, size, offset
   bool replicated = false;                          // levels address shared blocks through row maps

@@ -200,6 +200,22 @@ int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc,
                         const int64_t* R_ptr, const int32_t* R_idx, const double* R_val,
                         const double* dinv, double rho);
 int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv_dense);
+/* Smoothed-aggregation hierarchy set up on the device from a block's element
+ * matrices Ke (ne, 3 nnode, 3 nnode) FP64 (device pointer) and its prescribed
+ * DOFs (exfem_set_fixed): the set-up of AMG.__init__ (gfem/linalg.py:103-136,
+ * pyamg.smoothed_aggregation_solver with rigid-body modes, theta = 0 strength,
+ * standard aggregation, Jacobi-smoothed prolongator omega = 4/3 with absolute
+ * row-sum weighting, Galerkin R A P, max_coarse rows, <= 10 levels, 15-step
+ * power-iteration rho x 1.1, regularised Cholesky of the coarsest matrix) with
+ * the assembly and every matrix product on the GPU and only graph work on the
+ * host.  h must be empty (exfem_amg_create).  The mesh level stores no matrix
+ * unless keep_level0 is set; it is then smoothed with the block's matrix-free
+ * product (solvers, exfem_amg_vcycle with level0).  Synchronises the stream. */
+int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_coarse, int keep_level0,
+                          void* stream);
+/* level count (coarsest included) and, for the first cap levels, rows and
+ * operator nonzeros (AMG.info, gfem/linalg.py:135, 148-154). */
+int exfem_amg_info(exfem_amg h, int cap, int* nlevels, int64_t* rows, int64_t* nnz);
 /* Union of independent hierarchies (batched solves, no counterpart in the
  * reference): per-row spectral bounds of level `level` (n doubles; each row
  * smoothed with its own instance's Chebyshev coefficients, degree 2; a bound of 0
