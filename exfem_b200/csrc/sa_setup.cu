@@ -419,6 +419,7 @@ int power_rho(const BlockOp& A, const double* dinv, cudaStream_t s, double& rho)
     EX_LAUNCH_CHECK();
     nx = ny / std::max(ny, 1e-300);
   }
+  EX_CUDA(cudaStreamSynchronize(s));  // x and y are freed on return
   rho = 1.1 * lam;
   return EXFEM_OK;
 }
@@ -599,7 +600,7 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
   }
   // coarsest level: dense inverse through a regularised Cholesky factor
   const int64_t nc = A.nb * A.bs;
-  EX_ARG(nc <= 20000, "coarsest level of %lld rows is too large for a dense solve", (long long)nc);
+  EX_ARG(nc <= 5000, "coarsest level of %lld rows is too large for a dense solve", (long long)nc);
   std::vector<double> v;
   if ((st = down(v, A.val.p, A.pat.idx.size() * A.bs * A.bs, s))) return st;
   std::vector<double> D((size_t)nc * nc, 0.0), Ainv;

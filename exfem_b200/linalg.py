@@ -346,6 +346,43 @@ class AMG:
         return precond
 
 
+class DeviceAMG(AMG):
+    """Smoothed-aggregation AMG set up on the GPU (no counterpart in the reference,
+    whose set-up runs PyAMG on the host, gfem/linalg.py:103-136).
+
+    ``block``: a :class:`model.Block` with its prescribed DOFs set
+    (``Block.set_fixed``); ``Ke``: its FP64 element matrices (ne, 3 nnode, 3 nnode),
+    e.g. ``block.stiffness(u, state)``.  The same set-up as :func:`amg_setup` (rigid
+    body modes of the block's coordinates, standard aggregation on the theta = 0
+    strength graph, Jacobi-smoothed prolongator, Galerkin coarse operators), with
+    the assembly of A and every matrix product on the device; only the graph work
+    (adjacency, aggregates, sparsity patterns, per-aggregate orthonormalisation)
+    runs on the host.  For meshes whose assembled matrix is too large for the
+    host set-up.  The mesh level keeps no stored matrix unless ``keep_level0``:
+    the solvers smooth it with the block's matrix-free product."""
+
+    def __init__(self, block, Ke, max_coarse=300, degree=2, presmooth=1, keep_level0=False):
+        t0 = time.time()
+        _lib.require_cuda()
+        h = C.c_void_p()
+        check(lib.exfem_amg_create(C.byref(h)))
+        self._h = h
+        Ke = Ke.to(torch.float64).contiguous()
+        check(lib.exfem_amg_setup_block(h, block.handle, ptr(Ke), int(max_coarse), 1 if keep_level0 else 0,
+                                        stream_ptr()))
+        cap = 16
+        nl, rows, nnz = C.c_int(), (C.c_int64 * cap)(), (C.c_int64 * cap)()
+        check(lib.exfem_amg_info(h, cap, C.byref(nl), rows, nnz))
+        self.sizes = [int(rows[i]) for i in range(min(nl.value, cap))]
+        self.nnz = [int(nnz[i]) for i in range(min(nl.value, cap))]
+        self.levels, self.coarse, self.coarse_inv = None, None, None
+        self.degree, self.presmooth = degree, presmooth
+        self.complexity = float(sum(self.nnz) / max(self.nnz[0], 1))
+        self.nlevels = nl.value
+        self.keep_level0 = keep_level0
+        self.setup_time = time.time() - t0
+
+
 # ------------------------------------------------------------------ native solver
 class NativeSolver:
     """PCG / mixed-precision refinement in the library for one block.

@@ -127,8 +127,15 @@ class _LinearSystem:                                                    # solver
     """Solves (free K free + fixed I) x = b with the chosen back-end."""
 
     def __init__(self, model, method="auto", tangent="ebe", cg_tol=1e-9, cg_maxiter=20000, monitor=None,
-                 graph=True):
+                 graph=True, amg_setup="auto"):
         self.m = model
+        if amg_setup not in ("auto", "host", "device"):
+            raise ValueError(f"unknown AMG set-up {amg_setup!r}")
+        # where the hierarchy is set up: "host" (assembled CSR, worker-free host
+        # set-up), "device" (linalg.DeviceAMG), "auto" = device from the size at
+        # which the reference moves its set-up off the critical path
+        # (ndof >= 150000, gfem/solvers.py:445-452)
+        self.amg_setup = amg_setup
         if method == "auto":
             method = "direct" if model.ndof <= 20000 else "amg"
         if method not in ("direct", "amg", "jacobi", "mixed"):
@@ -175,8 +182,15 @@ class _LinearSystem:                                                    # solver
 
     def _build_amg(self, ops, setup, ctx):
         t0 = time.time()
-        A = self.assemble(self._setup_ops(ops, ctx), setup)
-        self.amg = linalg.AMG(A, self.m.X)
+        where = self.amg_setup
+        if where == "auto":
+            where = "device" if self.m.ndof >= 150000 else "host"
+        if where == "device":
+            Ke = self._setup_ops(ops, ctx)[0][1]
+            self.amg = linalg.DeviceAMG(self.m.blocks[0], Ke)
+        else:
+            A = self.assemble(self._setup_ops(ops, ctx), setup)
+            self.amg = linalg.AMG(A, self.m.X)
         self.amg_iters0 = None
         self._solvers = {}
         self.mon.log(f"    {self.amg.info()}  setup {time.time() - t0:.2f}s")
@@ -220,14 +234,15 @@ class _LinearSystem:                                                    # solver
 
 class StaticSolver:                                                     # solvers.py:481-683
     def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
-                 cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None):
+                 cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None,
+                 amg_setup="auto"):
         """``amg``: a prebuilt :class:`linalg.AMG` that every step starts from instead
         of assembling and setting up its own (the serving path keeps one resident
         per mesh); the rebuild rule still applies."""
         self.m, self.rtol, self.max_iter = model, rtol, max_iter
         self.mon = monitor or Monitor(verbose)
         self.line_search = line_search
-        self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph)
+        self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph, amg_setup)
         self.lin.pinned_amg = amg
         self.newton_iterations = 0
 

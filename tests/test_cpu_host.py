@@ -240,3 +240,42 @@ def test_random_cantilevers_follow_the_stated_ranges():
         mags = np.abs(tot).max(1)
         assert np.all((mags >= 100.0) & (mags <= 1000.0))
         np.testing.assert_allclose(np.sign(tot).astype(int), [[1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, -1]])
+
+
+def test_skin_and_pressure_vector_match_oracle():
+    """Config-3 load set-up: skin of a jittered C3D10 box, its z = 1 sub-surface and
+    the equivalent nodal forces of a -1 pressure against the oracle's restatement of
+    gfem/surfaces.py:182-242 and gfem/loads.py:37-49 (facets bit for bit, forces to
+    1e-14 of the largest: the closed-form shape-function derivatives round
+    differently from the oracle's AD ones in the last bit); the C3D8 skin
+    (QUAD4 facets) against the closed form: a pressure -p on the unit cube's top face
+    gives a total force p along +z and nothing else."""
+    from types import SimpleNamespace
+
+    from exfem_b200 import elements, loads, mesh, surfaces
+    from oracle import loads as oloads
+    X, c = tet10_box(1.0, 1.0, 1.0, 3, 3, 3, frac=0.1, seed=7)
+    blk = SimpleNamespace(conn=c, etype=elements.TET10)
+    top = mesh.nodes_where(X, lambda x, y, z: z > 1 - 1e-9)
+    sk = surfaces.skin(X, [blk])
+    osk = oloads.skin_tet10(X, c)
+    assert len(sk.groups) == 1 and sk.groups[0][0] is surfaces.TRI6
+    np.testing.assert_array_equal(sk.groups[0][1], osk)
+    sub = surfaces.sub_surface(sk, top)
+    osub = oloads.sub_surface(osk, top, len(X))
+    np.testing.assert_array_equal(sub.groups[0][1], osub)
+    f = loads.pressure_vector(X, sub, -1.0)
+    fo = oloads.pressure_vector(X, osub, -1.0)
+    np.testing.assert_allclose(f, fo, rtol=0, atol=1e-14 * np.abs(fo).max())
+    assert abs(f.reshape(-1, 3)[:, 2].sum() - 1.0) < 1e-12
+    Xh, ch = mesh.box_hex(1.0, 1.0, 1.0, 3, 3, 3)
+    Xh = mesh.jitter_interior(Xh, [1 / 3] * 3, 0.1, 3)
+    skh = surfaces.skin(Xh, [SimpleNamespace(conn=ch, etype=elements.HEX8)])
+    assert len(skh) == 6 * 9 and skh.groups[0][0] is surfaces.QUAD4
+    toph = mesh.nodes_where(Xh, lambda x, y, z: z > 1 - 1e-9)
+    fh = loads.pressure_vector(Xh, surfaces.sub_surface(skh, toph), -2.5).reshape(-1, 3)
+    np.testing.assert_allclose(fh.sum(0), [0.0, 0.0, 2.5], atol=1e-12)
+    w, area, nsum = skh.integrate(Xh)
+    assert abs(area - 6.0) < 1e-12 and np.abs(nsum).max() < 1e-12 and abs(w.sum() - 6.0) < 1e-12
+    ft = loads.traction_vector(Xh, surfaces.sub_surface(skh, toph), [1.0, 0.0, 0.0]).reshape(-1, 3)
+    np.testing.assert_allclose(ft.sum(0), [1.0, 0.0, 0.0], atol=1e-12)
