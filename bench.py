@@ -218,6 +218,43 @@ def solve_section(reps=10):
     return out
 
 
+def scale_solve_section(m, X, scale, cg_tol=1e-8):
+    """The mixed-precision scale case solved end to end on the bench's C3D10 cube:
+    z = 0 clamped, uniform 1 MPa outward normal traction on z = 1 (pressure -1 on the
+    top sub-surface of the skin), per-element E = 1 GPa x scale.  One
+    ``StaticSolver.solve`` per path, each with its own smoothed-aggregation
+    hierarchy set up on the device from the FP64 element matrices:
+    mixed = FP32 matrix-free product + FP32 V-cycle inside FP64 refinement to
+    cg_tol; plain_fp64 = FP64 matrix-free product + FP64 V-cycle, FP64 PCG to cg_tol."""
+    import torch
+    import exfem_b200 as xf
+    from exfem_b200 import loads, surfaces
+    fix = np.nonzero(X[:, 2] < 1e-9)[0]
+    top = np.nonzero(X[:, 2] > 1 - 1e-9)[0]
+    f = loads.pressure_vector(X, surfaces.sub_surface(surfaces.skin(X, m.blocks), top), -1.0)
+    step = xf.Step(bcs=[(fix, d, 0.0) for d in range(3)], dloads=[f])
+    out, sols = {}, {}
+    for name, method in (("mixed", "mixed"), ("plain_fp64", "amg")):
+        s = xf.StaticSolver(m, rtol=1e-6, linear_solver=method, tangent="mf", cg_tol=cg_tol, verbose=False,
+                            amg_setup="device")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, _, _ = s.solve(step, scale=[scale])
+        torch.cuda.synchronize()
+        total = time.perf_counter() - t0
+        amg = s.lin.amg
+        out[name] = dict(total_s=total, amg_setup_s=s.lin.last_setup_time, solve_s=total - s.lin.last_setup_time,
+                         pcg_iters=s.lin.last_iters, refinement_passes=s.lin.last_passes)
+        out["amg"] = dict(rows=amg.sizes, nnz=amg.nnz, complexity=amg.complexity)
+        sols[name] = u
+        del s, amg
+    out["rel_err_mixed_vs_fp64"] = float((sols["mixed"] - sols["plain_fp64"]).abs().max()
+                                         / sols["plain_fp64"].abs().max())
+    out["case"] = (f"C3D10 cube {m.nelem} el, {m.ndof} DOF, z=0 clamped, 1 MPa traction on z=1, "
+                   f"E log-uniform 1-10 GPa, cg_tol {cg_tol:g}, device SA set-up")
+    return out
+
+
 def batch_section(count=512, nplain=24, seed=0, workers=None):
     """Batched uneven solves (512 C3D8 cantilevers x 4 right-hand sides, FP32
     matrix-free AMG-PCG inside FP64 refinement to 1e-8) against the plain FP64
@@ -579,8 +616,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e_ms = float(t.item())
 
-    solve = None
+    solve = scale_res = None
     if rank == 0 and not args.no_solve:
+        scale_res = scale_solve_section(m, X, scale)
         solve = solve_section()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -607,7 +645,7 @@ def main():
         roofline=dict(bound="hbm", achieved=achieved, peak=pk, unit="GB/s", frac=achieved / pk,
                       traffic=TRAFFIC_BYTES, peak_source=f"{pk_src} (MEASURED_PEAKS.json hbm_gbs)",
                       algorithmic_bytes_per_step=alg_bytes),
-        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve)
+        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve, scale_solve=scale_res)
     print(json.dumps(line), flush=True)
 
 

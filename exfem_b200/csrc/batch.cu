@@ -195,7 +195,7 @@ struct exfem_batch_s {
   exfem::BatchScal S{};
   ~exfem_batch_s() {
     if (gexec) cudaGraphExecDestroy(gexec);
-    if (h_cnt) cudaFreeHost(h_cnt);
+    if (h_cnt) exfem::outside_captures([&] { return cudaFreeHost(h_cnt); });
   }
 };
 
@@ -291,6 +291,7 @@ static int batch_pcg32(exfem_batch_s* B, double tol, int maxiter, cudaStream_t s
     B->gexec = nullptr;
   }
   if (!B->gexec) {
+    CaptureScope cap;
     cudaGraph_t gr;
     EX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     int cs = EXFEM_OK;
@@ -378,7 +379,7 @@ int batch_alloc(exfem_batch_s* B, const int64_t* off_host) {
   DevBuf<float>* v32[] = {&B->x32, &B->r32, &B->z32, &B->p32, &B->Ap32, &B->t32, &B->dinv32};
   for (auto* v : v32)
     if ((s = v->alloc(std::max<int64_t>(B->n, 1)))) return s;
-  EX_CUDA(cudaMallocHost(&B->h_cnt, sizeof(int)));
+  EX_CUDA(outside_captures([&] { return cudaMallocHost(&B->h_cnt, sizeof(int)); }));
   return EXFEM_OK;
 }
 

@@ -110,6 +110,18 @@ static int mf_apply_cb(void* ctx, const T* x, T* y, const int* skip, cudaStream_
 
 // graphs cannot be captured on the legacy default stream: such calls run on a
 // private stream ordered after and before the caller's stream with events
+namespace exfem {
+std::shared_mutex& capture_lock() {
+  static std::shared_mutex m;
+  return m;
+}
+
+int& capturing_here() {
+  static thread_local int c = 0;
+  return c;
+}
+}  // namespace exfem
+
 struct StreamGuard {
   cudaStream_t user, work = nullptr;
   cudaEvent_t ev = nullptr;

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <vector>
 
@@ -37,6 +39,32 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line);
     }                                                                              \
   } while (0)
 
+// ---------------------------------------------------------------- captures and allocations
+// cudaFree and cudaFreeHost synchronise the whole device, and a device-wide
+// synchronisation invalidates a CUDA-graph capture that another host thread has in
+// progress.  Captures hold capture_lock() shared for their duration; allocations
+// and frees take it exclusively, so they wait for the captures in flight.  A
+// thread never allocates inside its own capture (the capture would fail anyway),
+// so it does not take the lock there (capturing_here()).
+std::shared_mutex& capture_lock();
+int& capturing_here();
+
+struct CaptureScope {
+  std::shared_lock<std::shared_mutex> lk;
+  CaptureScope() : lk(capture_lock()) { capturing_here() = 1; }
+  ~CaptureScope() { capturing_here() = 0; }
+  CaptureScope(const CaptureScope&) = delete;
+  CaptureScope& operator=(const CaptureScope&) = delete;
+};
+
+// run an allocation or free outside every other thread's capture
+template <class F>
+auto outside_captures(F f) -> decltype(f()) {
+  if (capturing_here()) return f();
+  std::unique_lock<std::shared_mutex> lk(capture_lock());
+  return f();
+}
+
 // ---------------------------------------------------------------- device buffer
 // Owning, non-copyable device allocation.  Allocation failures are reported
 // through the status of the function that asked for the buffer.
@@ -54,14 +82,14 @@ struct DevBuf {
   }
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) outside_captures([&] { return cudaFree(p); });
     p = nullptr;
     n = 0;
   }
   int alloc(size_t count) {
     release();
     if (count == 0) return EXFEM_OK;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    cudaError_t e = outside_captures([&] { return cudaMalloc(&p, count * sizeof(T)); });
     if (e != cudaSuccess) {
       p = nullptr;
       cudaGetLastError();

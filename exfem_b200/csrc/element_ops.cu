@@ -411,7 +411,9 @@ int build_geometry(exfem_block_s* b) {
     geometry_kernel<EXFEM_C3D10><<<grid, threads>>>(b->ne, b->X.p, b->conn_tile.p, b->order_dev.p, b->scale.p,
                                                     b->lam_e.p, b->mu_e.p, GS, b->geo64.p, b->geo32.p, b->tile);
   EX_LAUNCH_CHECK();
-  EX_CUDA(cudaDeviceSynchronize());
+  // the legacy stream only: a device-wide synchronisation would invalidate a graph
+  // capture in progress on another host thread
+  EX_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
   return EXFEM_OK;
 }
 

@@ -329,6 +329,7 @@ static int pcg_run(exfem_solver_s* S, double tol, int maxiter, int* iters, doubl
       S->gexec[gi] = nullptr;
     }
     if (!S->gexec[gi]) {
+      CaptureScope cap;
       cudaGraph_t g;
       EX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       int cs = EXFEM_OK;
@@ -411,6 +412,12 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
   if (bn == 0.0) bn = 1.0;
   int its = 0, p = 0;
   double rn = bn;
+  // Passes after the first stop their FP32 iteration at 4x the first pass's count:
+  // on large ill-conditioned meshes the FP32 recursion of a later pass (whose
+  // right-hand side is the rounding-level residual of the previous one) can stall
+  // above inner_tol, and iterating on gains nothing that the next FP64 residual
+  // and pass would not (the reference runs such a pass to cg_maxiter).
+  int cap = maxiter;
   for (p = 0; p < max_pass; ++p) {
     double sc;
     if ((s = norm64(S, S->r64.p, &sc, st))) return s;
@@ -419,9 +426,10 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
     EX_LAUNCH_CHECK();
     int k = 0;
     double rr;
-    s = pcg_run<float>(S, inner_tol, maxiter, &k, &rr, st);
+    s = pcg_run<float>(S, inner_tol, cap, &k, &rr, st);
     if (s < 0) return s;
     its += k;
+    if (p == 0) cap = std::min(maxiter, std::max(4 * k, 32));
     axpy_f32_kernel<<<eg, 256, 0, st>>>(n, x, S->x32.p, sc);
     EX_LAUNCH_CHECK();
     if ((s = launch_mf_matvec<double>(S->blk, x, S->Ap64.p, nullptr, st))) return s;
@@ -451,7 +459,7 @@ int solver_alloc(exfem_solver_s* S) {
   if ((s = S->counter.alloc(1))) return s;
   EX_CUDA(cudaMemset(S->counter.p, 0, sizeof(unsigned)));
   if ((s = S->scal.alloc(1))) return s;
-  EX_CUDA(cudaMallocHost(&S->h_scal, sizeof(PcgScal)));
+  EX_CUDA(outside_captures([&] { return cudaMallocHost(&S->h_scal, sizeof(PcgScal)); }));
   return EXFEM_OK;
 }
 
@@ -460,5 +468,5 @@ int solver_alloc(exfem_solver_s* S) {
 exfem_solver_s::~exfem_solver_s() {
   for (auto& g : gexec)
     if (g) cudaGraphExecDestroy(g);
-  if (h_scal) cudaFreeHost(h_scal);
+  if (h_scal) exfem::outside_captures([&] { return cudaFreeHost(h_scal); });
 }

@@ -311,7 +311,7 @@ class AMG:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.exfem_amg_destroy(h)
             self._h = None
 
@@ -407,7 +407,7 @@ class NativeSolver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h is not None and h.value:
+        if h is not None and h.value and lib is not None:
             lib.exfem_solver_destroy(h)
             self._h = None
 

@@ -152,6 +152,7 @@ class _LinearSystem:                                                    # solver
         self.amg_iters0 = None
         self.last_iters = 0
         self.last_passes = 0
+        self.last_setup_time = 0.0
         self._solvers = {}
 
     def reset(self):
@@ -193,7 +194,8 @@ class _LinearSystem:                                                    # solver
             self.amg = linalg.AMG(A, self.m.X)
         self.amg_iters0 = None
         self._solvers = {}
-        self.mon.log(f"    {self.amg.info()}  setup {time.time() - t0:.2f}s")
+        self.last_setup_time = time.time() - t0
+        self.mon.log(f"    {self.amg.info()}  setup {self.last_setup_time:.2f}s")
 
     def solve(self, ops, b, setup, jvp_args=None, rebuild=False):
         """ops: [(dofs, Ke)] (tangent="ebe") or None with jvp_args = (u, states, fields)
