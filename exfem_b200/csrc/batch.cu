@@ -23,6 +23,8 @@ constexpr int BT = 256;
 struct BatchScal {  // device arrays, one entry per instance
   double *rz, *pAp, *rr, *bb, *tol2, *alpha, *beta, *sc, *bn, *rn, *tmp;
   int *k, *done, *odone, *iters;
+  double* itol;  // inner tolerance of the current pass
+  int* cap;      // inner iteration limit of the current pass
 };
 
 enum BFin { BF_BB = 0, BF_RZ0, BF_RR0, BF_ALPHA, BF_BETA, BF_STORE };
@@ -63,13 +65,13 @@ bdot_kernel(const int64_t* __restrict__ off, const T* __restrict__ a, const T* _
   switch (F) {
     case BF_BB:
       S.bb[i] = s;
-      S.tol2[i] = tol * tol * fmax(s, 1e-300);
+      S.tol2[i] = S.itol[i] * S.itol[i] * fmax(s, 1e-300);
       break;
     case BF_RZ0: S.rz[i] = s; break;
     case BF_RR0:
       S.rr[i] = s;
       S.k[i] = 0;
-      S.done[i] = S.odone[i] || !(s > S.tol2[i] && 0 < maxiter);
+      S.done[i] = S.odone[i] || !(s > S.tol2[i] && 0 < S.cap[i]);
       break;
     case BF_ALPHA:
       S.pAp[i] = s;
@@ -79,7 +81,7 @@ bdot_kernel(const int64_t* __restrict__ off, const T* __restrict__ a, const T* _
       S.beta[i] = s / S.rz[i];
       S.rz[i] = s;
       S.k[i] += 1;
-      S.done[i] = !(S.rr[i] > S.tol2[i] && S.k[i] < maxiter);
+      S.done[i] = !(S.rr[i] > S.tol2[i] && S.k[i] < S.cap[i]);
       break;
     default: S.tmp[i] = s;
   }
@@ -161,7 +163,8 @@ __global__ void bresidual_kernel(const int64_t* __restrict__ off, const double* 
   }
 }
 
-__global__ void bnorm_init_kernel(const int64_t* __restrict__ off, const double* __restrict__ b, BatchScal S) {
+__global__ void bnorm_init_kernel(const int64_t* __restrict__ off, const double* __restrict__ b, BatchScal S,
+                                  double inner_tol, int maxiter) {
   const int i = blockIdx.x;
   double acc = 0.0;
   for (int64_t j = off[i] + threadIdx.x; j < off[i + 1]; j += BT) acc += b[j] * b[j];
@@ -173,7 +176,19 @@ __global__ void bnorm_init_kernel(const int64_t* __restrict__ off, const double*
     S.tmp[i] = s;
     S.odone[i] = 0;
     S.iters[i] = 0;
+    S.itol[i] = inner_tol;
+    S.cap[i] = maxiter;
   }
+}
+
+// after the first pass, per instance (the rule of the single-solve refinement):
+// later passes stop their FP32 recursion at the reduction the first pass attained
+// in FP64 (not below inner_tol) and at 4x the first pass's iterations
+__global__ void badapt_kernel(int m, BatchScal S, double inner_tol, int maxiter) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  S.cap[i] = min(maxiter, max(4 * S.k[i], 32));
+  S.itol[i] = fmin(fmax(inner_tol, S.rn[i] / S.sc[i]), 0.1);
 }
 
 }  // namespace exfem
@@ -266,9 +281,9 @@ static int batch_iteration(exfem_batch_s* B, int maxiter, cudaStream_t st) {
 }
 
 static int batch_count(exfem_batch_s* B, const int* flags, int* out, cudaStream_t st) {
-  count_kernel<<<1, 256, 0, st>>>(B->ninst, flags, B->si.p + 4 * B->ninst);
+  count_kernel<<<1, 256, 0, st>>>(B->ninst, flags, B->si.p + 5 * B->ninst);
   EX_LAUNCH_CHECK();
-  EX_CUDA(cudaMemcpyAsync(B->h_cnt, B->si.p + 4 * B->ninst, sizeof(int), cudaMemcpyDeviceToHost, st));
+  EX_CUDA(cudaMemcpyAsync(B->h_cnt, B->si.p + 5 * B->ninst, sizeof(int), cudaMemcpyDeviceToHost, st));
   EX_CUDA(cudaStreamSynchronize(st));
   *out = *B->h_cnt;
   return EXFEM_OK;
@@ -326,7 +341,7 @@ int batch_solve(exfem_batch_s* B, const double* b, double* x, double tol, double
   if ((s = amg_prepare(B->amg, EXFEM_F32))) return s;
   EX_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
   EX_CUDA(cudaMemcpyAsync(B->r64.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  bnorm_init_kernel<<<g, BT, 0, st>>>(B->off.p, b, B->S);
+  bnorm_init_kernel<<<g, BT, 0, st>>>(B->off.p, b, B->S, inner_tol, maxiter);
   EX_LAUNCH_CHECK();
   int p = 0;
   for (p = 0; p < max_pass; ++p) {
@@ -338,6 +353,10 @@ int batch_solve(exfem_batch_s* B, const double* b, double* x, double tol, double
     if ((s = launch_mf_matvec<double>(B->blk, x, B->t64.p, nullptr, st))) return s;
     bresidual_kernel<<<g, BT, 0, st>>>(B->off.p, b, B->t64.p, B->r64.p, B->S, tol);
     EX_LAUNCH_CHECK();
+    if (p == 0) {
+      badapt_kernel<<<(B->ninst + 255) / 256, 256, 0, st>>>(B->ninst, B->S, inner_tol, maxiter);
+      EX_LAUNCH_CHECK();
+    }
     // next pass scales by the new residual norms
     bdot_kernel<double><<<g, BT, 0, st>>>(B->off.p, B->r64.p, B->r64.p, B->S, BF_STORE, 0.0, 0, 0);
     EX_LAUNCH_CHECK();
@@ -366,13 +385,14 @@ int batch_alloc(exfem_batch_s* B, const int64_t* off_host) {
   int s;
   const int m = B->ninst;
   if ((s = B->off.upload(off_host, m + 1))) return s;
-  if ((s = B->sd.alloc((size_t)11 * m))) return s;
-  if ((s = B->si.alloc((size_t)4 * m + 1))) return s;
+  if ((s = B->sd.alloc((size_t)12 * m))) return s;
+  if ((s = B->si.alloc((size_t)5 * m + 1))) return s;
   EX_CUDA(cudaMemset(B->sd.p, 0, B->sd.bytes()));
   EX_CUDA(cudaMemset(B->si.p, 0, B->si.bytes()));
   double* d = B->sd.p;
   B->S = BatchScal{d, d + m, d + 2 * m, d + 3 * m, d + 4 * m, d + 5 * m, d + 6 * m, d + 7 * m, d + 8 * m, d + 9 * m,
-                   d + 10 * m, B->si.p, B->si.p + m, B->si.p + 2 * m, B->si.p + 3 * m};
+                   d + 10 * m, B->si.p, B->si.p + m, B->si.p + 2 * m, B->si.p + 3 * m, d + 11 * m,
+                   B->si.p + 4 * m};
   DevBuf<double>* v64[] = {&B->x64, &B->r64, &B->t64, &B->diag64, &B->dinv64};
   for (auto* v : v64)
     if ((s = v->alloc(std::max<int64_t>(B->n, 1)))) return s;

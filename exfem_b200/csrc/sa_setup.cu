@@ -19,7 +19,10 @@
 // reproducible.  The levels are handed to the V-cycle as scalar CSR (FP64 + an
 // FP32 copy); the mesh level keeps no stored matrix unless asked to (the
 // solvers smooth it with the matrix-free product).
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "sa.h"
@@ -106,12 +109,17 @@ __global__ void sa_rowinfo_kernel(int64_t nb, int bs, const int64_t* __restrict_
   }
 }
 
-__global__ void sa_nzflag_kernel(int64_t nblk, int bb, const double* __restrict__ A, uint8_t* __restrict__ f) {
+// nonzero flag per block, and the number of all-zero blocks
+__global__ void sa_nzflag_kernel(int64_t nblk, int bb, const double* __restrict__ A, uint8_t* __restrict__ f,
+                                 unsigned long long* __restrict__ nzero) {
+  unsigned long long z = 0;
   for (int64_t q = thread_id(); q < nblk; q += thread_count()) {
     uint8_t nz = 0;
     for (int k = 0; k < bb; ++k) nz |= (A[q * bb + k] != 0.0);
     f[q] = nz;
+    z += !nz;
   }
+  if (z) atomicAdd(nzero, z);
 }
 
 __global__ void sa_gather_blocks_kernel(int64_t nkeep, int bb, const int64_t* __restrict__ keep,
@@ -370,6 +378,20 @@ int down(std::vector<T>& h, const T* d, size_t n, cudaStream_t s) {
   return EXFEM_OK;
 }
 
+// phase timing of the set-up, printed to stderr when EXFEM_SETUP_TIMING is set
+struct PhaseClock {
+  bool on = std::getenv("EXFEM_SETUP_TIMING") != nullptr;
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  void mark(const char* what, cudaStream_t s, int level) {
+    if (!on) return;
+    cudaStreamSynchronize(s);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[sa setup] level %d %-22s %8.1f ms\n", level, what,
+                 std::chrono::duration<double, std::milli>(now - t).count());
+    t = now;
+  }
+};
+
 unsigned sa_grid(int64_t work, int block) { return grid_for((size_t)std::max<int64_t>(work, 1), block, 148u * 32u); }
 
 // block-sparse operator of one level while it is being coarsened
@@ -496,6 +518,7 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
   std::vector<int32_t> conn;
   std::vector<double> X;
   int st;
+  PhaseClock clk;
   if ((st = down(conn, b->conn.p, (size_t)b->ne * nnode, s))) return st;
   if ((st = down(X, b->X.p, (size_t)b->nn * 3, s))) return st;
   // level 0: node adjacency pattern, A_0 assembled from the element matrices
@@ -505,6 +528,7 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
   {
     Rows adj;
     if ((st = host_node_adjacency(b->nn, b->ne, nnode, conn.data(), adj))) return st;
+    clk.mark("node adjacency (host)", s, 0);
     if ((st = A.set_pattern(std::move(adj)))) return st;
   }
   if ((st = A.val.alloc(std::max<size_t>(A.pat.idx.size() * 9, 1)))) return st;
@@ -512,6 +536,7 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
       A.nb, nnode, b->vmax, b->plan.p, (int32_t)(b->ne * nnode), b->conn.p, Ke,
       b->node_fixed.n ? b->node_fixed.p : nullptr, A.ptr.p, A.idx.p, A.val.p);
   EX_LAUNCH_CHECK();
+  clk.mark("assembly", s, 0);
   std::vector<double> B;
   host_rigid_body_modes(b->nn, X.data(), B);
   std::vector<double>().swap(X);
@@ -523,13 +548,20 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
     const int64_t n = A.nb * bs, nblk = (int64_t)A.pat.idx.size();
     DevBuf<double> diag, dabs;
     DevBuf<uint8_t> flag;
-    if ((st = diag.alloc(n)) || (st = dabs.alloc(n)) || (st = flag.alloc(std::max<int64_t>(nblk, 1)))) return st;
+    DevBuf<unsigned long long> nzero;
+    if ((st = diag.alloc(n)) || (st = dabs.alloc(n)) || (st = flag.alloc(std::max<int64_t>(nblk, 1))) ||
+        (st = nzero.alloc(1)))
+      return st;
+    EX_CUDA(cudaMemsetAsync(nzero.p, 0, sizeof(unsigned long long), s));
     sa_rowinfo_kernel<<<sa_grid(n, 256), 256, 0, s>>>(A.nb, bs, A.ptr.p, A.idx.p, A.val.p, diag.p, dabs.p);
     EX_LAUNCH_CHECK();
-    sa_nzflag_kernel<<<sa_grid(nblk, 256), 256, 0, s>>>(nblk, bs * bs, A.val.p, flag.p);
+    sa_nzflag_kernel<<<sa_grid(nblk, 256), 256, 0, s>>>(nblk, bs * bs, A.val.p, flag.p, nzero.p);
     EX_LAUNCH_CHECK();
-    // strength graph (theta = 0): the nonzero blocks; A keeps only those
-    {
+    std::vector<unsigned long long> hz;
+    if ((st = down(hz, nzero.p, 1, s))) return st;
+    // strength graph (theta = 0): the nonzero blocks; A keeps only those (the
+    // pattern as it is when no block is all zero)
+    if (hz[0] > 0) {
       std::vector<uint8_t> f;
       if ((st = down(f, flag.p, (size_t)nblk, s))) return st;
       Rows S;
@@ -553,18 +585,23 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
         if ((st = A.set_pattern(std::move(S)))) return st;
       }
     }
+    const int lev = (int)h->levels.size();
+    clk.mark("strength graph", s, lev);
     std::vector<int32_t> agg(A.nb);
     int64_t nagg = 0;
     if ((st = host_standard_aggregation(A.nb, A.pat.ptr.data(), A.pat.idx.data(), agg.data(), nagg))) return st;
     if (nagg == 0) break;
     std::vector<double> Q, Bc;
+    clk.mark("aggregation (host)", s, lev);
     host_fit_candidates(A.nb, bs, K, agg.data(), nagg, B.data(), Q, Bc);
+    clk.mark("tentative P (host)", s, lev);
     Rows Pp, APp, PT, Acp;
     std::vector<int32_t> slot;
     host_p_pattern(A.pat, agg.data(), nagg, Pp);
     host_union_pattern(A.pat, Pp, nagg, APp);
     host_transpose_pattern(Pp, nagg, PT, slot);
     host_union_pattern(PT, APp, nagg, Acp);
+    clk.mark("patterns (host)", s, lev);
     auto L = std::make_unique<AmgLevel>();
     L->n = n;
     L->nc = nagg * K;
@@ -579,11 +616,13 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
     st = bs == 3 ? coarsen<3>(A, dagg, dQ, dabs, nagg, Pp, APp, PT, slot, Ac, *L, s)
                  : coarsen<6>(A, dagg, dQ, dabs, nagg, Pp, APp, PT, slot, Ac, *L, s);
     if (st) return st;
+    clk.mark("P, AP, RAP, P/R CSR", s, lev);
     // smoother data of this level: inverse diagonal, spectral bound, stored matrix
     if ((st = L->dinv64.alloc(n)) || (st = L->dinv32.alloc(n))) return st;
     sa_dinv_kernel<<<sa_grid(n, 256), 256, 0, s>>>(n, diag.p, L->dinv64.p, L->dinv32.p);
     EX_LAUNCH_CHECK();
     if ((st = power_rho(A, L->dinv64.p, s, L->rho))) return st;
+    clk.mark("spectral bound", s, lev);
     if (!h->levels.empty() || keep_level0) {
       if ((st = expand_blocks(L->A, A.nb, bs, bs, n, A.ptr, A.idx, A.val.p, (int64_t)A.pat.idx.size(), s))) return st;
     } else {
@@ -610,6 +649,7 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
         for (int j = 0; j < A.bs; ++j)
           D[(r * A.bs + i) * nc + (int64_t)A.pat.idx[q] * A.bs + j] = v[(q * A.bs + i) * A.bs + j];
   if ((st = host_coarse_inverse(nc, D, Ainv))) return st;
+  clk.mark("coarsest inverse", s, (int)h->levels.size());
   if ((st = h->Ainv.upload(Ainv.data(), Ainv.size()))) return st;
   h->nc = nc;
   h->coarse_nnz = nc * nc;
