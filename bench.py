@@ -268,6 +268,46 @@ def scale_solve_section(m, X, scale, cg_tol=1e-8, reps=3):
     return out
 
 
+def j2_section(nx=100, ny=20, nz=20, seed=0):
+    """The J2 Newton case: C3D8 cantilever 1000 x 200 x 200 mm of nx x ny x nz
+    elements, interior nodes jittered +-10% h (seeded), E = 210 GPa, nu = 0.3, yield
+    250 MPa with linear hardening H = 1 GPa, x = 0 clamped, tip -z displacement ramped
+    to 5 mm in 10 increments, Newton rtol 1e-6, cg_tol 1e-6.  Plain FP64 path (stored
+    FP64 Ke + FP64 AMG-PCG) against the mixed path (FP32 matrix-free consistent tangent
+    + FP32 V-cycle inside FP64 refinement); both full StaticSolver.solve runs."""
+    import torch
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    L, h = 1000.0, 1000.0 / nx
+    X, c = mesh.box_hex(L, 200.0, 200.0, nx, ny, nz)
+    X = mesh.jitter_interior(X, [h, 200.0 / ny, 200.0 / nz], 0.1, seed)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > L - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)] + [(tip, 2, -5.0)]
+    out, res = {}, {}
+    for name, kw in (("plain_fp64", dict(linear_solver="amg", tangent="ebe")),
+                     ("mixed", dict(linear_solver="mixed", tangent="mf"))):
+        m = xf.Model(X)
+        m.add_block(c, xf.HEX8, xf.J2Plasticity(210000.0, 0.3, [[250.0, 0.0], [1250.0, 1.0]]))
+        s = xf.StaticSolver(m, rtol=1e-6, cg_tol=1e-6, verbose=False, **kw)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        u, st, info = s.solve(xf.Step(bcs=bcs, dt_init=0.1, dt_max=0.1))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        newton = [int(hh[1]) for hh in info["history"]]
+        mises = m.stresses(u, st)[0]["MISES"]
+        out[name] = dict(total_s=dt, increments=len(newton), newton_per_increment=newton,
+                         newton_total=int(sum(newton)), max_peeq=float(st[0][..., 9].max()))
+        res[name] = (u, mises)
+    (u0, m0), (u1, m1) = res["plain_fp64"], res["mixed"]
+    out["rel_err_u_mixed_vs_fp64"] = float((u1 - u0).abs().max() / u0.abs().max())
+    out["rel_err_mises_mixed_vs_fp64"] = float((m1 - m0).abs().max() / m0.abs().max())
+    out["case"] = (f"C3D8 {nx}x{ny}x{nz} J2 cantilever ({len(c)} el, {3 * len(X)} DOF), tip -5 mm in 10 "
+                   f"increments, Newton rtol 1e-6, cg_tol 1e-6")
+    return out
+
+
 def batch_section(count=512, nplain=24, seed=0, workers=None):
     """Batched uneven solves (512 C3D8 cantilevers x 4 right-hand sides, FP32
     matrix-free AMG-PCG inside FP64 refinement to 1e-8) against the plain FP64
@@ -325,13 +365,15 @@ def batch_section(count=512, nplain=24, seed=0, workers=None):
                 max_rel_err_vs_plain_fp64=max(errs), host_setup_s=t_setup)
 
 
-def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e5), j2_frac=0.2, slots=8, seed=0,
+def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), j2_frac=0.2, slots=8, seed=0,
                   nplain=32):
     """Served request stream: a catalogue of seeded C3D8 / C3D10 jittered
     cantilever meshes (DOF log-uniform in `dof`), a fraction `j2_frac` of them J2
     (5 displacement increments), Poisson arrivals at each rate for `duration`
     seconds; p50/p99 latency and solves/s, against serial plain FP64 solves of a
-    sample of the same requests on the same GPU."""
+    sample of the same requests on the same GPU (FP64 matrix-free AMG-PCG with the
+    entry's hierarchy, one solve at a time, no graphs).  Hierarchies are set up on
+    the device by the server's set-up thread."""
     import threading
     import torch
     from exfem_b200 import elements, linalg, mesh, serve
@@ -392,7 +434,7 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e5), 
     out = dict(workload=f"{nmesh} seeded C3D8/C3D10 jittered cantilevers, DOF log-uniform in "
                         f"[{dof[0]:.0e}, {dof[1]:.0e}], {int(100 * j2_frac)}% of meshes J2 (5 increments)",
                slots=slots, rates={})
-    srv = serve.SolveServer(slots=slots, hbm_budget=150e9, setup_workers=8)
+    srv = serve.SolveServer(slots=slots, hbm_budget=150e9, amg_setup="device")
     try:
         t0 = time.time()
         srv.warm(specs)
@@ -430,16 +472,7 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e5), 
             ent = srv.entry(sp.key)
             served_x, _ = srv.submit(q).result()
             if sp.key not in plain_cache:
-                blk0 = Block(sp.conn, sp.etype, LinearElastic(sp.material.E, sp.material.nu), sp.X)
-                Ke = blk0.stiffness(torch.zeros(sp.ndof, dtype=torch.float64, device="cuda"), blk0.init_state())
-                dofs = (sp.conn.astype(np.int64)[:, :, None] * 3 + np.arange(3)).reshape(len(sp.conn), -1)
-                A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke.cpu().numpy())], sp.ndof),
-                                     (~sp.fixed).astype(float))
-                h = dict(levels=[dict(lv) for lv in ent.amg.levels], coarse=ent.amg.coarse,
-                         coarse_inv=ent.amg.coarse_inv, nnz=[1])
-                if h["levels"]:
-                    h["levels"][0]["A"] = A
-                amg = linalg.AMG.from_setup(h)
+                amg = ent.amg                                  # the entry's hierarchy, used in FP64
                 if sp.j2:
                     m = Model(sp.X)
                     m.add_block(sp.conn, sp.etype, sp.material)
@@ -533,7 +566,7 @@ def main():
     ap.add_argument("--count", type=int, default=512, help="cantilevers of the batch mode")
     ap.add_argument("--rates", default="50,200", help="arrival rates (solves/s) of the serve mode")
     ap.add_argument("--duration", type=float, default=15.0, help="seconds per arrival rate (serve mode)")
-    ap.add_argument("--max-dof", type=float, default=2e5, help="largest catalogue mesh (serve mode)")
+    ap.add_argument("--max-dof", type=float, default=2e6, help="largest catalogue mesh (serve mode)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -629,10 +662,11 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e_ms = float(t.item())
 
-    solve = scale_res = None
+    solve = scale_res = j2 = None
     if rank == 0 and not args.no_solve:
         scale_res = scale_solve_section(m, X, scale)
         solve = solve_section()
+        j2 = j2_section()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cv, ci = cpu_baseline()
@@ -658,7 +692,7 @@ def main():
         roofline=dict(bound="hbm", achieved=achieved, peak=pk, unit="GB/s", frac=achieved / pk,
                       traffic=TRAFFIC_BYTES, peak_source=f"{pk_src} (MEASURED_PEAKS.json hbm_gbs)",
                       algorithmic_bytes_per_step=alg_bytes),
-        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve, scale_solve=scale_res)
+        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve, scale_solve=scale_res, j2_newton=j2)
     print(json.dumps(line), flush=True)
 
 

@@ -105,9 +105,9 @@ def _host_setup(args):
 
 
 class _Entry:
-    def __init__(self, spec, setup, graph=True):
+    def __init__(self, spec, setup, graph=True, amg=None):
         self.spec = spec
-        self.amg = linalg.AMG.from_setup(setup)
+        self.amg = amg if amg is not None else linalg.AMG.from_setup(setup)
         if spec.j2:
             self.model = Model(spec.X)
             self.model.add_block(spec.conn, spec.etype, spec.material)
@@ -126,14 +126,19 @@ class SolveServer:
     """Continuous-batching solve server (see the module docstring).
 
     slots: requests in flight at once; hbm_budget: bytes of resident entries;
-    tol: relative residual of linear requests (FP64 refinement); setup_workers:
-    processes for the host aggregation set-up (0: in the set-up thread).
+    tol: relative residual of linear requests (FP64 refinement); amg_setup:
+    "device" (the hierarchy is set up on the GPU by the set-up thread,
+    linalg.DeviceAMG) or "host" (host aggregation set-up in ``setup_workers``
+    spawned processes, 0: in the set-up thread).
     ``solve_fn(entry, request)`` replaces the device solve (host-side tests)."""
 
     def __init__(self, slots=8, hbm_budget=150e9, tol=1e-8, inner_tol=2e-5, setup_workers=4, graph=True,
-                 solve_fn=None, setup_fn=None):
+                 solve_fn=None, setup_fn=None, amg_setup="device"):
+        if amg_setup not in ("device", "host"):
+            raise ValueError(f"unknown AMG set-up {amg_setup!r}")
         self.slots, self.budget, self.tol, self.inner_tol = slots, float(hbm_budget), tol, inner_tol
         self.graph = graph
+        self.amg_setup = amg_setup
         self._solve_fn = solve_fn or self._device_solve
         self._setup_fn = setup_fn or self._device_setup
         self._cv = threading.Condition()
@@ -146,7 +151,7 @@ class SolveServer:
         self.completed = []
         self.evictions = 0
         self._pool = (ProcessPoolExecutor(max_workers=setup_workers, mp_context=mp.get_context("spawn"))
-                      if setup_workers and setup_fn is None else None)
+                      if setup_workers and setup_fn is None and amg_setup == "host" else None)
         self._threads = [threading.Thread(target=self._worker, args=(i,), daemon=True) for i in range(slots)]
         self._threads.append(threading.Thread(target=self._setup_loop, daemon=True))
         for t in self._threads:
@@ -198,6 +203,11 @@ class SolveServer:
     def _device_setup(self, spec):
         blk = Block(spec.conn, spec.etype, LinearElastic(spec.material.E, spec.material.nu), spec.X)
         Ke = blk.stiffness(torch.zeros(spec.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
+        if self.amg_setup == "device":
+            blk.set_fixed(spec.fixed)
+            amg = linalg.DeviceAMG(blk, Ke)
+            del blk, Ke
+            return _Entry(spec, None, self.graph, amg=amg)
         dofs = (spec.conn.astype(np.int64)[:, :, None] * 3 + np.arange(3)).reshape(len(spec.conn), -1)
         job = (dofs, Ke.cpu().numpy(), spec.ndof, (~spec.fixed).astype(np.float64), spec.X)
         del blk, Ke

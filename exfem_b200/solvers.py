@@ -131,10 +131,9 @@ class _LinearSystem:                                                    # solver
         self.m = model
         if amg_setup not in ("auto", "host", "device"):
             raise ValueError(f"unknown AMG set-up {amg_setup!r}")
-        # where the hierarchy is set up: "host" (assembled CSR, worker-free host
-        # set-up), "device" (linalg.DeviceAMG), "auto" = device from the size at
-        # which the reference moves its set-up off the critical path
-        # (ndof >= 150000, gfem/solvers.py:445-452)
+        # where the hierarchy is set up: "host" (assembled CSR, host set-up),
+        # "device" (linalg.DeviceAMG: the same hierarchy, assembled and multiplied
+        # on the GPU); "auto" = device
         self.amg_setup = amg_setup
         if method == "auto":
             method = "direct" if model.ndof <= 20000 else "amg"
@@ -185,7 +184,7 @@ class _LinearSystem:                                                    # solver
         t0 = time.time()
         where = self.amg_setup
         if where == "auto":
-            where = "device" if self.m.ndof >= 150000 else "host"
+            where = "device"
         if where == "device":
             Ke = self._setup_ops(ops, ctx)[0][1]
             self.amg = linalg.DeviceAMG(self.m.blocks[0], Ke)
