@@ -36,6 +36,8 @@ int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int t
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
                    int& maxu);
 int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters, double* relres, cudaStream_t st);
+int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
+                    int maxiter, int* iters, int* updates, double* relres, cudaStream_t st);
 int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, double inner_tol, int max_pass,
                  int maxiter, int* iters, int* passes, double* relres, cudaStream_t st);
 int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st);
@@ -692,10 +694,22 @@ int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, d
   StreamGuard g;
   int st;
   if ((st = g.init(stream))) return st;
-  const int r = solver_mixed(s, b, x, tol, inner_tol, max_pass, maxiter, iters, passes, relres, g.work);
+  const int r = s->mixed_mode == 1
+                    ? solver_mixed_ru(s, b, x, tol, s->mixed_delta, 100 * max_pass, maxiter, iters, passes, relres,
+                                      g.work)
+                    : solver_mixed(s, b, x, tol, inner_tol, max_pass, maxiter, iters, passes, relres, g.work);
   if (r < 0) return r;
   const int w = block_wait_status(s->blk, g.work);
   return w < 0 ? w : r;
+}
+
+int exfem_solver_set_mixed_mode(exfem_solver s, int mode, double delta) {
+  EX_ARG(s, "solver is NULL");
+  EX_ARG(mode == 0 || mode == 1, "mixed mode must be 0 (restarted refinement) or 1 (reliable updates)");
+  EX_ARG(delta > 0 && delta < 1, "reliable-update reduction must lie in (0, 1), got %g", delta);
+  s->mixed_mode = mode;
+  s->mixed_delta = delta;
+  return EXFEM_OK;
 }
 
 int exfem_block_status(exfem_block b, void* stream) {

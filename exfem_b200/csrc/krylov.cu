@@ -180,6 +180,20 @@ __global__ void init_scal_kernel(PcgScal* sc, double tol, int maxiter) {
   sc->done = 0;
 }
 
+// start of a new segment of a PCG recursion that keeps its search direction:
+// stopping tolerance and iteration budget (the other scalars carry over)
+__global__ void segment_scal_kernel(PcgScal* sc, double tol, int maxiter) {
+  sc->spare = tol * tol;
+  sc->k = 0;
+  sc->maxiter = maxiter;
+  sc->done = 0;
+}
+
+__global__ void scale_f32_kernel(int64_t n, float* __restrict__ v, float a) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] *= a;
+}
+
 // ---------------------------------------------------------------- helpers
 static unsigned red_grid(int64_t n) {
   int64_t g = (n + RT * 4 - 1) / (RT * 4);
@@ -296,26 +310,16 @@ int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
   return EXFEM_OK;
 }
 
-// PCG on workspace vectors b (WB) -> x (WX) in precision T
+// hierarchy work vectors, inverse diagonal of the current operator, and (graphs
+// on) the captured chunk of PCG iterations in precision T
 template <class T>
-static int pcg_run(exfem_solver_s* S, double tol, int maxiter, int* iters, double* relres, cudaStream_t st) {
-  const int64_t n = S->n;
+static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
   const int gi = sizeof(T) == 8 ? 0 : 1;
   int s;
   if (S->pc == EXFEM_PC_AMG && !S->amg) { set_error("solver: AMG preconditioner without hierarchy"); return EXFEM_ERR_ARG; }
   if (S->pc == EXFEM_PC_AMG && (s = amg_prepare(S->amg, sizeof(T) == 8 ? EXFEM_F64 : EXFEM_F32))) return s;
   const bool stale = !S->diag_ready || S->diag_tan_gen != S->blk->tan_gen || S->diag_bc_gen != S->blk->bc_gen;
   if (stale && S->pc != EXFEM_PC_NONE && (s = solver_refresh_diagonal(S, st))) return s;
-  T *x = ws<T>(S, WX), *r = ws<T>(S, WR), *z = ws<T>(S, WZ), *p = ws<T>(S, WP), *b = ws<T>(S, WB);
-  init_scal_kernel<<<1, 1, 0, st>>>(S->scal.p, tol, maxiter);
-  EX_LAUNCH_CHECK();
-  EX_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, st));
-  EX_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
-  if ((s = dot<T>(S, b, b, FIN_BB, nullptr, 0, st))) return s;
-  if ((s = pc_apply<T>(S, r, z, nullptr, st))) return s;
-  EX_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
-  if ((s = dot<T>(S, r, z, FIN_RZ0, nullptr, 0, st))) return s;
-  if ((s = dot<T>(S, r, r, FIN_RR0, nullptr, 0, st))) return s;
   const int chunk = S->chunk > 0 ? S->chunk : 8;
   if (S->use_graph) {
     const double* keptr = S->op == EXFEM_OP_EBE_F64 ? S->Ke : nullptr;
@@ -343,6 +347,16 @@ static int pcg_run(exfem_solver_s* S, double tol, int maxiter, int* iters, doubl
       S->g_Ke[gi] = keptr;
     }
   }
+  return EXFEM_OK;
+}
+
+// chunks of PCG iterations until the device "done" flag is set (at most maxiter
+// iterations); the scalars are left in S->h_scal
+template <class T>
+static int pcg_chunks(exfem_solver_s* S, int maxiter, cudaStream_t st) {
+  const int gi = sizeof(T) == 8 ? 0 : 1;
+  const int chunk = S->chunk > 0 ? S->chunk : 8;
+  int s;
   const int max_chunks = maxiter / chunk + 2;
   for (int c = 0; c < max_chunks; ++c) {
     EX_CUDA(cudaMemcpyAsync(S->h_scal, S->scal.p, sizeof(PcgScal), cudaMemcpyDeviceToHost, st));
@@ -357,6 +371,26 @@ static int pcg_run(exfem_solver_s* S, double tol, int maxiter, int* iters, doubl
   }
   EX_CUDA(cudaMemcpyAsync(S->h_scal, S->scal.p, sizeof(PcgScal), cudaMemcpyDeviceToHost, st));
   EX_CUDA(cudaStreamSynchronize(st));
+  return EXFEM_OK;
+}
+
+// PCG on workspace vectors b (WB) -> x (WX) in precision T
+template <class T>
+static int pcg_run(exfem_solver_s* S, double tol, int maxiter, int* iters, double* relres, cudaStream_t st) {
+  const int64_t n = S->n;
+  int s;
+  if ((s = pcg_prepare<T>(S, st))) return s;
+  T *x = ws<T>(S, WX), *r = ws<T>(S, WR), *z = ws<T>(S, WZ), *p = ws<T>(S, WP), *b = ws<T>(S, WB);
+  init_scal_kernel<<<1, 1, 0, st>>>(S->scal.p, tol, maxiter);
+  EX_LAUNCH_CHECK();
+  EX_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * n, st));
+  EX_CUDA(cudaMemcpyAsync(r, b, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+  if ((s = dot<T>(S, b, b, FIN_BB, nullptr, 0, st))) return s;
+  if ((s = pc_apply<T>(S, r, z, nullptr, st))) return s;
+  EX_CUDA(cudaMemcpyAsync(p, z, sizeof(T) * n, cudaMemcpyDeviceToDevice, st));
+  if ((s = dot<T>(S, r, z, FIN_RZ0, nullptr, 0, st))) return s;
+  if ((s = dot<T>(S, r, r, FIN_RR0, nullptr, 0, st))) return s;
+  if ((s = pcg_chunks<T>(S, maxiter, st))) return s;
   const PcgScal& h = *S->h_scal;
   if (iters) *iters = h.k;
   const double rel = sqrt(h.rr / fmax(h.bb, 1e-300));
@@ -448,6 +482,92 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
   }
   if (iters) *iters = its;
   if (passes) *passes = p;
+  if (relres) *relres = rn / bn;
+  return (std::isfinite(rn) && rn <= tol * bn) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
+}
+
+// Mixed precision with reliable updates (Sleijpen & van der Vorst, "Reliable
+// updated residuals in hybrid Bi-CG methods", Computing 56, 1996; used for
+// mixed-precision CG by Clark, Babich, Barros, Brower & Rebbi, Comput. Phys.
+// Commun. 181, 2010): one FP32 PCG recursion (FP32 matrix-free product and V-cycle,
+// FP64 scalars) whose residual is replaced by the FP64 residual b - A64 x every
+// time the recursion has lowered it by `delta` since the last replacement; x is
+// accumulated in FP64 at each replacement.  Unlike restarted refinement the search
+// direction is kept across replacements (rescaled to the new residual's units), so
+// the FP32 iterations stay close to the FP64 PCG count instead of rebuilding the
+// Krylov space in every pass.  A replacement that does not halve the FP64 residual
+// restarts the recursion from the preconditioned residual.  Stops when
+// ||b - A64 x|| <= tol ||b||.  `updates` receives the number of replacements.
+int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
+                    int maxiter, int* iters, int* updates, double* relres, cudaStream_t st) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  if (S->op == EXFEM_OP_EBE_F64) {
+    set_error("mixed refinement needs a matrix-free operator (EXFEM_OP_MF_F32)");
+    return EXFEM_ERR_ARG;
+  }
+  int s;
+  if ((s = pcg_prepare<float>(S, st))) return s;
+  float *x32 = S->x32.p, *r32 = S->r32.p, *z32 = S->z32.p, *p32 = S->p32.p;
+  EX_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+  EX_CUDA(cudaMemcpyAsync(S->r64.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  double bn;
+  if ((s = norm64(S, b, &bn, st))) return s;
+  int its = 0, nup = 0;
+  double rn = bn;
+  if (bn == 0.0) {
+    if (iters) *iters = 0;
+    if (updates) *updates = 0;
+    if (relres) *relres = 0.0;
+    return EXFEM_OK;
+  }
+  double sc = bn, rn_prev = bn;
+  bool restart = true;
+  init_scal_kernel<<<1, 1, 0, st>>>(S->scal.p, 1.0, maxiter);
+  EX_LAUNCH_CHECK();
+  for (;;) {
+    // (re)start a segment from the FP64 residual r64, in units of sc
+    convert_kernel<double, float><<<eg, 256, 0, st>>>(n, S->r64.p, r32, 1.0 / sc, nullptr);
+    EX_LAUNCH_CHECK();
+    EX_CUDA(cudaMemsetAsync(x32, 0, sizeof(float) * n, st));
+    const double seg_tol = std::max(delta, tol * bn / rn);
+    segment_scal_kernel<<<1, 1, 0, st>>>(S->scal.p, seg_tol, std::max(maxiter - its, 0));
+    EX_LAUNCH_CHECK();
+    if ((s = dot<float>(S, r32, r32, FIN_BB, nullptr, 0, st))) return s;
+    if ((s = pc_apply<float>(S, r32, z32, nullptr, st))) return s;
+    if (restart) {
+      EX_CUDA(cudaMemcpyAsync(p32, z32, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    } else {
+      // the iteration that ended the last segment skipped its direction update
+      // (p = z + beta p, beta of that iteration): do it with the replaced residual
+      update_p_kernel<float><<<grid_for(n, 256), 256, 0, st>>>(n, p32, z32, S->scal.p);
+      EX_LAUNCH_CHECK();
+    }
+    if ((s = dot<float>(S, r32, z32, FIN_RZ0, nullptr, 0, st))) return s;
+    if ((s = dot<float>(S, r32, r32, FIN_RR0, nullptr, 0, st))) return s;
+    if ((s = pcg_chunks<float>(S, std::max(maxiter - its, 0), st))) return s;
+    its += S->h_scal->k;
+    // replacement: x += sc x32, r64 = b - A64 x
+    axpy_f32_kernel<<<eg, 256, 0, st>>>(n, x, x32, sc);
+    EX_LAUNCH_CHECK();
+    if ((s = launch_mf_matvec<double>(S->blk, x, S->Ap64.p, nullptr, st))) return s;
+    sub64_kernel<<<eg, 256, 0, st>>>(n, b, S->Ap64.p, S->r64.p);
+    EX_LAUNCH_CHECK();
+    if ((s = norm64(S, S->r64.p, &rn, st))) return s;
+    ++nup;
+    if (!std::isfinite(rn) || rn <= tol * bn || its >= maxiter || nup >= max_updates) break;
+    // keep the search direction in the new residual's units; restart when the
+    // replacement did not halve the FP64 residual (the recursion has stalled)
+    restart = !(rn <= 0.5 * rn_prev);
+    if (!restart) {
+      scale_f32_kernel<<<eg, 256, 0, st>>>(n, p32, (float)(sc / rn));
+      EX_LAUNCH_CHECK();
+    }
+    rn_prev = rn;
+    sc = rn;
+  }
+  if (iters) *iters = its;
+  if (updates) *updates = nup;
   if (relres) *relres = rn / bn;
   return (std::isfinite(rn) && rn <= tol * bn) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
 }

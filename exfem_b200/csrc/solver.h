@@ -73,6 +73,8 @@ struct exfem_solver_s {
   exfem::DevBuf<exfem::PcgScal> scal;
   exfem::PcgScal* h_scal = nullptr;  // pinned
   bool diag_ready = false;
+  int mixed_mode = 1;  // exfem_solver_mixed: 1 = reliable updates, 0 = restarted refinement (the reference's)
+  double mixed_delta = 0.1;  // reliable updates: replace the residual after this reduction
   uint64_t diag_tan_gen = 0, diag_bc_gen = 0, graph_bc_gen = 0;
   // CUDA graphs of `chunk` PCG iterations, one per precision
   int use_graph = 1, chunk = 8;

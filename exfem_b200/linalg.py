@@ -393,7 +393,12 @@ class NativeSolver:
     OPS = {"ebe64": _lib.OP_EBE_F64, "mf64": _lib.OP_MF_F64, "mf32": _lib.OP_MF_F32}
     PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG}
 
-    def __init__(self, block, op="mf32", pc="amg", amg=None, graph=True, chunk=8):
+    def __init__(self, block, op="mf32", pc="amg", amg=None, graph=True, chunk=8, mixed_mode="reliable",
+                 mixed_delta=0.1):
+        """mixed_mode: how :meth:`mixed` runs its FP32 work — "reliable" (one FP32
+        recursion whose residual is replaced by the FP64 one after each reduction by
+        mixed_delta) or "restart" (the reference's restarted refinement,
+        gfem/solvers.py:344-384)."""
         self.block, self.amg = block, amg
         self.op, self.pc = op, pc
         h = C.c_void_p()
@@ -401,6 +406,7 @@ class NativeSolver:
                                       amg.handle if amg is not None else None, C.byref(h)))
         self._h = h
         check(lib.exfem_solver_set_graph(h, 1 if graph else 0, chunk))
+        check(lib.exfem_solver_set_mixed_mode(h, {"reliable": 1, "restart": 0}[mixed_mode], float(mixed_delta)))
         self._Ke = None
         self.last_iters = 0
         self.last_passes = 0

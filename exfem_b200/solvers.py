@@ -127,8 +127,9 @@ class _LinearSystem:                                                    # solver
     """Solves (free K free + fixed I) x = b with the chosen back-end."""
 
     def __init__(self, model, method="auto", tangent="ebe", cg_tol=1e-9, cg_maxiter=20000, monitor=None,
-                 graph=True, amg_setup="auto"):
+                 graph=True, amg_setup="auto", mixed_mode="reliable"):
         self.m = model
+        self.mixed_mode = mixed_mode            # linalg.NativeSolver: "reliable" or "restart"
         if amg_setup not in ("auto", "host", "device"):
             raise ValueError(f"unknown AMG set-up {amg_setup!r}")
         # where the hierarchy is set up: "host" (assembled CSR, host set-up),
@@ -157,13 +158,16 @@ class _LinearSystem:                                                    # solver
     def reset(self):
         self.amg = self.pinned_amg
         self.amg_iters0 = None
-        self._solvers = {}
+        # solvers over a pinned hierarchy stay (with their captured graphs and the FP32
+        # pass tolerance their first mixed solve measured)
+        self._solvers = {k: v for k, v in self._solvers.items() if self.amg is not None and k[2] == id(self.amg)}
 
     def _solver(self, op, pc):
         key = (op, pc, id(self.amg))
         s = self._solvers.get(key)
         if s is None:
-            s = NativeSolver(self.m.blocks[0], op, pc, self.amg if pc == "amg" else None, graph=self.graph)
+            s = NativeSolver(self.m.blocks[0], op, pc, self.amg if pc == "amg" else None, graph=self.graph,
+                             mixed_mode=self.mixed_mode)
             self._solvers = {k: v for k, v in self._solvers.items() if k[2] == id(self.amg)}
             self._solvers[key] = s
         return s
@@ -236,14 +240,15 @@ class _LinearSystem:                                                    # solver
 class StaticSolver:                                                     # solvers.py:481-683
     def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
                  cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None,
-                 amg_setup="auto"):
+                 amg_setup="auto", mixed_mode="reliable"):
         """``amg``: a prebuilt :class:`linalg.AMG` that every step starts from instead
         of assembling and setting up its own (the serving path keeps one resident
         per mesh); the rebuild rule still applies."""
         self.m, self.rtol, self.max_iter = model, rtol, max_iter
         self.mon = monitor or Monitor(verbose)
         self.line_search = line_search
-        self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph, amg_setup)
+        self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph, amg_setup,
+                                 mixed_mode)
         self.lin.pinned_amg = amg
         self.newton_iterations = 0
 

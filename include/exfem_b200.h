@@ -277,12 +277,21 @@ int exfem_solver_set_graph(exfem_solver s, int enable, int chunk);
  * reference's warning condition, gfem/solvers.py:472-473). */
 int exfem_solver_pcg(exfem_solver s, const double* b, double* x, double tol, int maxiter,
                      int* iters, double* relres, void* stream);
-/* FP32 inner PCG (tolerance inner_tol) inside FP64 iterative refinement with an
- * FP64 matrix-free residual, at most max_pass passes, until
- * ||b - A x|| <= tol ||b|| (gfem/solvers.py:344-384 _LinearSystem._mixed). */
+/* FP32 matrix-free PCG with FP32 V-cycle inside FP64 iterative refinement with an
+ * FP64 matrix-free residual, until ||b - A x|| <= tol ||b|| (gfem/solvers.py:344-384
+ * _LinearSystem._mixed); how the FP32 work is organised: exfem_solver_set_mixed_mode. */
 int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, double inner_tol,
                        int max_pass, int maxiter, int* iters, int* passes, double* relres,
                        void* stream);
+/* How exfem_solver_mixed runs its FP32 work.  Mode 1 (default): one FP32 PCG
+ * recursion whose residual is replaced by the FP64 residual b - A x whenever it
+ * has dropped by delta (default 0.1) since the last replacement, the search direction kept
+ * (reliable updates, Sleijpen & van der Vorst 1996); inner_tol is not used, `passes`
+ * returns the number of replacements (at most 100 x max_pass).  Mode 0: the
+ * reference's restarted refinement (gfem/solvers.py:344-384): each pass a new FP32
+ * PCG to inner_tol on the scaled FP64 residual (passes after the first stop at the
+ * reduction the first pass attained, and at 4x its iterations). */
+int exfem_solver_set_mixed_mode(exfem_solver s, int mode, double delta);
 
 /* ------------------------------------------------------------ batched solves
  * Many independent linear-elastic systems in one set of launches (no counterpart
