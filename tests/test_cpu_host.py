@@ -279,3 +279,67 @@ def test_skin_and_pressure_vector_match_oracle():
     assert abs(area - 6.0) < 1e-12 and np.abs(nsum).max() < 1e-12 and abs(w.sum() - 6.0) < 1e-12
     ft = loads.traction_vector(Xh, surfaces.sub_surface(skh, toph), [1.0, 0.0, 0.0]).reshape(-1, 3)
     np.testing.assert_allclose(ft.sum(0), [1.0, 0.0, 0.0], atol=1e-12)
+
+
+def test_deck_reader_fixture():
+    """Input-deck reader (gfem/io/inp.py semantics) on the committed C3D10 fixture
+    (tests/golden/make_deck.py): nodes, connectivity in deck order through the
+    labels, generated and listed node sets, the element-face surface, the encastre,
+    the concentrated tip load and the pressure vector of the surface against the
+    oracle's skin / sub-surface / pressure restatement."""
+    import importlib.util
+
+    from exfem_b200 import deck
+    from oracle import loads as oloads
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_deck", os.path.join(here, "make_deck.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    ref = mk.case()
+    d = deck.InpDeck(os.path.join(here, "cantilever_c3d10.inp"))
+    np.testing.assert_array_equal(d.X, ref["X"])
+    np.testing.assert_array_equal(d.node_ids, ref["node_labels"])
+    assert len(d.blocks) == 1 and d.blocks[0]["etype"].name == "C3D10"
+    np.testing.assert_array_equal(d.blocks[0]["conn"], ref["conn"])
+    np.testing.assert_array_equal(d.blocks[0]["labels"], ref["elem_labels"])
+    np.testing.assert_array_equal(np.sort(d.node_indices("FIX")), np.sort(ref["fix"]))
+    np.testing.assert_array_equal(d.node_indices("FIRST_NODES"), np.arange(10))
+    m = d.blocks[0]["material"]
+    assert (m.E, m.nu) == (mk.E, mk.NU)
+    (st,) = d.step_objects()
+    assert st.name == "Load" and st.T == 1.0 and st.max_inc == 100
+    fixed = {(int(n), k) for nodes, k, v in st.bcs for n in nodes if v == 0.0}
+    assert fixed == {(int(n), k) for n in ref["fix"] for k in range(3)}
+    assert [(list(n), k, v) for n, k, v in st.loads] == [([ref["tip"]], 2, mk.TIP_LOAD)]
+    top = np.nonzero(ref["X"][:, 2] > 1 - 1e-9)[0]
+    skin = oloads.skin_tet10(ref["X"], ref["conn"])
+    fo = oloads.pressure_vector(ref["X"], oloads.sub_surface(skin, top, len(ref["X"])), mk.PRESSURE)
+    (f,) = st.dloads
+    np.testing.assert_allclose(f, fo, rtol=0, atol=1e-13 * np.abs(fo).max())
+    assert abs(f.reshape(-1, 3)[:, 2].sum() - (-mk.PRESSURE) * 4.0) < 1e-12
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/examples/decks"), reason="reference decks not present")
+def test_deck_reader_reference_examples():
+    """The reference's own static C3D10 example decks parse: node and element counts
+    against a plain count of their data lines, one static step each, the bracket's
+    concentrated loads and the plate's pressure (total force along +x)."""
+    from exfem_b200 import deck
+    for name, nload, ndl in (("bracket", 113, 0), ("plate_hole", 0, 1)):
+        path = f"/root/reference/examples/decks/{name}.inp"
+        counts, card = {"NODE": 0, "ELEMENT": 0}, None
+        with open(path) as fh:
+            for line in fh:
+                s = line.strip()
+                if s.startswith("**") or not s:
+                    continue
+                if s.startswith("*"):
+                    card = s[1:].split(",")[0].strip().upper()
+                elif card in counts:
+                    counts[card] += 1
+        d = deck.InpDeck(path)
+        assert len(d.X) == counts["NODE"] and sum(len(b["conn"]) for b in d.blocks) == counts["ELEMENT"]
+        (st,) = d.step_objects()
+        assert len(st.loads) == nload and len(st.dloads) == ndl and len(st.bcs) > 0
+        if ndl:
+            assert st.dloads[0].reshape(-1, 3).sum(0)[0] > 0

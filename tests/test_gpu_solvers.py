@@ -246,3 +246,31 @@ def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
     torch.cuda.synchronize()
     assert torch.isfinite(y).all()
     assert lib.exfem_block_status(blk.handle, stream_ptr()) == _lib.OK
+
+
+def test_deck_solve_matches_oracle(cuda):
+    """An input deck read by the deck reader (tests/golden/cantilever_c3d10.inp:
+    encastre, surface pressure, tip load) solved on the device (mixed path) against
+    the oracle's direct solve of the same problem built from the generator's arrays
+    and the oracle's own pressure restatement: 1e-8 relative."""
+    import importlib.util
+    import os
+
+    from exfem_b200 import deck
+    from oracle import loads as oloads
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_deck", os.path.join(here, "make_deck.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    ref = mk.case()
+    m, steps = deck.read_inp(os.path.join(here, "cantilever_c3d10.inp"))
+    import exfem_b200 as xf
+    up, _, _ = xf.StaticSolver(m, rtol=1e-6, linear_solver="mixed", cg_tol=1e-10, verbose=False).solve(steps[0])
+    X, c = ref["X"], ref["conn"]
+    top = np.nonzero(X[:, 2] > 1 - 1e-9)[0]
+    f = oloads.pressure_vector(X, oloads.sub_surface(oloads.skin_tet10(X, c), top, len(X)), mk.PRESSURE)
+    om = ofem.Model(X)
+    om.add_block(c, ofem.TET10, ofem.LinearElastic(mk.E, mk.NU))
+    st = osol.Step(bcs=[(ref["fix"], d, 0.0) for d in range(3)], loads=[([ref["tip"]], 2, mk.TIP_LOAD)], dloads=[f])
+    uo, _, _ = osol.StaticSolver(om, rtol=1e-6).solve(st)
+    assert rel_err(up, uo) < 1e-8
