@@ -181,14 +181,12 @@ __global__ void bnorm_init_kernel(const int64_t* __restrict__ off, const double*
   }
 }
 
-// after the first pass, per instance (the rule of the single-solve refinement):
-// later passes stop their FP32 recursion at the reduction the first pass attained
-// in FP64 (not below inner_tol) and at 4x the first pass's iterations
+// after the first pass, per instance (the rule of the single-solve restarted
+// refinement): later passes stop at 4x the first pass's iterations
 __global__ void badapt_kernel(int m, BatchScal S, double inner_tol, int maxiter) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   S.cap[i] = min(maxiter, max(4 * S.k[i], 32));
-  S.itol[i] = fmin(fmax(inner_tol, S.rn[i] / S.sc[i]), 0.1);
 }
 
 }  // namespace exfem

@@ -446,16 +446,13 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
   if (bn == 0.0) bn = 1.0;
   int its = 0, p = 0;
   double rn = bn;
-  // Passes after the first adapt to the accuracy FP32 attains on this operator.
-  // A pass can only lower the FP64 residual by the FP32 operator's attainable
-  // accuracy (about 1e-3 relative on a 12.5M-DOF C3D10 cube), however far its own
-  // recursion goes; so later passes stop their recursion at the reduction the first
-  // pass actually achieved in FP64 (never below inner_tol), and at 4x the first
-  // pass's iteration count.  The reference runs every pass to inner_tol and
-  // cg_maxiter; a later pass's recursion, whose right-hand side is the
-  // rounding-level residual of the previous one, can stall above inner_tol there.
+  // Passes after the first stop at 4x the first pass's iteration count: a pass can
+  // only lower the FP64 residual by the FP32 operator's attainable accuracy (about
+  // 1e-3 relative on a 12.5M-DOF C3D10 cube), and the recursion of a later pass,
+  // whose right-hand side is the rounding-level residual of the previous one, can
+  // stall above inner_tol there (the reference runs it to cg_maxiter).
   int cap = maxiter;
-  double itol = inner_tol;
+  const double itol = inner_tol;
   for (p = 0; p < max_pass; ++p) {
     double sc;
     if ((s = norm64(S, S->r64.p, &sc, st))) return s;
@@ -475,10 +472,7 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
     if ((s = norm64(S, S->r64.p, &rn, st))) return s;
     if (!std::isfinite(rn)) break;
     if (rn <= tol * bn) { ++p; break; }
-    if (p == 0) {
-      cap = std::min(maxiter, std::max(4 * k, 32));
-      itol = std::min(std::max(inner_tol, rn / sc), 0.1);
-    }
+    if (p == 0) cap = std::min(maxiter, std::max(4 * k, 32));
   }
   if (iters) *iters = its;
   if (passes) *passes = p;

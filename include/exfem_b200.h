@@ -289,8 +289,8 @@ int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, d
  * (reliable updates, Sleijpen & van der Vorst 1996); inner_tol is not used, `passes`
  * returns the number of replacements (at most 100 x max_pass).  Mode 0: the
  * reference's restarted refinement (gfem/solvers.py:344-384): each pass a new FP32
- * PCG to inner_tol on the scaled FP64 residual (passes after the first stop at the
- * reduction the first pass attained, and at 4x its iterations). */
+ * PCG to inner_tol on the scaled FP64 residual (passes after the first stop at 4x
+ * the first pass's iterations). */
 int exfem_solver_set_mixed_mode(exfem_solver s, int mode, double delta);
 
 /* ------------------------------------------------------------ batched solves
