@@ -93,6 +93,9 @@ _SIGS = {
     "exfem_host_gather_plan": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_colouring": ([I64, I64, C.c_int, P, P, C.POINTER(I32)], C.c_int),
     "exfem_host_standard_aggregation": ([I64, P, P, P, C.POINTER(I64)], C.c_int),
+    "exfem_host_node_adjacency": ([I64, I64, I32, P, C.POINTER(I64), P, P], C.c_int),
+    "exfem_host_fit_candidates": ([I64, I32, I32, P, I64, P, P, P], C.c_int),
+    "exfem_host_coarse_inverse": ([I64, P, P], C.c_int),
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
     "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
     "exfem_block_status": ([VP, VP], C.c_int),

@@ -792,6 +792,38 @@ int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn,
   return EXFEM_OK;
 }
 
+int exfem_host_node_adjacency(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int64_t* nnz, int64_t* ptr,
+                              int32_t* idx) {
+  EX_ARG(nn >= 0 && ne >= 0 && nnode > 0 && (ne == 0 || conn) && nnz && ptr, "invalid arguments");
+  Rows r;
+  int st;
+  if ((st = host_node_adjacency(nn, ne, nnode, conn, r))) return st;
+  *nnz = (int64_t)r.idx.size();
+  std::copy(r.ptr.begin(), r.ptr.end(), ptr);
+  if (idx) std::copy(r.idx.begin(), r.idx.end(), idx);
+  return EXFEM_OK;
+}
+
+int exfem_host_fit_candidates(int64_t nb, int bs, int K, const int32_t* agg, int64_t nagg, const double* B,
+                              double* Q, double* Bc) {
+  EX_ARG(nb >= 0 && bs > 0 && K > 0 && nagg >= 0 && agg && B && Q && Bc, "invalid arguments");
+  for (int64_t n = 0; n < nb; ++n) EX_ARG(agg[n] < nagg, "aggregate %d of node %lld out of range", agg[n], (long long)n);
+  std::vector<double> q, bc;
+  host_fit_candidates(nb, bs, K, agg, nagg, B, q, bc);
+  std::copy(q.begin(), q.end(), Q);
+  std::copy(bc.begin(), bc.end(), Bc);
+  return EXFEM_OK;
+}
+
+int exfem_host_coarse_inverse(int64_t n, const double* A, double* Ainv) {
+  EX_ARG(n > 0 && A && Ainv, "invalid arguments");
+  std::vector<double> a(A, A + n * n), inv;
+  int st;
+  if ((st = host_coarse_inverse(n, a, inv))) return st;
+  std::copy(inv.begin(), inv.end(), Ainv);
+  return EXFEM_OK;
+}
+
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
   EX_ARG(ptr && idx && agg && nagg, "NULL argument");
   return host_standard_aggregation(n, ptr, idx, agg, *nagg);

@@ -320,6 +320,22 @@ int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn,
                          int* ncolour);
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx,
                                     int32_t* agg, int64_t* nagg);
+/* Host graph steps of the device smoothed-aggregation set-up (exfem_amg_setup_block),
+ * exported for checking (no counterpart in the reference; pyamg does these steps
+ * inside smoothed_aggregation_solver, gfem/linalg.py:113-116):
+ * node adjacency of a mesh (row n: every node sharing an element with n, itself
+ * included, ascending) — call with idx NULL for ptr (nn+1) and *nnz, then with idx;
+ * tentative prolongator of an aggregation (per aggregate, modified Gram-Schmidt of
+ * the K near-null-space columns B (nb*bs, K) over its DOFs in increasing order,
+ * columns below 1e-10 of their norm dropped): Q (nb*bs, K) orthonormal rows of each
+ * DOF, Bc (nagg*K, K) the coarse near-null space;
+ * coarsest inverse: A (n, n) symmetrised, 1e-13 max|A| added to the diagonal,
+ * Cholesky, Ainv = L^-T L^-1 (gfem/linalg.py:122-133). */
+int exfem_host_node_adjacency(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int64_t* nnz, int64_t* ptr,
+                              int32_t* idx);
+int exfem_host_fit_candidates(int64_t nb, int bs, int K, const int32_t* agg, int64_t nagg, const double* B,
+                              double* Q, double* Bc);
+int exfem_host_coarse_inverse(int64_t n, const double* A, double* Ainv);
 /* tile order of the matrix-free operator (see exfem_block_tile_order) for a mesh
  * of ne elements with nnode nodes each, the first ncorner of them corners:
  * order (ne,) position -> element.  No counterpart in the reference. */

@@ -343,3 +343,50 @@ def test_deck_reader_reference_examples():
         assert len(st.loads) == nload and len(st.dloads) == ndl and len(st.bcs) > 0
         if ndl:
             assert st.dloads[0].reshape(-1, 3).sum(0)[0] > 0
+
+
+def test_device_setup_host_steps():
+    """Host graph steps of the device smoothed-aggregation set-up, checked on CPU:
+    the node adjacency against a brute-force set union over the elements, the
+    tentative prolongator against the host set-up's NumPy modified Gram-Schmidt
+    (linalg._fit_candidates) on a real aggregation of a C3D10 mesh with rigid-body
+    modes, and the regularised Cholesky inverse of the coarsest matrix against
+    NumPy."""
+    X, c = tet10_box(2.0, 1.0, 1.0, 4, 2, 2)
+    nn, ne = len(X), len(c)
+    conn = np.ascontiguousarray(c, dtype=np.int32)
+    nnz, ptr = C.c_int64(), np.zeros(nn + 1, np.int64)
+    _lib.check(_lib.lib.exfem_host_node_adjacency(nn, ne, 10, conn.ctypes.data, C.byref(nnz), ptr.ctypes.data, None))
+    idx = np.zeros(nnz.value, np.int32)
+    _lib.check(_lib.lib.exfem_host_node_adjacency(nn, ne, 10, conn.ctypes.data, C.byref(nnz), ptr.ctypes.data,
+                                                  idx.ctypes.data))
+    nb = [set() for _ in range(nn)]
+    for row in c:
+        for a in row:
+            nb[a].update(int(b) for b in row)
+    for n in range(nn):
+        np.testing.assert_array_equal(idx[ptr[n]:ptr[n + 1]], sorted(nb[n] | {n}))
+    # aggregation of the adjacency graph, tentative prolongator with rigid-body modes
+    agg = np.zeros(nn, np.int32)
+    nagg = C.c_int64()
+    _lib.check(_lib.lib.exfem_host_standard_aggregation(nn, ptr.ctypes.data, idx.ctypes.data, agg.ctypes.data,
+                                                        C.byref(nagg)))
+    B = np.ascontiguousarray(linalg.rigid_body_modes(X))
+    Q = np.zeros((3 * nn, 6))
+    Bc = np.zeros((nagg.value * 6, 6))
+    _lib.check(_lib.lib.exfem_host_fit_candidates(nn, 3, 6, agg.ctypes.data, nagg.value, B.ctypes.data, Q.ctypes.data,
+                                                  Bc.ctypes.data))
+    T, Bc_ref = linalg._fit_candidates(agg, nagg.value, B, 3)
+    Qref = np.zeros_like(Q)
+    Td = T.tocoo()
+    Qref[Td.row, Td.col % 6] = Td.data
+    np.testing.assert_allclose(Q, Qref, rtol=0, atol=1e-13)
+    np.testing.assert_allclose(Bc, Bc_ref, rtol=0, atol=1e-12 * np.abs(Bc_ref).max())
+    # coarsest inverse
+    rng = np.random.default_rng(4)
+    M = rng.standard_normal((30, 30))
+    A = M @ M.T + 30 * np.eye(30)
+    Ainv = np.zeros_like(A)
+    _lib.check(_lib.lib.exfem_host_coarse_inverse(30, np.ascontiguousarray(A).ctypes.data, Ainv.ctypes.data))
+    ref = np.linalg.inv(A + 1e-13 * np.abs(A).max() * np.eye(30))
+    np.testing.assert_allclose(Ainv, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
