@@ -698,9 +698,12 @@ template <class T>
 __global__ void mf_gather_kernel(int64_t nm, const int32_t* __restrict__ mnodes, const int32_t* __restrict__ mptr,
                                  const T* __restrict__ part, const T* __restrict__ v, T* __restrict__ y,
                                  const int* __restrict__ skip) {
-  constexpr int U = 4;
+  // U nodes per thread, the first R entries of each run loaded before any is added
+  // (every load in flight at once); entries are still added in run order
+  constexpr int U = 4, R = 2;
   if (skip && *skip) return;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const Node4<T>* P = reinterpret_cast<const Node4<T>*>(part);
   for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < nm; i0 += U * stride) {
     uint32_t id[U];
     int32_t q0[U], q1[U];
@@ -711,15 +714,28 @@ __global__ void mf_gather_kernel(int64_t nm, const int32_t* __restrict__ mnodes,
       q0[u] = i < nm ? mptr[i] : 0;
       q1[u] = i < nm ? mptr[i + 1] : 0;
     }
+    Node4<T> w[U][R];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (q0[u] + r < q1[u]) w[u][r] = P[q0[u] + r];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (i0 + u * stride >= nm) break;
       T s0 = T(0), s1 = T(0), s2 = T(0);
-      for (int32_t q = q0[u]; q < q1[u]; ++q) {
-        const Node4<T> w = reinterpret_cast<const Node4<T>*>(part)[q];
-        s0 += w.x;
-        s1 += w.y;
-        s2 += w.z;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (q0[u] + r < q1[u]) {
+          s0 += w[u][r].x;
+          s1 += w[u][r].y;
+          s2 += w[u][r].z;
+        }
+      for (int32_t q = q0[u] + R; q < q1[u]; ++q) {
+        const Node4<T> e = P[q];
+        s0 += e.x;
+        s1 += e.y;
+        s2 += e.z;
       }
       const int64_t d = 3 * (int64_t)(id[u] & 0x0FFFFFFFu);
       const uint32_t bits = id[u] >> 28;
