@@ -319,14 +319,21 @@ def test_deck_reader_fixture():
     assert abs(f.reshape(-1, 3)[:, 2].sum() - (-mk.PRESSURE) * 4.0) < 1e-12
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/examples/decks"), reason="reference decks not present")
+# the reference checkout (its example decks are read where they lie, when present)
+REF_DIR = os.environ.get("EXFEM_REFERENCE_DIR",
+                         os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                                      "reference"))
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REF_DIR, "examples", "decks")),
+                    reason="reference decks not present")
 def test_deck_reader_reference_examples():
     """The reference's own static C3D10 example decks parse: node and element counts
     against a plain count of their data lines, one static step each, the bracket's
     concentrated loads and the plate's pressure (total force along +x)."""
     from exfem_b200 import deck
     for name, nload, ndl in (("bracket", 113, 0), ("plate_hole", 0, 1)):
-        path = f"/root/reference/examples/decks/{name}.inp"
+        path = os.path.join(REF_DIR, "examples", "decks", f"{name}.inp")
         counts, card = {"NODE": 0, "ELEMENT": 0}, None
         with open(path) as fh:
             for line in fh:
