@@ -397,3 +397,75 @@ def test_device_setup_host_steps():
     _lib.check(_lib.lib.exfem_host_coarse_inverse(30, np.ascontiguousarray(A).ctypes.data, Ainv.ctypes.data))
     ref = np.linalg.inv(A + 1e-13 * np.abs(A).max() * np.eye(30))
     np.testing.assert_allclose(Ainv, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+
+
+def test_deck_reader_step_semantics(tmp_path):
+    """Boundary conditions and loads across steps as the reference reader carries
+    them (gfem/io/inp.py:518-616): *INCLUDE, GENERATE sets, DOF ranges with a value,
+    symmetry keywords, accumulation from step to step, OP=NEW, a later value of the
+    same node and DOF winning, and the static time increments."""
+    from exfem_b200 import deck
+    nodes = "\n".join(f"{10 + i}, {i % 3}.0, {(i // 3) % 3}.0, {i // 9}.0" for i in range(27))
+    (tmp_path / "nodes.inp").write_text("*NODE, NSET=ALLN\n" + nodes + "\n")
+    conn = [[0, 1, 4, 3, 9, 10, 13, 12], [1, 2, 5, 4, 10, 11, 14, 13], [3, 4, 7, 6, 12, 13, 16, 15],
+            [4, 5, 8, 7, 13, 14, 17, 16], [9, 10, 13, 12, 18, 19, 22, 21], [10, 11, 14, 13, 19, 20, 23, 22],
+            [12, 13, 16, 15, 21, 22, 25, 24], [13, 14, 17, 16, 22, 23, 26, 25]]
+    elems = "\n".join(f"{100 + e}, " + ", ".join(str(10 + n) for n in row) for e, row in enumerate(conn))
+    text = f"""*HEADING
+semantics
+*INCLUDE, INPUT=nodes.inp
+*ELEMENT, TYPE=C3D8R, ELSET=EALL
+{elems}
+*NSET, NSET=BASE, GENERATE
+10, 18, 1
+*NSET, NSET=TOPC
+36
+*SOLID SECTION, ELSET=EALL, MATERIAL=AL
+*MATERIAL, NAME=AL
+*ELASTIC
+70000., 0.33
+*PLASTIC
+100., 0.
+200., 0.5
+*BOUNDARY
+BASE, ZSYMM
+*STEP, NAME=one
+*STATIC
+0.1, 1., 1e-4, 0.25
+*BOUNDARY
+10, 1, 2
+*CLOAD
+TOPC, 3, -1.5
+36, 1, 2.0
+*END STEP
+*STEP, NAME=two
+*STATIC
+*BOUNDARY
+36, 1, 2, 0.25
+*CLOAD
+TOPC, 3, -3.0
+*END STEP
+*STEP, NAME=three
+*STATIC
+*BOUNDARY, OP=NEW
+11, 3, 3, 0.5
+*CLOAD, OP=NEW
+TOPC, 2, 1.0
+*END STEP
+"""
+    path = tmp_path / "sem.inp"
+    path.write_text(text)
+    d = deck.InpDeck(str(path))
+    assert len(d.X) == 27 and len(d.blocks) == 1 and d.blocks[0]["etype"].name == "C3D8"
+    m = d.blocks[0]["material"]
+    assert type(m).__name__ == "J2Plasticity"
+    one, two, three = d.step_objects()
+    flat = lambda items: {(int(n), k): v for ns, k, v in items for n in ns}
+    base = {(n, 2): 0.0 for n in range(9)}
+    assert (one.dt_init, one.T, one.dt_min, one.dt_max) == (0.1, 1.0, 1e-4, 0.25)
+    assert flat(one.bcs) == {**base, (0, 0): 0.0, (0, 1): 0.0}
+    assert flat(one.loads) == {(26, 2): -1.5, (26, 0): 2.0}
+    assert flat(two.bcs) == {**base, (0, 0): 0.0, (0, 1): 0.0, (26, 0): 0.25, (26, 1): 0.25}
+    assert flat(two.loads) == {(26, 2): -3.0, (26, 0): 2.0}
+    assert flat(three.bcs) == {**base, (1, 2): 0.5}
+    assert flat(three.loads) == {(26, 1): 1.0}
