@@ -101,6 +101,8 @@ _SIGS = {
     "exfem_block_status": ([VP, VP], C.c_int),
     "exfem_amg_setup_block": ([VP, VP, P, I32, I32, VP], C.c_int),
     "exfem_amg_info": ([VP, I32, P, P, P], C.c_int),
+    "exfem_amg_export_level": ([VP, I32, I32, P, P, P, P, P, P, P], C.c_int),
+    "exfem_amg_export_coarse": ([VP, P, P], C.c_int),
     "exfem_solver_set_mixed_mode": ([VP, I32, D], C.c_int),
     "exfem_selftest_bounded_wait": ([I32, VP], C.c_int),
     "exfem_block_tile_conn": ([VP, P], C.c_int),

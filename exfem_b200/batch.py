@@ -77,6 +77,21 @@ def _element_stiffness(p):
     return dofs, Ke.cpu().numpy()
 
 
+def device_setups(problems, max_coarse=300):
+    """Per-problem hierarchies set up on the device (linalg.DeviceAMG, the host
+    set-up's algorithm with the assembly and the products on the GPU), copied to the
+    host in the form :func:`host_setups` returns, one problem after the other."""
+    out = []
+    for p in problems:
+        blk = Block(p.conn, p.etype, p.material, p.X)
+        blk.set_fixed(p.fixed)
+        Ke = blk.stiffness(torch.zeros(p.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
+        amg = linalg.DeviceAMG(blk, Ke, max_coarse)
+        out.append(amg.to_setup())
+        del amg, Ke, blk
+    return out
+
+
 def host_setups(problems, max_coarse=300, workers=None, stiffness=None):
     """Per-problem host hierarchies.  Element stiffness matrices (``stiffness``, a
     list of (dofs, Ke) per problem) come from the GPU unless given; assembly and
@@ -155,7 +170,9 @@ class BatchSolver:
     displacement.  Instances are ordered problem by problem, right-hand side by
     right-hand side."""
 
-    def __init__(self, problems, max_coarse=300, workers=None, setups=None):
+    def __init__(self, problems, max_coarse=300, workers=None, setups=None, amg_setup="device"):
+        """amg_setup: "device" (per-problem hierarchies set up on the GPU, the
+        default) or "host" (assembled CSR and host set-up in ``workers`` processes)."""
         _lib.require_cuda()
         t0 = time.time()
         self.problems = list(problems)
@@ -165,7 +182,14 @@ class BatchSolver:
         if len(et) != 1:
             raise ValueError(f"one element type per batch, got {sorted(et)}")
         self.etype = self.problems[0].etype
-        self.setups = setups if setups is not None else host_setups(self.problems, max_coarse, workers)
+        if setups is not None:
+            self.setups = setups
+        elif amg_setup == "device":
+            self.setups = device_setups(self.problems, max_coarse)
+        elif amg_setup == "host":
+            self.setups = host_setups(self.problems, max_coarse, workers)
+        else:
+            raise ValueError(f"unknown AMG set-up {amg_setup!r}")
         self.t_host = time.time() - t0
         # instances: one per (problem, right-hand side)
         self.inst = [(k, r) for k, p in enumerate(self.problems) for r in range(len(p.rhs))]

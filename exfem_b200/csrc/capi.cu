@@ -736,6 +736,42 @@ int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_
   return st;
 }
 
+int exfem_amg_export_level(exfem_amg h, int level, int what, int64_t* rows, int64_t* cols, int64_t* nnz,
+                           int64_t* ptr, int32_t* idx, double* val, double* rho) {
+  EX_ARG(h && rows && cols && nnz, "NULL argument");
+  EX_ARG(level >= 0 && level < (int)h->levels.size(), "level %d out of range", level);
+  EX_ARG(!h->replicated, "replicated hierarchies are not exported");
+  EX_ARG(what >= 0 && what <= 3, "what must be 0 (A), 1 (P), 2 (R) or 3 (inverse diagonal)");
+  const AmgLevel& L = *h->levels[level];
+  if (rho) *rho = L.rho;
+  if (what == 3) {
+    *rows = L.n;
+    *cols = 1;
+    *nnz = L.n;
+    if (val && L.n) EX_CUDA(cudaMemcpy(val, L.dinv64.p, sizeof(double) * L.n, cudaMemcpyDeviceToHost));
+    return EXFEM_OK;
+  }
+  const Csr64& M = what == 0 ? L.A : what == 1 ? L.P : L.R;
+  *rows = M.n;
+  *cols = M.ncols;
+  *nnz = M.nnz;
+  if (ptr) {
+    if (M.ptr.p) EX_CUDA(cudaMemcpy(ptr, M.ptr.p, sizeof(int64_t) * (M.n + 1), cudaMemcpyDeviceToHost));
+    else std::fill(ptr, ptr + M.n + 1, (int64_t)0);
+  }
+  if (idx && M.nnz) EX_CUDA(cudaMemcpy(idx, M.idx.p, sizeof(int32_t) * M.nnz, cudaMemcpyDeviceToHost));
+  if (val && M.nnz) EX_CUDA(cudaMemcpy(val, M.v64.p, sizeof(double) * M.nnz, cudaMemcpyDeviceToHost));
+  return EXFEM_OK;
+}
+
+int exfem_amg_export_coarse(exfem_amg h, int64_t* nc, double* Ainv) {
+  EX_ARG(h && nc, "NULL argument");
+  EX_ARG(!h->replicated && !h->crow_s.p, "block-diagonal coarsest solves are not exported");
+  *nc = h->nc;
+  if (Ainv && h->nc) EX_CUDA(cudaMemcpy(Ainv, h->Ainv.p, sizeof(double) * h->nc * h->nc, cudaMemcpyDeviceToHost));
+  return EXFEM_OK;
+}
+
 int exfem_amg_info(exfem_amg h, int cap, int* nlevels, int64_t* rows, int64_t* nnz) {
   EX_ARG(h && nlevels, "NULL argument");
   const int nl = (int)h->levels.size() + (h->nc > 0 ? 1 : 0);

@@ -382,6 +382,39 @@ class DeviceAMG(AMG):
         self.keep_level0 = keep_level0
         self.setup_time = time.time() - t0
 
+    def _export(self, level, what):
+        rows, cols, nnz, rho = C.c_int64(), C.c_int64(), C.c_int64(), C.c_double()
+        check(lib.exfem_amg_export_level(self._h, level, what, C.byref(rows), C.byref(cols), C.byref(nnz), None, None,
+                                         None, C.byref(rho)))
+        if what == 3:
+            v = np.zeros(rows.value)
+            check(lib.exfem_amg_export_level(self._h, level, 3, C.byref(rows), C.byref(cols), C.byref(nnz), None,
+                                             None, v.ctypes.data, None))
+            return v, rho.value
+        ptr_ = np.zeros(rows.value + 1, np.int64)
+        idx = np.zeros(max(nnz.value, 1), np.int32)
+        val = np.zeros(max(nnz.value, 1))
+        check(lib.exfem_amg_export_level(self._h, level, what, C.byref(rows), C.byref(cols), C.byref(nnz),
+                                         ptr_.ctypes.data, idx.ctypes.data, val.ctypes.data, None))
+        return sp.csr_matrix((val[:nnz.value], idx[:nnz.value], ptr_), shape=(rows.value, cols.value)), rho.value
+
+    def to_setup(self):
+        """The hierarchy as the dict :func:`amg_setup` returns (levels with A — None
+        where no matrix is stored —, P, R, dinv, rho, n, nc; coarse_inv), e.g. to
+        merge it into a batched union (``batch.union_hierarchy``)."""
+        levels = []
+        for l in range(len(self.sizes) - 1):
+            A, _ = self._export(l, 0)
+            P, _ = self._export(l, 1)
+            R, _ = self._export(l, 2)
+            dinv, rho = self._export(l, 3)
+            levels.append(dict(A=A if A.nnz else None, P=P, R=R, dinv=dinv, rho=rho, n=P.shape[0], nc=P.shape[1]))
+        nc = C.c_int64()
+        check(lib.exfem_amg_export_coarse(self._h, C.byref(nc), None))
+        Ainv = np.zeros((nc.value, nc.value))
+        check(lib.exfem_amg_export_coarse(self._h, C.byref(nc), Ainv.ctypes.data))
+        return dict(levels=levels, coarse=None, coarse_inv=Ainv, nnz=list(self.nnz))
+
 
 # ------------------------------------------------------------------ native solver
 class NativeSolver:

@@ -216,6 +216,15 @@ int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_
 /* level count (coarsest included) and, for the first cap levels, rows and
  * operator nonzeros (AMG.info, gfem/linalg.py:135, 148-154). */
 int exfem_amg_info(exfem_amg h, int cap, int* nlevels, int64_t* rows, int64_t* nnz);
+/* copy one level of a (not replicated) hierarchy to the host: what 0 = A, 1 = P,
+ * 2 = R (scalar CSR: rows, cols, nnz; ptr (rows+1), idx, val when not NULL; a level
+ * without a stored matrix reports nnz 0), 3 = the inverse diagonal (rows values in
+ * val); rho (may be NULL) receives the level's spectral bound.  The coarsest
+ * level's dense inverse: exfem_amg_export_coarse (Ainv nc*nc, may be NULL).  Used to
+ * merge hierarchies set up on the device into a batched union. */
+int exfem_amg_export_level(exfem_amg h, int level, int what, int64_t* rows, int64_t* cols, int64_t* nnz,
+                           int64_t* ptr, int32_t* idx, double* val, double* rho);
+int exfem_amg_export_coarse(exfem_amg h, int64_t* nc, double* Ainv);
 /* Union of independent hierarchies (batched solves, no counterpart in the
  * reference): per-row spectral bounds of level `level` (n doubles; each row
  * smoothed with its own instance's Chebyshev coefficients, degree 2; a bound of 0

@@ -39,7 +39,7 @@ def _rel(a, b):
 
 def test_batch_matches_direct_and_single_solves(cuda):
     probs = _problems()
-    S = batch.BatchSolver(probs, workers=0)
+    S = batch.BatchSolver(probs, workers=0, amg_setup="host")   # the hierarchies of the single solves below
     x, info = S.solve(tol=1e-10)
     assert info["converged"], info
     assert np.all(info["relres"] <= 1e-10)
@@ -90,3 +90,22 @@ def test_batch_rejects_mixed_element_types_and_plastic_materials(cuda):
         batch.BatchSolver([a, b], workers=0)
     with pytest.raises(TypeError):
         batch.Problem(a.X, a.conn, a.etype, J2Plasticity(210e3, 0.3, [[250.0, 0.0], [1250.0, 1.0]]), a.fixed, a.rhs)
+
+
+def test_batch_with_device_setup(cuda):
+    """Per-problem hierarchies set up on the device and merged on the host: the
+    batched solution matches the direct solve of every instance and the batch
+    built from host set-ups, with the same level sizes per problem."""
+    probs = _problems()
+    dev = batch.BatchSolver(probs)
+    host = batch.BatchSolver(probs, workers=0, amg_setup="host")
+    for a, b in zip(dev.setups, host.setups):
+        assert [lv["n"] for lv in a["levels"]] == [lv["n"] for lv in b["levels"]]
+        assert a["coarse_inv"].shape == b["coarse_inv"].shape
+    xd, idv = dev.solve(tol=1e-10)
+    xh, ih = host.solve(tol=1e-10)
+    assert idv["converged"] and ih["converged"]
+    for i, (k, r) in enumerate(dev.inst):
+        xdir = _direct(probs[k], r)
+        assert _rel(dev.split(xd)[i], xdir) <= TOL_DIRECT
+        assert _rel(dev.split(xd)[i], host.split(xh)[i].cpu().numpy()) <= TOL_PAIR
