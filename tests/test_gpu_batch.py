@@ -109,3 +109,37 @@ def test_batch_with_device_setup(cuda):
         xdir = _direct(probs[k], r)
         assert _rel(dev.split(xd)[i], xdir) <= TOL_DIRECT
         assert _rel(dev.split(xd)[i], host.split(xh)[i].cpu().numpy()) <= TOL_PAIR
+
+
+def test_multi_load_cases_matches_oracle(cuda):
+    """optimize.multi_load_cases (gfem/optimize.py:116-143): three tip load cases on a
+    clamped cantilever, batched (default) and by the reference's per-case Jacobi-PCG,
+    against the oracle's sparse direct solve of each case: 1e-6 relative."""
+    import scipy.sparse.linalg as spla
+    import torch
+
+    import exfem_b200 as xf
+    from exfem_b200 import mesh, optimize
+    from oracle import fem as ofem
+    from oracle import linalg as olin
+    from oracle import solvers as osol
+    X, c = mesh.box_hex(60.0, 10.0, 10.0, 12, 2, 2)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > 60.0 - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)]
+    m = xf.Model(X)
+    m.add_block(c, xf.HEX8, xf.LinearElastic(210e3, 0.3))
+    F = np.zeros((3, m.ndof))
+    for k in range(3):
+        F[k, 3 * tip + k] = 100.0 / len(tip)
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.LinearElastic(210e3, 0.3))
+    setup = osol.Setup(om, osol.Step(bcs=bcs))
+    ops = [(d, K.numpy()) for d, K in om.stiffness_ops(torch.zeros(om.ndof, dtype=torch.float64), om.init_state())]
+    A = olin.bc_matrix(ofem.ops_assemble(ops, om.ndof), setup.free).tocsc()
+    ref = [spla.spsolve(A, F[k] * setup.free) for k in range(3)]
+    for method in ("batch", "jacobi"):
+        U = optimize.multi_load_cases(m, xf.Step(bcs=bcs), F, cg_tol=1e-10, method=method)
+        assert U.shape == (3, m.ndof)
+        for k in range(3):
+            assert _rel(U[k], ref[k]) < 1e-6, (method, k, _rel(U[k], ref[k]))
