@@ -18,7 +18,7 @@ C3D8, C3D10 = 0, 1
 LINEAR_ELASTIC, J2 = 0, 1
 F64, F32, BF16 = 0, 1, 2
 ASSEMBLE_GATHER, ASSEMBLE_COLOUR = 0, 1
-OP_EBE_F64, OP_MF_F64, OP_MF_F32 = 0, 1, 2
+OP_EBE_F64, OP_MF_F64, OP_MF_F32, OP_CSR_F64 = 0, 1, 2, 3
 PC_NONE, PC_JACOBI, PC_AMG = 0, 1, 2
 MAX_TABLE = 32
 

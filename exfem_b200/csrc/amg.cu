@@ -335,6 +335,11 @@ int amg_vcycle(exfem_amg_s* h, const T* b, T* x, const Level0Op<T>* op0, const i
 template int amg_vcycle<double>(exfem_amg_s*, const double*, double*, const Level0Op<double>*, const int*, cudaStream_t);
 template int amg_vcycle<float>(exfem_amg_s*, const float*, float*, const Level0Op<float>*, const int*, cudaStream_t);
 
+// y = A x with a stored FP64 CSR matrix (the assembled-operator solvers)
+int csr_apply(const Csr64& A, const double* x, double* y, const int* skip, cudaStream_t s) {
+  return spmv_lanes<double, SP_SET>(A, A.v64.p, x, y, nullptr, nullptr, nullptr, nullptr, 0.0, 0.0, skip, s);
+}
+
 // ---------------------------------------------------------------- upload
 static int upload_csr(Csr64& M, int64_t n, int64_t ncols, const int64_t* ptr, const int32_t* idx, const double* val) {
   M.n = n;

@@ -629,7 +629,7 @@ int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block
 int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out) {
   EX_ARG(b && out, "NULL argument");
   *out = nullptr;
-  EX_ARG(op_kind >= EXFEM_OP_EBE_F64 && op_kind <= EXFEM_OP_MF_F32, "unknown operator kind %d", op_kind);
+  EX_ARG(op_kind >= EXFEM_OP_EBE_F64 && op_kind <= EXFEM_OP_CSR_F64, "unknown operator kind %d", op_kind);
   EX_ARG(pc_kind >= EXFEM_PC_NONE && pc_kind <= EXFEM_PC_AMG, "unknown preconditioner %d", pc_kind);
   EX_ARG(pc_kind != EXFEM_PC_AMG || amg, "AMG preconditioner needs a hierarchy");
   EX_ARG(pc_kind != EXFEM_PC_AMG || amg->levels.empty() || amg->levels[0]->n == b->ndof(),
@@ -656,6 +656,13 @@ int exfem_solver_set_ke(exfem_solver s, const double* Ke) {
   EX_ARG(s, "solver is NULL");
   s->Ke = Ke;
   s->diag_ready = false;
+  if (s->op == EXFEM_OP_CSR_F64) {  // assemble now, with the block's current prescribed DOFs
+    StreamGuard g;
+    int st;
+    if ((st = g.init(nullptr))) return st;
+    if ((st = block_csr_assemble(s->blk, Ke, s->csr, g.work))) return st;
+    EX_CUDA(cudaStreamSynchronize(g.work));
+  }
   return EXFEM_OK;
 }
 

@@ -232,6 +232,10 @@ static int op_apply(exfem_solver_s* S, const T* v, T* y, const int* skip, cudaSt
       if (!S->Ke) { set_error("solver: stored-Ke operator without Ke (call exfem_solver_set_ke)"); return EXFEM_ERR_ARG; }
       return launch_ebe_matvec(S->blk, S->Ke, v, y, skip, st);
     }
+    if (S->op == EXFEM_OP_CSR_F64) {
+      if (!S->csr.ready) { set_error("solver: CSR operator not assembled (call exfem_solver_set_ke)"); return EXFEM_ERR_ARG; }
+      return csr_apply(S->csr.A, v, y, skip, st);
+    }
     return launch_mf_matvec<double>(S->blk, v, y, skip, st);
   } else {
     return launch_mf_matvec<float>(S->blk, v, y, skip, st);
@@ -295,7 +299,7 @@ static int pcg_iteration(exfem_solver_s* S, cudaStream_t st) {
 
 int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
   int s;
-  if (S->op == EXFEM_OP_EBE_F64) {
+  if (S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64) {
     if (!S->Ke) { set_error("solver: stored-Ke operator without Ke"); return EXFEM_ERR_ARG; }
     s = launch_ebe_diagonal(S->blk, S->Ke, S->diag64.p, st);
   } else {
@@ -433,7 +437,7 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
                  int maxiter, int* iters, int* passes, double* relres, cudaStream_t st) {
   const int64_t n = S->n;
   const unsigned eg = grid_for(n, 256);
-  if (S->op == EXFEM_OP_EBE_F64) {
+  if (S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64) {
     set_error("mixed refinement needs a matrix-free operator (EXFEM_OP_MF_F32)");
     return EXFEM_ERR_ARG;
   }
@@ -496,7 +500,7 @@ int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, d
                     int maxiter, int* iters, int* updates, double* relres, cudaStream_t st) {
   const int64_t n = S->n;
   const unsigned eg = grid_for(n, 256);
-  if (S->op == EXFEM_OP_EBE_F64) {
+  if (S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64) {
     set_error("mixed refinement needs a matrix-free operator (EXFEM_OP_MF_F32)");
     return EXFEM_ERR_ARG;
   }

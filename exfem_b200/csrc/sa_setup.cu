@@ -509,6 +509,37 @@ int coarsen(const BlockOp& A, const DevBuf<int32_t>& dagg, const DevBuf<double>&
 
 }  // namespace
 
+int block_csr_assemble(exfem_block_s* b, const double* Ke, BlockCsr& c, cudaStream_t s) {
+  EX_ARG(Ke || b->ne == 0, "element matrices are NULL");
+  const int64_t nn = b->nn, n = 3 * nn;
+  int st;
+  if (!c.ready) {
+    std::vector<int32_t> conn;
+    if ((st = down(conn, b->conn.p, (size_t)b->ne * b->nnode, s))) return st;
+    Rows adj;
+    if ((st = host_node_adjacency(nn, b->ne, b->nnode, conn.data(), adj))) return st;
+    c.nnzb = (int64_t)adj.idx.size();
+    if ((st = up(c.bptr, adj.ptr)) || (st = up(c.bidx, adj.idx)) ||
+        (st = c.bval.alloc(std::max<int64_t>(c.nnzb * 9, 1))))
+      return st;
+    c.A.n = c.A.ncols = n;
+    c.A.nnz = c.nnzb * 9;
+    if ((st = c.A.ptr.alloc(n + 1)) || (st = c.A.idx.alloc(std::max<int64_t>(c.A.nnz, 1))) ||
+        (st = c.A.v64.alloc(std::max<int64_t>(c.A.nnz, 1))) || (st = c.A.v32.alloc(std::max<int64_t>(c.A.nnz, 1))))
+      return st;
+    c.ready = true;
+  }
+  if (nn == 0) return EXFEM_OK;
+  sa_assemble0_kernel<<<sa_grid(nn * 32, 256), 256, 0, s>>>(
+      nn, b->nnode, b->vmax, b->plan.p, (int32_t)(b->ne * b->nnode), b->conn.p, Ke,
+      b->node_fixed.n ? b->node_fixed.p : nullptr, c.bptr.p, c.bidx.p, c.bval.p);
+  EX_LAUNCH_CHECK();
+  sa_expand_kernel<<<sa_grid(n, 256), 256, 0, s>>>(nn, 3, 3, c.bptr.p, c.bidx.p, c.bval.p, c.A.ptr.p, c.A.idx.p,
+                                                     c.A.v64.p, c.A.v32.p);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
 int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_coarse, int keep_level0,
                     cudaStream_t s) {
   EX_ARG(h->levels.empty() && h->nc == 0, "AMG handle already holds a hierarchy");

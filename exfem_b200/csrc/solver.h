@@ -22,6 +22,20 @@ struct AmgLevel {
   DevBuf<float> w32[NW];
 };
 
+// a block's element matrices assembled into one CSR matrix (EXFEM_OP_CSR_F64):
+// 3x3 node blocks on the node-adjacency pattern (built once, so the device
+// pointers a captured graph holds stay valid), expanded to scalar CSR
+struct BlockCsr {
+  bool ready = false;
+  int64_t nnzb = 0;
+  DevBuf<int64_t> bptr;
+  DevBuf<int32_t> bidx;
+  DevBuf<double> bval;
+  Csr64 A;
+};
+int block_csr_assemble(exfem_block_s* b, const double* Ke, BlockCsr& c, cudaStream_t s);
+int csr_apply(const Csr64& A, const double* x, double* y, const int* skip, cudaStream_t s);
+
 // level-0 operator override: y = A0(x) and its inverse diagonal
 template <class T>
 struct Level0Op {
@@ -64,6 +78,7 @@ struct exfem_solver_s {
   exfem_amg_s* amg = nullptr;
   int op = EXFEM_OP_MF_F32, pc = EXFEM_PC_AMG;
   const double* Ke = nullptr;
+  exfem::BlockCsr csr;  // EXFEM_OP_CSR_F64: the assembled operator
   int64_t n = 0;
   // workspace
   exfem::DevBuf<double> x64, r64, z64, p64, Ap64, b64, t64, dinv64, diag64;

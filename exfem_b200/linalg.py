@@ -420,10 +420,12 @@ class DeviceAMG(AMG):
 class NativeSolver:
     """PCG / mixed-precision refinement in the library for one block.
 
-    op: "ebe64" (stored Ke, FP64), "mf64" (matrix-free FP64), "mf32" (matrix-free
-    FP32); pc: "none", "jacobi", "amg"."""
+    op: "ebe64" (stored Ke, FP64), "csr64" (the stored Ke assembled on the device
+    into one FP64 CSR matrix, gfem/model.py:195-238), "mf64" (matrix-free FP64),
+    "mf32" (matrix-free FP32); pc: "none", "jacobi", "amg".  The stored-Ke operators
+    take their element matrices from :meth:`set_ke`."""
 
-    OPS = {"ebe64": _lib.OP_EBE_F64, "mf64": _lib.OP_MF_F64, "mf32": _lib.OP_MF_F32}
+    OPS = {"ebe64": _lib.OP_EBE_F64, "mf64": _lib.OP_MF_F64, "mf32": _lib.OP_MF_F32, "csr64": _lib.OP_CSR_F64}
     PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG}
 
     def __init__(self, block, op="mf32", pc="amg", amg=None, graph=True, chunk=8, mixed_mode="reliable",

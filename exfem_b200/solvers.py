@@ -127,8 +127,14 @@ class _LinearSystem:                                                    # solver
     """Solves (free K free + fixed I) x = b with the chosen back-end."""
 
     def __init__(self, model, method="auto", tangent="ebe", cg_tol=1e-9, cg_maxiter=20000, monitor=None,
-                 graph=True, amg_setup="auto", mixed_mode="reliable"):
+                 graph=True, amg_setup="auto", mixed_mode="reliable", operator="gather"):
         self.m = model
+        if operator not in ("gather", "csr"):
+            raise ValueError(f"unknown operator {operator!r}")
+        # stored-Ke operator of the "amg" / "jacobi" methods with tangent="ebe":
+        # "gather" = element-by-element products, "csr" = the element matrices
+        # assembled on the device into one CSR matrix (gfem/solvers.py:239-247, 406-412)
+        self.operator = operator
         self.mixed_mode = mixed_mode            # linalg.NativeSolver: "reliable" or "restart"
         if amg_setup not in ("auto", "host", "device"):
             raise ValueError(f"unknown AMG set-up {amg_setup!r}")
@@ -220,10 +226,10 @@ class _LinearSystem:                                                    # solver
             if not np.isfinite(rel) or rel > max(self.cg_tol * 10, 1e-3):
                 self.mon.log(f"    warning: mixed refinement not converged ({k} it, {p} passes, rel.res {rel:.2e})")
             return x
-        op = "ebe64" if self.tangent == "ebe" else "mf64"
+        op = ("csr64" if self.operator == "csr" else "ebe64") if self.tangent == "ebe" else "mf64"
         pc = "jacobi" if self.method == "jacobi" else "amg"
         S = self._solver(op, pc)
-        if op == "ebe64":
+        if op in ("ebe64", "csr64"):
             S.set_ke(ops[0][1])
         x, k, rr = S.pcg(b, tol=self.cg_tol, maxiter=self.cg_maxiter)
         if pc == "amg":
@@ -240,7 +246,7 @@ class _LinearSystem:                                                    # solver
 class StaticSolver:                                                     # solvers.py:481-683
     def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
                  cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None,
-                 amg_setup="auto", mixed_mode="reliable"):
+                 amg_setup="auto", mixed_mode="reliable", operator="gather"):
         """``amg``: a prebuilt :class:`linalg.AMG` that every step starts from instead
         of assembling and setting up its own (the serving path keeps one resident
         per mesh); the rebuild rule still applies."""
@@ -248,7 +254,7 @@ class StaticSolver:                                                     # solver
         self.mon = monitor or Monitor(verbose)
         self.line_search = line_search
         self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph, amg_setup,
-                                 mixed_mode)
+                                 mixed_mode, operator)
         self.lin.pinned_amg = amg
         self.newton_iterations = 0
 

@@ -49,7 +49,7 @@ enum { EXFEM_F64 = 0, EXFEM_F32 = 1, EXFEM_BF16 = 2 };
 /* assembly of element vectors into nodal vectors */
 enum { EXFEM_ASSEMBLE_GATHER = 0, EXFEM_ASSEMBLE_COLOUR = 1 };
 /* linear-operator kinds of a solver */
-enum { EXFEM_OP_EBE_F64 = 0, EXFEM_OP_MF_F64 = 1, EXFEM_OP_MF_F32 = 2 };
+enum { EXFEM_OP_EBE_F64 = 0, EXFEM_OP_MF_F64 = 1, EXFEM_OP_MF_F32 = 2, EXFEM_OP_CSR_F64 = 3 };
 /* preconditioners of a solver */
 enum { EXFEM_PC_NONE = 0, EXFEM_PC_JACOBI = 1, EXFEM_PC_AMG = 2 };
 
@@ -269,7 +269,11 @@ int exfem_amg_vcycle_noalloc(exfem_amg h, int dtype, const void* r, void* z, exf
 /* ------------------------------------------------------------ solvers
  * A solver binds an operator (EXFEM_OP_*) of a block, a preconditioner
  * (EXFEM_PC_*; an AMG handle for EXFEM_PC_AMG) and device workspace.
- * EXFEM_OP_EBE_F64 needs exfem_solver_set_ke before solving. */
+ * EXFEM_OP_EBE_F64 needs exfem_solver_set_ke before solving.  EXFEM_OP_CSR_F64 (the
+ * reference's operator="csr", gfem/model.py:195-238, gfem/solvers.py:406-412): the
+ * element matrices passed to exfem_solver_set_ke are assembled on the device into
+ * one FP64 CSR matrix (node-adjacency pattern, built once; prescribed DOFs as
+ * identity rows and columns), and the solver multiplies by it. */
 int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out);
 int exfem_solver_destroy(exfem_solver s);
 int exfem_solver_set_ke(exfem_solver s, const double* Ke);

@@ -67,15 +67,17 @@ def test_vcycle_matches_oracle(cuda):
     blk.set_fixed(None)
 
 
-@pytest.mark.parametrize("method,tangent", [("amg", "ebe"), ("amg", "mf"), ("mixed", "mf"), ("jacobi", "ebe")])
-def test_config1_linear_solve(cuda, method, tangent):
+@pytest.mark.parametrize("method,tangent,operator", [("amg", "ebe", "gather"), ("amg", "ebe", "csr"),
+                                                     ("amg", "mf", "gather"), ("mixed", "mf", "gather"),
+                                                     ("jacobi", "ebe", "gather"), ("jacobi", "ebe", "csr")])
+def test_config1_linear_solve(cuda, method, tangent, operator):
     import exfem_b200 as xf
     X, c, bcs, loads, pm, om = _config1()
     uo = _oracle_direct(om, bcs, loads)
     st = xf.Step(bcs=bcs, loads=loads)
     tol = 1e-10 if method != "mixed" else 1e-9
     up, s, info = xf.StaticSolver(pm, rtol=1e-6, linear_solver=method, tangent=tangent, cg_tol=tol,
-                                  verbose=False).solve(st)
+                                  verbose=False, operator=operator).solve(st)
     err = rel_err(up, uo)
     assert err < (1e-8 if method != "jacobi" else 1e-7), err
 
@@ -274,3 +276,30 @@ def test_deck_solve_matches_oracle(cuda):
     st = osol.Step(bcs=[(ref["fix"], d, 0.0) for d in range(3)], loads=[([ref["tip"]], 2, mk.TIP_LOAD)], dloads=[f])
     uo, _, _ = osol.StaticSolver(om, rtol=1e-6).solve(st)
     assert rel_err(up, uo) < 1e-8
+
+
+def test_csr_operator_matches_gather_product(cuda):
+    """The device-assembled CSR operator (operator="csr") applies the same matrix as
+    the element-by-element product of the same element matrices, prescribed DOFs as
+    identity rows (gfem/model.py:195-238 against 162-166): one PCG iteration on each
+    gives the same iterate to rounding, and J2 Newton counts stay those of the
+    oracle on one increment."""
+    import exfem_b200 as xf
+    from exfem_b200 import linalg
+    X, c, bcs, loads, pm, om = _config1()
+    blk = pm.blocks[0]
+    setup = osol.Setup(om, osol.Step(bcs=bcs, loads=loads))
+    blk.set_fixed(setup.fixed)
+    Ke = blk.stiffness(torch.zeros(pm.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
+    b = torch.as_tensor(np.random.default_rng(1).standard_normal(pm.ndof) * setup.free, device="cuda")
+    res = {}
+    for op in ("ebe64", "csr64"):
+        S = linalg.NativeSolver(blk, op, "jacobi", None, graph=False)
+        S.set_ke(Ke)
+        res[op] = S.pcg(b, tol=1e-12, maxiter=1)[0]
+    assert rel_err(res["csr64"], res["ebe64"]) < 1e-13
+    X2, bcs2, om2, uo, so, io, pm2 = _j2_case(1.0)
+    up, sp, ip = xf.StaticSolver(pm2, rtol=1e-6, linear_solver="amg", tangent="ebe", cg_tol=1e-10, verbose=False,
+                                 operator="csr").solve(xf.Step(bcs=bcs2, dt_init=1.0, dt_max=1.0))
+    assert [h[1] for h in ip["history"]] == [h[1] for h in io["history"]]
+    assert rel_err(up, uo) < 1e-6
