@@ -303,3 +303,54 @@ def test_csr_operator_matches_gather_product(cuda):
                                  operator="csr").solve(xf.Step(bcs=bcs2, dt_init=1.0, dt_max=1.0))
     assert [h[1] for h in ip["history"]] == [h[1] for h in io["history"]]
     assert rel_err(up, uo) < 1e-6
+
+
+def test_newton_cuts_back_on_nonfinite_residual(cuda):
+    """Failure detection on the host (gfem/solvers.py:562-563, 588-594, 663-664): a
+    non-finite internal force injected into the first increment's Newton loop makes
+    the increment fail and cut back (dt x 0.25), and the step completes with the
+    solution of an unfaulted run over the same increments."""
+    import exfem_b200 as xf
+
+    class Faulty(xf.StaticSolver):
+        calls = 0
+
+        def _fint(self, u, s, fields):
+            f, st = super()._fint(u, s, fields)
+            Faulty.calls += 1
+            if Faulty.calls == 1:
+                f = f.clone()
+                f[0] = float("nan")
+            return f, st
+
+    X, bcs, om, uo, so, io, pm = _j2_case(1.0)
+    uf, sf, inf_ = Faulty(pm, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-10,
+                          verbose=False).solve(xf.Step(bcs=bcs, dt_init=1.0, dt_max=1.0))
+    assert Faulty.calls > 1
+    assert inf_["increments"] == len(inf_["history"]) + 1          # one failed increment
+    assert inf_["history"][0][0] == 0.25                           # the cutback increment
+    X2, bcs2, om2, uo2, so2, io2, pm2 = _j2_case(1.0)
+    ur, sr, inr = xf.StaticSolver(pm2, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-10,
+                                  verbose=False).solve(xf.Step(bcs=bcs2, dt_init=0.25, dt_max=1.0))
+    assert [h[0] for h in inr["history"]] == [h[0] for h in inf_["history"]]
+    assert rel_err(uf, ur) < 1e-9
+
+
+def test_pcg_iteration_limit_reports_not_converged(cuda):
+    """PCG that runs out of iterations returns its iterate with the not-converged
+    status (a warning in the reference, gfem/solvers.py:472-473), not an error."""
+    from exfem_b200 import _lib, linalg
+    from exfem_b200._lib import lib
+    X, c, bcs, loads, pm, om = _config1()
+    blk = pm.blocks[0]
+    setup = osol.Setup(om, osol.Step(bcs=bcs, loads=loads))
+    blk.set_fixed(setup.fixed)
+    S = linalg.NativeSolver(blk, "mf64", "jacobi", None)
+    b = torch.as_tensor(np.random.default_rng(2).standard_normal(pm.ndof) * setup.free, device="cuda")
+    x, k, rr = S.pcg(b, tol=1e-14, maxiter=3)
+    assert k == 3 and rr > 1e-14 and torch.isfinite(x).all()
+    import ctypes as C
+    xo = torch.empty_like(b)
+    kk, r2 = C.c_int(), C.c_double()
+    st = lib.exfem_solver_pcg(S._h, _lib.ptr(b), _lib.ptr(xo), 1e-14, 3, C.byref(kk), C.byref(r2), _lib.stream_ptr())
+    assert st == _lib.NOT_CONVERGED and kk.value == 3
