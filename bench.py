@@ -365,6 +365,34 @@ def batch_section(count=512, nplain=24, seed=0, workers=None):
                 setup="per-problem smoothed aggregation on the device, merged on the host")
 
 
+def setup_section(n=80):
+    """Smoothed-aggregation set-up on the device for the C3D10 scale cube (z = 0
+    clamped): element matrices, then linalg.DeviceAMG; the phases print to stderr
+    when EXFEM_SETUP_TIMING is set."""
+    import torch
+    import exfem_b200 as xf
+    from exfem_b200 import linalg
+    X, c, scale = build_config3(n)
+    m = xf.Model(X)
+    blk = m.add_block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3))
+    blk.set_scale(scale)
+    fixed = np.zeros(m.ndof, bool)
+    for d in range(3):
+        fixed[3 * np.nonzero(X[:, 2] < 1e-9)[0] + d] = True
+    blk.set_fixed(fixed)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Ke = blk.stiffness(torch.zeros(m.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    amg = linalg.DeviceAMG(blk, Ke)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    return dict(workload=f"C3D10 {n}^3x6 cube ({len(c)} el, {m.ndof} DOF), device smoothed-aggregation set-up",
+                element_matrices_s=t1 - t0, setup_s=t2 - t1, rows=amg.sizes, nnz=amg.nnz,
+                complexity=amg.complexity)
+
+
 def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), j2_frac=0.2, slots=8, seed=0,
                   nplain=32):
     """Served request stream: a catalogue of seeded C3D8 / C3D10 jittered
@@ -560,7 +588,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default tile size (no autotuning)")
-    ap.add_argument("--mode", default="product", choices=["product", "batch", "serve", "stored_ke"],
+    ap.add_argument("--mode", default="product", choices=["product", "batch", "serve", "stored_ke", "setup"],
                     help="product: the C3D10 matrix-free product line (default); batch: batched uneven "
                          "solves; serve: served request stream")
     ap.add_argument("--count", type=int, default=512, help="cantilevers of the batch mode")
@@ -575,6 +603,8 @@ def main():
             sec = batch_section(args.count)
         elif args.mode == "stored_ke":
             sec = stored_ke_section()
+        elif args.mode == "setup":
+            sec = setup_section(args.n)
         else:
             sec = serve_section(rates=tuple(float(r) for r in args.rates.split(",")), duration=args.duration,
                                 dof=(1e3, args.max_dof))
