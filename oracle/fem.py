@@ -106,8 +106,8 @@ class LinearElastic:
     nstate = 1
     small_strain = True
 
-    def __init__(self, E, nu):
-        self.E, self.nu = float(E), float(nu)
+    def __init__(self, E, nu, density=1.0):
+        self.E, self.nu, self.density = float(E), float(nu), float(density)
         self.mu, self.lam = lame(self.E, self.nu)
 
     def pk1(self, F, s):
@@ -624,3 +624,18 @@ class Model:
             mises = torch.sqrt(1.5 * torch.sum(dev * dev, dim=(1, 2)))
             out.append(dict(S=sig, MISES=mises, PEEQ=ep, F=F))
         return out
+
+
+def lumped_mass(model):                                                # model.py:120-124, 501-510
+    """HRZ diagonal lumping per element, d_a = rho sum_g vol_g N_a(g)^2 scaled to
+    rho * element volume, summed at the nodes and repeated for the 3 DOFs."""
+    m = np.zeros(model.nn)
+    for b in model.blocks:
+        et, rho = b.etype, float(getattr(b.material, "density", 1.0))
+        Xe = model.X[torch.as_tensor(b.conn)]                           # (ne, nnode, 3)
+        Jac = torch.einsum("ean,gai->egni", Xe, et.dN)
+        vol = et.w[None, :] * torch.linalg.det(Jac)                     # (ne, ngp)
+        d = rho * torch.einsum("eg,ga->ea", vol, et.N * et.N)
+        d = d * (rho * vol.sum(1))[:, None] / d.sum(1)[:, None]
+        np.add.at(m, b.conn, d.numpy())
+    return np.repeat(m, 3)

@@ -469,3 +469,30 @@ TOPC, 2, 1.0
     assert flat(two.loads) == {(26, 2): -3.0, (26, 0): 2.0}
     assert flat(three.bcs) == {**base, (1, 2): 0.5}
     assert flat(three.loads) == {(26, 1): 1.0}
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_lumped_mass_matches_oracle(kind):
+    """HRZ-lumped mass of the modal analysis (gfem/model.py:120-124, 501-510) against
+    the oracle's restatement on jittered C3D8 and C3D10 meshes: 1e-13 relative, and
+    the total equals density x volume."""
+    from types import SimpleNamespace
+
+    from exfem_b200 import eigen, elements
+    from oracle import fem as ofem
+    if kind == "hex":
+        X, c = mesh.box_hex(3.0, 1.0, 1.0, 6, 2, 2)
+        X = mesh.jitter_interior(X, [0.5, 0.5, 0.5], 0.1, 5)
+        pet, oet = elements.HEX8, ofem.HEX8
+    else:
+        X, c = tet10_box(3.0, 1.0, 1.0, 3, 2, 2)
+        pet, oet = elements.TET10, ofem.TET10
+    rho = 7.85e-9
+    mat = SimpleNamespace(density=rho)
+    m = eigen.lumped_mass_host(X, [SimpleNamespace(conn=c, etype=pet, material=mat)])
+    om = ofem.Model(X)
+    om.add_block(c, oet, ofem.LinearElastic(210e3, 0.3, density=rho))
+    mo = ofem.lumped_mass(om)
+    np.testing.assert_allclose(m, mo, rtol=1e-13, atol=0)
+    assert abs(m.sum() / 3 - rho * 3.0) < 1e-12 * rho * 3.0
+    assert (m > 0).all()
