@@ -56,4 +56,7 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference checkout: argument, EXFEM_REFERENCE_DIR, or "reference" beside this repository
+    repo = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    default = os.environ.get("EXFEM_REFERENCE_DIR", os.path.join(os.path.dirname(repo), "reference"))
+    main(sys.argv[1] if len(sys.argv) > 1 else default)
