@@ -496,3 +496,29 @@ def test_lumped_mass_matches_oracle(kind):
     np.testing.assert_allclose(m, mo, rtol=1e-13, atol=0)
     assert abs(m.sum() / 3 - rho * 3.0) < 1e-12 * rho * 3.0
     assert (m > 0).all()
+
+
+def test_checkpoint_roundtrip(tmp_path):
+    """Checkpoint / resume data of a static analysis (the reference's State fields,
+    gfem/solvers.py:83-95): displacement, per-block material states, external force,
+    time and metadata survive a save / load round trip bit for bit, and the
+    per-increment callback writes one file per converged increment."""
+    import torch
+
+    from exfem_b200 import checkpoint
+    rng = np.random.default_rng(0)
+    u = torch.as_tensor(rng.standard_normal(30))
+    states = [torch.as_tensor(rng.standard_normal((4, 8, 19))), torch.as_tensor(rng.standard_normal((2, 4, 1)))]
+    fext = torch.as_tensor(rng.standard_normal(30))
+    path = tmp_path / "ck.npz"
+    checkpoint.save(path, u, states, time=0.75, fext=fext, increment=3)
+    u2, s2, t2, f2, meta = checkpoint.load(path, device="cpu")
+    assert torch.equal(u2, u) and all(torch.equal(a, b) for a, b in zip(s2, states)) and torch.equal(f2, fext)
+    assert t2 == 0.75 and int(meta["increment"]) == 3 and len(s2) == 2
+    cb = checkpoint.callback(str(tmp_path / "inc{inc:03d}.npz"))
+    for t in (0.25, 0.5):
+        cb(t, u * t, states)
+    files = sorted(p.name for p in tmp_path.glob("inc*.npz"))
+    assert files == ["inc001.npz", "inc002.npz"]
+    u3, _, t3, f3, meta3 = checkpoint.load(tmp_path / "inc002.npz", device="cpu")
+    assert t3 == 0.5 and f3 is None and torch.equal(u3, u * 0.5) and int(meta3["increment"]) == 2
