@@ -321,6 +321,23 @@ class SolveServer:
                 fut.set_exception(result)
 
 
+def request_records(reqs):
+    """One JSON-ready record per finished request: id, mesh key, kind, DOF, arrival
+    to start (queue) and start to done (service) times, latency, and the solver's info
+    (iterations, passes, relative residual, slot) — the raw data behind p50 / p99."""
+    out = []
+    for r in reqs:
+        if r.t_done is None:
+            continue
+        info = {k: (v.item() if hasattr(v, "item") else v) for k, v in r.info.items()
+                if isinstance(v, (int, float, str, bool, np.integer, np.floating))}
+        out.append(dict(id=int(r.id), mesh=r.spec.key, kind="j2" if r.spec.j2 else "linear", ndof=int(r.spec.ndof),
+                        queue_s=float(r.t_start - r.t_arrival) if r.t_start is not None else None,
+                        service_s=float(r.t_done - r.t_start) if r.t_start is not None else None,
+                        latency_s=float(r.latency), **info))
+    return out
+
+
 def latency_stats(reqs):
     """p50 / p99 latency (s), throughput (completed / makespan) of finished requests."""
     lat = np.array([r.latency for r in reqs if r.latency is not None])

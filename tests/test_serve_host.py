@@ -114,3 +114,27 @@ def test_request_kind_must_match_entry():
         serve.SolveRequest(sp)
     with pytest.raises(ValueError):
         serve.SolveRequest(sp, step=object())
+
+
+def test_request_records_for_latency_reports():
+    """Per-request records (the raw data behind p50 / p99): one JSON-serialisable
+    record per finished request with its queue, service and total times and the
+    solver's info, consistent with the latency statistics."""
+    import json
+    specs = [_spec(f"m{i}") for i in range(2)]
+    s, _ = _server(slots=2, budget=1e12, solve_time=0.01)
+    try:
+        futs = [s.submit(serve.SolveRequest(specs[i % 2], rhs=np.ones(specs[i % 2].ndof))) for i in range(6)]
+        for f in futs:
+            f.result(timeout=30)
+        recs = serve.request_records(list(s.completed))
+    finally:
+        s.close()
+    assert len(recs) == 6 and len({r["id"] for r in recs}) == 6
+    json.dumps(recs)
+    for r in recs:
+        assert r["kind"] == "linear" and r["mesh"] in ("m0", "m1") and r["iters"] == 1
+        assert r["queue_s"] >= 0 and r["service_s"] >= 0.01
+        assert abs(r["latency_s"] - (r["queue_s"] + r["service_s"])) < 1e-9
+    st = serve.latency_stats(list(s.completed))
+    assert abs(st["p50_s"] - float(np.percentile([r["latency_s"] for r in recs], 50))) < 1e-12
