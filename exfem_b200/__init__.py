@@ -11,7 +11,7 @@ interfaces so its Newton loop can run on them unchanged.
 """
 from . import _lib  # noqa: F401  (fails loudly when the CUDA library is missing)
 from .elements import ELEMENTS, HEX8, TET10  # noqa: F401
-from . import checkpoint, deck, eigen, loads, optimize, surfaces  # noqa: F401
+from . import checkpoint, deck, eigen, loads, optimize, results, surfaces  # noqa: F401
 from .linalg import AMG, DeviceAMG, NativeSolver, pcg  # noqa: F401
 from .materials import J2Plasticity, LinearElastic, from_props  # noqa: F401
 from .model import Block, Model  # noqa: F401

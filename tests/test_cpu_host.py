@@ -522,3 +522,45 @@ def test_checkpoint_roundtrip(tmp_path):
     assert files == ["inc001.npz", "inc002.npz"]
     u3, _, t3, f3, meta3 = checkpoint.load(tmp_path / "inc002.npz", device="cpu")
     assert t3 == 0.5 and f3 is None and torch.equal(u3, u * 0.5) and int(meta3["increment"]) == 2
+
+
+def test_vtu_writer_roundtrip(tmp_path):
+    """ParaView output (gfem/io/vtk.py:24-71 format): the .vtu of a C3D8 + C3D10
+    mesh parses as XML, and every binary DataArray decodes (UInt64 byte count, then
+    the values) to the written points, connectivity, offsets, cell types and result
+    arrays; the .pvd lists the frames."""
+    import base64
+    import xml.etree.ElementTree as ET
+    from types import SimpleNamespace
+
+    from exfem_b200 import elements, results
+    Xh, ch = mesh.box_hex(2.0, 1.0, 1.0, 2, 1, 1)
+    X10, c10 = tet10_box(1.0, 1.0, 1.0, 1, 1, 1)
+    X = np.vstack([Xh, X10 + [3.0, 0.0, 0.0]])
+    blocks = [SimpleNamespace(conn=ch, etype=elements.HEX8),
+              SimpleNamespace(conn=c10 + len(Xh), etype=elements.TET10)]
+    rng = np.random.default_rng(0)
+    U = rng.standard_normal((len(X), 3))
+    mises = rng.uniform(0, 300, len(ch) + len(c10))
+    path = tmp_path / "f.vtu"
+    results.write_vtu(path, X, blocks, point_data={"U": U}, cell_data={"MISES": mises})
+    root = ET.parse(path).getroot()
+    arrays = {}
+    for da in root.iter("DataArray"):
+        raw = base64.b64decode(da.text)
+        n = int(np.frombuffer(raw[:8], np.uint64)[0])
+        dt = {"Float64": np.float64, "Int64": np.int64, "UInt8": np.uint8}[da.get("type")]
+        arrays[da.get("Name")] = np.frombuffer(raw[8:8 + n], dt)
+    np.testing.assert_array_equal(arrays["Points"].reshape(-1, 3), X)
+    np.testing.assert_array_equal(arrays["connectivity"], np.concatenate([ch.ravel(), (c10 + len(Xh)).ravel()]))
+    np.testing.assert_array_equal(arrays["offsets"], np.cumsum([8] * len(ch) + [10] * len(c10)))
+    np.testing.assert_array_equal(arrays["types"], [12] * len(ch) + [24] * len(c10))
+    np.testing.assert_array_equal(arrays["U"].reshape(-1, 3), U)
+    np.testing.assert_array_equal(arrays["MISES"], mises)
+    piece = next(root.iter("Piece"))
+    assert int(piece.get("NumberOfPoints")) == len(X) and int(piece.get("NumberOfCells")) == len(mises)
+    results.write_pvd(tmp_path / "s.pvd", [(0.5, "f.vtu"), (1.0, "g.vtu")])
+    ds = [d.attrib for d in ET.parse(tmp_path / "s.pvd").getroot().iter("DataSet")]
+    assert ds == [{"timestep": "0.5", "file": "f.vtu"}, {"timestep": "1", "file": "g.vtu"}]
+    with pytest.raises(ValueError):
+        results.write_vtu(tmp_path / "bad.vtu", X, blocks, point_data={"U": U[:-1]})

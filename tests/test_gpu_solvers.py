@@ -390,3 +390,28 @@ def test_modal_lobpcg_matches_sparse_eigensolver(cuda):
         assert np.linalg.norm(r[free]) <= 1e-6 * w2[j] * np.linalg.norm(Mf * Phi[j])
     G = (Phi * Mf[None, :]) @ Phi.T
     np.testing.assert_allclose(G, np.eye(4), atol=1e-8)
+
+
+def test_result_frame_written_for_a_solution(cuda, tmp_path):
+    """Output of a device solution (deck output of served requests): displacement,
+    von Mises and PEEQ of the config-1 cantilever written to .vtu hold the solver's
+    values and the element stresses the oracle computes for the same displacement."""
+    import base64
+    import xml.etree.ElementTree as ET
+
+    import exfem_b200 as xf
+    from exfem_b200 import results
+    X, c, bcs, loads, pm, om = _config1()
+    u, states, _ = xf.StaticSolver(pm, rtol=1e-6, linear_solver="amg", cg_tol=1e-10, verbose=False).solve(
+        xf.Step(bcs=bcs, loads=loads))
+    results.write_frame(tmp_path / "r.vtu", pm, u, states)
+    arrays = {}
+    for da in ET.parse(tmp_path / "r.vtu").getroot().iter("DataArray"):
+        raw = base64.b64decode(da.text)
+        n = int(np.frombuffer(raw[:8], np.uint64)[0])
+        if da.get("type") == "Float64":
+            arrays[da.get("Name")] = np.frombuffer(raw[8:8 + n], np.float64)
+    np.testing.assert_array_equal(arrays["U"], u.cpu().numpy())
+    mo = om.stresses(torch.as_tensor(u.cpu()), om.init_state())[0]["MISES"]
+    assert rel_err(arrays["MISES"], mo) < 1e-10
+    assert np.all(arrays["PEEQ"] == 0.0)
