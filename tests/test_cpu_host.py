@@ -564,3 +564,29 @@ def test_vtu_writer_roundtrip(tmp_path):
     assert ds == [{"timestep": "0.5", "file": "f.vtu"}, {"timestep": "1", "file": "g.vtu"}]
     with pytest.raises(ValueError):
         results.write_vtu(tmp_path / "bad.vtu", X, blocks, point_data={"U": U[:-1]})
+
+
+def test_deck_reader_rejects_what_it_does_not_cover(tmp_path):
+    """The deck reader refuses, with a clear error, decks outside the static solid
+    path: other element types, dynamic / frequency steps, elements without a section,
+    node-based surfaces."""
+    from exfem_b200 import deck
+    head = "*NODE\n1, 0, 0, 0\n2, 1, 0, 0\n3, 0, 1, 0\n4, 0, 0, 1\n"
+    cases = {
+        "S4R shell": (head + "*ELEMENT, TYPE=S4R\n1, 1, 2, 3, 4\n", NotImplementedError),
+        "frequency": (head + "*ELEMENT, TYPE=C3D4\n1, 1, 2, 3, 4\n", NotImplementedError),
+        "no section": (None, ValueError),
+        "node surface": (None, NotImplementedError),
+    }
+    tet10 = ("*NODE\n" + "\n".join(f"{i + 1}, {x}, {y}, {z}" for i, (x, y, z) in enumerate(
+        [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (.5, 0, 0), (.5, .5, 0), (0, .5, 0), (0, 0, .5), (.5, 0, .5),
+         (0, .5, .5)])) + "\n*ELEMENT, TYPE=C3D10, ELSET=E\n1, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10\n")
+    cases["no section"] = (tet10 + "*MATERIAL, NAME=M\n*ELASTIC\n1., 0.3\n", ValueError)
+    cases["node surface"] = (tet10 + "*SURFACE, NAME=S, TYPE=NODE\n1, 1.\n", NotImplementedError)
+    cases["frequency"] = (tet10 + "*SOLID SECTION, ELSET=E, MATERIAL=M\n*MATERIAL, NAME=M\n*ELASTIC\n1., 0.3\n"
+                          "*STEP\n*FREQUENCY\n10\n*END STEP\n", NotImplementedError)
+    for name, (text, exc) in cases.items():
+        p = tmp_path / f"{name.replace(' ', '_')}.inp"
+        p.write_text(text)
+        with pytest.raises(exc):
+            deck.InpDeck(str(p))
