@@ -590,3 +590,22 @@ def test_deck_reader_rejects_what_it_does_not_cover(tmp_path):
         p.write_text(text)
         with pytest.raises(exc):
             deck.InpDeck(str(p))
+
+
+def test_coarse_inverse_singular_and_indefinite():
+    """Coarsest solve of the device set-up: a singular positive semidefinite matrix
+    (rigid-body null space of a floating structure) still factors through the
+    1e-13 max|A| shift, and the regularised inverse solves consistent systems; an
+    indefinite matrix is refused with a status instead of a wrong factor."""
+    rng = np.random.default_rng(2)
+    Bm = rng.standard_normal((12, 9))
+    A = Bm @ Bm.T                                        # rank 9 of 12
+    Ainv = np.zeros_like(A)
+    _lib.check(_lib.lib.exfem_host_coarse_inverse(12, np.ascontiguousarray(A).ctypes.data, Ainv.ctypes.data))
+    assert np.isfinite(Ainv).all()
+    b = A @ rng.standard_normal(12)                      # in the range of A
+    x = Ainv @ b
+    assert np.linalg.norm(A @ x - b) < 1e-3 * np.linalg.norm(b)
+    Neg = -np.eye(6)
+    st = _lib.lib.exfem_host_coarse_inverse(6, np.ascontiguousarray(Neg).ctypes.data, np.zeros((6, 6)).ctypes.data)
+    assert st < 0 and "positive definite" in _lib.last_error()
