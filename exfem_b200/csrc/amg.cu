@@ -531,21 +531,30 @@ namespace exfem {
 
 static __device__ __align__(256) unsigned char g_vcycle_scratch[EXFEM_VCYCLE_NOALLOC_BYTES];
 
-// device address of the scratch array, resolved once per device with that device
-// current (the host-side name of the array is not a device address)
+// device address of the scratch array, with the device current (the host-side
+// name of the array is not a device address).  Outside a stream capture the
+// address is looked up on every call, so a context that was destroyed and made
+// again (cudaDeviceReset) gets its new address; inside a capture the address
+// remembered from the last call on that device outside a capture is used, because
+// the look-up may load the module, which a capture does not permit.
 static std::mutex g_scratch_mu;
 static void* g_scratch_dev[64] = {nullptr};
 
-static int vcycle_scratch_address(void** out) {
+static int vcycle_scratch_address(cudaStream_t s, void** out) {
   int dev = 0;
   EX_CUDA(cudaGetDevice(&dev));
   EX_ARG(dev >= 0 && dev < 64, "device ordinal %d out of range", dev);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  EX_CUDA(cudaStreamIsCapturing(s, &cap));
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_dev[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     EX_CUDA(cudaGetSymbolAddress(&p, g_vcycle_scratch));
     g_scratch_dev[dev] = p;
   }
+  EX_ARG(g_scratch_dev[dev] != nullptr,
+         "allocation-free V-cycle: first call on device %d is inside a stream capture; call it once before capturing",
+         dev);
   *out = g_scratch_dev[dev];
   return EXFEM_OK;
 }
@@ -586,6 +595,10 @@ static int vcycle_level_noalloc(exfem_amg_s* h, size_t l, const T* b, T* x, cons
   if (l == h->levels.size()) return coarse_solve<T>(h, b, x, nullptr, s);
   AmgLevel& L = *h->levels[l];
   const bool mf = (l == 0 && op0 && op0->apply);
+  if (!mf && L.A.nnz == 0) {
+    set_error("AMG level %zu holds no stored matrix: smooth it with a level-0 block", l);
+    return EXFEM_ERR_ARG;
+  }
   const T* dinv = (l == 0 && op0 && op0->dinv) ? op0->dinv : lvdinv<T>(L);
   const T* rc = lvcoef<T>(L);  // per-row Chebyshev coefficients (union of independent hierarchies)
   const int64_t n = L.n;
@@ -665,9 +678,16 @@ static int mf_apply_noalloc(void* ctx, const T* x, T* y, const int* skip, cudaSt
 template <class T>
 static int vcycle_noalloc(exfem_amg_s* h, const T* r, T* z, exfem_block_s* level0, const T* dinv0, cudaStream_t s) {
   EX_ARG(!h->levels.empty() || h->nc > 0, "empty AMG hierarchy");
+  // every level smoothed with a stored matrix must hold one; checked before any
+  // launch (a hierarchy set up without its mesh-level matrix needs a level-0 block)
+  for (size_t l = 0; l < h->levels.size(); ++l)
+    if (!(l == 0 && level0) && h->levels[l]->A.nnz == 0) {
+      set_error("AMG level %zu holds no stored matrix: smooth it with a level-0 block", l);
+      return EXFEM_ERR_ARG;
+    }
   void* base = nullptr;
   int st;
-  if ((st = vcycle_scratch_address(&base))) return st;
+  if ((st = vcycle_scratch_address(s, &base))) return st;
   NoallocWork<T> w;
   if ((st = noalloc_carve<T>(h, static_cast<unsigned char*>(base), w))) return st;
   if (h->levels.empty()) return coarse_solve<T>(h, r, z, nullptr, s);
