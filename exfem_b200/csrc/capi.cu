@@ -32,6 +32,7 @@ int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx,
 int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
                     std::vector<int32_t>& order);
 int host_tile_pairs(int64_t ne, const int32_t* conn, std::vector<int32_t>& order, std::vector<int32_t>& conn_tile);
+int host_face_once(int64_t nface, const int64_t* keys, uint8_t* once);
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm,
                    int& maxu);
@@ -653,16 +654,31 @@ int exfem_solver_destroy(exfem_solver s) {
 }
 
 int exfem_solver_set_ke(exfem_solver s, const double* Ke) {
-  EX_ARG(s, "solver is NULL");
-  s->Ke = Ke;
+  return exfem_solver_set_ke_block(s, 0, Ke);
+}
+
+int exfem_solver_add_block(exfem_solver s, exfem_block b) {
+  EX_ARG(s && b, "NULL argument");
+  EX_ARG(b->nn == s->blk->nn, "an added block must share the solver's node set (%lld vs %lld nodes)",
+         (long long)b->nn, (long long)s->blk->nn);
+  for (auto& ge : s->gexec)
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  s->more.push_back(b);
+  s->more_Ke.push_back(nullptr);
   s->diag_ready = false;
-  if (s->op == EXFEM_OP_CSR_F64) {  // assemble now, with the block's current prescribed DOFs
-    StreamGuard g;
-    int st;
-    if ((st = g.init(nullptr))) return st;
-    if ((st = block_csr_assemble(s->blk, Ke, s->csr, g.work))) return st;
-    EX_CUDA(cudaStreamSynchronize(g.work));
-  }
+  s->csr_dirty = true;
+  return EXFEM_OK;
+}
+
+int exfem_solver_set_ke_block(exfem_solver s, int block, const double* Ke) {
+  EX_ARG(s, "solver is NULL");
+  EX_ARG(block >= 0 && block <= (int)s->more.size(), "block %d out of range (the solver has %zu)", block,
+         s->more.size() + 1);
+  if (block == 0) s->Ke = Ke;
+  else s->more_Ke[block - 1] = Ke;
+  s->diag_ready = false;
+  // EXFEM_OP_CSR_F64: assembled by the next solve, with the prescribed DOFs then in force
+  if (s->op == EXFEM_OP_CSR_F64) s->csr_dirty = true;
   return EXFEM_OK;
 }
 
@@ -730,10 +746,19 @@ int exfem_block_status(exfem_block b, void* stream) {
 int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_coarse, int keep_level0,
                           void* stream) {
   EX_ARG(h && b, "NULL handle");
+  return exfem_amg_setup_blocks(h, 1, &b, &Ke, max_coarse, keep_level0, stream);
+}
+
+int exfem_amg_setup_blocks(exfem_amg h, int nblk, const exfem_block* blocks, const double* const* Kes,
+                           int max_coarse, int keep_level0, void* stream) {
+  EX_ARG(h && nblk >= 1 && blocks && Kes, "NULL argument");
+  std::vector<exfem_block_s*> bl(blocks, blocks + nblk);
+  std::vector<const double*> ke(Kes, Kes + nblk);
+  for (int i = 0; i < nblk; ++i) EX_ARG(bl[i], "block %d is NULL", i);
   StreamGuard g;
   int st;
   if ((st = g.init(stream))) return st;
-  st = amg_setup_block(h, b, Ke, max_coarse, keep_level0, g.work);
+  st = amg_setup_blocks(h, bl, ke, max_coarse, keep_level0, g.work);
   if (st) {  // leave the handle empty rather than half built
     h->levels.clear();
     h->nc = 0;
@@ -870,6 +895,11 @@ int exfem_host_coarse_inverse(int64_t n, const double* A, double* Ainv) {
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
   EX_ARG(ptr && idx && agg && nagg, "NULL argument");
   return host_standard_aggregation(n, ptr, idx, agg, *nagg);
+}
+
+int exfem_host_face_once(int64_t nface, const int64_t* keys, uint8_t* once) {
+  EX_ARG(nface >= 0 && ((keys && once) || nface == 0), "NULL argument");
+  return host_face_once(nface, keys, once);
 }
 
 int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile) {

@@ -16,6 +16,11 @@
 //      pass 2: remaining nodes join the first neighbouring pass-1 aggregate;
 //      pass 3: still-unaggregated nodes seed new aggregates with their
 //              unaggregated neighbours.
+//  * boundary faces (no counterpart in the reference's code, which finds them
+//    with a row-wise np.unique, gfem/surfaces.py:182-221): every element face
+//    is keyed by its sorted corner nodes; the keys go into an open-addressing hash
+//    table (linear probing, power-of-two size at least twice the face count)
+//    that counts equal keys; a face is on the boundary when its key occurs once.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -364,6 +369,40 @@ int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx,
     ++next;
   }
   nagg = next;
+  return EXFEM_OK;
+}
+
+static inline uint64_t face_key_hash(const int64_t* k) {
+  uint64_t h = 0x9e3779b97f4a7c15ull;
+  for (int i = 0; i < 4; ++i) {  // splitmix64 steps over the four key words
+    uint64_t z = h + (uint64_t)k[i] + 0x9e3779b97f4a7c15ull * (uint64_t)(i + 1);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    h = z ^ (z >> 31);
+  }
+  return h;
+}
+
+int host_face_once(int64_t nface, const int64_t* keys, uint8_t* once) {
+  if (nface == 0) return EXFEM_OK;
+  size_t cap = 1;
+  while (cap < 2 * (size_t)nface) cap <<= 1;
+  std::vector<int64_t> slot(cap, -1);   // first face holding each distinct key
+  std::vector<int32_t> count(nface, 0);
+  std::vector<int64_t> first(nface);
+  for (int64_t f = 0; f < nface; ++f) {
+    const int64_t* k = keys + 4 * f;
+    size_t h = (size_t)face_key_hash(k) & (cap - 1);
+    for (;;) {
+      const int64_t g = slot[h];
+      if (g < 0) { slot[h] = f; first[f] = f; break; }
+      const int64_t* kg = keys + 4 * g;
+      if (kg[0] == k[0] && kg[1] == k[1] && kg[2] == k[2] && kg[3] == k[3]) { first[f] = g; break; }
+      h = (h + 1) & (cap - 1);
+    }
+    ++count[first[f]];
+  }
+  for (int64_t f = 0; f < nface; ++f) once[f] = count[first[f]] == 1 ? 1 : 0;
   return EXFEM_OK;
 }
 

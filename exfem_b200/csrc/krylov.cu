@@ -150,6 +150,16 @@ __global__ void jacobi_kernel(int64_t n, const T* __restrict__ dinv, const T* __
     z[i] = dinv[i] * r[i];
 }
 
+// y += t on the free DOFs (the product of a further block, whose prescribed rows
+// hold the identity the first block's product already wrote)
+template <class T>
+__global__ void add_free_kernel(int64_t n, const uint8_t* __restrict__ fixed, const T* __restrict__ t,
+                                T* __restrict__ y, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!(fixed && fixed[i])) y[i] += t[i];
+}
+
 __global__ void dinv_kernel(int64_t n, const double* __restrict__ d, const uint8_t* __restrict__ fixed,
                             double* __restrict__ d64, float* __restrict__ d32) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -225,21 +235,61 @@ template <class T> static const T* sdinv(exfem_solver_s* S);
 template <> const double* sdinv<double>(exfem_solver_s* S) { return S->dinv64.p; }
 template <> const float* sdinv<float>(exfem_solver_s* S) { return S->dinv32.p; }
 
+template <class T> static T* more_buf(exfem_solver_s* S);
+template <> double* more_buf<double>(exfem_solver_s* S) { return S->mb64.p; }
+template <> float* more_buf<float>(exfem_solver_s* S) { return S->mb32.p; }
+
+// generations of the tangent data / prescribed-DOF buffers over all blocks
+static uint64_t tan_gen_all(const exfem_solver_s* S) {
+  uint64_t g = S->blk->tan_gen;
+  for (auto* b : S->more) g += b->tan_gen;
+  return g;
+}
+static uint64_t bc_gen_all(const exfem_solver_s* S) {
+  uint64_t g = S->blk->bc_gen;
+  for (auto* b : S->more) g += b->bc_gen;
+  return g;
+}
+
+// matrix-free product of every block: y = opA_0(v) + sum over the further blocks of
+// free * K_b(free * v)
+template <class T>
+static int mf_apply_all(exfem_solver_s* S, const T* v, T* y, const int* skip, cudaStream_t st) {
+  int s;
+  if ((s = launch_mf_matvec<T>(S->blk, v, y, skip, st))) return s;
+  for (auto* b : S->more) {
+    T* t = more_buf<T>(S);
+    if ((s = launch_mf_matvec<T>(b, v, t, skip, st))) return s;
+    add_free_kernel<T><<<grid_for(S->n, 256), 256, 0, st>>>(S->n, S->blk->fixed.p, t, y, skip);
+    EX_LAUNCH_CHECK();
+  }
+  return EXFEM_OK;
+}
+
 template <class T>
 static int op_apply(exfem_solver_s* S, const T* v, T* y, const int* skip, cudaStream_t st) {
   if constexpr (sizeof(T) == 8) {
     if (S->op == EXFEM_OP_EBE_F64) {
       if (!S->Ke) { set_error("solver: stored-Ke operator without Ke (call exfem_solver_set_ke)"); return EXFEM_ERR_ARG; }
-      return launch_ebe_matvec(S->blk, S->Ke, v, y, skip, st);
+      int s;
+      if ((s = launch_ebe_matvec(S->blk, S->Ke, v, y, skip, st))) return s;
+      for (size_t i = 0; i < S->more.size(); ++i) {
+        if (!S->more_Ke[i]) {
+          set_error("solver: stored-Ke operator without Ke of block %zu (call exfem_solver_set_ke_block)", i + 1);
+          return EXFEM_ERR_ARG;
+        }
+        if ((s = launch_ebe_matvec(S->more[i], S->more_Ke[i], v, S->mb64.p, skip, st))) return s;
+        add_free_kernel<double><<<grid_for(S->n, 256), 256, 0, st>>>(S->n, S->blk->fixed.p, S->mb64.p, y, skip);
+        EX_LAUNCH_CHECK();
+      }
+      return EXFEM_OK;
     }
     if (S->op == EXFEM_OP_CSR_F64) {
       if (!S->csr.ready) { set_error("solver: CSR operator not assembled (call exfem_solver_set_ke)"); return EXFEM_ERR_ARG; }
       return csr_apply(S->csr.A, v, y, skip, st);
     }
-    return launch_mf_matvec<double>(S->blk, v, y, skip, st);
-  } else {
-    return launch_mf_matvec<float>(S->blk, v, y, skip, st);
   }
+  return mf_apply_all<T>(S, v, y, skip, st);
 }
 
 template <class T>
@@ -299,18 +349,24 @@ static int pcg_iteration(exfem_solver_s* S, cudaStream_t st) {
 
 int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
   int s;
-  if (S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64) {
-    if (!S->Ke) { set_error("solver: stored-Ke operator without Ke"); return EXFEM_ERR_ARG; }
-    s = launch_ebe_diagonal(S->blk, S->Ke, S->diag64.p, st);
-  } else {
-    s = launch_mf_diagonal(S->blk, S->diag64.p, st);
+  const bool stored = S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64;
+  for (size_t i = 0; i <= S->more.size(); ++i) {
+    exfem_block_s* b = i ? S->more[i - 1] : S->blk;
+    const double* Ke = i ? S->more_Ke[i - 1] : S->Ke;
+    double* d = i ? S->mb64.p : S->diag64.p;
+    if (stored && !Ke) { set_error("solver: stored-Ke operator without Ke of block %zu", i); return EXFEM_ERR_ARG; }
+    if ((s = stored ? launch_ebe_diagonal(b, Ke, d, st) : launch_mf_diagonal(b, d, st))) return s;
+    if (i) {
+      add_free_kernel<double><<<grid_for(S->n, 256), 256, 0, st>>>(S->n, S->blk->fixed.p, S->mb64.p, S->diag64.p,
+                                                                   nullptr);
+      EX_LAUNCH_CHECK();
+    }
   }
-  if (s) return s;
   dinv_kernel<<<grid_for(S->n, 256), 256, 0, st>>>(S->n, S->diag64.p, S->blk->fixed.p, S->dinv64.p, S->dinv32.p);
   EX_LAUNCH_CHECK();
   S->diag_ready = true;
-  S->diag_tan_gen = S->blk->tan_gen;
-  S->diag_bc_gen = S->blk->bc_gen;
+  S->diag_tan_gen = tan_gen_all(S);
+  S->diag_bc_gen = bc_gen_all(S);
   return EXFEM_OK;
 }
 
@@ -322,15 +378,29 @@ static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
   int s;
   if (S->pc == EXFEM_PC_AMG && !S->amg) { set_error("solver: AMG preconditioner without hierarchy"); return EXFEM_ERR_ARG; }
   if (S->pc == EXFEM_PC_AMG && (s = amg_prepare(S->amg, sizeof(T) == 8 ? EXFEM_F64 : EXFEM_F32))) return s;
-  const bool stale = !S->diag_ready || S->diag_tan_gen != S->blk->tan_gen || S->diag_bc_gen != S->blk->bc_gen;
+  if (S->op == EXFEM_OP_CSR_F64 && S->csr_dirty) {  // element matrices changed: assemble them again
+    std::vector<exfem_block_s*> blks{S->blk};
+    std::vector<const double*> kes{S->Ke};
+    blks.insert(blks.end(), S->more.begin(), S->more.end());
+    kes.insert(kes.end(), S->more_Ke.begin(), S->more_Ke.end());
+    for (size_t i = 0; i < kes.size(); ++i)
+      if (!kes[i]) { set_error("solver: CSR operator without Ke of block %zu", i); return EXFEM_ERR_ARG; }
+    if ((s = blocks_csr_assemble(blks, kes, S->csr, st))) return s;
+    S->csr_dirty = false;
+  }
+  const bool stale = !S->diag_ready || S->diag_tan_gen != tan_gen_all(S) || S->diag_bc_gen != bc_gen_all(S);
   if (stale && S->pc != EXFEM_PC_NONE && (s = solver_refresh_diagonal(S, st))) return s;
   const int chunk = S->chunk > 0 ? S->chunk : 8;
   if (S->use_graph) {
-    const double* keptr = S->op == EXFEM_OP_EBE_F64 ? S->Ke : nullptr;
-    if (S->graph_bc_gen != S->blk->bc_gen) {
+    std::vector<const double*> keptr;  // the element matrices a captured stored-Ke graph reads
+    if (S->op == EXFEM_OP_EBE_F64) {
+      keptr.push_back(S->Ke);
+      keptr.insert(keptr.end(), S->more_Ke.begin(), S->more_Ke.end());
+    }
+    if (S->graph_bc_gen != bc_gen_all(S)) {
       for (auto& ge : S->gexec)
         if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
-      S->graph_bc_gen = S->blk->bc_gen;
+      S->graph_bc_gen = bc_gen_all(S);
     }
     if (S->gexec[gi] && S->g_Ke[gi] != keptr) {
       cudaGraphExecDestroy(S->gexec[gi]);
@@ -470,7 +540,7 @@ int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, doub
     its += k;
     axpy_f32_kernel<<<eg, 256, 0, st>>>(n, x, S->x32.p, sc);
     EX_LAUNCH_CHECK();
-    if ((s = launch_mf_matvec<double>(S->blk, x, S->Ap64.p, nullptr, st))) return s;
+    if ((s = mf_apply_all<double>(S, x, S->Ap64.p, nullptr, st))) return s;
     sub64_kernel<<<eg, 256, 0, st>>>(n, b, S->Ap64.p, S->r64.p);
     EX_LAUNCH_CHECK();
     if ((s = norm64(S, S->r64.p, &rn, st))) return s;
@@ -548,7 +618,7 @@ int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, d
     // replacement: x += sc x32, r64 = b - A64 x
     axpy_f32_kernel<<<eg, 256, 0, st>>>(n, x, x32, sc);
     EX_LAUNCH_CHECK();
-    if ((s = launch_mf_matvec<double>(S->blk, x, S->Ap64.p, nullptr, st))) return s;
+    if ((s = mf_apply_all<double>(S, x, S->Ap64.p, nullptr, st))) return s;
     sub64_kernel<<<eg, 256, 0, st>>>(n, b, S->Ap64.p, S->r64.p);
     EX_LAUNCH_CHECK();
     if ((s = norm64(S, S->r64.p, &rn, st))) return s;
@@ -579,6 +649,7 @@ int solver_alloc(exfem_solver_s* S) {
   DevBuf<float>* v32[] = {&S->x32, &S->r32, &S->z32, &S->p32, &S->Ap32, &S->b32, &S->t32, &S->dinv32};
   for (auto* v : v32)
     if ((s = v->alloc(std::max<int64_t>(n, 1)))) return s;
+  if ((s = S->mb64.alloc(std::max<int64_t>(n, 1))) || (s = S->mb32.alloc(std::max<int64_t>(n, 1)))) return s;
   if ((s = S->partial.alloc(RED_MAX_BLOCKS))) return s;
   if ((s = S->dscr.alloc(4))) return s;
   if ((s = S->counter.alloc(1))) return s;

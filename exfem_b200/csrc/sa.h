@@ -43,5 +43,7 @@ int host_coarse_inverse(int64_t n, std::vector<double>& A, std::vector<double>& 
 // element matrices (sa_setup.cu)
 int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_coarse, int keep_level0,
                     cudaStream_t s);
+int amg_setup_blocks(exfem_amg_s* h, const std::vector<exfem_block_s*>& blks, const std::vector<const double*>& Kes,
+                     int max_coarse, int keep_level0, cudaStream_t s);
 
 }  // namespace exfem

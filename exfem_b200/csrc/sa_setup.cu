@@ -52,12 +52,14 @@ __device__ __forceinline__ int64_t thread_count() { return (int64_t)gridDim.x * 
 // A_0 node row n (3x3 blocks on the node adjacency row) = sum over the elements
 // of the gather plan row n (increasing slot order) of their Ke blocks; a lane
 // owns one (neighbour, entry) pair of an element at a time, and the warp
-// synchronises between elements, so every entry is summed in plan order.
+// synchronises between elements, so every entry is summed in plan order.  With
+// `accumulate` the rows are added to (the next block of a model of several blocks,
+// whose slots follow the previous blocks' in the model's plan) instead of set.
 __global__ void sa_assemble0_kernel(int64_t nn, int nnode, int vmax, const int32_t* __restrict__ plan,
                                     int32_t sentinel, const int32_t* __restrict__ conn,
                                     const double* __restrict__ Ke, const uint8_t* __restrict__ nfix,
                                     const int64_t* __restrict__ aptr, const int32_t* __restrict__ aidx,
-                                    double* __restrict__ A) {
+                                    double* __restrict__ A, int accumulate) {
   const int lane = threadIdx.x & 31;
   const int nd = 3 * nnode;
   for (int64_t n = warp_id(); n < nn; n += warp_count()) {
@@ -65,7 +67,8 @@ __global__ void sa_assemble0_kernel(int64_t nn, int nnode, int vmax, const int32
     const int len = (int)(aptr[n + 1] - r0);
     const int32_t* row = aidx + r0;
     double* Ar = A + r0 * 9;
-    for (int k = lane; k < len * 9; k += 32) Ar[k] = 0.0;
+    if (!accumulate)
+      for (int k = lane; k < len * 9; k += 32) Ar[k] = 0.0;
     __syncwarp();
     const uint32_t fn = nfix ? nfix[n] : 0u;
     for (int v = 0; v < vmax; ++v) {
@@ -509,6 +512,71 @@ int coarsen(const BlockOp& A, const DevBuf<int32_t>& dagg, const DevBuf<double>&
 
 }  // namespace
 
+// node adjacency of several blocks over one node set: each element's node list
+// padded to the widest element with its own first node (repeats are ignored)
+static int blocks_adjacency(const std::vector<exfem_block_s*>& blks, cudaStream_t s, Rows& adj) {
+  const int64_t nn = blks[0]->nn;
+  int wmax = 0;
+  int64_t ne = 0;
+  for (auto* b : blks) {
+    EX_ARG(b->nn == nn, "blocks of one operator must share their node set (%lld vs %lld nodes)",
+           (long long)b->nn, (long long)nn);
+    wmax = std::max(wmax, b->nnode);
+    ne += b->ne;
+  }
+  std::vector<int32_t> conn((size_t)ne * wmax), cb;
+  int64_t e0 = 0;
+  int st;
+  for (auto* b : blks) {
+    if ((st = down(cb, b->conn.p, (size_t)b->ne * b->nnode, s))) return st;
+    for (int64_t e = 0; e < b->ne; ++e)
+      for (int a = 0; a < wmax; ++a)
+        conn[(size_t)(e0 + e) * wmax + a] = cb[(size_t)e * b->nnode + (a < b->nnode ? a : 0)];
+    e0 += b->ne;
+  }
+  return host_node_adjacency(nn, ne, wmax, conn.data(), adj);
+}
+
+static void assemble_blocks(const std::vector<exfem_block_s*>& blks, const std::vector<const double*>& Kes,
+                            int64_t nn, const int64_t* aptr, const int32_t* aidx, double* A, cudaStream_t s) {
+  const uint8_t* nfix = blks[0]->node_fixed.n ? blks[0]->node_fixed.p : nullptr;
+  for (size_t i = 0; i < blks.size(); ++i) {
+    exfem_block_s* b = blks[i];
+    sa_assemble0_kernel<<<sa_grid(nn * 32, 256), 256, 0, s>>>(nn, b->nnode, b->vmax, b->plan.p,
+                                                               (int32_t)(b->ne * b->nnode), b->conn.p, Kes[i], nfix,
+                                                               aptr, aidx, A, i > 0 ? 1 : 0);
+  }
+}
+
+int blocks_csr_assemble(const std::vector<exfem_block_s*>& blks, const std::vector<const double*>& Kes, BlockCsr& c,
+                        cudaStream_t s) {
+  EX_ARG(!blks.empty() && blks.size() == Kes.size(), "need one element-matrix array per block");
+  for (size_t i = 0; i < blks.size(); ++i) EX_ARG(Kes[i] || blks[i]->ne == 0, "element matrices are NULL");
+  const int64_t nn = blks[0]->nn, n = 3 * nn;
+  int st;
+  if (!c.ready) {
+    Rows adj;
+    if ((st = blocks_adjacency(blks, s, adj))) return st;
+    c.nnzb = (int64_t)adj.idx.size();
+    if ((st = up(c.bptr, adj.ptr)) || (st = up(c.bidx, adj.idx)) ||
+        (st = c.bval.alloc(std::max<int64_t>(c.nnzb * 9, 1))))
+      return st;
+    c.A.n = c.A.ncols = n;
+    c.A.nnz = c.nnzb * 9;
+    if ((st = c.A.ptr.alloc(n + 1)) || (st = c.A.idx.alloc(std::max<int64_t>(c.A.nnz, 1))) ||
+        (st = c.A.v64.alloc(std::max<int64_t>(c.A.nnz, 1))) || (st = c.A.v32.alloc(std::max<int64_t>(c.A.nnz, 1))))
+      return st;
+    c.ready = true;
+  }
+  if (nn == 0) return EXFEM_OK;
+  assemble_blocks(blks, Kes, nn, c.bptr.p, c.bidx.p, c.bval.p, s);
+  EX_LAUNCH_CHECK();
+  sa_expand_kernel<<<sa_grid(n, 256), 256, 0, s>>>(nn, 3, 3, c.bptr.p, c.bidx.p, c.bval.p, c.A.ptr.p, c.A.idx.p,
+                                                     c.A.v64.p, c.A.v32.p);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
 int block_csr_assemble(exfem_block_s* b, const double* Ke, BlockCsr& c, cudaStream_t s) {
   EX_ARG(Ke || b->ne == 0, "element matrices are NULL");
   const int64_t nn = b->nn, n = 3 * nn;
@@ -532,7 +600,7 @@ int block_csr_assemble(exfem_block_s* b, const double* Ke, BlockCsr& c, cudaStre
   if (nn == 0) return EXFEM_OK;
   sa_assemble0_kernel<<<sa_grid(nn * 32, 256), 256, 0, s>>>(
       nn, b->nnode, b->vmax, b->plan.p, (int32_t)(b->ne * b->nnode), b->conn.p, Ke,
-      b->node_fixed.n ? b->node_fixed.p : nullptr, c.bptr.p, c.bidx.p, c.bval.p);
+      b->node_fixed.n ? b->node_fixed.p : nullptr, c.bptr.p, c.bidx.p, c.bval.p, 0);
   EX_LAUNCH_CHECK();
   sa_expand_kernel<<<sa_grid(n, 256), 256, 0, s>>>(nn, 3, 3, c.bptr.p, c.bidx.p, c.bval.p, c.A.ptr.p, c.A.idx.p,
                                                      c.A.v64.p, c.A.v32.p);
@@ -542,15 +610,25 @@ int block_csr_assemble(exfem_block_s* b, const double* Ke, BlockCsr& c, cudaStre
 
 int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_coarse, int keep_level0,
                     cudaStream_t s) {
+  return amg_setup_blocks(h, std::vector<exfem_block_s*>{b}, std::vector<const double*>{Ke}, max_coarse,
+                          keep_level0, s);
+}
+
+int amg_setup_blocks(exfem_amg_s* h, const std::vector<exfem_block_s*>& blks, const std::vector<const double*>& Kes,
+                     int max_coarse, int keep_level0, cudaStream_t s) {
   EX_ARG(h->levels.empty() && h->nc == 0, "AMG handle already holds a hierarchy");
-  EX_ARG(b->ne > 0 && Ke, "the block needs elements and their element matrices");
+  EX_ARG(!blks.empty() && blks.size() == Kes.size(), "need one element-matrix array per block");
+  int64_t ne = 0;
+  for (size_t i = 0; i < blks.size(); ++i) {
+    EX_ARG(blks[i]->ne == 0 || Kes[i], "block %zu needs its element matrices", i);
+    ne += blks[i]->ne;
+  }
+  EX_ARG(ne > 0, "the blocks need elements");
   EX_ARG(max_coarse >= 6, "max_coarse must be at least 6");
-  const int nnode = b->nnode;
-  std::vector<int32_t> conn;
+  exfem_block_s* b = blks[0];
   std::vector<double> X;
   int st;
   PhaseClock clk;
-  if ((st = down(conn, b->conn.p, (size_t)b->ne * nnode, s))) return st;
   if ((st = down(X, b->X.p, (size_t)b->nn * 3, s))) return st;
   // level 0: node adjacency pattern, A_0 assembled from the element matrices
   BlockOp A;
@@ -558,20 +636,23 @@ int amg_setup_block(exfem_amg_s* h, exfem_block_s* b, const double* Ke, int max_
   A.nb = b->nn;
   {
     Rows adj;
-    if ((st = host_node_adjacency(b->nn, b->ne, nnode, conn.data(), adj))) return st;
+    if (blks.size() == 1) {
+      std::vector<int32_t> conn;
+      if ((st = down(conn, b->conn.p, (size_t)b->ne * b->nnode, s))) return st;
+      if ((st = host_node_adjacency(b->nn, b->ne, b->nnode, conn.data(), adj))) return st;
+    } else if ((st = blocks_adjacency(blks, s, adj))) {
+      return st;
+    }
     clk.mark("node adjacency (host)", s, 0);
     if ((st = A.set_pattern(std::move(adj)))) return st;
   }
   if ((st = A.val.alloc(std::max<size_t>(A.pat.idx.size() * 9, 1)))) return st;
-  sa_assemble0_kernel<<<sa_grid(A.nb * 32, 256), 256, 0, s>>>(
-      A.nb, nnode, b->vmax, b->plan.p, (int32_t)(b->ne * nnode), b->conn.p, Ke,
-      b->node_fixed.n ? b->node_fixed.p : nullptr, A.ptr.p, A.idx.p, A.val.p);
+  assemble_blocks(blks, Kes, A.nb, A.ptr.p, A.idx.p, A.val.p, s);
   EX_LAUNCH_CHECK();
   clk.mark("assembly", s, 0);
   std::vector<double> B;
   host_rigid_body_modes(b->nn, X.data(), B);
   std::vector<double>().swap(X);
-  std::vector<int32_t>().swap(conn);
   constexpr int K = 6;
   const int max_levels = 10;
   while (A.nb * A.bs > max_coarse && (int)h->levels.size() < max_levels - 1) {

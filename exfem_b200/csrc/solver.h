@@ -34,6 +34,12 @@ struct BlockCsr {
   Csr64 A;
 };
 int block_csr_assemble(exfem_block_s* b, const double* Ke, BlockCsr& c, cudaStream_t s);
+// the same for several blocks over one node set, summed block after block in
+// gather-plan order (the prescribed DOFs of the first block)
+int blocks_csr_assemble(const std::vector<exfem_block_s*>& blks, const std::vector<const double*>& Kes, BlockCsr& c,
+                        cudaStream_t s);
+int amg_setup_blocks(exfem_amg_s* h, const std::vector<exfem_block_s*>& blks, const std::vector<const double*>& Kes,
+                     int max_coarse, int keep_level0, cudaStream_t s);
 int csr_apply(const Csr64& A, const double* x, double* y, const int* skip, cudaStream_t s);
 
 // level-0 operator override: y = A0(x) and its inverse diagonal
@@ -75,6 +81,14 @@ struct exfem_amg_s {
 
 struct exfem_solver_s {
   exfem_block_s* blk = nullptr;
+  // further element blocks over the same nodes (a model of several blocks,
+  // gfem/model.py:466-486): the operator is the sum of every block's product, the
+  // prescribed DOFs (identity rows of opA) those of the first block
+  std::vector<exfem_block_s*> more;
+  std::vector<const double*> more_Ke;
+  exfem::DevBuf<double> mb64;  // product of one further block
+  exfem::DevBuf<float> mb32;
+  bool csr_dirty = false;      // EXFEM_OP_CSR_F64: element matrices changed since the last assembly
   exfem_amg_s* amg = nullptr;
   int op = EXFEM_OP_MF_F32, pc = EXFEM_PC_AMG;
   const double* Ke = nullptr;
@@ -94,6 +108,6 @@ struct exfem_solver_s {
   // CUDA graphs of `chunk` PCG iterations, one per precision
   int use_graph = 1, chunk = 8;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
-  const double* g_Ke[2] = {nullptr, nullptr};
+  std::vector<const double*> g_Ke[2];
   ~exfem_solver_s();
 };

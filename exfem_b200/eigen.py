@@ -130,23 +130,29 @@ def lobpcg(A, B, T, X0, k, tol=1e-6, maxiter=500, log=None):
 
 
 def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=None):
-    """(w^2 (nmodes,), modes (nmodes, ndof)) of a single-block model under the
-    step's prescribed DOFs (gfem/eigen.py:99-124; ``nmodes`` is the reference step's
-    ``nmodes``)."""
-    if len(model.blocks) != 1:
-        raise NotImplementedError("modal analysis covers single-block models")
-    blk = model.blocks[0]
+    """(w^2 (nmodes,), modes (nmodes, ndof)) of a model under the step's prescribed
+    DOFs (gfem/eigen.py:99-124; ``nmodes`` is the reference step's ``nmodes``); the
+    stiffness of a model of several blocks is the sum over its blocks."""
     setup = _Setup(model, step, state or State(model))
     free = setup.free
-    blk.set_fixed(setup.fixed)
+    for blk in model.blocks:
+        blk.set_fixed(setup.fixed)
     nd = model.ndof
-    Ke = blk.stiffness(torch.zeros(nd, dtype=torch.float64, device="cuda"), blk.init_state())
-    amg = linalg.DeviceAMG(blk, Ke, keep_level0=True)
-    del Ke
+    zero = torch.zeros(nd, dtype=torch.float64, device="cuda")
+    Kes = [blk.stiffness(zero, blk.init_state()) for blk in model.blocks]
+    amg = linalg.DeviceAMG(model.blocks, Kes, keep_level0=True)
+    del Kes
     M = lumped_mass(model) * free
 
+    def K(v):
+        out = None
+        for blk in model.blocks:
+            y = blk.tangent_matvec(v)
+            out = y if out is None else out + y
+        return out
+
     def A(V):
-        return torch.stack([blk.tangent_matvec(V[:, j].contiguous()) for j in range(V.shape[1])], 1) * free[:, None]
+        return torch.stack([K(V[:, j].contiguous()) for j in range(V.shape[1])], 1) * free[:, None]
 
     def B(V):
         return M[:, None] * V

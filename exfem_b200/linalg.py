@@ -362,14 +362,23 @@ class DeviceAMG(AMG):
     the solvers smooth it with the block's matrix-free product."""
 
     def __init__(self, block, Ke, max_coarse=300, degree=2, presmooth=1, keep_level0=False):
+        """``block``, ``Ke``: one block and its element matrices, or lists of the
+        blocks of a model over one node set and their element matrices (A_0 is then
+        the sum over the blocks, with the first block's prescribed DOFs)."""
         t0 = time.time()
         _lib.require_cuda()
         h = C.c_void_p()
         check(lib.exfem_amg_create(C.byref(h)))
         self._h = h
-        Ke = Ke.to(torch.float64).contiguous()
-        check(lib.exfem_amg_setup_block(h, block.handle, ptr(Ke), int(max_coarse), 1 if keep_level0 else 0,
-                                        stream_ptr()))
+        blocks = list(block) if isinstance(block, (list, tuple)) else [block]
+        Kes = list(Ke) if isinstance(Ke, (list, tuple)) else [Ke]
+        if len(blocks) != len(Kes):
+            raise ValueError(f"{len(blocks)} blocks but {len(Kes)} element-matrix arrays")
+        Kes = [K.to(torch.float64).contiguous() for K in Kes]
+        hb = (C.c_void_p * len(blocks))(*[b.handle.value for b in blocks])
+        hk = (C.c_void_p * len(Kes))(*[K.data_ptr() for K in Kes])
+        check(lib.exfem_amg_setup_blocks(h, len(blocks), hb, hk, int(max_coarse), 1 if keep_level0 else 0,
+                                         stream_ptr()))
         cap = 16
         nl, rows, nnz = C.c_int(), (C.c_int64 * cap)(), (C.c_int64 * cap)()
         check(lib.exfem_amg_info(h, cap, C.byref(nl), rows, nnz))
@@ -418,12 +427,14 @@ class DeviceAMG(AMG):
 
 # ------------------------------------------------------------------ native solver
 class NativeSolver:
-    """PCG / mixed-precision refinement in the library for one block.
+    """PCG / mixed-precision refinement in the library for one block, or for the
+    blocks of a model (a list over one node set: every operator is the sum over the
+    blocks, gfem/model.py:466-486, with the first block's prescribed DOFs).
 
     op: "ebe64" (stored Ke, FP64), "csr64" (the stored Ke assembled on the device
     into one FP64 CSR matrix, gfem/model.py:195-238), "mf64" (matrix-free FP64),
     "mf32" (matrix-free FP32); pc: "none", "jacobi", "amg".  The stored-Ke operators
-    take their element matrices from :meth:`set_ke`."""
+    take their element matrices from :meth:`set_ke` (one array per block)."""
 
     OPS = {"ebe64": _lib.OP_EBE_F64, "mf64": _lib.OP_MF_F64, "mf32": _lib.OP_MF_F32, "csr64": _lib.OP_CSR_F64}
     PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG}
@@ -434,12 +445,15 @@ class NativeSolver:
         recursion whose residual is replaced by the FP64 one after each reduction by
         mixed_delta) or "restart" (the reference's restarted refinement,
         gfem/solvers.py:344-384)."""
-        self.block, self.amg = block, amg
+        self.blocks = list(block) if isinstance(block, (list, tuple)) else [block]
+        self.block, self.amg = self.blocks[0], amg
         self.op, self.pc = op, pc
         h = C.c_void_p()
-        check(lib.exfem_solver_create(block.handle, self.OPS[op], self.PCS[pc],
+        check(lib.exfem_solver_create(self.block.handle, self.OPS[op], self.PCS[pc],
                                       amg.handle if amg is not None else None, C.byref(h)))
         self._h = h
+        for b in self.blocks[1:]:
+            check(lib.exfem_solver_add_block(h, b.handle))
         check(lib.exfem_solver_set_graph(h, 1 if graph else 0, chunk))
         check(lib.exfem_solver_set_mixed_mode(h, {"reliable": 1, "restart": 0}[mixed_mode], float(mixed_delta)))
         self._Ke = None
@@ -453,8 +467,13 @@ class NativeSolver:
             self._h = None
 
     def set_ke(self, Ke):
-        self._Ke = Ke.contiguous()
-        check(lib.exfem_solver_set_ke(self._h, ptr(self._Ke)))
+        """Element matrices of the block (a tensor) or of every block (a list)."""
+        Kes = list(Ke) if isinstance(Ke, (list, tuple)) else [Ke]
+        if len(Kes) != len(self.blocks):
+            raise ValueError(f"{len(self.blocks)} blocks but {len(Kes)} element-matrix arrays")
+        self._Ke = [K.contiguous() for K in Kes]
+        for i, K in enumerate(self._Ke):
+            check(lib.exfem_solver_set_ke_block(self._h, i, ptr(K)))
 
     def pcg(self, b, tol=1e-8, maxiter=2000):
         b = b.to(torch.float64).contiguous()

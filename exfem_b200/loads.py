@@ -20,10 +20,13 @@ def cload_vector(ndof, nodes, dof, value):
 
 def pressure_vector(X, surface, p):
     X = np.asarray(X)
-    f = np.zeros_like(X, dtype=np.float64)
+    nn = len(X)
+    f = np.zeros((nn, 3))
     for ft, fac in surface.groups:
-        n = surface._jacobians(X, ft, fac)                           # (nf, ngp, 3)
-        np.add.at(f, fac, -p * np.einsum("fgi,ga->fai", n, ft.N))
+        n = ft.area_vectors(X, fac)                                   # (nf, ngp, 3)
+        fe = -p * np.matmul(ft.N.T, n)                                # (nf, nnode, 3)
+        for c in range(3):
+            f[:, c] += np.bincount(fac.reshape(-1), weights=fe[..., c].reshape(-1), minlength=nn)
     return f.ravel()
 
 

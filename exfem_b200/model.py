@@ -25,6 +25,22 @@ from . import _lib
 from ._lib import check, lib, ptr, stream_ptr
 
 
+def gather_plan(conns, nn):
+    """Atomic-free assembly plan of a list of element blocks (gfem/model.py:241-261):
+    for every node the flat slots ``offset_b + e*nnode_b + a`` of the blocks'
+    elements that touch it, in increasing order, padded with the total slot count
+    (a zero row) to the maximum valence; (nn, vmax) int32.  The library's counting
+    sort runs over the blocks' connectivities laid end to end as one slot list."""
+    flat = [np.asarray(c, dtype=np.int32).reshape(-1) for c in conns]
+    nslot = int(sum(f.size for f in flat))
+    flat = np.ascontiguousarray(np.concatenate(flat + [np.zeros(1, np.int32)]))   # one spare entry: never empty
+    vmax = C.c_int()
+    check(lib.exfem_host_gather_plan(int(nn), 1, nslot, flat.ctypes.data, None, C.byref(vmax)))
+    plan = np.empty((int(nn), vmax.value), np.int32)
+    check(lib.exfem_host_gather_plan(int(nn), 1, nslot, flat.ctypes.data, plan.ctypes.data, C.byref(vmax)))
+    return plan
+
+
 def _dev(x, dtype=torch.float64):
     if isinstance(x, torch.Tensor):
         return x.to(device="cuda", dtype=dtype).contiguous()
@@ -269,9 +285,10 @@ class Model:
         return [b.init_state() for b in self.blocks]
 
     def gather(self):
-        if len(self.blocks) != 1:
-            raise NotImplementedError("gather plan export covers single-block models")
-        return self.blocks[0].gather_plan()
+        """The gather plan over all blocks (gfem/model.py:421-429 with 241-261)."""
+        if len(self.blocks) == 1:
+            return self.blocks[0].gather_plan()
+        return gather_plan([b.conn for b in self.blocks], self.nn)
 
     def dof(self, nodes, d):
         return np.asarray(nodes, dtype=np.int64).ravel() * 3 + d

@@ -146,8 +146,6 @@ class _LinearSystem:                                                    # solver
             method = "direct" if model.ndof <= 20000 else "amg"
         if method not in ("direct", "amg", "jacobi", "mixed"):
             raise ValueError(f"unknown linear solver {method!r}")
-        if len(model.blocks) != 1:
-            raise NotImplementedError("the device linear solvers cover single-block models")
         self.method = method
         self.tangent = "mf" if tangent in ("mf", "jvp") or method == "mixed" else "ebe"
         self.cg_tol, self.cg_maxiter = cg_tol, cg_maxiter
@@ -172,7 +170,7 @@ class _LinearSystem:                                                    # solver
         key = (op, pc, id(self.amg))
         s = self._solvers.get(key)
         if s is None:
-            s = NativeSolver(self.m.blocks[0], op, pc, self.amg if pc == "amg" else None, graph=self.graph,
+            s = NativeSolver(self.m.blocks, op, pc, self.amg if pc == "amg" else None, graph=self.graph,
                              mixed_mode=self.mixed_mode)
             self._solvers = {k: v for k, v in self._solvers.items() if k[2] == id(self.amg)}
             self._solvers[key] = s
@@ -196,8 +194,8 @@ class _LinearSystem:                                                    # solver
         if where == "auto":
             where = "device"
         if where == "device":
-            Ke = self._setup_ops(ops, ctx)[0][1]
-            self.amg = linalg.DeviceAMG(self.m.blocks[0], Ke)
+            Kes = [K for _, K in self._setup_ops(ops, ctx)]
+            self.amg = linalg.DeviceAMG(self.m.blocks, Kes)
         else:
             A = self.assemble(self._setup_ops(ops, ctx), setup)
             self.amg = linalg.AMG(A, self.m.X)
@@ -209,8 +207,8 @@ class _LinearSystem:                                                    # solver
     def solve(self, ops, b, setup, jvp_args=None, rebuild=False):
         """ops: [(dofs, Ke)] (tangent="ebe") or None with jvp_args = (u, states, fields)
         (tangent="mf"; the block's tangent data must be current)."""
-        blk = self.m.blocks[0]
-        blk.set_fixed(setup.fixed)
+        for blk in self.m.blocks:
+            blk.set_fixed(setup.fixed)
         b = b.to(torch.float64)
         if self.method == "direct":
             A = self.assemble(self._setup_ops(ops, jvp_args), setup)
@@ -230,7 +228,7 @@ class _LinearSystem:                                                    # solver
         pc = "jacobi" if self.method == "jacobi" else "amg"
         S = self._solver(op, pc)
         if op in ("ebe64", "csr64"):
-            S.set_ke(ops[0][1])
+            S.set_ke([K for _, K in ops])
         x, k, rr = S.pcg(b, tol=self.cg_tol, maxiter=self.cg_maxiter)
         if pc == "amg":
             if self.amg_iters0 is None:

@@ -213,6 +213,13 @@ int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv_dense);
  * product (solvers, exfem_amg_vcycle with level0).  Synchronises the stream. */
 int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_coarse, int keep_level0,
                           void* stream);
+/* The same set-up for a model of several blocks over one node set (a list of
+ * element blocks, gfem/model.py:466-486, assembled into one matrix as
+ * gfem/model.py:176-192 does from the stiffness ops of all blocks): blocks[i] with
+ * its element matrices Kes[i]; A_0 sums the blocks in order through each block's
+ * gather plan; the prescribed DOFs are those of blocks[0]. */
+int exfem_amg_setup_blocks(exfem_amg h, int nblk, const exfem_block* blocks, const double* const* Kes,
+                           int max_coarse, int keep_level0, void* stream);
 /* level count (coarsest included) and, for the first cap levels, rows and
  * operator nonzeros (AMG.info, gfem/linalg.py:135, 148-154). */
 int exfem_amg_info(exfem_amg h, int cap, int* nlevels, int64_t* rows, int64_t* nnz);
@@ -258,10 +265,14 @@ int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block
  * EXFEM_VCYCLE_NOALLOC_BYTES that every GPU loading the library holds until exit,
  * and calls no cudaMalloc, cudaFree or allocating routine.  A hierarchy whose
  * work vectors (6 per level and 2 coarse, each rounded up to 256 bytes) exceed
- * the array is rejected with EXFEM_ERR_ARG.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race, so the caller must serialise them. */
+ * the array is rejected with EXFEM_ERR_ARG, and so, before any launch, is a
+ * level without a stored matrix that no level-0 block smooths (the device set-up
+ * without keep_level0).  A call outside a stream capture looks up the array's
+ * device address (cudaGetSymbolAddress) on the current device; a call inside a
+ * capture uses the address of the last call on that device outside one, so the
+ * first call on a device should come before any stream capture.  All calls
+ * share the array: calls that overlap on the GPU race, so the caller must
+ * serialise them. */
 #define EXFEM_VCYCLE_NOALLOC_BYTES (8u << 20)
 int exfem_amg_vcycle_noalloc(exfem_amg h, int dtype, const void* r, void* z, exfem_block level0,
                              const void* dinv0, void* stream);
@@ -277,6 +288,17 @@ int exfem_amg_vcycle_noalloc(exfem_amg h, int dtype, const void* r, void* z, exf
 int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out);
 int exfem_solver_destroy(exfem_solver s);
 int exfem_solver_set_ke(exfem_solver s, const double* Ke);
+/* A model of several element blocks (gfem/model.py:466-486: the reference's
+ * operators loop over the blocks and its gather plan covers all of them,
+ * gfem/model.py:241-261): add_block adds a further block over the solver block's
+ * node set; every operator of the solver (products, diagonal, the FP64 residual
+ * of the mixed solves, the level-0 smoothing) is then the sum over the blocks, with
+ * the prescribed DOFs of the first block (give every block the same mask).
+ * set_ke_block sets the stored element matrices of block i (0 = the solver's own
+ * block, as exfem_solver_set_ke); EXFEM_OP_CSR_F64 assembles all blocks into one
+ * matrix at the next solve. */
+int exfem_solver_add_block(exfem_solver s, exfem_block b);
+int exfem_solver_set_ke_block(exfem_solver s, int block, const double* Ke);
 /* Refresh the Jacobi / level-0 inverse diagonal from the current operator
  * (gfem/solvers.py:312-313 dinv0). Called automatically by the first solve. */
 int exfem_solver_refresh_diagonal(exfem_solver s, void* stream);
@@ -325,8 +347,10 @@ int exfem_batch_solve(exfem_batch b, const double* rhs, double* x, double tol, d
 /* ------------------------------------------------------------ host index builders
  * Host-side, no device work.  Gather plan of one connectivity exactly as
  * gfem/model.py:241-261 (plan must hold nn*vmax entries; call with plan = NULL to
- * get vmax); greedy colouring; standard aggregation of a symmetric strength
- * graph (CSR pattern) for the smoothed-aggregation set-up. */
+ * get vmax; the plan of several blocks is that of their connectivities
+ * concatenated as one flat list: ne = 1, nnode = the total slot count); greedy
+ * colouring; standard aggregation of a symmetric strength graph (CSR pattern)
+ * for the smoothed-aggregation set-up. */
 int exfem_host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* plan,
                            int* vmax);
 int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* colour,
@@ -360,6 +384,11 @@ int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const 
  * the second (both positively oriented), so the product loads and adds their six
  * shared nodes once.  No counterpart in the reference. */
 int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile);
+/* boundary faces: keys (nface, 4) int64, each face's corner nodes sorted
+ * ascending (triangles padded in front with -1); once[f] = 1 when no other face
+ * has the same key, else 0.  The face matching of gfem/surfaces.py:182-221
+ * (skin), by hashing the keys. */
+int exfem_host_face_once(int64_t nface, const int64_t* keys, uint8_t* once);
 
 #ifdef __cplusplus
 }

@@ -609,3 +609,55 @@ def test_coarse_inverse_singular_and_indefinite():
     Neg = -np.eye(6)
     st = _lib.lib.exfem_host_coarse_inverse(6, np.ascontiguousarray(Neg).ctypes.data, np.zeros((6, 6)).ctypes.data)
     assert st < 0 and "positive definite" in _lib.last_error()
+
+
+def _ref_fixture_cases():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_index_fixtures.npz")
+    z = np.load(path)
+    names = sorted({k.split("_")[0] for k in z.files})
+    return z, names
+
+
+@pytest.mark.parametrize("case", ["c1", "tet10", "hex", "two", "mixed"])
+def test_index_maps_and_surfaces_match_reference_output(case):
+    """The gather plan (gfem/model.py:241-261) over one or several blocks, the skin
+    (gfem/surfaces.py:182-221, with its outward orientation 150-162), the z = max
+    sub-surface (234-242), the surface integrals (103-120) and the pressure and
+    traction load vectors (gfem/loads.py:39-57), against the output of the
+    reference's own code (tests/golden/make_golden.py runs it on these meshes):
+    index maps and facet lists bit for bit, load vectors to 1e-14 of the largest
+    entry (shape-function derivatives in closed form here, by a complex-step
+    derivative there)."""
+    from types import SimpleNamespace
+
+    from exfem_b200 import elements, loads, surfaces
+    from exfem_b200.model import gather_plan
+    z, _ = _ref_fixture_cases()
+    X = z[f"{case}_X"]
+    conns = [z[f"{case}_b{i}_conn"] for i in range(int(z[f"{case}_nblk"]))]
+    ets = [elements.ELEMENTS[str(z[f"{case}_b{i}_etype"])] for i in range(len(conns))]
+    np.testing.assert_array_equal(gather_plan(conns, len(X)), z[f"{case}_plan"])
+    blocks = [SimpleNamespace(conn=c, etype=et) for c, et in zip(conns, ets)]
+    sk = surfaces.skin(X, blocks)
+    top = np.nonzero(X[:, 2] > X[:, 2].max() - 1e-9)[0]
+    sub = surfaces.sub_surface(sk, top)
+    for tag, s in (("skin", sk), ("sub", sub)):
+        assert [ft.name for ft, _ in s.groups] == list(z[f"{case}_{tag}_types"])
+        for g, (_, f) in enumerate(s.groups):
+            np.testing.assert_array_equal(f, z[f"{case}_{tag}_g{g}"])
+    for name, got in (("pressure", loads.pressure_vector(X, sub, -1.0)),
+                      ("traction", loads.traction_vector(X, sub, [1.0, 0.5, -0.25]))):
+        ref = z[f"{case}_{name}"]
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-14 * np.abs(ref).max())
+    w, area, nsum = sk.integrate(X)
+    np.testing.assert_allclose(w, z[f"{case}_skin_w"], rtol=0, atol=1e-14 * np.abs(z[f"{case}_skin_w"]).max())
+    assert abs(area - float(z[f"{case}_skin_area"])) <= 1e-13 * area
+    np.testing.assert_allclose(nsum, z[f"{case}_skin_nsum"], rtol=0, atol=1e-12 * area)
+
+
+def test_face_hash_counts_shared_keys():
+    """exfem_host_face_once: a key that occurs once is flagged, twice or more not."""
+    keys = np.array([[-1, 0, 1, 2], [0, 1, 2, 3], [-1, 0, 1, 2], [-1, 0, 1, 3], [-1, 0, 1, 2]], np.int64)
+    once = np.zeros(len(keys), np.uint8)
+    assert _lib.lib.exfem_host_face_once(len(keys), keys.ctypes.data, once.ctypes.data) == 0
+    np.testing.assert_array_equal(once, [0, 1, 0, 1, 0])
