@@ -23,8 +23,10 @@ solve  = solves/s and p50/p99 latency of the cantilever of the small plain-metho
          case (C3D8 20x4x4, 1,575 DOF) by the mixed FP32/FP64 AMG-PCG path and by
          the plain FP64 path, with the relative displacement error between them;
 cpu_baseline = the CPU oracle (restated reference, torch FP64 forward-mode AD of
-         the internal force = the reference's Model.tangent_jvp) on a 30^3-hex
-         C3D10 sub-mesh with all host threads.
+         the internal force = the reference's Model.tangent_jvp) on the same
+         whole mesh with all host threads; ``--impl reference`` times the same
+         product for K steps after W warm-ups and imports nothing of the CUDA
+         product (its mesh comes from the oracle's restatement of gfem/mesh.py).
 
 Multi-GPU: replicas only — every rank runs the same workload on its own GPU;
 value is the sum over ranks divided by the slowest rank's time.
@@ -110,19 +112,22 @@ class ClockSampler:
 
 
 class CpuOracleProduct:
-    """The CPU oracle's matrix-free product (FP64 forward-mode AD JVP of the
-    internal force, the restated Model.tangent_jvp) on a bounded C3D10 sub-mesh
-    with all host threads."""
+    """The reference's matrix-free tangent product on the host cores: the CPU
+    oracle's FP64 forward-mode AD JVP of the internal force (the restated
+    Model.tangent_jvp, gfem/model.py:488-490, which the FP32 matrix-free product
+    replaces) over the whole benchmark mesh, with all host threads.  The mesh comes
+    from the oracle's own restatement of gfem/mesh.py, so this arm loads nothing of
+    the CUDA product."""
 
-    def __init__(self, n=30):
+    def __init__(self, n=80):
         import torch
-        from exfem_b200 import mesh
         from oracle import fem as ofem
+        from oracle import mesh as omesh
         self.cores = os.cpu_count()
         torch.set_num_threads(self.cores)
-        X, c = mesh.box_hex(1.0, 1.0, 1.0, n, n, n)
-        X = mesh.jitter_interior(X, 1.0 / n, 0.1, 0)
-        X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+        X, c = omesh.box_hex(1.0, 1.0, 1.0, n, n, n)
+        X = omesh.jitter_interior(X, 1.0 / n, 0.1, 0)
+        X, c = omesh.tet4_to_tet10(*omesh.hex_to_tet4(X, c))
         self.m = ofem.Model(X)
         self.m.add_block(c, ofem.TET10, ofem.LinearElastic(1000.0, 0.3), chunk=1 << 20)
         self.scale = [np.exp(np.random.default_rng(1).uniform(0, np.log(10.0), size=len(c)))]
@@ -130,15 +135,17 @@ class CpuOracleProduct:
         self.v = torch.randn(self.m.ndof, dtype=torch.float64, generator=torch.Generator().manual_seed(0))
         self.s = self.m.init_state()
         self.ndof = self.m.ndof
-        self.sample = (f"C3D10 {n}^3x6 sub-mesh of the same construction ({len(c)} el, {self.m.ndof} DOF), "
-                       f"FP64 AD JVP of the internal force (restated Model.tangent_jvp), torch threads={self.cores}")
+        self.sample = (f"the whole C3D10 {n}^3x6 cube ({len(c)} el, {self.m.ndof} DOF), FP64 forward-mode AD "
+                       f"JVP of the internal force (restated Model.tangent_jvp, gfem/model.py:488-490), "
+                       f"torch threads={self.cores}")
 
     def step(self):
         self.m.tangent_jvp(self.u, self.s, self.v, self.scale)
 
 
-def cpu_baseline(steps=3, n=30):
-    """(DOF·matvec/s, info) of the CPU oracle product, timed after one warm-up."""
+def cpu_baseline(steps=2, n=80):
+    """(DOF·matvec/s, info) of the CPU oracle product on the whole mesh, timed
+    after one warm-up."""
     p = CpuOracleProduct(n)
     p.step()
     t0 = time.perf_counter()
@@ -177,7 +184,7 @@ def run_reference(args):
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
                 ms_per_step=dt * 1e3, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
                 data="synthetic", impl="reference",
-                config=dict(workload=WORKLOAD, sample=p.sample),
+                config=dict(workload=WORKLOAD, sample=p.sample, same_mesh=True),
                 cpu_baseline=dict(value=value, unit=UNIT, cores=p.cores, kind="port", sample=p.sample),
                 e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
@@ -199,7 +206,7 @@ def solve_section(reps=10):
     sols = {}
     for name, kw in (("plain_fp64", dict(linear_solver="amg", tangent="ebe", graph=False)),
                      ("mixed", dict(linear_solver="mixed", tangent="mf", graph=True))):
-        s = xf.StaticSolver(m, rtol=1e-6, cg_tol=1e-10 if name == "plain_fp64" else 1e-9, verbose=False, **kw)
+        s = xf.StaticSolver(m, rtol=1e-6, cg_tol=1e-10, verbose=False, **kw)     # config 1: AMG-PCG to 1e-10
         u, _, _ = s.solve(xf.Step(bcs=bcs, loads=loads))          # warm-up, builds the hierarchy
         lat = []
         for _ in range(reps):

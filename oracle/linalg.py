@@ -147,10 +147,13 @@ def bc_matrix(A, free):                                                # linalg.
 
 
 class Direct:                                                          # linalg.py:199-210
-    def __init__(self, A):
+    def __init__(self, A, permc_spec="COLAMD"):
+        """``permc_spec``: SuperLU's column ordering (the reference's COLAMD by
+        default; "MMD_AT_PLUS_A" factors large 3D stiffness matrices with far less
+        fill, same solution to rounding)."""
         self.n = A.shape[0]
         try:
-            self.lu = spla.splu(A.tocsc(), permc_spec="COLAMD")
+            self.lu = spla.splu(A.tocsc(), permc_spec=permc_spec)
             self._solve = self.lu.solve
         except RuntimeError:
             self._solve = spla.factorized(A.tocsc())

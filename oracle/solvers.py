@@ -66,8 +66,10 @@ class Setup:                                                           # solvers
 
 
 class StaticSolver:                                                    # solvers.py:481-683
-    def __init__(self, model, rtol=5e-3, max_iter=16, line_search=True, scale=None, log=None):
+    def __init__(self, model, rtol=5e-3, max_iter=16, line_search=True, scale=None, log=None,
+                 permc_spec="COLAMD"):
         self.m, self.rtol, self.max_iter = model, rtol, max_iter
+        self.permc_spec = permc_spec
         self.line_search = line_search
         self.scale = scale
         self.log = log or (lambda s: None)
@@ -84,7 +86,7 @@ class StaticSolver:                                                    # solvers
         ops = [(d, K.numpy()) for d, K in self._ops(u, s)]
         A = linalg.bc_matrix(fem.ops_assemble(ops, self.m.ndof), setup.free)
         self.linear_solves += 1
-        return linalg.Direct(A).solve(b)
+        return linalg.Direct(A, self.permc_spec).solve(b)
 
     def solve(self, step, u0=None, states=None):
         m = self.m

@@ -126,3 +126,31 @@ def test_oracle_colouring_is_proper():
     for k in range(col.max() + 1):
         nodes = c[col == k].ravel()
         assert len(nodes) == len(np.unique(nodes))
+
+
+def test_oracle_mesh_matches_reference_fixtures():
+    """The oracle's restatement of gfem/mesh.py (the CPU reference arm's mesh source)
+    against the reference's own output, bit for bit, and its node jitter against the
+    product's (both build the benchmark meshes)."""
+    import os
+
+    import numpy as np
+
+    from exfem_b200 import mesh as pmesh
+    from oracle import mesh as omesh
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mesh_fixtures.npz"))
+    for name, args in {"c1": (100.0, 20.0, 20.0, 20, 4, 4), "small": (1.0, 1.0, 1.0, 2, 3, 4),
+                       "cant": (10.0, 1.0, 1.0, 20, 2, 2)}.items():
+        X, c = omesh.box_hex(*args)
+        np.testing.assert_array_equal(X, z[f"{name}_hex_X"])
+        np.testing.assert_array_equal(c, z[f"{name}_hex_conn"])
+    _, c = omesh.box_hex(1.0, 1.0, 1.0, 3, 3, 3)
+    for name in ("t", "tj"):
+        Xt, t4 = omesh.hex_to_tet4(z[f"{name}_hexX"], c)
+        np.testing.assert_array_equal(t4, z[f"{name}_tet4"])
+        X10, c10 = omesh.tet4_to_tet10(Xt, t4)
+        np.testing.assert_array_equal(X10, z[f"{name}_X10"])
+        np.testing.assert_array_equal(c10, z[f"{name}_tet10"])
+    X, c = omesh.box_hex(1.0, 1.0, 1.0, 6, 5, 4)
+    np.testing.assert_array_equal(omesh.jitter_interior(X, [1 / 6, 1 / 5, 1 / 4], 0.1, 9),
+                                  pmesh.jitter_interior(X, [1 / 6, 1 / 5, 1 / 4], 0.1, 9))
