@@ -230,6 +230,39 @@ def test_tet10_mixed_vs_direct(cuda):
     assert rel_err(up, uo) < 1e-8
 
 
+@pytest.mark.parametrize("method", ["mixed", "amg"])
+def test_config3_construction_matches_oracle(cuda, method):
+    """The mixed-precision scale case built exactly as at full size, on a sub-cube
+    the oracle's direct solve handles (8^3 hexahedra x 6 Kuhn C3D10, 14,739 DOF):
+    interior jitter +-10% h, per-element E log-uniform in [1, 10] GPa through the
+    stiffness scale, z = 0 clamped, 1 MPa outward traction on z = 1 as the pressure
+    vector of the top sub-surface of the skin.  The mixed FP32/FP64 path and the
+    plain FP64 path (device set-up of the hierarchy) against the oracle's load
+    vector and sparse direct solution: 1e-8 relative displacement."""
+    import exfem_b200 as xf
+    from exfem_b200 import loads, mesh, surfaces
+    from oracle import loads as oloads
+    n = 8
+    X, c = mesh.box_hex(1.0, 1.0, 1.0, n, n, n)
+    X = mesh.jitter_interior(X, 1.0 / n, 0.1, 0)
+    X, c = mesh.tet4_to_tet10(*mesh.hex_to_tet4(X, c))
+    sc = np.exp(np.random.default_rng(1).uniform(0.0, np.log(10.0), size=len(c)))
+    fix = np.nonzero(X[:, 2] < 1e-9)[0]
+    top = np.nonzero(X[:, 2] > 1 - 1e-9)[0]
+    bcs = [(fix, d, 0.0) for d in range(3)]
+    fo = oloads.pressure_vector(X, oloads.sub_surface(oloads.skin_tet10(X, c), top, len(X)), -1.0)
+    om = ofem.Model(X)
+    om.add_block(c, ofem.TET10, ofem.LinearElastic(1000.0, 0.3))
+    uo, _, _ = osol.StaticSolver(om, rtol=1e-6, scale=[sc]).solve(osol.Step(bcs=bcs, dloads=[fo]))
+    pm = xf.Model(X)
+    pm.add_block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3))
+    f = loads.pressure_vector(X, surfaces.sub_surface(surfaces.skin(X, pm.blocks), top), -1.0)
+    assert np.abs(f - fo).max() <= 1e-14 * np.abs(fo).max()
+    up, _, _ = xf.StaticSolver(pm, rtol=1e-6, linear_solver=method, tangent="mf", cg_tol=1e-11, verbose=False,
+                               amg_setup="device").solve(xf.Step(bcs=bcs, dloads=[f]), scale=[sc])
+    assert rel_err(up, uo) < 1e-8, rel_err(up, uo)
+
+
 def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
     """Failure detection without a GPU fault: a kernel whose barrier nothing arrives
     on must give up after its poll limit and report EXFEM_ERR_TIMEOUT; the next
