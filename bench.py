@@ -345,7 +345,7 @@ def batch_section(count=512, nplain=24, seed=0, workers=None):
     for i in sample:
         k, r = S.inst[i]
         p = probs[k]
-        blk = Block(p.conn, p.etype, p.material, p.X)
+        blk = Block(p.conn, p.etype, p.material, X=p.X)
         blk.set_fixed(p.fixed)
         dofs, Ke = batch._element_stiffness(p)
         A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke)], p.ndof), (~p.fixed).astype(float))
@@ -513,7 +513,7 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), 
                     m.add_block(sp.conn, sp.etype, sp.material)
                     plain_cache[sp.key] = ("j2", m, amg)
                 else:
-                    blk = Block(sp.conn, sp.etype, sp.material, sp.X)
+                    blk = Block(sp.conn, sp.etype, sp.material, X=sp.X)
                     blk.set_fixed(sp.fixed)
                     plain_cache[sp.key] = ("lin", linalg.NativeSolver(blk, "mf64", "amg", amg, graph=False), amg)
             kind, obj, amg = plain_cache[sp.key]

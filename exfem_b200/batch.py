@@ -71,7 +71,7 @@ def _setup_worker(args):
 
 
 def _element_stiffness(p):
-    blk = Block(p.conn, p.etype, p.material, p.X)
+    blk = Block(p.conn, p.etype, p.material, X=p.X)
     Ke = blk.stiffness(torch.zeros(p.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
     dofs = (p.conn.astype(np.int64)[:, :, None] * 3 + np.arange(3)).reshape(len(p.conn), -1)
     return dofs, Ke.cpu().numpy()
@@ -83,7 +83,7 @@ def device_setups(problems, max_coarse=300):
     host in the form :func:`host_setups` returns, one problem after the other."""
     out = []
     for p in problems:
-        blk = Block(p.conn, p.etype, p.material, p.X)
+        blk = Block(p.conn, p.etype, p.material, X=p.X)
         blk.set_fixed(p.fixed)
         Ke = blk.stiffness(torch.zeros(p.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
         amg = linalg.DeviceAMG(blk, Ke, max_coarse)
@@ -205,7 +205,7 @@ class BatchSolver:
             mus.append(np.full(len(p.conn), mu))
             fixed.append(p.fixed)
             node0 += len(p.X)
-        self.block = Block(np.concatenate(cs), self.etype, self.problems[0].material, np.concatenate(Xs))
+        self.block = Block(np.concatenate(cs), self.etype, self.problems[0].material, X=np.concatenate(Xs))
         self.block.set_lame(np.concatenate(lams), np.concatenate(mus))
         self.fixed = np.concatenate(fixed)
         self.block.set_fixed(self.fixed)

@@ -39,10 +39,13 @@ class Material:
 class LinearElastic(Material):
     linear = True
 
-    def __init__(self, E, nu, density=1.0, name=None, **kw):
+    def __init__(self, E, nu, density=1.0, name=None, alpha=0.0, tref=0.0, **kw):
         self.E, self.nu = float(E), float(nu)
         self.mu, self.lam = lame(self.E, self.nu)
         self.density = float(density)
+        # thermal expansion (gfem/materials.py:28-30); a temperature field that would
+        # strain the material is refused by the model (the kernels have no thermal strain)
+        self.alpha, self.tref = float(alpha), float(tref)
         if name:
             self.name = name
 
@@ -55,12 +58,13 @@ class LinearElastic(Material):
 class J2Plasticity(Material):
     nstate = 19
 
-    def __init__(self, E, nu, table, Hk=0.0, density=1.0, name=None, **kw):
+    def __init__(self, E, nu, table, Hk=0.0, density=1.0, name=None, alpha=0.0, tref=0.0, **kw):
         self.E, self.nu = float(E), float(nu)
         self.mu, self.lam = lame(self.E, self.nu)
         self.K = self.lam + 2 * self.mu / 3
         self.Hk = float(Hk)
         self.density = float(density)
+        self.alpha, self.tref = float(alpha), float(tref)
         if name:
             self.name = name
         t = np.asarray(table, dtype=np.float64).reshape(-1, 2)
@@ -85,14 +89,17 @@ class J2Plasticity(Material):
 
 
 def from_props(p, name=None):
-    """Property dictionary -> material, for the two small-strain models covered."""
-    plastic = "plastic" in p or "yield" in p or p.get("model") == "plastic"
-    if plastic:
-        table = p.get("plastic")
-        if table is None:
-            Et = p.get("tangent", 0.0)                                 # bilinear (ANSYS BISO style)
-            E = p["E"]
-            Hp = E * Et / (E - Et) if Et > 0 else 0.0
-            table = [[p["yield"], 0.0], [p["yield"] + Hp * 1.0, 1.0]]
-        return J2Plasticity(p["E"], p["nu"], table, Hk=p.get("Hk", 0.0), name=name)
-    return LinearElastic(p["E"], p["nu"], name=name)
+    """Material from a property dictionary (the keys of gfem/materials.py:335-391)
+    for the two small-strain models covered.  A plastic material takes a hardening
+    table, or a yield stress with an optional elastic-plastic tangent modulus Et:
+    the plastic modulus of that straight line is H = E Et / (E - Et), giving the
+    two-row table (sy, 0), (sy + H, 1)."""
+    common = dict(density=p.get("density", 1.0), alpha=p.get("alpha", 0.0), tref=p.get("tref", 0.0), name=name)
+    if not ("plastic" in p or "yield" in p or p.get("model") == "plastic"):
+        return LinearElastic(p["E"], p["nu"], **common)
+    table = p.get("plastic")
+    if table is None:
+        E, Et, sy = float(p["E"]), float(p.get("tangent", 0.0)), float(p["yield"])
+        H = E * Et / (E - Et) if Et > 0.0 else 0.0
+        table = [[sy, 0.0], [sy + H, 1.0]]
+    return J2Plasticity(p["E"], p["nu"], table, Hk=p.get("Hk", 0.0), **common)

@@ -41,6 +41,18 @@ def gather_plan(conns, nn):
     return plan
 
 
+def _check_thermal(material, Te, where):
+    """Temperatures give a thermal strain alpha (T - T0) (gfem/model.py:54-59); the
+    element kernels cover materials without thermal expansion only, so a field that
+    would strain them is refused instead of ignored."""
+    if Te is None or float(getattr(material, "alpha", 0.0)) == 0.0:
+        return
+    T = torch.as_tensor(Te, dtype=torch.float64)
+    if bool(torch.any(T[..., 0] != T[..., 1])):
+        raise NotImplementedError(f"{where()}: thermal strain (alpha = {material.alpha:g}, T != T0) is not covered "
+                                  "by the element kernels")
+
+
 def _dev(x, dtype=torch.float64):
     if isinstance(x, torch.Tensor):
         return x.to(device="cuda", dtype=dtype).contiguous()
@@ -48,25 +60,40 @@ def _dev(x, dtype=torch.float64):
 
 
 class Block:
-    """Element block bound to node coordinates ``X`` (library handle)."""
+    """Element block: connectivity, element type and material (gfem/model.py:21-26,
+    same positional arguments).  The global operators need the block bound to the
+    model's node coordinates ``X`` (``Model.add_block`` binds it; a library handle
+    then holds the device data); ``force``/``stiff`` on gathered element arrays work
+    on an unbound block too."""
 
-    def __init__(self, conn, etype, material, X, name="block"):
-        _lib.require_cuda()
+    def __init__(self, conn, etype, material, name="block", X=None):
         self.conn = np.ascontiguousarray(np.asarray(conn, dtype=np.int32))
         self.etype, self.material, self.name = etype, material, name
         self.ne = int(self.conn.shape[0])
-        X = np.ascontiguousarray(np.asarray(X, dtype=np.float64))
-        self.nn = int(X.shape[0])
         if self.ne and self.conn.shape[1] != etype.nnode:
             raise ValueError(f"{etype.name} needs {etype.nnode} nodes per element, got {self.conn.shape[1]}")
-        h = C.c_void_p()
-        m = material.to_c()
-        check(lib.exfem_block_create(etype.code, C.byref(m), self.nn, X.ctypes.data, self.ne,
-                                     self.conn.ctypes.data if self.ne else None, C.byref(h)))
-        self._h = h
+        self._h = None
         self._scale_key = None
         self._fixed_key = None
+        self._local = None                  # (key, disjoint block) of the gathered-array signatures
+        self.nn = 0
+        if X is not None:
+            self.bind(X)
+
+    def bind(self, X):
+        """Create the library handle over node coordinates X (nn, 3)."""
+        _lib.require_cuda()
+        if self._h is not None:
+            raise RuntimeError(f"block {self.name} is already bound to node coordinates")
+        X = np.ascontiguousarray(np.asarray(X, dtype=np.float64))
+        self.nn = int(X.shape[0])
+        h = C.c_void_p()
+        m = self.material.to_c()
+        check(lib.exfem_block_create(self.etype.code, C.byref(m), self.nn, X.ctypes.data, self.ne,
+                                     self.conn.ctypes.data if self.ne else None, C.byref(h)))
+        self._h = h
         self.conn_dev = torch.as_tensor(self.conn, device="cuda")
+        return self
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -76,13 +103,15 @@ class Block:
 
     @property
     def handle(self):
+        if self._h is None:
+            raise RuntimeError(f"block {self.name} is not bound to node coordinates (Model.add_block binds it)")
         return self._h
 
     # ---------------- info and index maps
     def query(self):
         ne, nn, vmax, ncol, aff, nb = C.c_int64(), C.c_int64(), C.c_int(), C.c_int(), C.c_int(), C.c_int64()
         nnode, ngp, ns = C.c_int(), C.c_int(), C.c_int()
-        check(lib.exfem_block_query(self._h, C.byref(ne), C.byref(nn), C.byref(nnode), C.byref(ngp), C.byref(ns),
+        check(lib.exfem_block_query(self.handle, C.byref(ne), C.byref(nn), C.byref(nnode), C.byref(ngp), C.byref(ns),
                                     C.byref(vmax), C.byref(ncol), C.byref(aff), C.byref(nb)))
         return dict(ne=ne.value, nn=nn.value, nnode=nnode.value, ngp=ngp.value, nstate=ns.value,
                     vmax=vmax.value, ncolour=ncol.value, affine=bool(aff.value), device_bytes=nb.value)
@@ -90,38 +119,38 @@ class Block:
     def gather_plan(self):
         q = self.query()
         out = np.empty((self.nn, q["vmax"]), np.int32)
-        check(lib.exfem_block_gather_plan(self._h, out.ctypes.data))
+        check(lib.exfem_block_gather_plan(self.handle, out.ctypes.data))
         return out
 
     def colours(self):
         out = np.empty(self.ne, np.int32)
-        check(lib.exfem_block_colours(self._h, out.ctypes.data))
+        check(lib.exfem_block_colours(self.handle, out.ctypes.data))
         return out
 
     def tile_maps(self):
         """(ptr, nodes, nend, perm) element-tile maps of the matrix-free operator."""
         nt, nl, mu = C.c_int64(), C.c_int64(), C.c_int()
-        check(lib.exfem_block_tile_info(self._h, C.byref(nt), C.byref(nl), C.byref(mu)))
+        check(lib.exfem_block_tile_info(self.handle, C.byref(nt), C.byref(nl), C.byref(mu)))
         tile, _ = self.tile_order()
         ptr_ = np.empty(nt.value + 1, np.int32)
         nodes = np.empty(max(nl.value, 1), np.int32)
         nend = np.empty(max(nl.value, 1), np.uint16)
         perm = np.empty((nt.value, self.etype.nnode * tile), np.uint16)
-        check(lib.exfem_block_tile_maps(self._h, ptr_.ctypes.data, nodes.ctypes.data, nend.ctypes.data,
+        check(lib.exfem_block_tile_maps(self.handle, ptr_.ctypes.data, nodes.ctypes.data, nend.ctypes.data,
                                         perm.ctypes.data))
         return ptr_, nodes[:nl.value], nend[:nl.value], perm
 
     def tile_conn(self):
         """(ne, nnode) connectivity of every tile position in the tiles' numbering."""
         out = np.empty((max(self.ne, 1), self.etype.nnode), np.int32)
-        check(lib.exfem_block_tile_conn(self._h, out.ctypes.data))
+        check(lib.exfem_block_tile_conn(self.handle, out.ctypes.data))
         return out[:self.ne]
 
     def tile_order(self):
         """(tile, order): elements per tile and the tile order (position -> element)."""
         tile = C.c_int()
         order = np.empty(max(self.ne, 1), np.int32)
-        check(lib.exfem_block_tile_order(self._h, C.byref(tile), order.ctypes.data))
+        check(lib.exfem_block_tile_order(self.handle, C.byref(tile), order.ctypes.data))
         return tile.value, order[:self.ne]
 
     def init_state(self):                                              # model.py:154-155
@@ -135,14 +164,14 @@ class Block:
         """Per-element stiffness scale (fields["scale"], model.py:449-463)."""
         if scale is None:
             if self._scale_key is not None:
-                check(lib.exfem_block_set_scale(self._h, None))
+                check(lib.exfem_block_set_scale(self.handle, None))
                 self._scale_key = None
             return
         s = np.ascontiguousarray(np.asarray(scale.cpu() if isinstance(scale, torch.Tensor) else scale,
                                             dtype=np.float64).reshape(-1))
         key = (s.size, hash(s.tobytes()))
         if key != self._scale_key:
-            check(lib.exfem_block_set_scale(self._h, s.ctypes.data))
+            check(lib.exfem_block_set_scale(self.handle, s.ctypes.data))
             self._scale_key = key
 
     def set_lame(self, lam, mu):
@@ -150,25 +179,25 @@ class Block:
         many linear-elastic instances with their own E and nu); None, None = the
         block material's."""
         if lam is None and mu is None:
-            check(lib.exfem_block_set_lame(self._h, None, None))
+            check(lib.exfem_block_set_lame(self.handle, None, None))
             return
         lam = np.ascontiguousarray(np.asarray(lam, dtype=np.float64).reshape(-1))
         mu = np.ascontiguousarray(np.asarray(mu, dtype=np.float64).reshape(-1))
         if lam.size != self.ne or mu.size != self.ne:
             raise ValueError(f"need {self.ne} Lame pairs, got {lam.size} and {mu.size}")
-        check(lib.exfem_block_set_lame(self._h, lam.ctypes.data, mu.ctypes.data))
+        check(lib.exfem_block_set_lame(self.handle, lam.ctypes.data, mu.ctypes.data))
 
     def set_fixed(self, fixed):
         """Prescribed-DOF mask (ndof of this block's node set) used by opA."""
         if fixed is None:
             if self._fixed_key is not None:
-                check(lib.exfem_block_set_fixed(self._h, None))
+                check(lib.exfem_block_set_fixed(self.handle, None))
                 self._fixed_key = None
             return
         f = np.ascontiguousarray(np.asarray(fixed).astype(np.uint8).reshape(-1))
         key = hash(f.tobytes())
         if key != self._fixed_key:
-            check(lib.exfem_block_set_fixed(self._h, f.ctypes.data))
+            check(lib.exfem_block_set_fixed(self.handle, f.ctypes.data))
             self._fixed_key = key
 
     # ---------------- kernels on global vectors
@@ -178,7 +207,7 @@ class Block:
         s_old = _dev(state) if j2 else None
         s_new = torch.empty_like(s_old) if j2 else None
         f = torch.empty(3 * self.nn, dtype=torch.float64, device="cuda")
-        check(lib.exfem_internal_force(self._h, ptr(u), ptr(s_old), ptr(s_new), ptr(fe), ptr(f), assembly,
+        check(lib.exfem_internal_force(self.handle, ptr(u), ptr(s_old), ptr(s_new), ptr(fe), ptr(f), assembly,
                                        stream_ptr()))
         return f, (s_new if j2 else state)
 
@@ -188,23 +217,23 @@ class Block:
         s_old = _dev(state) if self.material.nstate > 1 else None
         nd = self.etype.nd
         Ke = torch.empty((self.ne, nd, nd), dtype=dtype, device="cuda")
-        check(lib.exfem_element_stiffness(self._h, ptr(u), ptr(s_old), code, ptr(Ke), stream_ptr()))
+        check(lib.exfem_element_stiffness(self.handle, ptr(u), ptr(s_old), code, ptr(Ke), stream_ptr()))
         return Ke
 
     def tangent_update(self, u, state):
         if self.material.nstate > 1:
-            check(lib.exfem_tangent_update(self._h, ptr(_dev(u)), ptr(_dev(state)), stream_ptr()))
+            check(lib.exfem_tangent_update(self.handle, ptr(_dev(u)), ptr(_dev(state)), stream_ptr()))
 
     def tangent_matvec(self, v, out=None, apply_bc=True):
         v = v.contiguous()
         code = _lib.F64 if v.dtype == torch.float64 else _lib.F32
         y = torch.empty_like(v) if out is None else out
-        check(lib.exfem_tangent_matvec(self._h, code, ptr(v), ptr(y), 1 if apply_bc else 0, stream_ptr()))
+        check(lib.exfem_tangent_matvec(self.handle, code, ptr(v), ptr(y), 1 if apply_bc else 0, stream_ptr()))
         return y
 
     def tangent_diagonal(self):
         d = torch.empty(3 * self.nn, dtype=torch.float64, device="cuda")
-        check(lib.exfem_tangent_diagonal(self._h, ptr(d), stream_ptr()))
+        check(lib.exfem_tangent_diagonal(self.handle, ptr(d), stream_ptr()))
         return d
 
     def ebe_matvec_multi(self, Ke_bf16, V, apply_bc=True):
@@ -213,19 +242,19 @@ class Block:
         to BF16, FP32 accumulation)."""
         V = V.to(torch.float32).contiguous()
         Y = torch.empty_like(V)
-        check(lib.exfem_ebe_matvec_bf16_multi(self._h, ptr(Ke_bf16.contiguous()), V.shape[1], ptr(V), ptr(Y),
+        check(lib.exfem_ebe_matvec_bf16_multi(self.handle, ptr(Ke_bf16.contiguous()), V.shape[1], ptr(V), ptr(Y),
                                               1 if apply_bc else 0, stream_ptr()))
         return Y
 
     def ebe_matvec(self, Ke, v, apply_bc=True):
         v = _dev(v)
         y = torch.empty_like(v)
-        check(lib.exfem_ebe_matvec(self._h, ptr(Ke.contiguous()), ptr(v), ptr(y), 1 if apply_bc else 0, stream_ptr()))
+        check(lib.exfem_ebe_matvec(self.handle, ptr(Ke.contiguous()), ptr(v), ptr(y), 1 if apply_bc else 0, stream_ptr()))
         return y
 
     def ebe_diagonal(self, Ke):
         d = torch.empty(3 * self.nn, dtype=torch.float64, device="cuda")
-        check(lib.exfem_ebe_diagonal(self._h, ptr(Ke.contiguous()), ptr(d), stream_ptr()))
+        check(lib.exfem_ebe_diagonal(self.handle, ptr(Ke.contiguous()), ptr(d), stream_ptr()))
         return d
 
     def cauchy(self, u, state):
@@ -233,22 +262,39 @@ class Block:
         mises = torch.empty(self.ne, dtype=torch.float64, device="cuda")
         peeq = torch.empty(self.ne, dtype=torch.float64, device="cuda")
         s = _dev(state) if self.material.nstate > 1 else None
-        check(lib.exfem_stresses(self._h, ptr(_dev(u)), ptr(s), ptr(S), ptr(mises), ptr(peeq), stream_ptr()))
+        check(lib.exfem_stresses(self.handle, ptr(_dev(u)), ptr(s), ptr(S), ptr(mises), ptr(peeq), stream_ptr()))
         return S, mises, peeq
 
     # ---------------- reference per-element signatures (model.py:70-111)
-    @staticmethod
-    def _disjoint(etype, material, Xe):
-        ne, nnode = Xe.shape[0], Xe.shape[1]
-        conn = np.arange(ne * nnode, dtype=np.int32).reshape(ne, nnode)
-        return Block(conn, etype, material, np.asarray(Xe.detach().cpu() if isinstance(Xe, torch.Tensor) else Xe,
-                                                       dtype=np.float64).reshape(-1, 3))
+    def _disjoint(self, Xe):
+        """A block of the same type and material whose elements own their nodes,
+        over the gathered coordinates Xe (ne, nnode, 3); kept while Xe is unchanged,
+        so repeated calls on one mesh build its geometry streams once."""
+        Xh = np.ascontiguousarray(np.asarray(Xe.detach().cpu() if isinstance(Xe, torch.Tensor) else Xe,
+                                             dtype=np.float64))
+        key = (Xh.shape, hash(Xh.tobytes()))
+        if self._local is None or self._local[0] != key:
+            ne, nnode = Xh.shape[0], Xh.shape[1]
+            conn = np.arange(ne * nnode, dtype=np.int32).reshape(ne, nnode)
+            self._local = (key, Block(conn, self.etype, self.material, self.name, X=Xh.reshape(-1, 3)))
+        return self._local[1]
+
+    def _element_fields(self, b, Te, scv):
+        """Stiffness scale of the gathered-array signatures; temperature and
+        eigenstrain fields are checked, because the element kernels cover neither."""
+        _check_thermal(self.material, Te, lambda: f"block {self.name}")
+        if scv is None:
+            b.set_scale(None)
+            return
+        scv = torch.as_tensor(scv, dtype=torch.float64)
+        if scv.shape[-1] > 1 and bool(torch.any(scv[:, 1:] != 0)):
+            raise NotImplementedError(f"block {self.name}: eigenstrain fields are not covered by the element kernels")
+        b.set_scale(np.asarray(scv[:, 0].cpu()))
 
     def force(self, Xe, ue, se=None, Te=None, scv=None):
         """Element forces from gathered arrays Xe, ue (ne, nnode, 3): (fe, s_new)."""
-        b = Block._disjoint(self.etype, self.material, Xe)
-        if scv is not None:
-            b.set_scale(np.asarray(torch.as_tensor(scv)[:, 0].cpu()))
+        b = self._disjoint(Xe)
+        self._element_fields(b, Te, scv)
         st = se if se is not None else b.init_state()
         fe = torch.empty((b.ne, self.etype.nnode, 3), dtype=torch.float64, device="cuda")
         _, sn = b.internal_force(_dev(ue).reshape(-1), st, fe=fe)
@@ -256,9 +302,8 @@ class Block:
 
     def stiff(self, Xe, ue, se=None, Te=None, scv=None):
         """Element tangents from gathered arrays: Ke (ne, nd, nd)."""
-        b = Block._disjoint(self.etype, self.material, Xe)
-        if scv is not None:
-            b.set_scale(np.asarray(torch.as_tensor(scv)[:, 0].cpu()))
+        b = self._disjoint(Xe)
+        self._element_fields(b, Te, scv)
         st = se if se is not None else b.init_state()
         return b.stiffness(_dev(ue).reshape(-1), st)
 
@@ -277,7 +322,7 @@ class Model:
         self.T0 = None
 
     def add_block(self, conn, etype, material, name=None):
-        b = Block(conn, etype, material, self.X, name or f"block{len(self.blocks)}")
+        b = Block(conn, etype, material, name or f"block{len(self.blocks)}", X=self.X)
         self.blocks.append(b)
         return b
 
@@ -304,9 +349,23 @@ class Model:
         return dict(scale=[None] * len(self.blocks))
 
     def _apply_fields(self, fields):
-        sc = (fields or {}).get("scale") or [None] * len(self.blocks)
+        """fields (gfem/model.py:446-463): "scale" per block is applied; "T" (nodal
+        temperatures against the initial ``T0``) and "eig" (per-element
+        eigenstrains) are refused where they would change the result, because the
+        element kernels cover neither."""
+        fields = fields or {}
+        sc = fields.get("scale") or [None] * len(self.blocks)
         for b, s in zip(self.blocks, sc):
             b.set_scale(s)
+        T = fields.get("T")
+        if T is not None:
+            T = torch.as_tensor(T, dtype=torch.float64).reshape(-1)
+            T0 = torch.zeros_like(T) if self.T0 is None else torch.as_tensor(self.T0, dtype=torch.float64).reshape(-1)
+            for b in self.blocks:
+                _check_thermal(b.material, torch.stack([T, T0], 1), lambda: f"block {b.name}")
+        for b, e in zip(self.blocks, fields.get("eig") or []):
+            if e is not None and bool(torch.any(torch.as_tensor(e) != 0)):
+                raise NotImplementedError(f"block {b.name}: eigenstrain fields are not covered by the element kernels")
 
     # ---------- global operators
     def internal_force(self, u, states, fields=None, assembly=_lib.ASSEMBLE_GATHER):

@@ -114,7 +114,7 @@ class _Entry:
             self.block, self.solver = self.model.blocks[0], None
         else:
             self.model = None
-            self.block = Block(spec.conn, spec.etype, spec.material, spec.X)
+            self.block = Block(spec.conn, spec.etype, spec.material, X=spec.X)
             self.block.set_fixed(spec.fixed)
             self.solver = linalg.NativeSolver(self.block, "mf32", "amg", self.amg, graph=graph)
         self.bytes = spec.device_bytes_estimate()
@@ -201,7 +201,7 @@ class SolveServer:
 
     # ------------------------------------------------------------------ set-up
     def _device_setup(self, spec):
-        blk = Block(spec.conn, spec.etype, LinearElastic(spec.material.E, spec.material.nu), spec.X)
+        blk = Block(spec.conn, spec.etype, LinearElastic(spec.material.E, spec.material.nu), X=spec.X)
         Ke = blk.stiffness(torch.zeros(spec.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
         if self.amg_setup == "device":
             blk.set_fixed(spec.fixed)

@@ -272,6 +272,24 @@ class StaticSolver:                                                     # solver
         ops = self._ops(u, s, fields)
         return self.lin.solve(ops, b, setup, (u, s, fields) if ops is None else None)
 
+    # increment control (gfem/solvers.py:525-605): an increment that converges in at
+    # most GROW_AFTER Newton corrections lets the next one grow by GROW (capped by the
+    # step's dt_max); a failed increment is retried at CUT of its size, and the step
+    # fails once that drops below dt_min or the step runs out of increments
+    GROW, GROW_AFTER, CUT = 1.5, 5, 0.25
+
+    def _try_increment(self, u, states, t_new, fields, setup, inc):
+        """Predictor and Newton iterations of one increment ending at t_new:
+        (converged, corrections, u, states); a non-finite residual fails it."""
+        fext = setup.fext(t_new)
+        start = torch.where(setup.fixed_j, setup.prescribed(t_new), u)
+        try:
+            start = self._predictor(u, states, start, fext, fields, setup)
+            ok, its, u_new, s_new, _ = self._newton(start, states, fext, fields, setup, inc)
+        except FloatingPointError:
+            return False, 0, u, states
+        return ok, its, u_new, s_new
+
     def solve(self, step, u0=None, states=None, fext0=None, callback=None, state=None, scale=None):
         m = self.m
         st = state or State(m)
@@ -284,45 +302,41 @@ class StaticSolver:                                                     # solver
         setup = _Setup(m, step, st)
         self.setup = setup
         self.lin.reset()
-        u, states = st.u, st.states
-        t, dt, inc, history = 0.0, min(step.dt_init, step.T), 0, []
-        t0 = time.time()
-        total = 0
         self.qref = 0.0
         fields = self._fields(scale)
-        while t < step.T * (1 - 1e-12):
-            if self.mon.should_stop():
-                self.mon.log("  stopped by user")
-                break
-            inc += 1
-            if inc > step.max_inc:
-                raise RuntimeError("max increments exceeded")
+        u, states = st.u, st.states
+        t, dt = 0.0, min(step.dt_init, step.T)
+        history, attempts, total = [], 0, 0
+        clock = time.time()
+        end = step.T * (1 - 1e-12)
+        while t < end and not self.mon.should_stop():
+            attempts += 1
+            if attempts > step.max_inc:
+                raise RuntimeError(f"step {step.name!r}: {step.max_inc} increments used before t reached "
+                                   f"{step.T:g} (now {t:.4g})")
             dt = min(dt, step.T - t)
-            tn = t + dt
-            fext = setup.fext(tn)
-            ut = torch.where(setup.fixed_j, setup.prescribed(tn), u)
-            try:
-                ut = self._predictor(u, states, ut, fext, fields, setup)
-                ok, it, ui, s_try, rh = self._newton(ut, states, fext, fields, setup, inc)
-            except FloatingPointError:
-                ok, it, ui, s_try, rh = False, 0, u, states, []
-            total += it
-            if ok:
-                u, states, t = ui, s_try, tn
-                history.append((t, it))
-                self.mon.log(f"  inc {inc:4d}  t={t:.4g}  dt={dt:.3g}  iters={it}  lin={self.lin.last_iters}")
-                self.mon.increment(step=step.name, inc=inc, t=t, dt=dt, iters=it, ok=True)
-                if callback:
-                    callback(t, u, states)
-                if it <= 5:
-                    dt = min(dt * 1.5, step.dt_max)
-            else:
-                dt *= 0.25
-                self.mon.log(f"  inc {inc:4d}  cutback -> dt={dt:.3g}")
-                self.mon.increment(step=step.name, inc=inc, t=t, dt=dt, iters=it, ok=False)
+            ok, its, u_new, s_new = self._try_increment(u, states, t + dt, fields, setup, attempts)
+            total += its
+            self.mon.increment(step=step.name, inc=attempts, t=t + dt if ok else t, dt=dt, iters=its, ok=ok)
+            if not ok:
+                dt *= self.CUT
+                self.mon.log(f"  increment {attempts}: no convergence, retrying with dt {dt:.3g}")
                 if dt < step.dt_min:
-                    raise RuntimeError("time increment smaller than minimum")
-        self.mon.log(f"  step '{step.name}' done: {inc} incs, {total} iterations, {time.time() - t0:.2f}s")
+                    raise RuntimeError(f"step {step.name!r}: increment size {dt:.3g} fell below dt_min "
+                                       f"{step.dt_min:g} at t = {t:.4g}")
+                continue
+            u, states, t = u_new, s_new, t + dt
+            history.append((t, its))
+            self.mon.log(f"  increment {attempts}: t {t:.4g} (dt {dt:.3g}), {its} Newton corrections, "
+                         f"last linear solve {self.lin.last_iters} iterations")
+            if callback:
+                callback(t, u, states)
+            if its <= self.GROW_AFTER:
+                dt = min(self.GROW * dt, step.dt_max)
+        if t < end:
+            self.mon.log(f"  step {step.name!r} stopped at t = {t:.4g} on request")
+        self.mon.log(f"  step {step.name!r}: {attempts} increments, {total} Newton corrections, "
+                     f"{time.time() - clock:.2f} s")
         fint, _ = self._fint(u, states, fields)
         reactions = (fint - setup.fext(step.T)) * setup.fixed_j
         fe = setup.fext_final()
@@ -331,7 +345,7 @@ class StaticSolver:                                                     # solver
         st.reactions = reactions
         self.newton_iterations = total
         return u, states, dict(history=history, reactions=reactions, fext=fe, state=st, iterations=total,
-                               increments=inc)
+                               increments=attempts)
 
     def _predictor(self, uc, s_old, ut, fext, fields, setup):           # solvers.py:607-624
         delta = ut - uc

@@ -78,7 +78,7 @@ def autotune(etypes=(elements.HEX8, elements.TET10), n=None, reps=20, candidates
             try:
                 for tile in candidates:
                     apply(et, tile)
-                    blk = Block(c, et, LinearElastic(1000.0, 0.3), X)
+                    blk = Block(c, et, LinearElastic(1000.0, 0.3), X=X)
                     blk.set_fixed(fixed)
                     times[tile] = _time_product(blk, 3 * len(X), reps)
                     del blk

@@ -63,7 +63,7 @@ def test_batch_matches_direct_and_single_solves(cuda):
         xd = _direct(p, r)
         assert _rel(xs[i], xd) <= TOL_DIRECT, (i, _rel(xs[i], xd))
         # the single-solve mixed path with the problem's own hierarchy
-        blk = Block(p.conn, p.etype, p.material, p.X)
+        blk = Block(p.conn, p.etype, p.material, X=p.X)
         blk.set_fixed(p.fixed)
         dofs, Ke = batch._element_stiffness(p)
         A = linalg.bc_matrix(linalg.ops_assemble([(dofs, Ke)], p.ndof), (~p.fixed).astype(float))

@@ -193,7 +193,7 @@ def test_autotuner_picks_a_tile_and_both_tiles_agree(cuda):
     ys = {}
     for t in tuning.CANDIDATES:
         tuning.apply(xf.TET10, t)
-        blk = Block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3), X)
+        blk = Block(c, xf.TET10, xf.LinearElastic(1000.0, 0.3), X=X)
         assert blk.tile_order()[0] == t
         ys[t] = blk.tangent_matvec(v.float()).double()
         y64 = blk.tangent_matvec(v)
