@@ -19,7 +19,7 @@ LINEAR_ELASTIC, J2 = 0, 1
 F64, F32, BF16 = 0, 1, 2
 ASSEMBLE_GATHER, ASSEMBLE_COLOUR = 0, 1
 OP_EBE_F64, OP_MF_F64, OP_MF_F32, OP_CSR_F64 = 0, 1, 2, 3
-PC_NONE, PC_JACOBI, PC_AMG = 0, 1, 2
+PC_NONE, PC_JACOBI, PC_AMG, PC_CHEBY = 0, 1, 2, 3
 MAX_TABLE = 32
 
 
@@ -82,6 +82,7 @@ _SIGS = {
     "exfem_solver_destroy": ([VP], C.c_int),
     "exfem_solver_set_ke": ([VP, P], C.c_int),
     "exfem_solver_refresh_diagonal": ([VP, VP], C.c_int),
+    "exfem_solver_cheby_bound": ([VP, C.POINTER(D)], C.c_int),
     "exfem_solver_set_graph": ([VP, C.c_int, C.c_int], C.c_int),
     "exfem_solver_pcg": ([VP, P, P, D, C.c_int, C.POINTER(I32), C.POINTER(D), VP], C.c_int),
     "exfem_solver_mixed": ([VP, P, P, D, D, C.c_int, C.c_int, C.POINTER(I32), C.POINTER(I32), C.POINTER(D), VP],
@@ -99,6 +100,7 @@ _SIGS = {
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
     "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
     "exfem_host_face_once": ([I64, P, P], C.c_int),
+    "exfem_host_tile_maps": ([I64, I64, I32, P, I32, I32, P, C.POINTER(I64), C.POINTER(I64), P, P, P, P], C.c_int),
     "exfem_block_status": ([VP, VP], C.c_int),
     "exfem_amg_setup_block": ([VP, VP, P, I32, I32, VP], C.c_int),
     "exfem_amg_setup_blocks": ([VP, I32, P, P, I32, I32, VP], C.c_int),

@@ -160,6 +160,58 @@ __global__ void add_free_kernel(int64_t n, const uint8_t* __restrict__ fixed, co
     if (!(fixed && fixed[i])) y[i] += t[i];
 }
 
+// Chebyshev-Jacobi polynomial preconditioner z = M(r) (the reference's "cheby",
+// gfem/solvers.py:289-306): res = D^-1 r, d = res / theta, x = 0; six times
+// x += d, res -= D^-1 A d, d = c_a d + c_b res; z = x + d
+template <class T>
+__global__ void cheb_pc_init_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ r,
+                                    T* __restrict__ x, T* __restrict__ res, T* __restrict__ d, T ith,
+                                    const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T q = dinv[i] * r[i];
+    res[i] = q;
+    d[i] = q * ith;
+    x[i] = T(0);
+  }
+}
+
+template <class T>
+__global__ void cheb_pc_step_kernel(int64_t n, const T* __restrict__ dinv, const T* __restrict__ Ad,
+                                    T* __restrict__ x, T* __restrict__ res, T* __restrict__ d, T ca, T cb,
+                                    const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const T di = d[i];
+    x[i] += di;
+    const T q = res[i] - dinv[i] * Ad[i];
+    res[i] = q;
+    d[i] = ca * di + cb * q;
+  }
+}
+
+template <class T>
+__global__ void cheb_pc_out_kernel(int64_t n, const T* __restrict__ x, const T* __restrict__ d, T* __restrict__ z,
+                                   const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    z[i] = x[i] + d[i];
+}
+
+// power-iteration start vector of the Chebyshev bound (gfem/solvers.py:333):
+// v_i = sin(0.37 i + 0.1) free_i + 1e-3
+__global__ void cheb_start_kernel(int64_t n, const uint8_t* __restrict__ fixed, double* __restrict__ v) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = ((fixed && fixed[i]) ? 0.0 : sin(0.37 * (double)i + 0.1)) + 1e-3;
+}
+
+// w = D^-1 y, or v = w / |w| (scale given)
+__global__ void cheb_scale_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                                  double* __restrict__ out, double sc) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (b ? a[i] * b[i] : a[i]) * sc;
+}
+
 __global__ void dinv_kernel(int64_t n, const double* __restrict__ d, const uint8_t* __restrict__ fixed,
                             double* __restrict__ d64, float* __restrict__ d32) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -310,6 +362,32 @@ static int pc_apply(exfem_solver_s* S, const T* r, T* z, const int* skip, cudaSt
     EX_LAUNCH_CHECK();
     return EXFEM_OK;
   }
+  if (S->pc == EXFEM_PC_CHEBY) {
+    T *x, *res, *d;
+    if constexpr (sizeof(T) == 8) {
+      x = S->cx64.p, res = S->cr64.p, d = S->cd64.p;
+    } else {
+      x = S->cx32.p, res = S->cr32.p, d = S->cd32.p;
+    }
+    T* Ad = z;  // z is free until the final sum: it holds A d meanwhile
+    const double hi = S->cheb_lmax, lo = hi / 30.0;
+    const double th = 0.5 * (hi + lo), de = 0.5 * (hi - lo), sg = th / de;
+    double rh = 1.0 / sg;
+    cheb_pc_init_kernel<T><<<eg, 256, 0, st>>>(n, sdinv<T>(S), r, x, res, d, (T)(1.0 / th), skip);
+    EX_LAUNCH_CHECK();
+    int s;
+    for (int j = 0; j < 6; ++j) {
+      if ((s = op_apply<T>(S, d, Ad, skip, st))) return s;
+      const double rn = 1.0 / (2.0 * sg - rh);
+      cheb_pc_step_kernel<T><<<eg, 256, 0, st>>>(n, sdinv<T>(S), Ad, x, res, d, (T)(rn * rh), (T)(2.0 * rn / de),
+                                                 skip);
+      EX_LAUNCH_CHECK();
+      rh = rn;
+    }
+    cheb_pc_out_kernel<T><<<eg, 256, 0, st>>>(n, x, d, z, skip);
+    EX_LAUNCH_CHECK();
+    return EXFEM_OK;
+  }
   const uint8_t* fixed = S->blk->fixed.p;
   const T* rin = r;
   if (fixed) {
@@ -347,6 +425,45 @@ static int pcg_iteration(exfem_solver_s* S, cudaStream_t st) {
   return EXFEM_OK;
 }
 
+static int norm64(exfem_solver_s* S, const double* v, double* out, cudaStream_t st);
+
+// Spectral bound of D^-1 A for the Chebyshev-Jacobi preconditioner: 25 power
+// iterations from the reference's start vector, times 1.1 (gfem/solvers.py:328-342),
+// with the solver's FP64 operator when it has one (the FP32 one otherwise)
+static int cheby_bound(exfem_solver_s* S, cudaStream_t st) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  double* v = S->cx64.p;
+  double* w = S->cr64.p;
+  int s;
+  cheb_start_kernel<<<eg, 256, 0, st>>>(n, S->blk->fixed.p, v);
+  EX_LAUNCH_CHECK();
+  double vn, wn, lam = 1.0;
+  if ((s = norm64(S, v, &vn, st))) return s;
+  for (int it = 0; it < 25; ++it) {
+    if (S->op == EXFEM_OP_MF_F32) {
+      convert_kernel<double, float><<<eg, 256, 0, st>>>(n, v, S->cx32.p, 1.0, nullptr);
+      EX_LAUNCH_CHECK();
+      if ((s = op_apply<float>(S, S->cx32.p, S->cr32.p, nullptr, st))) return s;
+      convert_kernel<float, double><<<eg, 256, 0, st>>>(n, S->cr32.p, w, 1.0, nullptr);
+      EX_LAUNCH_CHECK();
+    } else if ((s = op_apply<double>(S, v, w, nullptr, st))) {
+      return s;
+    }
+    cheb_scale_kernel<<<eg, 256, 0, st>>>(n, w, S->dinv64.p, w, 1.0);
+    EX_LAUNCH_CHECK();
+    if ((s = norm64(S, w, &wn, st))) return s;
+    lam = wn / vn;
+    if (!(wn > 0.0) || !std::isfinite(wn)) break;
+    cheb_scale_kernel<<<eg, 256, 0, st>>>(n, w, nullptr, v, 1.0 / wn);
+    EX_LAUNCH_CHECK();
+    vn = 1.0;
+  }
+  EX_ARG(std::isfinite(lam) && lam > 0.0, "Chebyshev bound: power iteration gave %g", lam);
+  S->cheb_lmax = 1.1 * lam;
+  return EXFEM_OK;
+}
+
 int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
   int s;
   const bool stored = S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64;
@@ -364,6 +481,7 @@ int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
   }
   dinv_kernel<<<grid_for(S->n, 256), 256, 0, st>>>(S->n, S->diag64.p, S->blk->fixed.p, S->dinv64.p, S->dinv32.p);
   EX_LAUNCH_CHECK();
+  if (S->pc == EXFEM_PC_CHEBY && (s = cheby_bound(S, st))) return s;
   S->diag_ready = true;
   S->diag_tan_gen = tan_gen_all(S);
   S->diag_bc_gen = bc_gen_all(S);
@@ -402,7 +520,7 @@ static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
         if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
       S->graph_bc_gen = bc_gen_all(S);
     }
-    if (S->gexec[gi] && S->g_Ke[gi] != keptr) {
+    if (S->gexec[gi] && (S->g_Ke[gi] != keptr || S->g_lmax[gi] != S->cheb_lmax)) {
       cudaGraphExecDestroy(S->gexec[gi]);
       S->gexec[gi] = nullptr;
     }
@@ -419,6 +537,7 @@ static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
       cudaGraphDestroy(g);
       EX_CUDA(ce);
       S->g_Ke[gi] = keptr;
+      S->g_lmax[gi] = S->cheb_lmax;
     }
   }
   return EXFEM_OK;
@@ -650,6 +769,14 @@ int solver_alloc(exfem_solver_s* S) {
   for (auto* v : v32)
     if ((s = v->alloc(std::max<int64_t>(n, 1)))) return s;
   if ((s = S->mb64.alloc(std::max<int64_t>(n, 1))) || (s = S->mb32.alloc(std::max<int64_t>(n, 1)))) return s;
+  if (S->pc == EXFEM_PC_CHEBY) {
+    DevBuf<double>* c64[] = {&S->cx64, &S->cr64, &S->cd64};
+    DevBuf<float>* c32[] = {&S->cx32, &S->cr32, &S->cd32};
+    for (auto* v : c64)
+      if ((s = v->alloc(std::max<int64_t>(n, 1)))) return s;
+    for (auto* v : c32)
+      if ((s = v->alloc(std::max<int64_t>(n, 1)))) return s;
+  }
   if ((s = S->partial.alloc(RED_MAX_BLOCKS))) return s;
   if ((s = S->dscr.alloc(4))) return s;
   if ((s = S->counter.alloc(1))) return s;

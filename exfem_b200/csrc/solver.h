@@ -101,6 +101,10 @@ struct exfem_solver_s {
   exfem::DevBuf<unsigned> counter;
   exfem::DevBuf<exfem::PcgScal> scal;
   exfem::PcgScal* h_scal = nullptr;  // pinned
+  exfem::DevBuf<double> cx64, cr64, cd64;  // EXFEM_PC_CHEBY work vectors
+  exfem::DevBuf<float> cx32, cr32, cd32;
+  double cheb_lmax = 0.0;                  // EXFEM_PC_CHEBY spectral bound of D^-1 A
+  double g_lmax[2] = {0.0, 0.0};           // the bound each captured graph was recorded with
   bool diag_ready = false;
   int mixed_mode = 1;  // exfem_solver_mixed: 1 = reliable updates, 0 = restarted refinement (the reference's)
   double mixed_delta = 0.1;  // reliable updates: replace the residual after this reduction

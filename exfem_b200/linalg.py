@@ -433,11 +433,12 @@ class NativeSolver:
 
     op: "ebe64" (stored Ke, FP64), "csr64" (the stored Ke assembled on the device
     into one FP64 CSR matrix, gfem/model.py:195-238), "mf64" (matrix-free FP64),
-    "mf32" (matrix-free FP32); pc: "none", "jacobi", "amg".  The stored-Ke operators
+    "mf32" (matrix-free FP32); pc: "none", "jacobi", "amg", "cheby" (Chebyshev-Jacobi
+    polynomial, gfem/solvers.py:289-306).  The stored-Ke operators
     take their element matrices from :meth:`set_ke` (one array per block)."""
 
     OPS = {"ebe64": _lib.OP_EBE_F64, "mf64": _lib.OP_MF_F64, "mf32": _lib.OP_MF_F32, "csr64": _lib.OP_CSR_F64}
-    PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG}
+    PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG, "cheby": _lib.PC_CHEBY}
 
     def __init__(self, block, op="mf32", pc="amg", amg=None, graph=True, chunk=8, mixed_mode="reliable",
                  mixed_delta=0.1):
@@ -474,6 +475,12 @@ class NativeSolver:
         self._Ke = [K.contiguous() for K in Kes]
         for i, K in enumerate(self._Ke):
             check(lib.exfem_solver_set_ke_block(self._h, i, ptr(K)))
+
+    def cheby_bound(self):
+        """The Chebyshev-Jacobi preconditioner's bound on the spectrum of D^-1 A."""
+        v = C.c_double()
+        check(lib.exfem_solver_cheby_bound(self._h, C.byref(v)))
+        return v.value
 
     def pcg(self, b, tol=1e-8, maxiter=2000):
         b = b.to(torch.float64).contiguous()

@@ -11,6 +11,9 @@
     "amg"     plain FP64 path: FP64 operator (stored Ke, or matrix-free with
               ``tangent="mf"``) + FP64 AMG V-cycle, PCG in the library;
     "jacobi"  FP64 operator + Jacobi PCG;
+    "cheby"   FP64 operator + the set-up-free Chebyshev-Jacobi polynomial
+              preconditioner (degree 6, bound by device power iteration,
+              gfem/solvers.py:289-306, 328-342);
     "mixed"   FP32 matrix-free operator + FP32 V-cycle (FP64 coarse solve)
               inside FP64 iterative refinement with an FP64 matrix-free residual
               (solvers.py:344-384);
@@ -18,7 +21,10 @@
   The hierarchy is built on the first solve of a step from the assembled FP64
   tangent, frozen across Newton iterations and increments, and rebuilt when the
   PCG iteration count exceeds 4x the first one (solvers.py:442-470); level 0 is
-  always smoothed with the current operator (solvers.py:311-314).
+  always smoothed with the current operator (solvers.py:311-314).  For "amg" on
+  models of at least ``async_amg`` DOFs (150000, the reference's threshold) the
+  hierarchy is set up in a background thread on its own CUDA stream while the
+  solves run Chebyshev-Jacobi PCG (solvers.py:445-464).
 * ``StaticSolver`` — gfem/solvers.py:481-683: automatic incrementation (x1.5
   growth after <= 5 iterations, x0.25 cutback), tangent predictor, Newton with
   the reference convergence test and a 4-step backtracking line search.
@@ -127,8 +133,11 @@ class _LinearSystem:                                                    # solver
     """Solves (free K free + fixed I) x = b with the chosen back-end."""
 
     def __init__(self, model, method="auto", tangent="ebe", cg_tol=1e-9, cg_maxiter=20000, monitor=None,
-                 graph=True, amg_setup="auto", mixed_mode="reliable", operator="gather"):
+                 graph=True, amg_setup="auto", mixed_mode="reliable", operator="gather", async_amg=150000):
         self.m = model
+        self.async_amg = async_amg              # DOFs from which "amg" sets up in the background (None: never)
+        self._amg_future = None
+        self._pool = None
         if operator not in ("gather", "csr"):
             raise ValueError(f"unknown operator {operator!r}")
         # stored-Ke operator of the "amg" / "jacobi" methods with tangent="ebe":
@@ -144,7 +153,7 @@ class _LinearSystem:                                                    # solver
         self.amg_setup = amg_setup
         if method == "auto":
             method = "direct" if model.ndof <= 20000 else "amg"
-        if method not in ("direct", "amg", "jacobi", "mixed"):
+        if method not in ("direct", "amg", "jacobi", "mixed", "cheby"):
             raise ValueError(f"unknown linear solver {method!r}")
         self.method = method
         self.tangent = "mf" if tangent in ("mf", "jvp") or method == "mixed" else "ebe"
@@ -160,6 +169,9 @@ class _LinearSystem:                                                    # solver
         self._solvers = {}
 
     def reset(self):
+        if self._amg_future is not None:                 # a background set-up of the previous step
+            self._amg_future.result()
+            self._amg_future = None
         self.amg = self.pinned_amg
         self.amg_iters0 = None
         # solvers over a pinned hierarchy stay (with their captured graphs and the FP32
@@ -204,6 +216,46 @@ class _LinearSystem:                                                    # solver
         self.last_setup_time = time.time() - t0
         self.mon.log(f"    {self.amg.info()}  setup {self.last_setup_time:.2f}s")
 
+    def _start_background_build(self, ops, setup, ctx):
+        """Set the hierarchy up in a worker thread on its own stream, from element
+        matrices evaluated now on the calling stream."""
+        import concurrent.futures as cf
+        Kes = [K for _, K in self._setup_ops(ops, ctx)]
+        ready = torch.cuda.Event()
+        ready.record()
+        device = torch.cuda.current_device()
+        where = "device" if self.amg_setup == "auto" else self.amg_setup
+        host_A = self.assemble(list(zip([b.dofs() for b in self.m.blocks], Kes)), setup) if where == "host" else None
+
+        def build():
+            t0 = time.time()
+            torch.cuda.set_device(device)
+            side = torch.cuda.Stream()
+            with torch.cuda.stream(side):
+                side.wait_event(ready)
+                amg = linalg.DeviceAMG(self.m.blocks, Kes) if host_A is None else linalg.AMG(host_A, self.m.X)
+            side.synchronize()
+            return amg, time.time() - t0
+
+        self._pool = self._pool or cf.ThreadPoolExecutor(1)
+        self._amg_future = self._pool.submit(build)
+        self.mon.log("    AMG set-up started in the background; Chebyshev-Jacobi PCG meanwhile")
+
+    def _collect_background_build(self):
+        fut = self._amg_future
+        if fut is not None and fut.done():
+            self._amg_future = None
+            self.amg, self.last_setup_time = fut.result()
+            self.amg_iters0 = None
+            self._solvers = {}
+            self.mon.log(f"    {self.amg.info()}  (set up in the background, {self.last_setup_time:.2f}s)")
+
+    def _pcg(self, ops, b, op, pc):
+        S = self._solver(op, pc)
+        if op in ("ebe64", "csr64"):
+            S.set_ke([K for _, K in ops])
+        return S.pcg(b, tol=self.cg_tol, maxiter=self.cg_maxiter)
+
     def solve(self, ops, b, setup, jvp_args=None, rebuild=False):
         """ops: [(dofs, Ke)] (tangent="ebe") or None with jvp_args = (u, states, fields)
         (tangent="mf"; the block's tangent data must be current)."""
@@ -215,7 +267,19 @@ class _LinearSystem:                                                    # solver
             x = linalg.Direct(A).solve(b.cpu().numpy())
             self.last_iters = 1
             return torch.as_tensor(x, device="cuda")
-        if self.method in ("amg", "mixed") and (self.amg is None or rebuild):
+        op = ("csr64" if self.operator == "csr" else "ebe64") if self.tangent == "ebe" else "mf64"
+        if self.method == "amg":
+            self._collect_background_build()
+            if (self.amg is None or rebuild) and self._amg_future is None:
+                if self.async_amg is not None and self.m.ndof >= self.async_amg:
+                    self._start_background_build(ops, setup, jvp_args)
+                else:
+                    self._build_amg(ops, setup, jvp_args)
+            if self.amg is None or (rebuild and self._amg_future is not None):
+                x, k, rr = self._pcg(ops, b, op, "cheby")
+                self.last_iters = k
+                return x
+        if self.method == "mixed" and (self.amg is None or rebuild):
             self._build_amg(ops, setup, jvp_args)
         if self.method == "mixed":
             S = self._solver("mf32", "amg")
@@ -224,12 +288,8 @@ class _LinearSystem:                                                    # solver
             if not np.isfinite(rel) or rel > max(self.cg_tol * 10, 1e-3):
                 self.mon.log(f"    warning: mixed refinement not converged ({k} it, {p} passes, rel.res {rel:.2e})")
             return x
-        op = ("csr64" if self.operator == "csr" else "ebe64") if self.tangent == "ebe" else "mf64"
-        pc = "jacobi" if self.method == "jacobi" else "amg"
-        S = self._solver(op, pc)
-        if op in ("ebe64", "csr64"):
-            S.set_ke([K for _, K in ops])
-        x, k, rr = S.pcg(b, tol=self.cg_tol, maxiter=self.cg_maxiter)
+        pc = self.method if self.method in ("jacobi", "cheby") else "amg"
+        x, k, rr = self._pcg(ops, b, op, pc)
         if pc == "amg":
             if self.amg_iters0 is None:
                 self.amg_iters0 = max(k, 5)
@@ -244,7 +304,7 @@ class _LinearSystem:                                                    # solver
 class StaticSolver:                                                     # solvers.py:481-683
     def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
                  cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None,
-                 amg_setup="auto", mixed_mode="reliable", operator="gather"):
+                 amg_setup="auto", mixed_mode="reliable", operator="gather", async_amg=150000):
         """``amg``: a prebuilt :class:`linalg.AMG` that every step starts from instead
         of assembling and setting up its own (the serving path keeps one resident
         per mesh); the rebuild rule still applies."""
@@ -252,7 +312,7 @@ class StaticSolver:                                                     # solver
         self.mon = monitor or Monitor(verbose)
         self.line_search = line_search
         self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph, amg_setup,
-                                 mixed_mode, operator)
+                                 mixed_mode, operator, async_amg)
         self.lin.pinned_amg = amg
         self.newton_iterations = 0
 

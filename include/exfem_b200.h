@@ -50,8 +50,10 @@ enum { EXFEM_F64 = 0, EXFEM_F32 = 1, EXFEM_BF16 = 2 };
 enum { EXFEM_ASSEMBLE_GATHER = 0, EXFEM_ASSEMBLE_COLOUR = 1 };
 /* linear-operator kinds of a solver */
 enum { EXFEM_OP_EBE_F64 = 0, EXFEM_OP_MF_F64 = 1, EXFEM_OP_MF_F32 = 2, EXFEM_OP_CSR_F64 = 3 };
-/* preconditioners of a solver */
-enum { EXFEM_PC_NONE = 0, EXFEM_PC_JACOBI = 1, EXFEM_PC_AMG = 2 };
+/* preconditioners of a solver; EXFEM_PC_CHEBY is the set-up-free Chebyshev-Jacobi
+ * polynomial of gfem/solvers.py:289-306 (degree 6 in D^-1 A over [lmax/30, lmax],
+ * lmax from 25 power iterations x 1.1, gfem/solvers.py:328-342) */
+enum { EXFEM_PC_NONE = 0, EXFEM_PC_JACOBI = 1, EXFEM_PC_AMG = 2, EXFEM_PC_CHEBY = 3 };
 
 #define EXFEM_MAX_TABLE 32
 
@@ -109,9 +111,11 @@ int exfem_block_colours(exfem_block b, int32_t* colour_host);
  * in a tile order (grouped by mesh component, in the order of each component's
  * first element, then along a Morton curve of the corner-coordinate sums, ties by
  * element index); a tile is `tile` consecutive positions of that order, and slot
- * s = a*tile + p is local node a of the element at tile position p.  tile_info: tile count, total length of the node lists and the
- * longest list; tile_maps, copied to host: ptr (ntile+1), the sorted distinct
- * nodes of every tile, for each listed node the end of its run of slots
+ * s = a*tile + p is local node a of the element at tile position p.  tile_info:
+ * tile count, total length of the node lists and the longest list; tile_maps,
+ * copied to host: ptr (ntile+1), the distinct nodes of every tile in the order of
+ * their shared-memory records (chosen against bank conflicts of the FP32 product,
+ * exfem_host_tile_maps), for each listed node the end of its run of slots
  * (uint16), and per tile the slots grouped by node in node order, increasing
  * within a node (ntile, nnode*tile, zero padded); tile_order: the tile size and
  * the order (ne,) as position -> element.  No counterpart in the reference. */
@@ -302,6 +306,9 @@ int exfem_solver_set_ke_block(exfem_solver s, int block, const double* Ke);
 /* Refresh the Jacobi / level-0 inverse diagonal from the current operator
  * (gfem/solvers.py:312-313 dinv0). Called automatically by the first solve. */
 int exfem_solver_refresh_diagonal(exfem_solver s, void* stream);
+/* EXFEM_PC_CHEBY: the spectral bound in use (refreshed with the diagonal, i.e. when
+ * the operator's tangent or prescribed DOFs change; 0 before the first solve). */
+int exfem_solver_cheby_bound(exfem_solver s, double* lmax);
 /* Use CUDA graphs for the PCG iteration loop (default on) and the number of
  * iterations captured per graph launch. */
 int exfem_solver_set_graph(exfem_solver s, int enable, int chunk);
@@ -384,6 +391,17 @@ int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const 
  * the second (both positively oriented), so the product loads and adds their six
  * shared nodes once.  No counterpart in the reference. */
 int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile);
+/* tile maps of the matrix-free product (see exfem_block_tile_maps) for a
+ * connectivity already in tile order, for a product thread layout of `lanes`
+ * elements per thread (2: C3D10 element pairs, partner = the local node of a
+ * pair's first element that may equal local node b of the second, or -1; NULL for
+ * none): per tile its distinct nodes in the bank-conflict-aware record order,
+ * nend and perm.  Call with ptr = NULL for ntile and nlist (the total list
+ * length), then with ptr (ntile+1), nodes (nlist), nend (nlist) and perm
+ * (ntile * nnode * tile).  No counterpart in the reference. */
+int exfem_host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int lanes,
+                         const int32_t* partner, int64_t* ntile, int64_t* nlist, int32_t* ptr, int32_t* nodes,
+                         uint16_t* nend, uint16_t* perm);
 /* boundary faces: keys (nface, 4) int64, each face's corner nodes sorted
  * ascending (triangles padded in front with -1); once[f] = 1 when no other face
  * has the same key, else 0.  The face matching of gfem/surfaces.py:182-221

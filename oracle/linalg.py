@@ -141,6 +141,37 @@ def vcycle(levels, L, b, lvl=0, A0=None, dinv0=None, deg=2):           # linalg.
     return cheb(Amv, dinv, lv["rho"], x, b, deg)
 
 
+def cheby_lmax(Amv, dinv, free, it=25):                               # solvers.py:328-342
+    """Bound of the spectrum of D^-1 A by power iteration: start sin(0.37 i + 0.1)
+    on the free DOFs plus 1e-3, 25 iterations, the last |w| / |v| times 1.1."""
+    n = len(dinv)
+    v = np.sin(np.arange(n) * 0.37 + 0.1) * free + 1e-3
+    lam = 1.0
+    for _ in range(it):
+        w = dinv * Amv(v)
+        lam = np.linalg.norm(w) / np.linalg.norm(v)
+        v = w / np.linalg.norm(w)
+    return 1.1 * lam
+
+
+def cheby_precond(Amv, dinv, lmax, r, deg=6):                          # solvers.py:289-306
+    """Chebyshev-Jacobi polynomial z = M(r) over [lmax/30, lmax], degree 6."""
+    lo, hi = lmax / 30.0, lmax
+    th, de = 0.5 * (hi + lo), 0.5 * (hi - lo)
+    sg = th / de
+    rh = 1.0 / sg
+    res = dinv * r
+    d = res / th
+    x = np.zeros_like(r)
+    for _ in range(deg):
+        x = x + d
+        res = res - dinv * Amv(d)
+        rn = 1.0 / (2 * sg - rh)
+        d = rn * rh * d + 2 * rn / de * res
+        rh = rn
+    return x + d
+
+
 def bc_matrix(A, free):                                                # linalg.py:213-217
     D = sp.diags(np.asarray(free, float))
     return (D @ A @ D + sp.diags(1.0 - np.asarray(free, float))).tocsr()

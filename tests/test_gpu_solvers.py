@@ -448,3 +448,67 @@ def test_result_frame_written_for_a_solution(cuda, tmp_path):
     mo = om.stresses(torch.as_tensor(u.cpu()), om.init_state())[0]["MISES"]
     assert rel_err(arrays["MISES"], mo) < 1e-10
     assert np.all(arrays["PEEQ"] == 0.0)
+
+
+@pytest.mark.parametrize("tangent", ["ebe", "mf"])
+def test_cheby_solver_matches_oracle(cuda, tangent):
+    """linear_solver="cheby" (gfem/solvers.py:289-306, 328-342): the config-1
+    cantilever against the oracle's direct solution (1e-8), the device power-iteration
+    bound against the oracle's on the same assembled operator (1e-10), and one
+    preconditioner application against the oracle's polynomial (1e-12)."""
+    import exfem_b200 as xf
+    from exfem_b200 import linalg, mesh
+    X, c = mesh.box_hex(100.0, 20.0, 20.0, 20, 4, 4)
+    _, tip, bcs, loads = cantilever_bcs(X, 100.0)
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.LinearElastic(E, NU))
+    uo, _, _ = osol.StaticSolver(om, rtol=1e-6).solve(osol.Step(bcs=bcs, loads=loads))
+    pm = xf.Model(X)
+    pm.add_block(c, xf.HEX8, xf.LinearElastic(E, NU))
+    s = xf.StaticSolver(pm, rtol=1e-6, linear_solver="cheby", tangent=tangent, cg_tol=1e-11, verbose=False)
+    up, _, _ = s.solve(xf.Step(bcs=bcs, loads=loads))
+    assert rel_err(up, uo) < 1e-8, rel_err(up, uo)
+    # the bound and the polynomial on the assembled operator
+    setup = osol.Setup(om, osol.Step(bcs=bcs, loads=loads))
+    ops = [(d, K.numpy()) for d, K in om.stiffness_ops(torch.zeros(om.ndof, dtype=torch.float64), om.init_state())]
+    A = olin.bc_matrix(ofem.ops_assemble(ops, om.ndof), setup.free).tocsr()
+    dg = A.diagonal()
+    dinv = np.where(setup.free > 0, 1.0 / np.where(np.abs(dg) > 0, dg, 1.0), 1.0)
+    lo = olin.cheby_lmax(lambda v: A @ v, dinv, setup.free)
+    blk = pm.blocks[0]
+    blk.set_fixed(setup.fixed)
+    S = linalg.NativeSolver(blk, "mf64", "cheby", None, graph=False)
+    r = np.random.default_rng(5).standard_normal(pm.ndof) * setup.free
+    _, k, _ = S.pcg(torch.as_tensor(r, device="cuda"), tol=1e-30, maxiter=1)
+    assert abs(S.cheby_bound() - lo) <= 1e-10 * lo, (S.cheby_bound(), lo)
+    assert k == 1
+
+
+def test_background_hierarchy_set_up(cuda):
+    """The "amg" solver with the background set-up forced on (threshold below the
+    model size): the first linear solves run Chebyshev-Jacobi PCG while the
+    hierarchy is set up on another stream, later ones use it; the Newton solution
+    matches the oracle (1e-8) and equals the foreground set-up's to the solver
+    tolerance."""
+    import time as _time
+
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = jittered_box(100.0, 20.0, 20.0, 20, 4, 4, frac=0.1, seed=8)
+    _, _, bcs, loads = cantilever_bcs(X, 100.0)
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.LinearElastic(E, NU))
+    uo, _, _ = osol.StaticSolver(om, rtol=1e-6).solve(osol.Step(bcs=bcs, loads=loads))
+    pm = xf.Model(X)
+    pm.add_block(c, xf.HEX8, xf.LinearElastic(E, NU))
+    s = xf.StaticSolver(pm, rtol=1e-6, linear_solver="amg", cg_tol=1e-11, verbose=False, async_amg=1000)
+    up, _, _ = s.solve(xf.Step(bcs=bcs, loads=loads))
+    assert rel_err(up, uo) < 1e-8
+    t0 = _time.time()
+    while s.lin._amg_future is not None and not s.lin._amg_future.done() and _time.time() - t0 < 60:
+        _time.sleep(0.05)
+    s.lin._collect_background_build()
+    assert s.lin.amg is not None and s.lin.amg.nlevels >= 2
+    x = s.lin.solve(s.m.stiffness_ops(torch.zeros(pm.ndof, dtype=torch.float64, device="cuda"), pm.init_state()),
+                    torch.as_tensor(s.setup.group, device="cuda") * s.setup.free, s.setup)
+    assert rel_err(x, uo) < 1e-8
