@@ -70,6 +70,7 @@ _SIGS = {
     "exfem_ebe_matvec_bf16_multi": ([VP, P, I32, P, P, I32, VP], C.c_int),
     "exfem_ebe_diagonal": ([VP, P, P, VP], C.c_int),
     "exfem_stresses": ([VP, P, P, P, P, P, VP], C.c_int),
+    "exfem_geometric_stiffness": ([VP, P, P, VP], C.c_int),
     "exfem_amg_create": ([C.POINTER(VP)], C.c_int),
     "exfem_amg_destroy": ([VP], C.c_int),
     "exfem_amg_add_level": ([VP, I64, I64, P, P, P, P, P, P, P, P, P, P, D], C.c_int),

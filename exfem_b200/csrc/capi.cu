@@ -538,6 +538,14 @@ int exfem_ebe_diagonal(exfem_block b, const double* Ke, double* diag, void* stre
   return launch_ebe_diagonal(b, Ke, diag, as_stream(stream));
 }
 
+int exfem_geometric_stiffness(exfem_block b, const double* S, double* Kg, void* stream) {
+  EX_ARG(b && (S || b->ne == 0) && (Kg || b->ne == 0), "NULL argument");
+  StreamGuard g;
+  int st;
+  if ((st = g.init(stream))) return st;
+  return launch_geo_stiffness(b, S, Kg, g.work);
+}
+
 int exfem_stresses(exfem_block b, const double* u, const double* state, double* S, double* mises, double* peeq,
                    void* stream) {
   EX_ARG(b && u, "NULL argument");

@@ -621,6 +621,70 @@ int launch_stiffness(exfem_block_s* b, const double* u, const double* st_old, in
   return EXFEM_OK;
 }
 
+// ---------------------------------------------------------------- initial-stress stiffness
+// K_sigma of an element under a constant Cauchy stress sigma (gfem/model.py:113-117
+// geo_stiff): k_ab = sum_g vol_g dN_a/dX . sigma . dN_b/dX with the plain
+// (not B-bar) shape-function gradients and vol_g = w_g det J, expanded as
+// K[3a+i, 3b+j] = k_ab delta_ij.  One thread per (element, node a) writes rows
+// 3a .. 3a+2.
+template <int ET>
+__global__ void __launch_bounds__(128)
+geo_stiffness_kernel(int64_t ne, const double* __restrict__ X, const int32_t* __restrict__ conn,
+                     const double* __restrict__ S, double* __restrict__ Kg) {
+  constexpr int NN = ElemTraits<ET>::nnode, NG = ElemTraits<ET>::ngp, ND = 3 * NN;
+  const double w = ET == EXFEM_C3D8 ? 1.0 : 1.0 / 24.0;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < ne * NN; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / NN;
+    const int a = (int)(t - e * NN);
+    const int32_t* ce = conn + e * NN;
+    double sg[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sg[k] = S[e * 9 + k];
+    double k_ab[NN];
+#pragma unroll
+    for (int b = 0; b < NN; ++b) k_ab[b] = 0.0;
+    for (int g = 0; g < NG; ++g) {
+      double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, iJ[9];
+      for (int c = 0; c < NN; ++c) {
+        const double* xc = X + 3 * (int64_t)ce[c];
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+          for (int i = 0; i < 3; ++i) J[3 * n + i] += xc[n] * elem_dN(ET, g, c, i);
+      }
+      const double vol = w * inv3(J, iJ);
+      double ga[3], sa[3];                                   // dN_a/dX and sigma . dN_a/dX
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        ga[j] = elem_dN(ET, g, a, 0) * iJ[j] + elem_dN(ET, g, a, 1) * iJ[3 + j] + elem_dN(ET, g, a, 2) * iJ[6 + j];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) sa[j] = ga[0] * sg[j] + ga[1] * sg[3 + j] + ga[2] * sg[6 + j];
+      for (int b = 0; b < NN; ++b) {
+        double gb[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          gb[j] = elem_dN(ET, g, b, 0) * iJ[j] + elem_dN(ET, g, b, 1) * iJ[3 + j] + elem_dN(ET, g, b, 2) * iJ[6 + j];
+        k_ab[b] += vol * (sa[0] * gb[0] + sa[1] * gb[1] + sa[2] * gb[2]);
+      }
+    }
+    double* K = Kg + e * (int64_t)ND * ND;
+    for (int i = 0; i < 3; ++i)
+      for (int b = 0; b < NN; ++b)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) K[(int64_t)(3 * a + i) * ND + 3 * b + j] = i == j ? k_ab[b] : 0.0;
+  }
+}
+
+int launch_geo_stiffness(exfem_block_s* b, const double* S, double* Kg, cudaStream_t s) {
+  if (b->ne == 0) return EXFEM_OK;
+  const int64_t work = b->ne * b->nnode;
+  const unsigned grid = (unsigned)std::min<int64_t>((work + 127) / 128, 1 << 20);
+  if (b->etype == EXFEM_C3D8) geo_stiffness_kernel<EXFEM_C3D8><<<grid, 128, 0, s>>>(b->ne, b->X.p, b->conn.p, S, Kg);
+  else geo_stiffness_kernel<EXFEM_C3D10><<<grid, 128, 0, s>>>(b->ne, b->X.p, b->conn.p, S, Kg);
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
 // ---------------------------------------------------------------- stored-Ke products
 // ys[e, r] = sum_j Ke[e, r, j] * (free*v)[dofs[e, j]]   (one thread per element row)
 __global__ void ebe_rows_kernel(int64_t ne, int nnode, const int32_t* __restrict__ conn,

@@ -97,6 +97,7 @@ int launch_colour_assemble(exfem_block_s* b, const double* fe, double* f, cudaSt
 int launch_ebe_matvec(exfem_block_s* b, const double* Ke, const double* v, double* y,
                       const int* skip, cudaStream_t s, bool bc = true);
 int launch_ebe_diagonal(exfem_block_s* b, const double* Ke, double* diag, cudaStream_t s);
+int launch_geo_stiffness(exfem_block_s* b, const double* S, double* Kg, cudaStream_t s);
 // matrix-free operator (matfree.cu)
 template <class T>
 int launch_mf_matvec(exfem_block_s* b, const T* v, T* y, const int* skip, cudaStream_t s, bool bc = true);

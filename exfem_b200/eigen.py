@@ -1,5 +1,11 @@
-"""Modal analysis by block LOBPCG on the device operators (drop-in for
-``gfem.eigen.lobpcg`` / ``modal_lobpcg``, gfem/eigen.py:32-124).
+"""Modal and buckling analysis by block LOBPCG on the device operators (drop-in for
+``gfem.eigen.lobpcg`` / ``modal_lobpcg`` / ``buckling_lobpcg``, gfem/eigen.py:32-151,
+and the linear buckling procedure of gfem/solvers.py:1074-1110).
+
+Buckling: K0 phi = -lambda KG phi through the smallest mu of KG phi = mu K0 phi
+(A = the initial-stress stiffness KG of the stresses of the linear response to the
+step's loads, element matrices from the library's geometric-stiffness kernel; B =
+the stiffness K0 at u = 0; T = a device V-cycle of K0), lambda = -1/mu.
 
 K phi = w^2 M phi for the smallest eigenvalues: A = the block's FP64 matrix-free
 tangent product (prescribed DOFs held at zero), B = the HRZ-lumped mass matrix
@@ -165,3 +171,66 @@ def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=Non
     X0 = torch.randn(nd, m, dtype=torch.float64, device="cuda", generator=g) * free[:, None]
     lam, V, it = lobpcg(A, B, T, X0, nmodes, tol=tol, maxiter=maxiter, log=log)
     return np.maximum(lam, 0.0), V.T.contiguous()
+
+
+def _ops_block(ops, free):
+    """(n, m) -> (n, m): V -> free * sum_b K_b (free * V) of stored element ops
+    [(dofs, Ke)] on their blocks, column by column (gfem/eigen.py:97-110)."""
+    def apply(V):
+        cols = []
+        for j in range(V.shape[1]):
+            v = (V[:, j] * free).contiguous()
+            y = None
+            for blk, K in ops:
+                t = blk.ebe_matvec(K, v, apply_bc=False)
+                y = t if y is None else y + t
+            cols.append(y * free)
+        return torch.stack(cols, 1)
+    return apply
+
+
+def buckling_lobpcg(model, K0ops, KGops, setup, nmodes, monitor=None, tol=1e-6, maxiter=500):
+    """Buckling loads of K0 phi = -lambda KG phi (gfem/eigen.py:137-151): the
+    smallest mu of KG phi = mu K0 phi by LOBPCG with A = KG, B = K0 and a device
+    AMG V-cycle of K0 as preconditioner; lambda = -1/mu for mu < 0 (infinity
+    otherwise).  K0ops, KGops: per block (Block, Ke) stored FP64 element matrices.
+    Returns (lambda (nmodes,), modes (nmodes, ndof))."""
+    from .solvers import Monitor
+    mon = monitor or Monitor(False)
+    free = setup.free
+    for blk in model.blocks:
+        blk.set_fixed(setup.fixed)
+    A = _ops_block(KGops, free)
+    B = _ops_block(K0ops, free)
+    amg = linalg.DeviceAMG([b for b, _ in K0ops], [K for _, K in K0ops], keep_level0=True)
+    mon.log(f"  buckling (device LOBPCG): {int(setup.free_np.sum())} free dofs, {amg.info()}")
+
+    def T(R):
+        return torch.stack([amg.vcycle(R[:, j].contiguous()) for j in range(R.shape[1])], 1) * free[:, None]
+
+    m = nmodes + max(4, nmodes // 2)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    X0 = torch.randn(model.ndof, m, dtype=torch.float64, device="cuda", generator=g) * free[:, None]
+    mu, V, it = lobpcg(A, B, T, X0, nmodes, tol=tol, maxiter=maxiter, log=mon.log)
+    lam = np.where(mu < 0, -1.0 / np.where(mu < 0, mu, -1.0), np.inf)
+    order = np.argsort(lam)
+    mon.log(f"  LOBPCG converged in {it} iterations")
+    return lam[order], V.T[order].contiguous()
+
+
+def buckling(model, step, nmodes, state=None, monitor=None, tol=1e-6, linear_solver="auto"):
+    """Linear (eigenvalue) buckling (gfem/solvers.py:1074-1110): the linear response
+    to the step's loads with its prescribed DOFs held at zero, the element stresses
+    of that response, K0 at u = 0 and the initial-stress stiffness KG, then
+    :func:`buckling_lobpcg`.  Returns (load factors (nmodes,), modes (nmodes, ndof))."""
+    from .solvers import Step, StaticSolver
+    base = Step("base", bcs=[(b[0], b[1], 0.0) for b in step.bcs], loads=step.loads, dloads=step.dloads)
+    solver = StaticSolver(model, linear_solver=linear_solver, cg_tol=1e-10, verbose=False)
+    u, states, _ = solver.solve(base, state=State(model))
+    stress = model.stresses(u, states)
+    zero = torch.zeros(model.ndof, dtype=torch.float64, device="cuda")
+    K0ops = [(b, b.stiffness(zero, b.init_state())) for b in model.blocks]
+    KGops = [(b, b.geometric_stiffness(st["S"])) for b, st in zip(model.blocks, stress)]
+    setup = _Setup(model, base, state or State(model))
+    return buckling_lobpcg(model, K0ops, KGops, setup, nmodes, monitor, tol)
+

@@ -257,6 +257,15 @@ class Block:
         check(lib.exfem_ebe_diagonal(self.handle, ptr(Ke.contiguous()), ptr(d), stream_ptr()))
         return d
 
+    def geometric_stiffness(self, S):
+        """Initial-stress stiffness of every element under its Cauchy stress S
+        (ne, 3, 3) (gfem/model.py:113-117): Kg (ne, nd, nd) FP64."""
+        S = _dev(S).reshape(self.ne, 3, 3).contiguous()
+        nd = self.etype.nd
+        Kg = torch.empty((self.ne, nd, nd), dtype=torch.float64, device="cuda")
+        check(lib.exfem_geometric_stiffness(self.handle, ptr(S), ptr(Kg), stream_ptr()))
+        return Kg
+
     def cauchy(self, u, state):
         S = torch.empty((self.ne, 3, 3), dtype=torch.float64, device="cuda")
         mises = torch.empty(self.ne, dtype=torch.float64, device="cuda")
@@ -426,6 +435,11 @@ class Model:
             S, mises, peeq = b.cauchy(u, s)
             out.append(dict(S=S, MISES=mises, PEEQ=peeq))
         return out
+
+    def geometric_ops(self, stresses, u=None, states=None):
+        """Initial-stress stiffness ops [(dofs, Kg)] of the solid blocks from their
+        element stresses (``stresses()[b]["S"]``; gfem/model.py:541-553)."""
+        return [(b.dofs(), b.geometric_stiffness(st["S"])) for b, st in zip(self.blocks, stresses)]
 
     def summary(self):
         lines = [f"{self.nn} nodes, {self.nelem} elements, {self.ndof} dofs"]

@@ -183,6 +183,11 @@ int exfem_ebe_matvec_bf16_multi(exfem_block b, const void* Ke_bf16, int nrhs, co
                                 int apply_bc, void* stream);
 /* Diagonal of stored Ke (gfem/model.py:169-173 ops_diagonal), FP64 (ndof). */
 int exfem_ebe_diagonal(exfem_block b, const double* Ke, double* diag, void* stream);
+/* Initial-stress (geometric) stiffness of every element under its constant
+ * Cauchy stress S (ne, 3, 3) FP64 (gfem/model.py:113-117 geo_stiff, 541-553
+ * geometric_ops, with the stresses of Model.stresses): Kg (ne, 3 nnode, 3 nnode)
+ * FP64 row-major, K[3a+i, 3b+j] = delta_ij sum_g vol_g dN_a/dX . S . dN_b/dX. */
+int exfem_geometric_stiffness(exfem_block b, const double* S, double* Kg, void* stream);
 /* Volume-averaged Cauchy stress (ne, 3, 3), von Mises (ne) and PEEQ (ne)
  * (gfem/model.py:530-539 Model.stresses over Block.cauchy 129-137). */
 int exfem_stresses(exfem_block b, const double* u, const double* state, double* S,

@@ -295,8 +295,15 @@ class Block:
             return (torch.einsum("g,gij->ij", wv, P), torch.einsum("g,g->", wv, mat.eqps(snew)),
                     torch.einsum("g,gij->ij", wv, F))
 
+        def geo_stiff(Xe, sig):                                        # model.py:113-117
+            dNdX, vol = geom(Xe)
+            k = torch.einsum("gai,ij,gbj,g->ab", dNdX, sig, dNdX, vol)
+            n = k.shape[0]
+            return torch.einsum("ab,ij->aibj", k, I3).reshape(n * 3, n * 3)
+
         self._geom, self._defgrad = geom, defgrad
         self._force, self._stiff, self._cauchy = vmap(force), vmap(stiff), vmap(cauchy)
+        self._geo_stiff = vmap(geo_stiff)
 
     def _chunks(self, fn, *args):
         outs = []
@@ -314,6 +321,9 @@ class Block:
 
     def cauchy(self, Xe, ue, se, scv):
         return self._chunks(self._cauchy, Xe, ue, se, scv)
+
+    def geo_stiff(self, Xe, sig):
+        return self._chunks(self._geo_stiff, Xe, sig)
 
     def init_state(self):                                              # model.py:154-155
         return torch.zeros((self.ne, self.etype.ngp, self.material.nstate), dtype=DT)
@@ -697,6 +707,9 @@ class Model:
     def tangent_jvp(self, u, states, v, scale=None):                   # model.py:488-490
         u = torch.as_tensor(u)
         return jvp(lambda x: self.internal_force(x, states, scale)[0], (u,), (torch.as_tensor(v),))[1]
+
+    def geometric_ops(self, stresses):                                 # model.py:541-553
+        return [(b.dofs(), b.geo_stiff(self.X[b.conn], st["S"])) for b, st in zip(self.blocks, stresses)]
 
     def stresses(self, u, states, scale=None):                         # model.py:530-539
         U = torch.as_tensor(u).reshape(-1, 3)

@@ -512,3 +512,65 @@ def test_background_hierarchy_set_up(cuda):
     x = s.lin.solve(s.m.stiffness_ops(torch.zeros(pm.ndof, dtype=torch.float64, device="cuda"), pm.init_state()),
                     torch.as_tensor(s.setup.group, device="cuda") * s.setup.free, s.setup)
     assert rel_err(x, uo) < 1e-8
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_geometric_stiffness_matches_oracle(cuda, kind):
+    """Initial-stress stiffness of every element under a random symmetric Cauchy
+    stress (gfem/model.py:113-117) against the oracle's: 1e-12 relative."""
+    import exfem_b200 as xf
+    X, c = jittered_box(2.0, 1.0, 1.0, 3, 2, 2, frac=0.1, seed=9)
+    et, oet = xf.HEX8, ofem.HEX8
+    if kind == "tet":
+        X, c = tet10_box(2.0, 1.0, 1.0, 3, 2, 2, frac=0.1, seed=9)
+        et, oet = xf.TET10, ofem.TET10
+    S = np.random.default_rng(3).standard_normal((len(c), 3, 3))
+    S = S + S.transpose(0, 2, 1)
+    pm = xf.Model(X)
+    pm.add_block(c, et, xf.LinearElastic(E, NU))
+    om = ofem.Model(X)
+    om.add_block(c, oet, ofem.LinearElastic(E, NU))
+    kp = pm.geometric_ops([dict(S=torch.as_tensor(S, device="cuda"))])[0][1]
+    ko = om.geometric_ops([dict(S=torch.as_tensor(S))])[0][1]
+    assert rel_err(kp, ko) < 1e-12, rel_err(kp, ko)
+
+
+def test_buckling_matches_oracle(cuda):
+    """Linear buckling of a clamped slender column under a unit compressive tip load
+    (gfem/solvers.py:1074-1110 with the device LOBPCG of gfem/eigen.py:137-151):
+    the two lowest load factors (the square section buckles alike in y and z)
+    against the oracle's: base response by a direct solve, element stresses,
+    K0 and KG from the oracle's element matrices, and SciPy's Lanczos on
+    -KG phi = mu K0 phi (the reference's small-model path): 1e-6 relative."""
+    import scipy.sparse.linalg as spla
+
+    import exfem_b200 as xf
+    from exfem_b200 import eigen, mesh
+    L = 20.0
+    X, c = mesh.box_hex(L, 1.0, 1.0, 20, 2, 2)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > L - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)]
+    loads = [(tip, 0, -1.0 / len(tip))]
+    pm = xf.Model(X)
+    pm.add_block(c, xf.HEX8, xf.LinearElastic(E, NU))
+    lam, modes = eigen.buckling(pm, xf.Step(bcs=bcs, loads=loads), 2, tol=1e-9)
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.LinearElastic(E, NU))
+    uo, so, _ = osol.StaticSolver(om, rtol=1e-9).solve(osol.Step(bcs=bcs, loads=loads))
+    stress = om.stresses(torch.as_tensor(uo), so)
+    zero = torch.zeros(om.ndof, dtype=torch.float64)
+    K0 = ofem.ops_assemble([(d, K.numpy()) for d, K in om.stiffness_ops(zero, om.init_state())], om.ndof).tocsr()
+    KG = ofem.ops_assemble([(d, K.numpy()) for d, K in om.geometric_ops(stress)], om.ndof).tocsr()
+    setup = osol.Setup(om, osol.Step(bcs=bcs))
+    free = np.nonzero(setup.free > 0)[0]
+    K0f, KGf = K0[free][:, free].tocsc(), KG[free][:, free].tocsc()
+    lu = spla.splu(K0f)
+    mu = spla.eigsh(-KGf, k=4, M=K0f, Minv=spla.LinearOperator(K0f.shape, matvec=lu.solve), which="LA",
+                    return_eigenvectors=False)
+    ref = np.sort(1.0 / mu[mu > 0])[:2]
+    np.testing.assert_allclose(lam[:2], ref, rtol=1e-6)
+    # Euler's clamped-free column, P_cr = pi^2 E I / (4 L^2): the coarse trilinear
+    # mesh (two elements through the section) is stiffer in bending, not wrong by more
+    euler = np.pi ** 2 * E * (1.0 / 12) / (4 * L * L)
+    assert euler < lam[0] < 1.5 * euler, (lam[0], euler)
