@@ -665,27 +665,27 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     __syncthreads();
     // node sums back to T: a node listed by this tile only goes to y directly
     // (prescribed DOFs take v), the others' sums are stored (not added) at their
-    // partials positions; the accumulators are cleared for the next tile.  One
-    // lane per (node, component): the three lanes of a node are adjacent, so a
-    // warp's stores of neighbouring nodes (runs of consecutive ids in the sorted
-    // list) share sectors.  No barrier closes the phase: the next tile's first
-    // shared-memory writes (its atomics, its destinations buffer) come after its
-    // own barriers, which every thread reaches only after finishing this loop.
+    // partials positions; the accumulators are cleared for the next tile
     const int32_t* td = tdb + s * mu;
     const T nan = std::numeric_limits<T>::quiet_NaN();
-    for (int j = tid; j < 3 * nu; j += NT) {
-      const int k = j / 3, c = j - 3 * k;
-      I* a = sums(k) + c;
-      const T r = bad ? nan : from_fixed(*a, T(0)) * iq;
-      *a = I(0);
+    for (int k = tid; k < nu; k += NT) {
+      I* a = sums(k);
+      T r[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        r[c] = bad ? nan : from_fixed(a[c], T(0)) * iq;
+        a[c] = I(0);
+      }
       const int32_t d = td[k];
       if (d < 0) {
-        const int64_t q = 3 * (int64_t)(d & 0x0FFFFFFF) + c;
-        y[q] = (((uint32_t)d >> (28 + c)) & 1u) ? v[q] : r;
+        const int64_t n3 = 3 * (int64_t)(d & 0x0FFFFFFF);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) y[n3 + c] = (((uint32_t)d >> (28 + c)) & 1u) ? v[n3 + c] : r[c];
       } else {
-        part[4 * (int64_t)d + c] = r;
+        reinterpret_cast<Node4<T>*>(part)[d] = Node4<T>{r[0], r[1], r[2], T(0)};   // one 16-byte entry
       }
     }
+    __syncthreads();
   }
   cp_async_wait<0>();
 }

@@ -156,7 +156,7 @@ def test_noalloc_vcycle_refuses_level0_without_matrix(cuda):
     output untouched), as exfem_amg_vcycle refuses it; with the block it runs."""
     from exfem_b200 import _lib
     m, fixed, amg = _device_hierarchy(keep_level0=False)
-    assert amg.nnz[0] == 0
+    assert amg._export(0, 0)[0].nnz == 0                 # level 0 stores no matrix
     r = torch.ones(m.ndof, dtype=torch.float64, device="cuda")
     z = torch.full_like(r, 7.0)
     torch.cuda.synchronize()
