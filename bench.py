@@ -491,10 +491,18 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), 
                 if dt > 0:
                     time.sleep(dt)
                 futs.append(srv.submit(q))
+            # the window closes when the stream ends: requests not yet started are
+            # withdrawn (the backlog of a saturated server), those running finish
+            dt = tstart + duration - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            withdrawn = srv.cancel_pending()
             for f in futs:
-                f.result()
+                if not f.cancelled():
+                    f.result()
             st = serve.latency_stats(list(srv.completed))
             st["offered_per_s"] = float(len(arrivals) / duration)
+            st["withdrawn_at_window_end"] = withdrawn
             st["j2_requests"] = int(sum(q.spec.j2 for q in reqs))
             out["rates"][str(int(rate))] = st
         # serial plain FP64 solves of a sample of requests (hierarchies prebuilt)
@@ -723,11 +731,17 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e_ms = float(t.item())
 
-    solve = scale_res = j2 = None
+    tile_used = blk.tile_order()[0]
+    solve = scale_res = j2 = served = batched = None
     if rank == 0 and not args.no_solve:
         scale_res = scale_solve_section(m, X, scale)
         solve = solve_section()
         j2 = j2_section()
+    if rank == 0 and world == 1 and not args.no_solve:
+        del blk, m
+        torch.cuda.empty_cache()
+        batched = batch_section()
+        served = serve_section(rates=(50.0,), duration=60.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cv, ci = cpu_baseline()
@@ -746,7 +760,7 @@ def main():
         ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
         data="synthetic",
         config=dict(workload=WORKLOAD, ne=ne, nodes=nn, ndof=ndof, parallelism=f"replicas x{world}",
-                    l2="per-step stream 600 MB > 126 MB L2, no flush", seed=0, tile=blk.tile_order()[0],
+                    l2="per-step stream 600 MB > 126 MB L2, no flush", seed=0, tile=tile_used,
                     autotune=tuned),
         e2e=dict(value=world * ndof / (e_ms * 1e-3), unit=UNIT, h2d_bytes_per_step=4 * ndof,
                  d2h_bytes_per_step=4 * ndof, ms_per_step=e_ms,
@@ -755,7 +769,8 @@ def main():
         roofline=dict(bound="hbm", achieved=achieved, peak=pk, unit="GB/s", frac=achieved / pk,
                       traffic=TRAFFIC_BYTES, peak_source=f"{pk_src} (MEASURED_PEAKS.json hbm_gbs)",
                       algorithmic_bytes_per_step=alg_bytes),
-        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve, scale_solve=scale_res, j2_newton=j2)
+        cpu_baseline=cpu, clocks=clocks, gpu_launches=2 * args.steps, solve=solve, scale_solve=scale_res, j2_newton=j2,
+        batch=batched, serve=served)
     print(json.dumps(line), flush=True)
 
 

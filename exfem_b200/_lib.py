@@ -20,6 +20,7 @@ F64, F32, BF16 = 0, 1, 2
 ASSEMBLE_GATHER, ASSEMBLE_COLOUR = 0, 1
 OP_EBE_F64, OP_MF_F64, OP_MF_F32, OP_CSR_F64 = 0, 1, 2, 3
 PC_NONE, PC_JACOBI, PC_AMG, PC_CHEBY = 0, 1, 2, 3
+REQ_PENDING, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 MAX_TABLE = 32
 
 
@@ -113,6 +114,13 @@ _SIGS = {
     "exfem_solver_set_mixed_mode": ([VP, I32, D], C.c_int),
     "exfem_selftest_bounded_wait": ([I32, VP], C.c_int),
     "exfem_block_tile_conn": ([VP, P], C.c_int),
+    "exfem_queue_create": ([I32, C.POINTER(VP)], C.c_int),
+    "exfem_queue_destroy": ([VP], C.c_int),
+    "exfem_queue_submit": ([VP, VP, P, D, C.POINTER(I64)], C.c_int),
+    "exfem_queue_poll": ([VP, I64, C.POINTER(I32), C.POINTER(I32), C.POINTER(D)], C.c_int),
+    "exfem_queue_wait": ([VP, I64, D, C.POINTER(I32)], C.c_int),
+    "exfem_queue_result": ([VP, I64, P, C.POINTER(I32), C.POINTER(I32), C.POINTER(D)], C.c_int),
+    "exfem_queue_cancel": ([VP, I64, C.POINTER(I32)], C.c_int),
 }
 for _name, (_args, _res) in _SIGS.items():
     _f = getattr(lib, _name)

@@ -89,6 +89,104 @@ static int spmv_lanes(const Csr64& A, const T* val, const T* x, T* y, const T* b
   return EXFEM_OK;
 }
 
+// Block-sparse product with the same fused modes as spmv_kernel: L lanes per block
+// row stride over its blocks (consecutive blocks are contiguous in memory, so a
+// group's loads coalesce), each lane keeps the R row sums of its blocks, and the
+// group reduces them in a fixed order; lane 0 finishes the R rows.
+template <class T, int R, int C, int L, int MODE>
+__global__ void __launch_bounds__(256)
+bsr_kernel(int64_t nb, const int64_t* __restrict__ ptr, const int32_t* __restrict__ idx, const T* __restrict__ val,
+           const T* __restrict__ x, T* __restrict__ y, const T* __restrict__ b, const T* __restrict__ dinv,
+           T* __restrict__ d2, T* __restrict__ xo, T c1, T c2, const int* __restrict__ skip) {
+  if (skip && *skip) return;
+  constexpr int GPW = 32 / L;
+  const int lane = threadIdx.x & (L - 1);
+  const int grp = (threadIdx.x & 31) / L;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = warp * GPW; base < nb; base += nwarps * GPW) {
+    const int64_t br = base + grp;
+    T acc[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) acc[i] = T(0);
+    if (br < nb) {
+      const int64_t k1 = ptr[br + 1];
+      for (int64_t k = ptr[br] + lane; k < k1; k += L) {
+        const T* v = val + k * (R * C);
+        const T* xx = x + (int64_t)idx[k] * C;
+        T xv[C];
+#pragma unroll
+        for (int j = 0; j < C; ++j) xv[j] = xx[j];
+#pragma unroll
+        for (int i = 0; i < R; ++i)
+#pragma unroll
+          for (int j = 0; j < C; ++j) acc[i] += v[i * C + j] * xv[j];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i)
+#pragma unroll
+      for (int o = L / 2; o > 0; o >>= 1) acc[i] += __shfl_down_sync(0xffffffffu, acc[i], o, L);
+    if (br < nb && lane == 0) {
+#pragma unroll
+      for (int i = 0; i < R; ++i) {
+        const int64_t row = br * R + i;
+        const T sv = acc[i];
+        if (MODE == SP_SET) {
+          y[row] = sv;
+        } else if (MODE == SP_ADD) {
+          y[row] += sv;
+        } else if (MODE == SP_RES) {
+          y[row] = b[row] - sv;
+        } else if (MODE == SP_RESINIT) {
+          const T r = dinv[row] * (b[row] - sv);
+          y[row] = r;
+          d2[row] = r * c1;
+        } else {  // SP_CHEB: x is the direction d
+          const T d = x[row];
+          xo[row] += d;
+          const T r = y[row] - dinv[row] * sv;
+          y[row] = r;
+          d2[row] = c1 * d + c2 * r;
+        }
+      }
+    }
+  }
+}
+
+template <class T, int R, int C, int MODE>
+static void bsr_launch(const Bsr& M, const T* val, const T* x, T* y, const T* b, const T* dinv, T* d2, T* xo, T c1,
+                       T c2, const int* skip, cudaStream_t s) {
+  const double avg = M.nb ? (double)M.nnzb / (double)M.nb : 0.0;
+  const int threads = 256;
+  const unsigned grid = grid_for((size_t)((M.nb + 7) / 8) * 32, threads, 148u * 24u);
+#define EXF_BSR(L) bsr_kernel<T, R, C, L, MODE><<<grid, threads, 0, s>>>(M.nb, M.ptr.p, M.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, skip)
+  if (avg <= 2) EXF_BSR(1);
+  else if (avg <= 6) EXF_BSR(4);
+  else if (avg <= 16) EXF_BSR(8);
+  else if (avg <= 40) EXF_BSR(16);
+  else EXF_BSR(32);
+#undef EXF_BSR
+}
+
+template <class T, int MODE>
+static int bsr_apply(const Bsr& M, const T* x, T* y, const T* b, const T* dinv, T* d2, T* xo, T c1, T c2,
+                     const int* skip, cudaStream_t s) {
+  const T* val;
+  if constexpr (sizeof(T) == 8) val = M.v64.p;
+  else val = M.v32.p;
+  if (M.R == 3 && M.C == 6) bsr_launch<T, 3, 6, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else if (M.R == 6 && M.C == 3) bsr_launch<T, 6, 3, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else if (M.R == 6 && M.C == 6) bsr_launch<T, 6, 6, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else if (M.R == 3 && M.C == 3) bsr_launch<T, 3, 3, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else {
+    set_error("no block-sparse product for %d x %d blocks", M.R, M.C);
+    return EXFEM_ERR_UNSUPPORTED;
+  }
+  EX_LAUNCH_CHECK();
+  return EXFEM_OK;
+}
+
 template <class T>
 static const T* csr_vals(const Csr64& A);
 template <> const double* csr_vals<double>(const Csr64& A) { return A.v64.p; }
@@ -243,6 +341,11 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
   }
   const T* dinv = (l == 0 && op0 && op0->dinv) ? op0->dinv : lvdinv<T>(L);
   const T* rc = lvcoef<T>(L);  // per-row Chebyshev coefficients (union of independent hierarchies)
+  // block-sparse forms where the device set-up kept them (never with per-row
+  // coefficients or replicated levels, whose scalar rows are remapped)
+  const bool blocks_ok = !rc && !h->replicated;
+  const bool useA = blocks_ok && L.bA.on();
+  const bool useT = blocks_ok && L.bP.on() && L.bR.on();
   const int64_t n = L.n;
   T* r = lvbuf<T>(L, AmgLevel::WR);
   T* d = lvbuf<T>(L, AmgLevel::WD);
@@ -273,9 +376,12 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
                                                  rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr);
         EX_LAUNCH_CHECK();
       } else {
-        if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s,
-                                         rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr)))
+        if (useA) {
+          if ((st = bsr_apply<T, SP_CHEB>(L.bA, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s))) return st;
+        } else if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s,
+                                                rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr))) {
           return st;
+        }
       }
       std::swap(d, d2);
     }
@@ -293,7 +399,11 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
     sub_kernel<T><<<eg, 256, 0, s>>>(n, b, t, skip);
     EX_LAUNCH_CHECK();
   } else {
-    if ((st = spmv_lanes<T, SP_RES>(L.A, vals, x, t, b, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+    if (useA) {
+      if ((st = bsr_apply<T, SP_RES>(L.bA, x, t, b, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+    } else if ((st = spmv_lanes<T, SP_RES>(L.A, vals, x, t, b, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) {
+      return st;
+    }
   }
   T* bc;
   T* xc;
@@ -305,18 +415,31 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
     if constexpr (sizeof(T) == 8) { bc = (T*)h->cb64.p; xc = (T*)h->cx64.p; }
     else { bc = (T*)h->cb32.p; xc = (T*)h->cx32.p; }
   }
-  if ((st = spmv_lanes<T, SP_SET>(L.R, csr_vals<T>(L.R), t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  if (useT) {
+    if ((st = bsr_apply<T, SP_SET>(L.bR, t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  } else if ((st = spmv_lanes<T, SP_SET>(L.R, csr_vals<T>(L.R), t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0),
+                                         skip, s))) {
+    return st;
+  }
   if ((st = vcycle_level<T>(h, l + 1, bc, xc, nullptr, skip, s))) return st;
-  if ((st = spmv_lanes<T, SP_ADD>(L.P, csr_vals<T>(L.P), xc, x, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  if (useT) {
+    if ((st = bsr_apply<T, SP_ADD>(L.bP, xc, x, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+  } else if ((st = spmv_lanes<T, SP_ADD>(L.P, csr_vals<T>(L.P), xc, x, nullptr, nullptr, nullptr, nullptr, T(0), T(0),
+                                         skip, s))) {
+    return st;
+  }
   // post-smoothing from the corrected x
   if (mf) {
     if ((st = op0->apply(op0->ctx, x, t, skip, s))) return st;
     resinit_kernel<T><<<eg, 256, 0, s>>>(n, b, t, dinv, r, d, ith, skip, rc ? rc + 4 : nullptr);
     EX_LAUNCH_CHECK();
   } else {
-    if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), skip, s,
-                                        rc ? rc + 4 : nullptr)))
+    if (useA) {
+      if ((st = bsr_apply<T, SP_RESINIT>(L.bA, x, r, b, dinv, d, nullptr, ith, T(0), skip, s))) return st;
+    } else if ((st = spmv_lanes<T, SP_RESINIT>(L.A, vals, x, r, b, dinv, d, nullptr, ith, T(0), skip, s,
+                                               rc ? rc + 4 : nullptr))) {
       return st;
+    }
   }
   return smooth_steps();
 }

@@ -466,9 +466,11 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     int32_t u0, nu;
     uint32_t pk[GK];
   };
-  auto load_ids = [&](int64_t t, Ids& d) {
-    d.u0 = tptr[t];
-    d.nu = tptr[t + 1] - d.u0;
+  // (the list bounds come from registers loaded one tile earlier, so the id loads
+  // never wait on a dependent load of tptr)
+  auto load_ids = [&](int32_t u0, int32_t u1, Ids& d) {
+    d.u0 = u0;
+    d.nu = u1 - u0;
 #pragma unroll
     for (int i = 0; i < GK; ++i) {
       const int k = tid + i * NT;
@@ -507,11 +509,17 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
   Ids cur, nxt;
   cur.nu = nxt.nu = 0;
   if ((int64_t)blockIdx.x < ntile) {
-    load_ids(blockIdx.x, cur);
+    load_ids(tptr[blockIdx.x], tptr[blockIdx.x + 1], cur);
     copies(cur, 0);
   }
   cp_async_commit();
-  if ((int64_t)blockIdx.x + gridDim.x < ntile) load_ids(blockIdx.x + gridDim.x, nxt);
+  if ((int64_t)blockIdx.x + gridDim.x < ntile)
+    load_ids(tptr[blockIdx.x + gridDim.x], tptr[blockIdx.x + gridDim.x + 1], nxt);
+  int32_t pu0 = 0, pu1 = 0;                                           // list bounds three tiles ahead
+  if ((int64_t)blockIdx.x + 2 * (int64_t)gridDim.x < ntile) {
+    pu0 = tptr[blockIdx.x + 2 * (int64_t)gridDim.x];
+    pu1 = tptr[blockIdx.x + 2 * (int64_t)gridDim.x + 1];
+  }
   int it = 0;
   for (int64_t t = blockIdx.x; t < ntile; t += gridDim.x, ++it) {
     const int s = it & 1;
@@ -618,7 +626,11 @@ mf_tile_kernel(int64_t ne, int64_t ntile, const T* __restrict__ geo, const uint1
     if (tn < ntile) copies(nxt, s ^ 1);
     cp_async_commit();
     cur = nxt;
-    if (tn + gridDim.x < ntile) load_ids(tn + gridDim.x, nxt);
+    if (tn + gridDim.x < ntile) load_ids(pu0, pu1, nxt);
+    if (tn + 2 * (int64_t)gridDim.x < ntile) {
+      pu0 = tptr[tn + 2 * (int64_t)gridDim.x];
+      pu1 = tptr[tn + 2 * (int64_t)gridDim.x + 1];
+    }
     const bool bad = !(M <= std::numeric_limits<T>::max());            // NaN or infinity in the tile
     int e = 0;
     if (!bad && M > T(0)) {

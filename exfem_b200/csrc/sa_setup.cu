@@ -284,6 +284,27 @@ __global__ void sa_expand_kernel(int64_t nbr, int R, int C, const int64_t* __res
 
 // R = P^T as scalar CSR: row g*K + k lists, for the fine nodes n holding g
 // (increasing), the BS DOFs of n with P[n, g][r][k]
+// FP32 copy of FP64 values
+__global__ void sa_to_f32_kernel(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// blocks of R = P^T in block form: block q of aggregate row a is the transpose of
+// P's block tslot[q] (BS x K -> K x BS), FP64 and FP32
+__global__ void sa_transpose_blocks_kernel(int64_t nq, int BS, int K, const int32_t* __restrict__ tslot,
+                                           const double* __restrict__ P, double* __restrict__ r64,
+                                           float* __restrict__ r32) {
+  const int E = BS * K;
+  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nq * E; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = t / E;
+    const int e = (int)(t - q * E), i = e / BS, j = e - i * BS;   // entry (i, j) of the K x BS block
+    const double v = P[(int64_t)tslot[q] * E + j * K + i];
+    r64[t] = v;
+    r32[t] = (float)v;
+  }
+}
+
 __global__ void sa_expand_rt_kernel(int64_t nagg, int BS, int K, const int64_t* __restrict__ tptr,
                                     const int32_t* __restrict__ tidx, const int32_t* __restrict__ tslot,
                                     const int64_t* __restrict__ pptr, const double* __restrict__ P,
@@ -505,6 +526,30 @@ int coarsen(const BlockOp& A, const DevBuf<int32_t>& dagg, const DevBuf<double>&
     sa_expand_rt_kernel<<<sa_grid(R.n, 256), 256, 0, s>>>(nagg, BS, K, tptr.p, tidx.p, tslot.p, pptr.p, P.p, R.ptr.p,
                                                            R.idx.p, R.v64.p, R.v32.p);
     EX_LAUNCH_CHECK();
+  }
+  // the same P and R in block form for the V-cycle (one index per block)
+  {
+    const int64_t nq = (int64_t)Pp.idx.size();
+    Bsr& bp = L.bP;
+    bp.R = BS, bp.C = K, bp.nb = A.nb, bp.nnzb = nq;
+    if ((st = bp.v32.alloc(std::max<int64_t>(nq * E, 1))) || (st = L.bR.v64.alloc(std::max<int64_t>(nq * E, 1))) ||
+        (st = L.bR.v32.alloc(std::max<int64_t>(nq * E, 1))))
+      return st;
+    if (nq) {
+      sa_to_f32_kernel<<<sa_grid(nq * E, 256), 256, 0, s>>>(nq * E, P.p, bp.v32.p);
+      EX_LAUNCH_CHECK();
+      sa_transpose_blocks_kernel<<<sa_grid(nq * E, 256), 256, 0, s>>>(nq, BS, K, tslot.p, P.p, L.bR.v64.p,
+                                                                        L.bR.v32.p);
+      EX_LAUNCH_CHECK();
+    }
+    Bsr& br = L.bR;
+    br.R = K, br.C = BS, br.nb = nagg, br.nnzb = nq;
+    EX_CUDA(cudaStreamSynchronize(s));
+    bp.ptr = std::move(pptr);
+    bp.idx = std::move(pidx);
+    bp.v64 = std::move(P);
+    br.ptr = std::move(tptr);
+    br.idx = std::move(tidx);
   }
   EX_CUDA(cudaStreamSynchronize(s));  // the temporaries are freed on return
   return EXFEM_OK;
@@ -737,6 +782,21 @@ int amg_setup_blocks(exfem_amg_s* h, const std::vector<exfem_block_s*>& blks, co
     clk.mark("spectral bound", s, lev);
     if (!h->levels.empty() || keep_level0) {
       if ((st = expand_blocks(L->A, A.nb, bs, bs, n, A.ptr, A.idx, A.val.p, (int64_t)A.pat.idx.size(), s))) return st;
+      // and in block form (A is replaced by the coarse operator below, so its
+      // device arrays move into the level)
+      Bsr& ba = L->bA;
+      ba.R = ba.C = bs;
+      ba.nb = A.nb;
+      ba.nnzb = (int64_t)A.pat.idx.size();
+      if ((st = ba.v32.alloc(std::max<int64_t>(ba.nnzb * bs * bs, 1)))) return st;
+      if (ba.nnzb) {
+        sa_to_f32_kernel<<<sa_grid(ba.nnzb * bs * bs, 256), 256, 0, s>>>(ba.nnzb * bs * bs, A.val.p, ba.v32.p);
+        EX_LAUNCH_CHECK();
+      }
+      EX_CUDA(cudaStreamSynchronize(s));
+      ba.ptr = std::move(A.ptr);
+      ba.idx = std::move(A.idx);
+      ba.v64 = std::move(A.val);
     } else {
       L->A.n = n;
       L->A.ncols = n;

@@ -8,12 +8,26 @@
 
 namespace exfem {
 
+// a level matrix kept in block-sparse form (R x C dense blocks, row-major) by the
+// device set-up: the V-cycle applies it with one index per block instead of one
+// per entry (the scalar CSR copy stays for exports and replicated unions)
+struct Bsr {
+  int R = 0, C = 0;
+  int64_t nb = 0, nnzb = 0;  // block rows, stored blocks
+  DevBuf<int64_t> ptr;
+  DevBuf<int32_t> idx;
+  DevBuf<double> v64;
+  DevBuf<float> v32;
+  bool on() const { return nnzb > 0; }
+};
+
 struct AmgLevel {
   enum { WB = 0, WX = 1, WR = 2, WD = 3, WD2 = 4, WTMP = 5, NW = 6 };
   int64_t n = 0, nc = 0;
   double rho = 1.0;
   int64_t op_nnz = 0;     // nonzeros of the level operator when it is not stored (device set-up)
   Csr64 A, P, R;
+  Bsr bA, bP, bR;         // the same matrices in block form (device set-up only)
   DevBuf<double> dinv64;
   DevBuf<float> dinv32;
   DevBuf<double> coef64;  // optional per-row Chebyshev coefficients (5 per row)

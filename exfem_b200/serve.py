@@ -170,6 +170,28 @@ class SolveServer:
             self._cv.notify_all()
         return fut
 
+    def cancel(self, req):
+        """Withdraw a request that has not started; its future raises
+        CancelledError.  Returns False when it already runs or has finished."""
+        with self._cv:
+            if req not in self._pending:
+                return False
+            self._pending.remove(req)
+            fut = self._futures.pop(req.id)
+        fut.cancel()
+        return True
+
+    def cancel_pending(self):
+        """Withdraw every request that has not started (e.g. the backlog at the end
+        of a measurement window); returns how many were withdrawn."""
+        with self._cv:
+            reqs = list(self._pending)
+            self._pending.clear()
+            futs = [self._futures.pop(r.id) for r in reqs]
+        for f in futs:
+            f.cancel()
+        return len(reqs)
+
     def warm(self, specs):
         """Set up entries ahead of the stream (blocks until they are resident)."""
         for sp in specs:

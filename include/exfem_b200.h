@@ -75,6 +75,7 @@ typedef struct exfem_block_s* exfem_block;
 typedef struct exfem_amg_s* exfem_amg;
 typedef struct exfem_solver_s* exfem_solver;
 typedef struct exfem_batch_s* exfem_batch;
+typedef struct exfem_queue_s* exfem_queue;
 
 /* ------------------------------------------------------------ library */
 int exfem_version(void);
@@ -355,6 +356,33 @@ int exfem_batch_create(exfem_block blk, exfem_amg amg, int ninst, const int64_t*
 int exfem_batch_destroy(exfem_batch b);
 int exfem_batch_solve(exfem_batch b, const double* rhs, double* x, double tol, double inner_tol, int max_pass,
                       int maxiter, int* iters, int* passes, double* relres, void* stream);
+
+/* ------------------------------------------------------------ request queue
+ * Linear solves queued against resident solver handles, for hosts that are not
+ * Python (the served stream behind the C ABI; no counterpart in the reference,
+ * which solves one model per StaticSolver.solve call, gfem/solvers.py:481-605).
+ * exfem_queue_create starts `workers` host threads on the current device, each
+ * with its own CUDA stream.  exfem_queue_submit copies a right-hand side (the
+ * solver's ndof FP64 values, host memory) and returns a request id; a worker
+ * takes the oldest pending request whose solver is idle (one request per solver
+ * handle at a time; requests of different handles run concurrently) and runs
+ * exfem_solver_mixed with it to `tol` (the handle must be EXFEM_OP_MF_F32 with its
+ * preconditioner set; the handle must not be used elsewhere while the queue holds
+ * requests for it).  poll reports the state (EXFEM_REQ_*), iterations and relative
+ * residual; wait blocks up to timeout_s seconds; result copies a finished request's
+ * solution to x_host and forgets the request (returns the solve's status, or the
+ * error of a failed or withdrawn one); cancel withdraws a request that has not
+ * started (*withdrawn = 1) and leaves running or finished ones alone
+ * (*withdrawn = 0).  destroy withdraws what is pending and waits for the running. */
+enum { EXFEM_REQ_PENDING = 0, EXFEM_REQ_RUNNING = 1, EXFEM_REQ_DONE = 2, EXFEM_REQ_FAILED = 3,
+       EXFEM_REQ_CANCELLED = 4 };
+int exfem_queue_create(int workers, exfem_queue* out);
+int exfem_queue_destroy(exfem_queue q);
+int exfem_queue_submit(exfem_queue q, exfem_solver s, const double* rhs_host, double tol, int64_t* id);
+int exfem_queue_poll(exfem_queue q, int64_t id, int* state, int* iters, double* relres);
+int exfem_queue_wait(exfem_queue q, int64_t id, double timeout_s, int* state);
+int exfem_queue_result(exfem_queue q, int64_t id, double* x_host, int* iters, int* passes, double* relres);
+int exfem_queue_cancel(exfem_queue q, int64_t id, int* withdrawn);
 
 /* ------------------------------------------------------------ host index builders
  * Host-side, no device work.  Gather plan of one connectivity exactly as

@@ -73,3 +73,59 @@ def test_served_results_match_direct_and_alone(cuda):
     with serve.SolveServer(slots=1, setup_workers=0) as srv:
         ua, _ = srv.submit(serve.SolveRequest(j2spec, step=step)).result(timeout=600)
     np.testing.assert_array_equal(ua, out[-1][0])
+
+
+def test_c_abi_request_queue(cuda):
+    """The request queue of the C ABI (exfem_queue_*), as a host that is not Python
+    drives it: right-hand sides for two resident mixed-solver handles submitted,
+    polled, waited for and collected, one request withdrawn before it starts; every
+    result equals the same handle's direct mixed solve bit for bit, and to 1e-8 the
+    oracle's direct solution."""
+    import ctypes as C
+
+    from exfem_b200 import _lib
+    from exfem_b200._lib import lib
+    from exfem_b200.model import Block
+    specs = [_linear_spec("q0", (12, 3, 2), elements.HEX8, 210e3, 0.3),
+             _linear_spec("q1", (4, 2, 2), elements.TET10, 95e3, 0.35)]
+    solvers = []
+    for sp, _ in specs:
+        blk = Block(sp.conn, sp.etype, sp.material, X=sp.X)
+        blk.set_fixed(sp.fixed)
+        Ke = blk.stiffness(torch.zeros(sp.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
+        amg = linalg.DeviceAMG(blk, Ke)
+        solvers.append((blk, amg, linalg.NativeSolver(blk, "mf32", "amg", amg)))
+    q = C.c_void_p()
+    assert lib.exfem_queue_create(2, C.byref(q)) == _lib.OK
+    try:
+        ids, want = [], []
+        for k in range(6):
+            (sp, rhs), (_, _, ns) = specs[k % 2], solvers[k % 2]
+            b = np.ascontiguousarray(rhs * (1.0 + 0.5 * k))
+            i = C.c_int64()
+            assert lib.exfem_queue_submit(q, ns._h, b.ctypes.data, 1e-10, C.byref(i)) == _lib.OK, _lib.last_error()
+            ids.append(i.value)
+            want.append((sp, b))
+        wd = C.c_int()
+        assert lib.exfem_queue_cancel(q, ids[5], C.byref(wd)) == _lib.OK
+        for k, i in enumerate(ids):
+            st = C.c_int()
+            assert lib.exfem_queue_wait(q, i, 120.0, C.byref(st)) == _lib.OK
+            if k == 5 and wd.value:
+                assert st.value == _lib.REQ_CANCELLED
+                assert lib.exfem_queue_result(q, i, None, None, None, None) == _lib.ERR_ARG
+                continue
+            assert st.value == _lib.REQ_DONE, (k, st.value, _lib.last_error())
+            sp, b = want[k]
+            x = np.empty(sp.ndof)
+            it, ps, rr = C.c_int(), C.c_int(), C.c_double()
+            assert lib.exfem_queue_result(q, i, x.ctypes.data, C.byref(it), C.byref(ps), C.byref(rr)) == _lib.OK
+            assert rr.value <= 1e-10 and it.value > 0
+            xd, _, _, _ = solvers[k % 2][2].mixed(torch.as_tensor(b, device="cuda"), tol=1e-10)
+            np.testing.assert_array_equal(x, xd.cpu().numpy())
+            xo = _direct(sp, b)
+            assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+        st = C.c_int()
+        assert lib.exfem_queue_poll(q, ids[0], C.byref(st), None, None) == _lib.ERR_ARG     # already collected
+    finally:
+        assert lib.exfem_queue_destroy(q) == _lib.OK

@@ -138,3 +138,22 @@ def test_request_records_for_latency_reports():
         assert abs(r["latency_s"] - (r["queue_s"] + r["service_s"])) < 1e-9
     st = serve.latency_stats(list(s.completed))
     assert abs(st["p50_s"] - float(np.percentile([r["latency_s"] for r in recs], 50))) < 1e-12
+
+
+def test_pending_requests_can_be_withdrawn():
+    """Requests that have not started can be withdrawn (one by one or the whole
+    backlog); their futures report cancellation, running ones still finish."""
+    sp = _spec("m0")
+    s, _ = _server(slots=1, budget=1e12, solve_time=0.2)
+    try:
+        futs = [s.submit(serve.SolveRequest(sp, rhs=np.full(sp.ndof, float(i)))) for i in range(6)]
+        time.sleep(0.05)                                   # the first request is running
+        reqs = list(s._pending)
+        assert s.cancel(reqs[0]) and not s.cancel(reqs[0])
+        n = s.cancel_pending()
+        assert n == len(reqs) - 1
+        x, _ = futs[0].result(timeout=30)
+        np.testing.assert_array_equal(x, np.zeros(sp.ndof))
+        assert all(f.cancelled() for f in futs[1:])
+    finally:
+        s.close()
