@@ -102,7 +102,7 @@ _SIGS = {
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
     "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
     "exfem_host_face_once": ([I64, P, P], C.c_int),
-    "exfem_host_tile_maps": ([I64, I64, I32, P, I32, I32, P, C.POINTER(I64), C.POINTER(I64), P, P, P, P], C.c_int),
+    "exfem_host_tile_maps": ([I64, I64, I32, P, I32, C.POINTER(I64), C.POINTER(I64), P, P, P, P], C.c_int),
     "exfem_block_status": ([VP, VP], C.c_int),
     "exfem_amg_setup_block": ([VP, VP, P, I32, I32, VP], C.c_int),
     "exfem_amg_setup_blocks": ([VP, I32, P, P, I32, I32, VP], C.c_int),

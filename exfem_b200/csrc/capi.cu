@@ -33,9 +33,8 @@ int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double
                     std::vector<int32_t>& order);
 int host_tile_pairs(int64_t ne, const int32_t* conn, std::vector<int32_t>& order, std::vector<int32_t>& conn_tile);
 int host_face_once(int64_t nface, const int64_t* keys, uint8_t* once);
-int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int lanes, const int* partner,
-                   std::vector<int32_t>& ptr, std::vector<int32_t>& nodes, std::vector<uint16_t>& nend,
-                   std::vector<uint16_t>& perm, int& maxu);
+int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
+                   std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm, int& maxu);
 int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters, double* relres, cudaStream_t st);
 int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
                     int maxiter, int* iters, int* updates, double* relres, cudaStream_t st);
@@ -227,16 +226,7 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
     if ((s = b->conn_tile.upload(conn_ord.data(), std::max<size_t>(conn_ord.size(), 1)))) return s;
     std::vector<int32_t> tp, tn;
     std::vector<uint16_t> te, tq;
-    {
-      // record order for the FP32 product's thread layout: C3D10 element pairs per
-      // thread with face partners (local corners 0-1-2 of a pair's shared face),
-      // one C3D8 element per thread
-      static const int tet10_partner[10] = {1, 0, 2, -1, 4, 6, 5, -1, -1, -1};
-      const bool pairs = b->etype == EXFEM_C3D10;
-      if ((s = host_tile_maps(nn, ne, b->nnode, conn_ord.data(), b->tile, pairs ? 2 : 1, pairs ? tet10_partner : nullptr,
-                              tp, tn, te, tq, b->maxu)))
-        return s;
-    }
+    if ((s = host_tile_maps(nn, ne, b->nnode, conn_ord.data(), b->tile, tp, tn, te, tq, b->maxu))) return s;
     b->ntile = (int64_t)tp.size() - 1;
     if ((s = b->tile_ptr.upload(tp.data(), tp.size()))) return s;
     if ((s = b->tile_nodes.upload(tn.data(), std::max<size_t>(tn.size(), 1)))) return s;
@@ -920,22 +910,17 @@ int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t
   return host_standard_aggregation(n, ptr, idx, agg, *nagg);
 }
 
-int exfem_host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int lanes,
-                         const int32_t* partner, int64_t* ntile, int64_t* nlist, int32_t* ptr, int32_t* nodes,
-                         uint16_t* nend, uint16_t* perm) {
+int exfem_host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int64_t* ntile,
+                         int64_t* nlist, int32_t* ptr, int32_t* nodes, uint16_t* nend, uint16_t* perm) {
   EX_ARG(ne >= 0 && nnode > 0 && (conn || ne == 0) && ntile && nlist, "NULL argument");
   EX_ARG(tile == 128 || tile == 256, "tile must be 128 or 256, got %d", tile);
-  EX_ARG(lanes == 1 || lanes == 2, "lanes must be 1 or 2, got %d", lanes);
   for (int64_t k = 0; k < ne * nnode; ++k)
     EX_ARG(conn[k] >= 0 && conn[k] < nn, "connectivity entry %d at slot %lld is outside [0, %lld)", conn[k],
            (long long)k, (long long)nn);
-  std::vector<int> part;
-  if (partner) part.assign(partner, partner + nnode);
   std::vector<int32_t> tp, tn;
   std::vector<uint16_t> te, tq;
   int maxu = 0, s;
-  if ((s = host_tile_maps(nn, ne, nnode, conn, tile, lanes, partner ? part.data() : nullptr, tp, tn, te, tq, maxu)))
-    return s;
+  if ((s = host_tile_maps(nn, ne, nnode, conn, tile, tp, tn, te, tq, maxu))) return s;
   *ntile = (int64_t)tp.size() - 1;
   *nlist = (int64_t)tn.size();
   if (ptr) memcpy(ptr, tp.data(), tp.size() * sizeof(int32_t));

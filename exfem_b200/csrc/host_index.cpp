@@ -17,8 +17,8 @@
 //      pass 3: still-unaggregated nodes seed new aggregates with their
 //              unaggregated neighbours.
 //  * tile maps of the matrix-free product: per tile of consecutive positions of
-//    the tile order, its distinct nodes in a bank-conflict-aware record order
-//    (bank_record_order below) and the slots grouped by node;
+//    the tile order, its sorted distinct nodes and the slots grouped by node
+//    (tiles in parallel);
 //  * boundary faces (no counterpart in the reference's code, which finds them
 //    with a row-wise np.unique, gfem/surfaces.py:182-221): every element face
 //    is keyed by its sorted corner nodes; the keys go into an open-addressing hash
@@ -293,152 +293,31 @@ int host_tile_pairs(int64_t ne, const int32_t* conn, std::vector<int32_t>& order
 // slots in increasing slot order, concatenated into `perm` (tile-major, padded
 // to nnode*tile entries per tile); and `nend`, the end of each node's run in
 // perm (aligned with the node list).
-// Record order of a tile's distinct nodes (the shared-memory records of the
-// matrix-free product), chosen against shared-memory bank conflicts.  The product's
-// threads read node values and add node sums at records r with word addresses
-// 7 r + const, so the bank of an access is fixed by r mod 32 (7 is invertible
-// mod 32): a warp instruction takes as many passes as the largest number of its
-// lanes that hit one residue class (distinct records for loads, every lane for the
-// atomic additions).  Access groups follow the kernel: thread j of NT = tile/lanes
-// threads handles tile positions lanes*j (+1 with lanes = 2), warps are 32
-// consecutive threads, one group per warp and local node (and per pair half);
-// with lanes = 2 the second element skips a node its face partner (local node
-// partner[b] of the first) already holds.  Greedy: nodes by decreasing weight
-// (group memberships counted once for loads plus the multiplicity for atomics),
-// ties by list position; each takes the residue class, among those with room
-// (class c holds the records c, c+32, ... < nu), that adds least to the groups'
-// largest class counts, ties by the emptier class, then the lower class; the
-// records of a class go to its nodes in list order.  Returns the record of each
-// list position (a permutation of 0..nu-1).
-static void bank_record_order(const int32_t* lpos, int cnt, int tile, int nnode, int lanes, const int* partner,
-                              int nu, std::vector<int>& rec) {
-  const int NT = tile / lanes, NW = (NT + 31) / 32;
-  struct Mem {
-    int g, m;
-  };
-  std::vector<std::vector<Mem>> mem(nu);
-  std::vector<int> cntbuf(nu, 0), touched;
-  int ngroup = 0;
-  auto add_group = [&](const std::vector<int>& members) {
-    touched.clear();
-    for (int n : members) {
-      if (cntbuf[n] == 0) touched.push_back(n);
-      ++cntbuf[n];
-    }
-    for (int n : touched) {
-      mem[n].push_back(Mem{ngroup, cntbuf[n]});
-      cntbuf[n] = 0;
-    }
-    ++ngroup;
-  };
-  std::vector<int> g;
-  for (int w = 0; w < NW; ++w) {
-    const int j0 = 32 * w, j1 = std::min(NT, 32 * w + 32);
-    if (lanes == 2) {
-      for (int a = 0; a < nnode; ++a) {
-        g.clear();
-        for (int j = j0; j < j1; ++j)
-          if (2 * j < cnt) g.push_back(lpos[(size_t)(2 * j) * nnode + a]);
-        add_group(g);
-      }
-      for (int b = 0; b < nnode; ++b) {
-        g.clear();
-        for (int j = j0; j < j1; ++j) {
-          if (2 * j + 1 >= cnt) continue;
-          const int n1 = lpos[(size_t)(2 * j + 1) * nnode + b];
-          const int sb = partner ? partner[b] : -1;
-          if (sb >= 0 && n1 == lpos[(size_t)(2 * j) * nnode + sb]) continue;
-          g.push_back(n1);
-        }
-        add_group(g);
-      }
-    } else {
-      for (int a = 0; a < nnode; ++a) {
-        g.clear();
-        for (int j = j0; j < j1; ++j)
-          if (j < cnt) g.push_back(lpos[(size_t)j * nnode + a]);
-        add_group(g);
-      }
-    }
-  }
-  std::vector<int> weight(nu, 0), order(nu);
-  for (int n = 0; n < nu; ++n)
-    for (const Mem& e : mem[n]) weight[n] += 1 + e.m;
-  for (int n = 0; n < nu; ++n) order[n] = n;
-  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return weight[x] > weight[y]; });
-  std::vector<int> hl((size_t)ngroup * 32, 0), ha((size_t)ngroup * 32, 0), ml(ngroup, 0), ma(ngroup, 0);
-  int cap[32], used[32] = {0};
-  for (int c = 0; c < 32; ++c) cap[c] = nu / 32 + (c < nu % 32 ? 1 : 0);
-  std::vector<int> colour(nu, 0);
-  for (int n : order) {
-    int best = -1;
-    long bcost = 0;
-    for (int c = 0; c < 32; ++c) {
-      if (used[c] >= cap[c]) continue;
-      long add = 0;
-      for (const Mem& e : mem[n]) {
-        add += std::max(0, hl[(size_t)e.g * 32 + c] + 1 - ml[e.g]);
-        add += std::max(0, ha[(size_t)e.g * 32 + c] + e.m - ma[e.g]);
-      }
-      if (best < 0 || add < bcost || (add == bcost && used[c] < used[best])) {
-        best = c;
-        bcost = add;
-      }
-    }
-    colour[n] = best;
-    ++used[best];
-    for (const Mem& e : mem[n]) {
-      int& l = hl[(size_t)e.g * 32 + best];
-      int& a = ha[(size_t)e.g * 32 + best];
-      l += 1;
-      a += e.m;
-      ml[e.g] = std::max(ml[e.g], l);
-      ma[e.g] = std::max(ma[e.g], a);
-    }
-  }
-  rec.assign(nu, 0);
-  int next[32];
-  for (int c = 0; c < 32; ++c) next[c] = c;
-  for (int n = 0; n < nu; ++n) {
-    rec[n] = next[colour[n]];
-    next[colour[n]] += 32;
-  }
-}
-
-int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int lanes, const int* partner,
-                   std::vector<int32_t>& ptr, std::vector<int32_t>& nodes, std::vector<uint16_t>& nend,
+int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr, std::vector<int32_t>& nodes, std::vector<uint16_t>& nend,
                    std::vector<uint16_t>& perm, int& maxu) {
   const int64_t ntile = (ne + tile - 1) / tile;
   const int nslot = nnode * tile;
   ptr.assign(ntile + 1, 0);
   nend.clear();
   perm.assign((size_t)ntile * nslot, 0);
-  // per tile: the sorted distinct nodes, then their record order (independent per
-  // tile, so the tiles are processed in parallel and concatenated in tile order)
+  // per tile: the sorted distinct nodes (independent per tile, so the tiles are
+  // processed in parallel and concatenated in tile order)
   std::vector<std::vector<int32_t>> lists(ntile);
   std::vector<std::vector<uint16_t>> ends(ntile);
   const int nth = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
   std::vector<std::thread> pool;
   std::atomic<int64_t> next_tile(0);
   auto work = [&]() {
-    std::vector<int32_t> pos(nn, 0), lpos, cntv, start;
-    std::vector<int> rec;
+    std::vector<int32_t> pos(nn, 0), cntv, start;
     for (;;) {
       const int64_t t = next_tile.fetch_add(1);
       if (t >= ntile) break;
       const int64_t e0 = t * tile, e1 = std::min<int64_t>(ne, e0 + tile);
-      const int cnt = (int)(e1 - e0);
       std::vector<int32_t> list(conn + e0 * nnode, conn + e1 * nnode);
       std::sort(list.begin(), list.end());
       list.erase(std::unique(list.begin(), list.end()), list.end());
       const int nu = (int)list.size();
       for (int i = 0; i < nu; ++i) pos[list[i]] = i;
-      lpos.resize((size_t)cnt * nnode);
-      for (int64_t k = 0; k < (int64_t)cnt * nnode; ++k) lpos[k] = pos[conn[e0 * nnode + k]];
-      bank_record_order(lpos.data(), cnt, tile, nnode, lanes, partner, nu, rec);
-      std::vector<int32_t> ordered(nu);
-      for (int i = 0; i < nu; ++i) ordered[rec[i]] = list[i];
-      for (int i = 0; i < nu; ++i) pos[ordered[i]] = i;
       cntv.assign(nu, 0);
       for (int a = 0; a < nnode; ++a)
         for (int64_t e = e0; e < e1; ++e) ++cntv[pos[conn[e * nnode + a]]];
@@ -450,7 +329,7 @@ int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int t
         for (int64_t e = e0; e < e1; ++e) pm[cntv[pos[conn[e * nnode + a]]]++] = (uint16_t)(a * tile + (e - e0));
       std::vector<uint16_t> en(nu);
       for (int i = 0; i < nu; ++i) en[i] = (uint16_t)start[i + 1];
-      lists[t] = std::move(ordered);
+      lists[t] = std::move(list);
       ends[t] = std::move(en);
     }
   };

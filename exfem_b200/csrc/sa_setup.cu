@@ -290,16 +290,19 @@ __global__ void sa_to_f32_kernel(int64_t n, const double* __restrict__ a, float*
     b[i] = (float)a[i];
 }
 
-// blocks of R = P^T in block form: block q of aggregate row a is the transpose of
-// P's block tslot[q] (BS x K -> K x BS), FP64 and FP32
-__global__ void sa_transpose_blocks_kernel(int64_t nq, int BS, int K, const int32_t* __restrict__ tslot,
+// blocks of R = P^T in block form: block q of aggregate row a (fine node tidx[q])
+// is the transpose of P's block at position tslot[q] of that node's row
+// (BS x K -> K x BS), FP64 and FP32
+__global__ void sa_transpose_blocks_kernel(int64_t nq, int BS, int K, const int32_t* __restrict__ tidx,
+                                           const int32_t* __restrict__ tslot, const int64_t* __restrict__ pptr,
                                            const double* __restrict__ P, double* __restrict__ r64,
                                            float* __restrict__ r32) {
   const int E = BS * K;
   for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nq * E; t += (int64_t)gridDim.x * blockDim.x) {
     const int64_t q = t / E;
     const int e = (int)(t - q * E), i = e / BS, j = e - i * BS;   // entry (i, j) of the K x BS block
-    const double v = P[(int64_t)tslot[q] * E + j * K + i];
+    const int64_t blk = pptr[tidx[q]] + tslot[q];
+    const double v = P[blk * E + j * K + i];
     r64[t] = v;
     r32[t] = (float)v;
   }
@@ -538,8 +541,8 @@ int coarsen(const BlockOp& A, const DevBuf<int32_t>& dagg, const DevBuf<double>&
     if (nq) {
       sa_to_f32_kernel<<<sa_grid(nq * E, 256), 256, 0, s>>>(nq * E, P.p, bp.v32.p);
       EX_LAUNCH_CHECK();
-      sa_transpose_blocks_kernel<<<sa_grid(nq * E, 256), 256, 0, s>>>(nq, BS, K, tslot.p, P.p, L.bR.v64.p,
-                                                                        L.bR.v32.p);
+      sa_transpose_blocks_kernel<<<sa_grid(nq * E, 256), 256, 0, s>>>(nq, BS, K, tidx.p, tslot.p, pptr.p, P.p,
+                                                                        L.bR.v64.p, L.bR.v32.p);
       EX_LAUNCH_CHECK();
     }
     Bsr& br = L.bR;

@@ -114,9 +114,8 @@ int exfem_block_colours(exfem_block b, int32_t* colour_host);
  * element index); a tile is `tile` consecutive positions of that order, and slot
  * s = a*tile + p is local node a of the element at tile position p.  tile_info:
  * tile count, total length of the node lists and the longest list; tile_maps,
- * copied to host: ptr (ntile+1), the distinct nodes of every tile in the order of
- * their shared-memory records (chosen against bank conflicts of the FP32 product,
- * exfem_host_tile_maps), for each listed node the end of its run of slots
+ * copied to host: ptr (ntile+1), the sorted distinct nodes of every tile (the
+ * order of its shared-memory records), for each listed node the end of its run of slots
  * (uint16), and per tile the slots grouped by node in node order, increasing
  * within a node (ntile, nnode*tile, zero padded); tile_order: the tile size and
  * the order (ne,) as position -> element.  No counterpart in the reference. */
@@ -425,16 +424,12 @@ int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const 
  * shared nodes once.  No counterpart in the reference. */
 int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile);
 /* tile maps of the matrix-free product (see exfem_block_tile_maps) for a
- * connectivity already in tile order, for a product thread layout of `lanes`
- * elements per thread (2: C3D10 element pairs, partner = the local node of a
- * pair's first element that may equal local node b of the second, or -1; NULL for
- * none): per tile its distinct nodes in the bank-conflict-aware record order,
- * nend and perm.  Call with ptr = NULL for ntile and nlist (the total list
- * length), then with ptr (ntile+1), nodes (nlist), nend (nlist) and perm
+ * connectivity already in tile order: per tile its sorted distinct nodes, nend
+ * and perm.  Call with ptr = NULL for ntile and nlist (the total list length),
+ * then with ptr (ntile+1), nodes (nlist), nend (nlist) and perm
  * (ntile * nnode * tile).  No counterpart in the reference. */
-int exfem_host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int lanes,
-                         const int32_t* partner, int64_t* ntile, int64_t* nlist, int32_t* ptr, int32_t* nodes,
-                         uint16_t* nend, uint16_t* perm);
+int exfem_host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int64_t* ntile,
+                         int64_t* nlist, int32_t* ptr, int32_t* nodes, uint16_t* nend, uint16_t* perm);
 /* boundary faces: keys (nface, 4) int64, each face's corner nodes sorted
  * ascending (triangles padded in front with -1); once[f] = 1 when no other face
  * has the same key, else 0.  The face matching of gfem/surfaces.py:182-221

@@ -536,93 +536,13 @@ def tile_pairs(order, conn, window=16):
     return np.asarray(out_o, np.int32), np.asarray(out_c, np.int32).reshape(-1, conn.shape[1])
 
 
-TET10_PARTNER = (1, 0, 2, -1, 4, 6, 5, -1, -1, -1)
-
-
-def bank_record_order(lpos, tile, lanes, partner, nu):
-    """Record of each sorted-list node of one tile (no counterpart in the reference):
-    the greedy bank-conflict-aware order of the matrix-free product's shared-memory
-    node records.  lpos (cnt, nnode): list position of every slot's node.  Access
-    groups: per warp of 32 threads (thread j handles positions lanes*j, +1 for
-    lanes = 2), per local node a, lanes in order; with lanes = 2 first the groups
-    of the even positions, then those of the odd ones, where a node equal to the
-    even element's node at local partner[b] is left out.  Nodes by decreasing
-    weight (sum over their groups of 1 + multiplicity; ties by list position) take
-    the residue class c (records c, c+32, ...; room nu//32 + (c < nu%32)) that adds
-    least to the groups' largest class counts (loads count a node once, additions
-    every lane), ties by fewer nodes already in the class, then lower c; each
-    class's records go to its nodes in list order."""
-    cnt, nnode = lpos.shape
-    NT = tile // lanes
-    groups = []
-    for w in range(-(-NT // 32)):
-        js = np.arange(32 * w, min(NT, 32 * w + 32))
-        if lanes == 2:
-            ev = js[2 * js < cnt]
-            for a in range(nnode):
-                groups.append(lpos[2 * ev, a])
-            od = js[2 * js + 1 < cnt]
-            for b in range(nnode):
-                g = lpos[2 * od + 1, b]
-                sb = partner[b] if partner is not None else -1
-                if sb >= 0:
-                    g = g[g != lpos[2 * od, sb]]
-                groups.append(g)
-        else:
-            ok = js[js < cnt]
-            for a in range(nnode):
-                groups.append(lpos[ok, a])
-    mem = [[] for _ in range(nu)]
-    for gi, g in enumerate(groups):
-        nodes, mult = np.unique(g, return_counts=True)
-        for n, m in zip(nodes, mult):
-            mem[int(n)].append((gi, int(m)))
-    weight = np.array([sum(1 + m for _, m in mem[n]) for n in range(nu)])
-    order = np.argsort(-weight, kind="stable")
-    G = len(groups)
-    hl, ha = np.zeros((G, 32), np.int64), np.zeros((G, 32), np.int64)
-    ml, ma = np.zeros(G, np.int64), np.zeros(G, np.int64)
-    cap = np.array([nu // 32 + (1 if c < nu % 32 else 0) for c in range(32)])
-    used = np.zeros(32, np.int64)
-    colour = np.zeros(nu, np.int64)
-    for n in order:
-        gs = np.array([g for g, _ in mem[n]], np.int64)
-        ms = np.array([m for _, m in mem[n]], np.int64)
-        if len(gs):
-            add = (np.maximum(0, hl[gs] + 1 - ml[gs, None]).sum(0) +
-                   np.maximum(0, ha[gs] + ms[:, None] - ma[gs, None]).sum(0))
-        else:
-            add = np.zeros(32, np.int64)
-        best = -1
-        for c in range(32):
-            if used[c] >= cap[c]:
-                continue
-            if best < 0 or add[c] < add[best] or (add[c] == add[best] and used[c] < used[best]):
-                best = c
-        colour[n] = best
-        used[best] += 1
-        if len(gs):
-            hl[gs, best] += 1
-            ha[gs, best] += ms
-            ml[gs] = np.maximum(ml[gs], hl[gs, best])
-            ma[gs] = np.maximum(ma[gs], ha[gs, best])
-    rec = np.zeros(nu, np.int64)
-    nxt = np.arange(32)
-    for n in range(nu):
-        rec[n] = nxt[colour[n]]
-        nxt[colour[n]] += 32
-    return rec
-
-
-def tile_maps(conn, tile, lanes=1, partner=None):
+def tile_maps(conn, tile):
     """Element-tile maps used by the matrix-free product (no counterpart in the
     reference), for conn given in tile order.  Positions [t*tile, (t+1)*tile) form
     tile t; slot s = a*tile + p is local node a of the element at tile position p.
-    Per tile: the distinct nodes in record order (:func:`bank_record_order` of the
-    sorted list, for the product's thread layout: ``lanes`` elements per thread and
-    the face ``partner`` map of element pairs); for each node (in that order) its
-    slots in increasing order, concatenated into perm (padded with zeros to
-    nnode*tile per tile); nend = end of each node's run.
+    Per tile: the sorted distinct nodes; for each node (in that order) its slots in
+    increasing order, concatenated into perm (padded with zeros to nnode*tile per
+    tile); nend = end of each node's run.
     Returns (ptr (ntile+1,), nodes, nend, perm (ntile, nnode*tile))."""
     conn = np.asarray(conn, dtype=np.int64)
     ne, nnode = conn.shape
@@ -631,11 +551,8 @@ def tile_maps(conn, tile, lanes=1, partner=None):
     perm = np.zeros((ntile, nnode * tile), np.uint16)
     for t in range(ntile):
         blk = conn[t * tile:(t + 1) * tile]
-        srt = np.unique(blk)
-        rec = bank_record_order(np.searchsorted(srt, blk), tile, lanes, partner, len(srt))
-        u = np.empty_like(srt)
-        u[rec] = srt
-        slot_node = rec[np.searchsorted(srt, blk.T.reshape(-1))]  # record of each slot, order a*tile + p
+        u = np.unique(blk)
+        slot_node = np.searchsorted(u, blk.T.reshape(-1))        # slot order a*tile + p (valid p only)
         la = np.arange(blk.shape[0])
         slots = (np.arange(nnode)[:, None] * tile + la[None, :]).reshape(-1)
         order = np.argsort(slot_node, kind="stable")

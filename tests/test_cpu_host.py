@@ -663,12 +663,10 @@ def test_face_hash_counts_shared_keys():
     np.testing.assert_array_equal(once, [0, 1, 0, 1, 0])
 
 
-def _host_tile_maps(conn, nn, tile, lanes, partner):
+def _host_tile_maps(conn, nn, tile):
     c32 = np.ascontiguousarray(conn, dtype=np.int32)
-    part = None if partner is None else np.ascontiguousarray(partner, dtype=np.int32)
     nt, nl = C.c_int64(), C.c_int64()
-    args = [nn, len(c32), c32.shape[1], c32.ctypes.data, tile, lanes, part.ctypes.data if part is not None else None,
-            C.byref(nt), C.byref(nl)]
+    args = [nn, len(c32), c32.shape[1], c32.ctypes.data, tile, C.byref(nt), C.byref(nl)]
     assert _lib.lib.exfem_host_tile_maps(*args, None, None, None, None) == 0, _lib.last_error()
     ptr = np.zeros(nt.value + 1, np.int32)
     nodes = np.zeros(max(nl.value, 1), np.int32)
@@ -679,63 +677,20 @@ def _host_tile_maps(conn, nn, tile, lanes, partner):
     return ptr, nodes[:nl.value], nend[:nl.value], perm
 
 
-def _bank_passes(conn, ptr, nodes, tile, lanes, partner):
-    """Shared-memory passes of the product's record loads and additions (largest
-    residue-class count per warp access group) summed over the tiles."""
-    loads = adds = 0
-    nnode = conn.shape[1]
-    for t in range(len(ptr) - 1):
-        rec = {int(n): i for i, n in enumerate(nodes[ptr[t]:ptr[t + 1]])}
-        blk = conn[t * tile:(t + 1) * tile]
-        r = np.vectorize(rec.get)(blk)
-        cnt = len(blk)
-        for w in range(tile // lanes // 32):
-            js = np.arange(32 * w, 32 * w + 32)
-            grp = []
-            if lanes == 2:
-                ev, od = js[2 * js < cnt], js[2 * js + 1 < cnt]
-                grp += [r[2 * ev, a] for a in range(nnode)]
-                for b in range(nnode):
-                    g = r[2 * od + 1, b]
-                    if partner is not None and partner[b] >= 0:
-                        g = g[g != r[2 * od, partner[b]]]
-                    grp.append(g)
-            else:
-                ok = js[js < cnt]
-                grp += [r[ok, a] for a in range(nnode)]
-            for g in grp:
-                if len(g):
-                    loads += np.bincount(np.unique(g) % 32, minlength=32).max()
-                    adds += np.bincount(g % 32, minlength=32).max()
-    return loads, adds
-
-
 @pytest.mark.parametrize("kind", ["tet", "hex"])
-def test_tile_record_order_bit_exact_and_fewer_bank_conflicts(kind):
-    """The tile maps' record order (a greedy choice against shared-memory bank
-    conflicts of the FP32 product, no counterpart in the reference) equals the
-    oracle's restatement bit for bit, lists every tile's distinct nodes once, and
-    cuts the product's shared-memory passes against the sorted order."""
+def test_host_tile_maps_bit_exact(kind):
+    """The tile maps of the matrix-free product (no counterpart in the reference),
+    built by the library's threaded host code, equal the oracle's restatement bit
+    for bit on a tile-ordered C3D10 (face-paired) and C3D8 mesh, both tile sizes."""
     from oracle import fem as ofem
     if kind == "tet":
         X, c = tet10_box(1.0, 1.0, 1.0, 6, 5, 5, frac=0.1, seed=2)
         order = fem.tile_order(X, c, 4)
         order, ct = fem.tile_pairs(order, c)
-        lanes, partner = 2, ofem.TET10_PARTNER
     else:
         X, c = mesh.box_hex(1.0, 1.0, 1.0, 10, 8, 8)
         ct = c[fem.tile_order(X, c, 8)]
-        lanes, partner = 1, None
     ct = np.asarray(ct)
     for tile in (128, 256):
-        got = _host_tile_maps(ct, len(X), tile, lanes, partner)
-        want = ofem.tile_maps(ct, tile, lanes, partner)
-        for g, w in zip(got, want):
+        for g, w in zip(_host_tile_maps(ct, len(X), tile), ofem.tile_maps(ct, tile)):
             np.testing.assert_array_equal(g, w)
-        ptr, nodes = got[0], got[1]
-        for t in range(len(ptr) - 1):
-            np.testing.assert_array_equal(np.sort(nodes[ptr[t]:ptr[t + 1]]), np.unique(ct[t * tile:(t + 1) * tile]))
-        sorted_nodes = np.concatenate([np.unique(ct[t * tile:(t + 1) * tile]) for t in range(len(ptr) - 1)])
-        l0, a0 = _bank_passes(ct, ptr, sorted_nodes, tile, lanes, partner)
-        l1, a1 = _bank_passes(ct, ptr, nodes, tile, lanes, partner)
-        assert l1 < 0.8 * l0 and a1 < 0.9 * a0, (tile, l0, l1, a0, a1)

@@ -146,8 +146,7 @@ def test_index_maps_bit_exact(cuda, kind):
         want_order, want_conn = ofem.tile_pairs(want_order, c)
     np.testing.assert_array_equal(order, want_order)
     np.testing.assert_array_equal(pmod.blocks[0].tile_conn(), want_conn)
-    lanes, partner = (2, ofem.TET10_PARTNER) if kind == "tet" else (1, None)
-    for got, want in zip(pmod.blocks[0].tile_maps(), ofem.tile_maps(want_conn, tile, lanes, partner)):
+    for got, want in zip(pmod.blocks[0].tile_maps(), ofem.tile_maps(want_conn, tile)):
         np.testing.assert_array_equal(got, want)
 
 
