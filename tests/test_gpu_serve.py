@@ -97,6 +97,7 @@ def test_c_abi_request_queue(cuda):
         solvers.append((blk, amg, linalg.NativeSolver(blk, "mf32", "amg", amg)))
     q = C.c_void_p()
     assert lib.exfem_queue_create(2, C.byref(q)) == _lib.OK
+    got = {}
     try:
         ids, want = [], []
         for k in range(6):
@@ -121,11 +122,15 @@ def test_c_abi_request_queue(cuda):
             it, ps, rr = C.c_int(), C.c_int(), C.c_double()
             assert lib.exfem_queue_result(q, i, x.ctypes.data, C.byref(it), C.byref(ps), C.byref(rr)) == _lib.OK
             assert rr.value <= 1e-10 and it.value > 0
-            xd, _, _, _ = solvers[k % 2][2].mixed(torch.as_tensor(b, device="cuda"), tol=1e-10)
-            np.testing.assert_array_equal(x, xd.cpu().numpy())
-            xo = _direct(sp, b)
-            assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
+            got[k] = x
         st = C.c_int()
         assert lib.exfem_queue_poll(q, ids[0], C.byref(st), None, None) == _lib.ERR_ARG     # already collected
     finally:
         assert lib.exfem_queue_destroy(q) == _lib.OK
+    # the handles are free again once the queue is gone: direct solves to compare with
+    for k, x in got.items():
+        sp, b = want[k]
+        xd, _, _, _ = solvers[k % 2][2].mixed(torch.as_tensor(b, device="cuda"), tol=1e-10)
+        np.testing.assert_array_equal(x, xd.cpu().numpy())
+        xo = _direct(sp, b)
+        assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-8
