@@ -244,7 +244,8 @@ def scale_solve_section(m, X, scale, cg_tol=1e-8, reps=3):
     step = xf.Step(bcs=[(fix, d, 0.0) for d in range(3)], dloads=[f])
     out, sols = {}, {}
     for name, method in (("mixed", "mixed"), ("plain_fp64", "amg")):
-        kw = dict(rtol=1e-6, linear_solver=method, tangent="mf", cg_tol=cg_tol, verbose=False, amg_setup="device")
+        kw = dict(rtol=1e-6, linear_solver=method, tangent="mf", cg_tol=cg_tol, verbose=False, amg_setup="device",
+                  async_amg=None)
         s = xf.StaticSolver(m, **kw)
         torch.cuda.synchronize()
         t0 = time.perf_counter()

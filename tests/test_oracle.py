@@ -154,3 +154,24 @@ def test_oracle_mesh_matches_reference_fixtures():
     X, c = omesh.box_hex(1.0, 1.0, 1.0, 6, 5, 4)
     np.testing.assert_array_equal(omesh.jitter_interior(X, [1 / 6, 1 / 5, 1 / 4], 0.1, 9),
                                   pmesh.jitter_interior(X, [1 / 6, 1 / 5, 1 / 4], 0.1, 9))
+
+
+def test_config2_fixture_describes_this_mesh():
+    """The full-size J2 fixture was made on the mesh the GPU test rebuilds (digest of
+    the jittered 100 x 20 x 20 C3D8 cantilever), and holds a Newton history that
+    converged: ten increments, each residual-ratio history ending below rtol 1e-6."""
+    import hashlib
+    import os
+    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "config2_j2_oracle.npz"))
+    L = 1000.0
+    X, c = mesh.box_hex(L, 200.0, 200.0, 100, 20, 20)
+    X = mesh.jitter_interior(X, [L / 100, 200.0 / 20, 200.0 / 20], 0.1, 0)
+    digest = hashlib.sha256(np.ascontiguousarray(X).tobytes() +
+                            np.ascontiguousarray(c, dtype=np.int64).tobytes()).hexdigest()
+    assert digest == str(ref["mesh_digest"])
+    assert ref["newton"].shape == (10,) and ref["u"].shape == (3 * len(X),)
+    assert ref["mises"].shape == (len(c),) and np.all(np.isfinite(ref["u"]))
+    tip = X[:, 0] > L - 1e-9
+    assert np.allclose(ref["u"].reshape(-1, 3)[tip, 2], -5.0)
+    for row in ref["ratios"]:
+        assert row[np.isfinite(row)][-1] < 1e-6
