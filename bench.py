@@ -48,11 +48,11 @@ METRIC = "DOF·matvec/s, solves/s, p50/p99 latency at 1e-8 rel err vs plain FP64
 UNIT = "DOF·matvec/s"
 WORKLOAD = "C3D10 80^3x6 unit cube (3,072,000 el, 12,519,843 DOF), FP32 matrix-free tangent product"
 # DRAM bytes per product (tile pass + node pass) from one ncu capture of the
-# 56^3-cube case (dram__bytes_read.sum + dram__bytes_write.sum: 128.0 MB over
-# 1,053,696 elements in the tile pass and 41.5 MB over 1,442,897 nodes in the node
-# pass), scaled to the 80^3 cube by elements and nodes; the traffic of both passes
-# grows in proportion to them.
-TRAFFIC_BYTES = int(3072000 * 121.49 + 4173281 * 28.75)
+# 56^3-cube case (dram__bytes_read.sum + dram__bytes_write.sum: 128.6 MB over
+# 1,053,696 elements in the tile pass and 41.2 MB over 1,442,897 nodes in the node
+# pass; profiles/mf_matvec_c3d10_80cube.md), scaled to the 80^3 cube by elements
+# and nodes; the traffic of both passes grows in proportion to them.
+TRAFFIC_BYTES = int(3072000 * 122.04 + 4173281 * 28.55)
 
 
 def peaks():
@@ -450,6 +450,22 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), 
         specs.append(serve.MeshSpec(f"m{i}", X, c, et, mat, fixed))
         extra.append(dict(fix=fix, tip=tip, L=L))
 
+    # each linear request takes one of `npool` seeded tip loads of its mesh, so that a
+    # stream of 2,000/s for a minute holds no more than a few hundred MB of loads
+    npool = 4
+    pr = np.random.default_rng(seed + 3)
+    loads = []
+    for sp, ex in zip(specs, extra):
+        lst = []
+        for _ in range(0 if sp.j2 else npool):
+            f = pr.standard_normal(3)
+            f *= pr.uniform(100.0, 1000.0) / np.linalg.norm(f)
+            rhs = np.zeros(sp.ndof)
+            for k in range(3):
+                rhs[3 * ex["tip"] + k] = f[k] / len(ex["tip"])
+            lst.append(rhs)
+        loads.append(lst)
+
     def make_request(r):
         i = int(r.integers(0, nmesh))
         sp, ex = specs[i], extra[i]
@@ -457,12 +473,7 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), 
             d = -L_over(ex) * r.uniform(0.5, 1.0)
             step = Step(bcs=[(ex["fix"], k, 0.0) for k in range(3)] + [(ex["tip"], 2, d)], dt_init=0.2, dt_max=0.2)
             return serve.SolveRequest(sp, step=step)
-        f = r.standard_normal(3)
-        f *= r.uniform(100.0, 1000.0) / np.linalg.norm(f)
-        rhs = np.zeros(sp.ndof)
-        for k in range(3):
-            rhs[3 * ex["tip"] + k] = f[k] / len(ex["tip"])
-        return serve.SolveRequest(sp, rhs=rhs)
+        return serve.SolveRequest(sp, rhs=loads[i][int(r.integers(0, npool))])
 
     def L_over(ex):
         return ex["L"] / 400.0
@@ -742,7 +753,7 @@ def main():
         del blk, m
         torch.cuda.empty_cache()
         batched = batch_section()
-        served = serve_section(rates=(50.0,), duration=60.0)
+        served = serve_section(rates=(50.0, 2000.0), duration=60.0)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cv, ci = cpu_baseline()

@@ -77,9 +77,8 @@ static int spmv_lanes(const Csr64& A, const T* val, const T* x, T* y, const T* b
   const int64_t nsrc = A.ptr.n ? (int64_t)A.ptr.n - 1 : A.n;  // stored rows (fewer when blocks are replicated)
   const double avg = nsrc ? (double)A.nnz / (double)nsrc : 0.0;
   const int threads = 256;
-  const int64_t warps_needed = (A.n + 7) / 8;
-  const unsigned grid = grid_for((size_t)warps_needed * 32, threads, 148u * 24u);
-#define EXF_SP(L) spmv_kernel<T, L, MODE><<<grid, threads, 0, s>>>(A.n, A.ptr.p, A.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, rc1, rc2, A.rmap.p, A.cshift.p, skip)
+  // one group of L lanes per row: 32 / L rows per warp
+#define EXF_SP(L) spmv_kernel<T, L, MODE><<<grid_for((size_t)((A.n + 32 / L - 1) / (32 / L)) * 32, threads, 148u * 24u), threads, 0, s>>>(A.n, A.ptr.p, A.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, rc1, rc2, A.rmap.p, A.cshift.p, skip)
   if (avg <= 8) EXF_SP(4);
   else if (avg <= 24) EXF_SP(8);
   else if (avg <= 64) EXF_SP(16);
@@ -87,6 +86,35 @@ static int spmv_lanes(const Csr64& A, const T* val, const T* x, T* y, const T* b
 #undef EXF_SP
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
+}
+
+// N values of T from p into registers with the widest loads that p's alignment A
+// (bytes, a multiple of 4) allows: 16-byte, 8-byte or single loads.
+template <class T, int N, int A>
+__device__ __forceinline__ void load_regs(const T* __restrict__ p, T (&o)[N]) {
+  constexpr int BYTES = N * (int)sizeof(T);
+  if constexpr (A % 16 == 0 && BYTES % 16 == 0) {
+#pragma unroll
+    for (int i = 0; i < BYTES / 16; ++i) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i);
+      memcpy(reinterpret_cast<char*>(o) + 16 * i, &v, 16);
+    }
+  } else if constexpr (A % 8 == 0 && BYTES % 8 == 0) {
+#pragma unroll
+    for (int i = 0; i < BYTES / 8; ++i) {
+      const float2 v = __ldg(reinterpret_cast<const float2*>(p) + i);
+      memcpy(reinterpret_cast<char*>(o) + 8 * i, &v, 8);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < N; ++i) o[i] = __ldg(p + i);
+  }
+}
+
+// alignment in bytes of element k * n of a 256-byte aligned array of T
+template <class T, int N>
+constexpr int stride_align() {
+  return (N * (int)sizeof(T)) % 16 == 0 ? 16 : (N * (int)sizeof(T)) % 8 == 0 ? 8 : 4;
 }
 
 // Block-sparse product with the same fused modes as spmv_kernel: L lanes per block
@@ -112,11 +140,9 @@ bsr_kernel(int64_t nb, const int64_t* __restrict__ ptr, const int32_t* __restric
     if (br < nb) {
       const int64_t k1 = ptr[br + 1];
       for (int64_t k = ptr[br] + lane; k < k1; k += L) {
-        const T* v = val + k * (R * C);
-        const T* xx = x + (int64_t)idx[k] * C;
-        T xv[C];
-#pragma unroll
-        for (int j = 0; j < C; ++j) xv[j] = xx[j];
+        T v[R * C], xv[C];
+        load_regs<T, R * C, stride_align<T, R * C>()>(val + k * (R * C), v);
+        load_regs<T, C, stride_align<T, C>()>(x + (int64_t)idx[k] * C, xv);
 #pragma unroll
         for (int i = 0; i < R; ++i)
 #pragma unroll
@@ -155,18 +181,24 @@ bsr_kernel(int64_t nb, const int64_t* __restrict__ ptr, const int32_t* __restric
 }
 
 template <class T, int R, int C, int MODE>
-static void bsr_launch(const Bsr& M, const T* val, const T* x, T* y, const T* b, const T* dinv, T* d2, T* xo, T c1,
+static int bsr_launch(const Bsr& M, const T* val, const T* x, T* y, const T* b, const T* dinv, T* d2, T* xo, T c1,
                        T c2, const int* skip, cudaStream_t s) {
+  // the vector loads of the kernel assume the alignment of a 256-byte aligned array
+  if ((uintptr_t)x % stride_align<T, C>() || (uintptr_t)val % stride_align<T, R * C>()) {
+    set_error("block-sparse product: misaligned operand (x %p, blocks %p)", (const void*)x, (const void*)val);
+    return EXFEM_ERR_ARG;
+  }
   const double avg = M.nb ? (double)M.nnzb / (double)M.nb : 0.0;
   const int threads = 256;
-  const unsigned grid = grid_for((size_t)((M.nb + 7) / 8) * 32, threads, 148u * 24u);
-#define EXF_BSR(L) bsr_kernel<T, R, C, L, MODE><<<grid, threads, 0, s>>>(M.nb, M.ptr.p, M.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, skip)
+  // one group of L lanes per block row: 32 / L block rows per warp
+#define EXF_BSR(L) bsr_kernel<T, R, C, L, MODE><<<grid_for((size_t)((M.nb + 32 / L - 1) / (32 / L)) * 32, threads, 148u * 24u), threads, 0, s>>>(M.nb, M.ptr.p, M.idx.p, val, x, y, b, dinv, d2, xo, c1, c2, skip)
   if (avg <= 2) EXF_BSR(1);
   else if (avg <= 6) EXF_BSR(4);
   else if (avg <= 16) EXF_BSR(8);
   else if (avg <= 40) EXF_BSR(16);
   else EXF_BSR(32);
 #undef EXF_BSR
+  return EXFEM_OK;
 }
 
 template <class T, int MODE>
@@ -175,14 +207,16 @@ static int bsr_apply(const Bsr& M, const T* x, T* y, const T* b, const T* dinv, 
   const T* val;
   if constexpr (sizeof(T) == 8) val = M.v64.p;
   else val = M.v32.p;
-  if (M.R == 3 && M.C == 6) bsr_launch<T, 3, 6, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
-  else if (M.R == 6 && M.C == 3) bsr_launch<T, 6, 3, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
-  else if (M.R == 6 && M.C == 6) bsr_launch<T, 6, 6, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
-  else if (M.R == 3 && M.C == 3) bsr_launch<T, 3, 3, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  int st;
+  if (M.R == 3 && M.C == 6) st = bsr_launch<T, 3, 6, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else if (M.R == 6 && M.C == 3) st = bsr_launch<T, 6, 3, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else if (M.R == 6 && M.C == 6) st = bsr_launch<T, 6, 6, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
+  else if (M.R == 3 && M.C == 3) st = bsr_launch<T, 3, 3, MODE>(M, val, x, y, b, dinv, d2, xo, c1, c2, skip, s);
   else {
     set_error("no block-sparse product for %d x %d blocks", M.R, M.C);
     return EXFEM_ERR_UNSUPPORTED;
   }
+  if (st) return st;
   EX_LAUNCH_CHECK();
   return EXFEM_OK;
 }

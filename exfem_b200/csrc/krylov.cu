@@ -17,7 +17,7 @@
 namespace exfem {
 
 constexpr int RT = 256;          // reduction block size
-constexpr int RED_MAX_BLOCKS = 296;
+constexpr int RED_MAX_BLOCKS = 592;   // 4 CTAs of 256 per SM
 
 enum Fin { FIN_BB = 0, FIN_RZ0, FIN_RR0, FIN_ALPHA, FIN_RR, FIN_BETA, FIN_STORE };
 
@@ -88,10 +88,21 @@ __global__ void __launch_bounds__(RT)
 dot_kernel(int64_t n, const T* __restrict__ a, const T* __restrict__ b, double* partial, unsigned* counter,
            PcgScal* sc, double* out, int F, int check_done) {
   if (check_done && sc->done) return;
-  double acc = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n; i += (int64_t)gridDim.x * RT)
-    acc += (double)a[i] * (double)b[i];
-  block_finish(acc, partial, counter, F, sc, out);
+  // four independent strided loads in flight per thread, four accumulators summed
+  // in a fixed order at the end (deterministic for a given grid)
+  const int64_t S = (int64_t)gridDim.x * RT;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x;
+  for (; i + 3 * S < n; i += 4 * S) {
+    const T x0 = a[i], x1 = a[i + S], x2 = a[i + 2 * S], x3 = a[i + 3 * S];
+    const T y0 = b[i], y1 = b[i + S], y2 = b[i + 2 * S], y3 = b[i + 3 * S];
+    a0 += (double)x0 * (double)y0;
+    a1 += (double)x1 * (double)y1;
+    a2 += (double)x2 * (double)y2;
+    a3 += (double)x3 * (double)y3;
+  }
+  for (; i < n; i += S) a0 += (double)a[i] * (double)b[i];
+  block_finish((a0 + a1) + (a2 + a3), partial, counter, F, sc, out);
 }
 
 template <class T>
@@ -100,14 +111,33 @@ update_xr_kernel(int64_t n, T* __restrict__ x, T* __restrict__ r, const T* __res
                  const T* __restrict__ Ap, double* partial, unsigned* counter, PcgScal* sc) {
   if (sc->done) return;
   const T alpha = (T)sc->alpha;
-  double acc = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n; i += (int64_t)gridDim.x * RT) {
+  const int64_t S = (int64_t)gridDim.x * RT;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x;
+  for (; i + 3 * S < n; i += 4 * S) {
+    T xv[4], pv[4], rv[4], av[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      xv[u] = x[i + u * S];
+      pv[u] = p[i + u * S];
+      rv[u] = r[i + u * S];
+      av[u] = Ap[i + u * S];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      x[i + u * S] = xv[u] + alpha * pv[u];
+      const T ri = rv[u] - alpha * av[u];
+      r[i + u * S] = ri;
+      acc[u] += (double)ri * (double)ri;
+    }
+  }
+  for (; i < n; i += S) {
     x[i] += alpha * p[i];
     const T ri = r[i] - alpha * Ap[i];
     r[i] = ri;
-    acc += (double)ri * (double)ri;
+    acc[0] += (double)ri * (double)ri;
   }
-  block_finish(acc, partial, counter, FIN_RR, sc, nullptr);
+  block_finish((acc[0] + acc[1]) + (acc[2] + acc[3]), partial, counter, FIN_RR, sc, nullptr);
 }
 
 template <class T>

@@ -143,6 +143,8 @@ class SolveServer:
         self._setup_fn = setup_fn or self._device_setup
         self._cv = threading.Condition()
         self._pending = collections.deque()
+        self._waiting = collections.Counter()           # mesh key -> pending requests (no scans of a long backlog)
+        self._waiting_spec = {}                          # mesh key -> its spec, while it has pending requests
         self._entries = collections.OrderedDict()       # key -> _Entry (LRU order)
         self._setting_up = set()
         self._futures = {}
@@ -167,6 +169,7 @@ class SolveServer:
             req.t_arrival = time.perf_counter()
             self._futures[req.id] = fut
             self._pending.append(req)
+            self._hold(req)
             self._cv.notify_all()
         return fut
 
@@ -177,6 +180,7 @@ class SolveServer:
             if req not in self._pending:
                 return False
             self._pending.remove(req)
+            self._release(req)
             fut = self._futures.pop(req.id)
         fut.cancel()
         return True
@@ -187,6 +191,8 @@ class SolveServer:
         with self._cv:
             reqs = list(self._pending)
             self._pending.clear()
+            self._waiting.clear()
+            self._waiting_spec.clear()
             futs = [self._futures.pop(r.id) for r in reqs]
         for f in futs:
             f.cancel()
@@ -221,6 +227,18 @@ class SolveServer:
         with self._cv:
             return self._entries.get(key)
 
+    def _hold(self, req):
+        k = req.spec.key
+        self._waiting[k] += 1
+        self._waiting_spec[k] = req.spec
+
+    def _release(self, req):
+        k = req.spec.key
+        self._waiting[k] -= 1
+        if self._waiting[k] <= 0:
+            del self._waiting[k]
+            self._waiting_spec.pop(k, None)
+
     # ------------------------------------------------------------------ set-up
     def _device_setup(self, spec):
         blk = Block(spec.conn, spec.etype, LinearElastic(spec.material.E, spec.material.nu), X=spec.X)
@@ -243,7 +261,7 @@ class SolveServer:
         with self._cv:
             while self.resident_bytes + need > self.budget:
                 victim = next((k for k, e in self._entries.items()
-                               if not e.busy and not any(r.spec.key == k for r in self._pending)), None)
+                               if not e.busy and not self._waiting[k]), None)
                 if victim is None:
                     if not self._entries:
                         break                                 # an entry larger than the budget runs alone
@@ -272,8 +290,8 @@ class SolveServer:
                 while spec is None:
                     if self._stop:
                         return
-                    spec = next((r.spec for r in self._pending
-                                 if r.spec.key not in self._entries and r.spec.key not in self._setting_up), None)
+                    spec = next((sp for k, sp in self._waiting_spec.items()
+                                 if k not in self._entries and k not in self._setting_up), None)
                     if spec is None:
                         self._cv.wait(0.05)
             try:
@@ -282,6 +300,7 @@ class SolveServer:
                 with self._cv:
                     for r in [r for r in self._pending if r.spec.key == spec.key]:
                         self._pending.remove(r)
+                        self._release(r)
                         self._futures.pop(r.id).set_exception(exc)
 
     # ------------------------------------------------------------------ solving
@@ -315,6 +334,7 @@ class SolveServer:
                     if req is None:
                         self._cv.wait(0.05)
                 self._pending.remove(req)
+                self._release(req)
                 entry.busy = True
                 entry.last_used = time.time()
                 self._entries.move_to_end(req.spec.key)
