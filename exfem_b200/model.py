@@ -169,10 +169,11 @@ class Block:
             return
         s = np.ascontiguousarray(np.asarray(scale.cpu() if isinstance(scale, torch.Tensor) else scale,
                                             dtype=np.float64).reshape(-1))
-        key = (s.size, hash(s.tobytes()))
-        if key != self._scale_key:
+        # compared with a kept copy of the last one set (a memory compare, cheaper
+        # than hashing the array on every call)
+        if self._scale_key is None or self._scale_key.shape != s.shape or not np.array_equal(self._scale_key, s):
             check(lib.exfem_block_set_scale(self.handle, s.ctypes.data))
-            self._scale_key = key
+            self._scale_key = s.copy()
 
     def set_lame(self, lam, mu):
         """Per-element Lame parameters of the matrix-free operator (a block holding
@@ -194,11 +195,11 @@ class Block:
                 check(lib.exfem_block_set_fixed(self.handle, None))
                 self._fixed_key = None
             return
-        f = np.ascontiguousarray(np.asarray(fixed).astype(np.uint8).reshape(-1))
-        key = hash(f.tobytes())
-        if key != self._fixed_key:
+        f = np.ascontiguousarray(np.asarray(fixed).reshape(-1)).view(np.uint8) if np.asarray(fixed).dtype == bool \
+            else np.ascontiguousarray(np.asarray(fixed).astype(np.uint8).reshape(-1))
+        if self._fixed_key is None or self._fixed_key.shape != f.shape or not np.array_equal(self._fixed_key, f):
             check(lib.exfem_block_set_fixed(self.handle, f.ctypes.data))
-            self._fixed_key = key
+            self._fixed_key = f.copy()
 
     # ---------------- kernels on global vectors
     def internal_force(self, u, state, assembly=_lib.ASSEMBLE_GATHER, fe=None):

@@ -101,20 +101,38 @@ class _Setup:                                                           # solver
             d = model.dof(nodes, dof)
             self.fixed[d] = True
             self.target[d] = val
-        g = np.zeros(nd)
-        for ld in step.loads:
-            nodes, dof, val = ld[:3]
-            np.add.at(g, model.dof(nodes, dof), val)
+        # point loads summed on the host (few entries), distributed load vectors
+        # summed on the device; masks and targets scattered on the device from the
+        # prescribed DOFs, so only index-sized arrays and the load vectors cross PCIe
+        g = torch.zeros(nd, dtype=torch.float64, device="cuda")
+        if step.loads:
+            gp = np.zeros(nd)
+            for ld in step.loads:
+                nodes, dof, val = ld[:3]
+                np.add.at(gp, model.dof(nodes, dof), val)
+            nz = np.nonzero(gp)[0]
+            g[torch.as_tensor(nz, device="cuda")] = torch.as_tensor(gp[nz], device="cuda")
         for dl in step.dloads:
             vec = dl[0] if isinstance(dl, (tuple, list)) else dl
-            g += np.asarray(vec.cpu() if isinstance(vec, torch.Tensor) else vec, float)
-        self.group = torch.as_tensor(g, device="cuda")
+            g += torch.as_tensor(np.asarray(vec, float) if not isinstance(vec, torch.Tensor) else vec,
+                                 dtype=torch.float64, device="cuda").reshape(-1)
+        self.group = g
         self.fprev = state.fext
         self.ustart = state.u.clone()
-        self.free_np = (~self.fixed).astype(float)
-        self.free = torch.as_tensor(self.free_np, device="cuda")
-        self.fixed_j = torch.as_tensor(self.fixed, device="cuda")
-        self.target_j = torch.as_tensor(self.target, device="cuda")
+        idx = np.nonzero(self.fixed)[0]
+        idx_j = torch.as_tensor(idx, device="cuda")
+        self.fixed_j = torch.zeros(nd, dtype=torch.bool, device="cuda")
+        self.fixed_j[idx_j] = True
+        self.target_j = torch.zeros(nd, dtype=torch.float64, device="cuda")
+        self.target_j[idx_j] = torch.as_tensor(self.target[idx], device="cuda")
+        self.free = (~self.fixed_j).to(torch.float64)
+        self._free_np = None
+
+    @property
+    def free_np(self):
+        if self._free_np is None:
+            self._free_np = (~self.fixed).astype(float)
+        return self._free_np
 
     def fext(self, t):
         r = _ramp(t, self.step.T)
