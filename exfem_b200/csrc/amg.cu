@@ -21,7 +21,10 @@
 
 namespace exfem {
 
-enum SpmvMode { SP_SET = 0, SP_ADD = 1, SP_RES = 2, SP_RESINIT = 3, SP_CHEB = 4 };
+// SP_CHEBLAST: the last Chebyshev step of a smoothing, which also adds the new
+// direction to x (x = (x + d) + d2) and stores neither r nor d2; SP_SETDIFF (block
+// products): y = M (b - x), the restriction of a residual whose product A x is in x.
+enum SpmvMode { SP_SET = 0, SP_ADD = 1, SP_RES = 2, SP_RESINIT = 3, SP_CHEB = 4, SP_CHEBLAST = 5, SP_SETDIFF = 6 };
 
 template <class T, int LANES, int MODE>
 __global__ void __launch_bounds__(256)
@@ -30,6 +33,7 @@ spmv_kernel(int64_t n, const int64_t* __restrict__ ptr, const int32_t* __restric
             const T* __restrict__ b, const T* __restrict__ dinv, T* __restrict__ d2,
             T* __restrict__ xo, T c1, T c2, const T* __restrict__ rc1, const T* __restrict__ rc2,
             const int64_t* __restrict__ rmap, const int64_t* __restrict__ cshift, const int* __restrict__ skip) {
+  static_assert(MODE <= SP_CHEB, "the scalar product has the first five modes only");
   if (skip && *skip) return;
   constexpr int GPW = 32 / LANES;  // row groups per warp
   const int lane = threadIdx.x & (LANES - 1);
@@ -143,6 +147,12 @@ bsr_kernel(int64_t nb, const int64_t* __restrict__ ptr, const int32_t* __restric
         T v[R * C], xv[C];
         load_regs<T, R * C, stride_align<T, R * C>()>(val + k * (R * C), v);
         load_regs<T, C, stride_align<T, C>()>(x + (int64_t)idx[k] * C, xv);
+        if constexpr (MODE == SP_SETDIFF) {
+          T bv[C];
+          load_regs<T, C, stride_align<T, C>()>(b + (int64_t)idx[k] * C, bv);
+#pragma unroll
+          for (int j = 0; j < C; ++j) xv[j] = bv[j] - xv[j];
+        }
 #pragma unroll
         for (int i = 0; i < R; ++i)
 #pragma unroll
@@ -168,12 +178,19 @@ bsr_kernel(int64_t nb, const int64_t* __restrict__ ptr, const int32_t* __restric
           const T r = dinv[row] * (b[row] - sv);
           y[row] = r;
           d2[row] = r * c1;
-        } else {  // SP_CHEB: x is the direction d
+        } else if (MODE == SP_CHEB) {  // x is the direction d
           const T d = x[row];
           xo[row] += d;
           const T r = y[row] - dinv[row] * sv;
           y[row] = r;
           d2[row] = c1 * d + c2 * r;
+        } else if (MODE == SP_CHEBLAST) {
+          const T d = x[row];
+          const T r = y[row] - dinv[row] * sv;
+          const T dn = c1 * d + c2 * r;
+          xo[row] = (xo[row] + d) + dn;
+        } else {  // SP_SETDIFF
+          y[row] = sv;
         }
       }
     }
@@ -184,7 +201,8 @@ template <class T, int R, int C, int MODE>
 static int bsr_launch(const Bsr& M, const T* val, const T* x, T* y, const T* b, const T* dinv, T* d2, T* xo, T c1,
                        T c2, const int* skip, cudaStream_t s) {
   // the vector loads of the kernel assume the alignment of a 256-byte aligned array
-  if ((uintptr_t)x % stride_align<T, C>() || (uintptr_t)val % stride_align<T, R * C>()) {
+  if ((uintptr_t)x % stride_align<T, C>() || (uintptr_t)val % stride_align<T, R * C>() ||
+      (MODE == SP_SETDIFF && (uintptr_t)b % stride_align<T, C>())) {
     set_error("block-sparse product: misaligned operand (x %p, blocks %p)", (const void*)x, (const void*)val);
     return EXFEM_ERR_ARG;
   }
@@ -244,14 +262,19 @@ template <class T>
 __global__ void cheb_update_kernel(int64_t n, T* __restrict__ x, const T* __restrict__ d, T* __restrict__ r,
                                    const T* __restrict__ Ad, const T* __restrict__ dinv, T* __restrict__ d2,
                                    T c1, T c2, const int* __restrict__ skip, const T* __restrict__ rc1 = nullptr,
-                                   const T* __restrict__ rc2 = nullptr) {
+                                   const T* __restrict__ rc2 = nullptr, int last = 0) {
   if (skip && *skip) return;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const T di = d[i];
-    x[i] += di;
     const T ri = r[i] - dinv[i] * Ad[i];
-    r[i] = ri;
-    d2[i] = (rc1 ? rc1[5 * i] : c1) * di + (rc2 ? rc2[5 * i] : c2) * ri;
+    const T dn = (rc1 ? rc1[5 * i] : c1) * di + (rc2 ? rc2[5 * i] : c2) * ri;
+    if (last) {  // the smoothing's last step: x = (x + d) + d2, r and d2 not kept
+      x[i] = (x[i] + di) + dn;
+    } else {
+      x[i] += di;
+      r[i] = ri;
+      d2[i] = dn;
+    }
   }
 }
 
@@ -402,16 +425,26 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
   const unsigned eg = grid_for(n, 256);
   const T* vals = csr_vals<T>(L.A);
   int st;
+  // the last step of the matrix-free and block-sparse smoothings adds the final
+  // direction itself (x = (x + d) + d2); the scalar-CSR smoothing adds it after
   auto smooth_steps = [&]() -> int {
+    const bool fused_last = mf || useA;
     for (int j = 0; j < h->degree; ++j) {
+      const bool last = fused_last && j == h->degree - 1;
       if (mf) {
         if ((st = op0->apply(op0->ctx, d, t, skip, s))) return st;
         cheb_update_kernel<T><<<eg, 256, 0, s>>>(n, x, d, r, t, dinv, d2, (T)ca[j], (T)cb[j], skip,
-                                                 rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr);
+                                                 rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr,
+                                                 last ? 1 : 0);
         EX_LAUNCH_CHECK();
       } else {
         if (useA) {
-          if ((st = bsr_apply<T, SP_CHEB>(L.bA, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s))) return st;
+          if (last) {
+            if ((st = bsr_apply<T, SP_CHEBLAST>(L.bA, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s)))
+              return st;
+          } else if ((st = bsr_apply<T, SP_CHEB>(L.bA, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s))) {
+            return st;
+          }
         } else if ((st = spmv_lanes<T, SP_CHEB>(L.A, vals, d, r, nullptr, dinv, d2, x, (T)ca[j], (T)cb[j], skip, s,
                                                 rc ? rc + 2 * j : nullptr, rc ? rc + 2 * j + 1 : nullptr))) {
           return st;
@@ -419,8 +452,10 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
       }
       std::swap(d, d2);
     }
-    add_kernel<T><<<eg, 256, 0, s>>>(n, d, x, skip);
-    EX_LAUNCH_CHECK();
+    if (!(fused_last && h->degree > 0)) {
+      add_kernel<T><<<eg, 256, 0, s>>>(n, d, x, skip);
+      EX_LAUNCH_CHECK();
+    }
     return EXFEM_OK;
   };
   // pre-smoothing from x = 0
@@ -430,8 +465,10 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
   // residual and restriction
   if (mf) {
     if ((st = op0->apply(op0->ctx, x, t, skip, s))) return st;
-    sub_kernel<T><<<eg, 256, 0, s>>>(n, b, t, skip);
-    EX_LAUNCH_CHECK();
+    if (!useT) {  // the block-sparse restriction below forms b - t itself
+      sub_kernel<T><<<eg, 256, 0, s>>>(n, b, t, skip);
+      EX_LAUNCH_CHECK();
+    }
   } else {
     if (useA) {
       if ((st = bsr_apply<T, SP_RES>(L.bA, x, t, b, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
@@ -450,7 +487,11 @@ static int vcycle_level(exfem_amg_s* h, size_t l, const T* b, T* x, const Level0
     else { bc = (T*)h->cb32.p; xc = (T*)h->cx32.p; }
   }
   if (useT) {
-    if ((st = bsr_apply<T, SP_SET>(L.bR, t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+    if (mf) {
+      if ((st = bsr_apply<T, SP_SETDIFF>(L.bR, t, bc, b, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) return st;
+    } else if ((st = bsr_apply<T, SP_SET>(L.bR, t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0), skip, s))) {
+      return st;
+    }
   } else if ((st = spmv_lanes<T, SP_SET>(L.R, csr_vals<T>(L.R), t, bc, nullptr, nullptr, nullptr, nullptr, T(0), T(0),
                                          skip, s))) {
     return st;
