@@ -86,6 +86,7 @@ _SIGS = {
     "exfem_solver_refresh_diagonal": ([VP, VP], C.c_int),
     "exfem_solver_cheby_bound": ([VP, C.POINTER(D)], C.c_int),
     "exfem_solver_set_graph": ([VP, C.c_int, C.c_int], C.c_int),
+    "exfem_solver_set_loop": ([VP, C.c_int], C.c_int),
     "exfem_solver_pcg": ([VP, P, P, D, C.c_int, C.POINTER(I32), C.POINTER(D), VP], C.c_int),
     "exfem_solver_mixed": ([VP, P, P, D, D, C.c_int, C.c_int, C.POINTER(I32), C.POINTER(I32), C.POINTER(D), VP],
                            C.c_int),

@@ -710,6 +710,14 @@ int exfem_solver_set_graph(exfem_solver s, int enable, int chunk) {
   return EXFEM_OK;
 }
 
+int exfem_solver_set_loop(exfem_solver s, int device_loop) {
+  EX_ARG(s, "solver is NULL");
+  for (auto& g : s->gexec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  s->device_loop = device_loop ? 1 : 0;
+  return EXFEM_OK;
+}
+
 int exfem_solver_pcg(exfem_solver s, const double* b, double* x, double tol, int maxiter, int* iters, double* relres,
                      void* stream) {
   EX_ARG(s && b && x, "NULL argument");

@@ -281,6 +281,17 @@ __global__ void segment_scal_kernel(PcgScal* sc, double tol, int maxiter) {
   sc->done = 0;
 }
 
+// Condition of the device-side iteration loop (the conditional while node of the
+// PCG graph): run the body again while the recursion is not done.  `pad` counts the
+// passes of this launch; maxiter + 2 passes end the loop even if the done flag were
+// never set, so the loop always terminates.
+__global__ void loop_cond_kernel(cudaGraphConditionalHandle h, PcgScal* sc, int head) {
+  if (head) sc->pad = 0;
+  else sc->pad += 1;
+  const bool more = !sc->done && sc->k < sc->maxiter && (long long)sc->pad <= (long long)sc->maxiter + 1;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
 __global__ void scale_f32_kernel(int64_t n, float* __restrict__ v, float a) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     v[i] *= a;
@@ -518,8 +529,59 @@ int solver_refresh_diagonal(exfem_solver_s* S, cudaStream_t st) {
   return EXFEM_OK;
 }
 
+// Graph of the whole PCG loop: a head kernel sets the loop condition from the
+// device scalars, then a conditional while node runs one captured iteration plus
+// the condition kernel until the recursion is done (or maxiter + 2 passes)
+template <class T>
+static int loop_graph(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* out) {
+  cudaGraph_t g = nullptr;
+  EX_CUDA(cudaGraphCreate(&g, 0));
+  auto fail = [&](cudaError_t e, const char* what) {
+    cudaGraphDestroy(g);
+    set_error("PCG loop graph: %s: %s", what, cudaGetErrorString(e));
+    return EXFEM_ERR_CUDA;
+  };
+  cudaGraphConditionalHandle h;
+  cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 0, 0);
+  if (e != cudaSuccess) return fail(e, "condition handle");
+  PcgScal* sc = S->scal.p;
+  int head = 1;
+  void* args[] = {&h, &sc, &head};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void*)loop_cond_kernel;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(1);
+  kp.kernelParams = args;
+  cudaGraphNode_t n_head, n_loop;
+  if ((e = cudaGraphAddKernelNode(&n_head, g, nullptr, 0, &kp)) != cudaSuccess) return fail(e, "head node");
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if ((e = cudaGraphAddNode(&n_loop, g, &n_head, 1, &cp)) != cudaSuccess) return fail(e, "while node");
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if ((e = cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)) !=
+      cudaSuccess)
+    return fail(e, "capture of the loop body");
+  int cs = pcg_iteration<T>(S, st);
+  if (!cs) {
+    loop_cond_kernel<<<1, 1, 0, st>>>(h, sc, 0);
+    if (cudaGetLastError() != cudaSuccess) cs = EXFEM_ERR_CUDA;
+  }
+  cudaGraph_t captured = nullptr;
+  e = cudaStreamEndCapture(st, &captured);
+  if (cs) {
+    cudaGraphDestroy(g);
+    return cs;
+  }
+  if (e != cudaSuccess) return fail(e, "end of the body capture");
+  *out = g;
+  return EXFEM_OK;
+}
+
 // hierarchy work vectors, inverse diagonal of the current operator, and (graphs
-// on) the captured chunk of PCG iterations in precision T
+// on) the captured PCG iterations in precision T
 template <class T>
 static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
   const int gi = sizeof(T) == 8 ? 0 : 1;
@@ -556,16 +618,21 @@ static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
     }
     if (!S->gexec[gi]) {
       CaptureScope cap;
-      cudaGraph_t g;
-      EX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      int cs = EXFEM_OK;
-      for (int i = 0; i < chunk && !cs; ++i) cs = pcg_iteration<T>(S, st);
-      cudaError_t ce = cudaStreamEndCapture(st, &g);
-      if (cs) { if (ce == cudaSuccess) cudaGraphDestroy(g); return cs; }
-      EX_CUDA(ce);
-      ce = cudaGraphInstantiate(&S->gexec[gi], g, 0);
+      cudaGraph_t g = nullptr;
+      if (S->device_loop) {
+        if ((s = loop_graph<T>(S, st, &g))) return s;
+      } else {
+        EX_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int cs = EXFEM_OK;
+        for (int i = 0; i < chunk && !cs; ++i) cs = pcg_iteration<T>(S, st);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (cs) { if (ce == cudaSuccess) cudaGraphDestroy(g); return cs; }
+        EX_CUDA(ce);
+      }
+      cudaError_t ce = cudaGraphInstantiate(&S->gexec[gi], g, 0);
       cudaGraphDestroy(g);
       EX_CUDA(ce);
+      S->gloop[gi] = S->device_loop != 0;
       S->g_Ke[gi] = keptr;
       S->g_lmax[gi] = S->cheb_lmax;
     }
@@ -580,6 +647,12 @@ static int pcg_chunks(exfem_solver_s* S, int maxiter, cudaStream_t st) {
   const int gi = sizeof(T) == 8 ? 0 : 1;
   const int chunk = S->chunk > 0 ? S->chunk : 8;
   int s;
+  if (S->use_graph && S->gexec[gi] && S->gloop[gi]) {  // one launch runs the loop to the end
+    EX_CUDA(cudaGraphLaunch(S->gexec[gi], st));
+    EX_CUDA(cudaMemcpyAsync(S->h_scal, S->scal.p, sizeof(PcgScal), cudaMemcpyDeviceToHost, st));
+    EX_CUDA(cudaStreamSynchronize(st));
+    return EXFEM_OK;
+  }
   const int max_chunks = maxiter / chunk + 2;
   for (int c = 0; c < max_chunks; ++c) {
     EX_CUDA(cudaMemcpyAsync(S->h_scal, S->scal.p, sizeof(PcgScal), cudaMemcpyDeviceToHost, st));

@@ -123,9 +123,13 @@ struct exfem_solver_s {
   int mixed_mode = 1;  // exfem_solver_mixed: 1 = reliable updates, 0 = restarted refinement (the reference's)
   double mixed_delta = 0.1;  // reliable updates: replace the residual after this reduction
   uint64_t diag_tan_gen = 0, diag_bc_gen = 0, graph_bc_gen = 0;
-  // CUDA graphs of `chunk` PCG iterations, one per precision
-  int use_graph = 1, chunk = 8;
+  // CUDA graphs of the PCG iterations, one per precision: with device_loop a
+  // graph whose conditional while node repeats one iteration until the device
+  // scalars say done (no host round trips between iterations), else a graph of
+  // `chunk` iterations launched from the host until done
+  int use_graph = 1, chunk = 8, device_loop = 1;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  bool gloop[2] = {false, false};
   std::vector<const double*> g_Ke[2];
   ~exfem_solver_s();
 };

@@ -441,11 +441,13 @@ class NativeSolver:
     PCS = {"none": _lib.PC_NONE, "jacobi": _lib.PC_JACOBI, "amg": _lib.PC_AMG, "cheby": _lib.PC_CHEBY}
 
     def __init__(self, block, op="mf32", pc="amg", amg=None, graph=True, chunk=8, mixed_mode="reliable",
-                 mixed_delta=0.1):
+                 mixed_delta=0.1, device_loop=True):
         """mixed_mode: how :meth:`mixed` runs its FP32 work — "reliable" (one FP32
         recursion whose residual is replaced by the FP64 one after each reduction by
         mixed_delta) or "restart" (the reference's restarted refinement,
-        gfem/solvers.py:344-384)."""
+        gfem/solvers.py:344-384).  device_loop (with graph): the PCG loop runs to its
+        stopping test inside one graph launch (conditional while node); False
+        launches graphs of `chunk` iterations from the host."""
         self.blocks = list(block) if isinstance(block, (list, tuple)) else [block]
         self.block, self.amg = self.blocks[0], amg
         self.op, self.pc = op, pc
@@ -456,6 +458,7 @@ class NativeSolver:
         for b in self.blocks[1:]:
             check(lib.exfem_solver_add_block(h, b.handle))
         check(lib.exfem_solver_set_graph(h, 1 if graph else 0, chunk))
+        check(lib.exfem_solver_set_loop(h, 1 if device_loop else 0))
         check(lib.exfem_solver_set_mixed_mode(h, {"reliable": 1, "restart": 0}[mixed_mode], float(mixed_delta)))
         self._Ke = None
         self.last_iters = 0

@@ -315,8 +315,14 @@ int exfem_solver_refresh_diagonal(exfem_solver s, void* stream);
  * the operator's tangent or prescribed DOFs change; 0 before the first solve). */
 int exfem_solver_cheby_bound(exfem_solver s, double* lmax);
 /* Use CUDA graphs for the PCG iteration loop (default on) and the number of
- * iterations captured per graph launch. */
+ * iterations captured per graph launch (host-driven loop only). */
 int exfem_solver_set_graph(exfem_solver s, int enable, int chunk);
+/* With graphs on: 1 (default) runs the whole PCG loop inside one graph launch, a
+ * conditional while node repeating one captured iteration until the device-side
+ * stopping test (r.r <= tol^2 b.b or k >= maxiter) ends it, so no host round trip
+ * falls between iterations; 0 launches graphs of `chunk` iterations from the host
+ * and reads the stopping test after each. */
+int exfem_solver_set_loop(exfem_solver s, int device_loop);
 /* PCG in the operator's precision with FP64 scalars and dot products
  * (gfem/linalg.py:21-47): x0 = 0, stop when r.r <= tol^2 b.b or k >= maxiter.
  * b, x: FP64 device (ndof).  Synchronises the stream to read the iteration count.

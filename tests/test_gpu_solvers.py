@@ -95,6 +95,40 @@ def test_graph_and_eager_pcg_agree(cuda):
     np.testing.assert_array_equal(res[0][0], res[1][0])       # deterministic reductions
 
 
+def test_device_loop_matches_host_driven_loop(cuda):
+    """The PCG loop run to its stopping test inside one graph launch (conditional
+    while node) gives the same iterates, bit for bit, as graphs of 8 iterations
+    launched from the host and as eager launches; an iteration limit ends it."""
+    from exfem_b200 import linalg
+    X, c, bcs, loads, pm, om = _config1()
+    blk = pm.blocks[0]
+    setup = osol.Setup(om, osol.Step(bcs=bcs, loads=loads))
+    blk.set_fixed(setup.fixed)
+    blk.tangent_update(torch.zeros(pm.ndof, device="cuda"), pm.init_state()[0])
+    ops = [(d, K.numpy()) for d, K in om.stiffness_ops(torch.zeros(om.ndof, dtype=torch.float64), om.init_state())]
+    import exfem_b200 as xf
+    amg = xf.AMG(olin.bc_matrix(ofem.ops_assemble(ops, om.ndof), setup.free), X)
+    b = torch.as_tensor(np.random.default_rng(3).standard_normal(pm.ndof) * setup.free, device="cuda")
+    modes = [dict(graph=True, device_loop=True), dict(graph=True, device_loop=False), dict(graph=False)]
+    for op in ("mf64", "mf32"):
+        res = []
+        for kw in modes:
+            S = linalg.NativeSolver(blk, op, "amg", amg, **kw)
+            if op == "mf64":
+                x, k, rr = S.pcg(b, tol=1e-10)
+                res.append((x.cpu().numpy(), k))
+                xl, kl, _ = S.pcg(b, tol=1e-14, maxiter=3)
+                assert kl == 3
+            else:
+                x, k, p, rel = S.mixed(b, tol=1e-9)
+                res.append((x.cpu().numpy(), (k, p)))
+                assert rel < 1e-9
+        for x, k in res[1:]:
+            assert k == res[0][1]
+            np.testing.assert_array_equal(x, res[0][0])
+    blk.set_fixed(None)
+
+
 def _j2_case(dt):
     import exfem_b200 as xf
     from exfem_b200 import mesh
