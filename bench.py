@@ -562,9 +562,11 @@ def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), 
 
 def stored_ke_section(n=(160, 40, 40), reps=20):
     """Multi-right-hand-side products on one C3D8 mesh (n hexahedra, jittered,
-    linear elastic, x = 0 clamped): the BF16 stored-Ke tensor-core product for 4
-    and 16 right-hand sides against the FP32 matrix-free product applied to each
-    right-hand side.  Reported as DOF x right-hand sides x products / s."""
+    linear elastic, x = 0 clamped): the BF16 stored-Ke product for 4 and 16
+    right-hand sides on the tensor cores ("tc") and on the CUDA cores ("cuda")
+    against the FP32 matrix-free product applied to each right-hand side, and the
+    FP64 stored-Ke product of 4 and 16 right-hand sides against the single one.
+    Reported as DOF x right-hand sides x products / s."""
     import torch
     import exfem_b200 as xf
     from exfem_b200 import mesh
@@ -595,13 +597,27 @@ def stored_ke_section(n=(160, 40, 40), reps=20):
     v = torch.randn(m.ndof, dtype=torch.float32, device="cuda")
     ms_mf = timed(lambda: blk.tangent_matvec(v))
     out["mf_fp32_ms_per_rhs"] = ms_mf
+    pk, _ = peaks()
+    # algorithmic bytes per product: Ke once, V read and Y written once per DOF and
+    # right-hand side, the element rows written and read back by the node sums
     for nr in (4, 16):
         V = torch.randn(m.ndof, nr, dtype=torch.float32, device="cuda")
-        ms = timed(lambda: blk.ebe_matvec_multi(Kb, V))
-        out[f"tc_bf16_{nr}rhs"] = dict(ms=ms, dof_rhs_per_s=m.ndof * nr / (ms * 1e-3),
-                                       mf_fp32_dof_rhs_per_s=m.ndof / (ms_mf * 1e-3),
-                                       speedup_vs_mf=ms_mf * nr / ms,
-                                       ke_gbs=Kb.numel() * 2 / (ms * 1e-3) / 1e9)
+        for eng in ("tc", "cuda"):
+            ms = timed(lambda: blk.ebe_matvec_multi(Kb, V, engine=eng))
+            alg = Kb.numel() * 2 + 2 * 4 * m.ndof * nr + 2 * 4 * Kb.shape[0] * Kb.shape[1] * nr
+            out[f"{eng}_bf16_{nr}rhs"] = dict(ms=ms, dof_rhs_per_s=m.ndof * nr / (ms * 1e-3),
+                                              mf_fp32_dof_rhs_per_s=m.ndof / (ms_mf * 1e-3),
+                                              speedup_vs_mf=ms_mf * nr / ms,
+                                              ke_gbs=Kb.numel() * 2 / (ms * 1e-3) / 1e9,
+                                              hbm_frac=alg / (ms * 1e-3) / 1e9 / pk)
+    K64 = blk.stiffness(zero, blk.init_state())
+    v64 = torch.randn(m.ndof, dtype=torch.float64, device="cuda")
+    ms1 = timed(lambda: blk.ebe_matvec(K64, v64))
+    for nr in (4, 16):
+        V = torch.randn(m.ndof, nr, dtype=torch.float64, device="cuda")
+        ms = timed(lambda: blk.ebe_matvec_multi(K64, V))
+        out[f"cuda_fp64_{nr}rhs"] = dict(ms=ms, single_rhs_fp64_ms=ms1, speedup_vs_single=ms1 * nr / ms,
+                                         ke_gbs=K64.numel() * 8 / (ms * 1e-3) / 1e9)
     return out
 
 

@@ -69,6 +69,8 @@ _SIGS = {
     "exfem_tangent_diagonal": ([VP, P, VP], C.c_int),
     "exfem_ebe_matvec": ([VP, P, P, P, C.c_int, VP], C.c_int),
     "exfem_ebe_matvec_bf16_multi": ([VP, P, I32, P, P, I32, VP], C.c_int),
+    "exfem_ebe_matvec_multi": ([VP, VP, C.c_int, C.c_int, VP, VP, C.c_int, VP], C.c_int),
+    "exfem_multi_pcg": ([VP, VP, C.c_int, VP, VP, C.c_double, C.c_int, VP, VP, VP], C.c_int),
     "exfem_ebe_diagonal": ([VP, P, P, VP], C.c_int),
     "exfem_stresses": ([VP, P, P, P, P, P, VP], C.c_int),
     "exfem_geometric_stiffness": ([VP, P, P, VP], C.c_int),

@@ -518,6 +518,25 @@ int exfem_ebe_matvec_bf16_multi(exfem_block b, const void* Ke_bf16, int nrhs, co
   return launch_ebe_matvec_tc(b, (const __nv_bfloat16*)Ke_bf16, nrhs, V, Y, g.work, apply_bc != 0);
 }
 
+int exfem_ebe_matvec_multi(exfem_block b, const void* Ke, int ke_dtype, int nrhs, const void* V, void* Y,
+                           int apply_bc, void* stream) {
+  EX_ARG(b && (b->ne == 0 || Ke) && V && Y, "NULL argument");
+  StreamGuard g;
+  int s;
+  if ((s = g.init(stream))) return s;
+  return launch_ebe_matvec_multi(b, Ke, ke_dtype, nrhs, V, Y, apply_bc != 0, g.work);
+}
+
+int exfem_multi_pcg(exfem_block b, const double* Ke, int nrhs, const double* B, double* X, double tol, int maxiter,
+                    int* iters, double* relres, void* stream) {
+  EX_ARG(b && (b->ne == 0 || Ke) && B && X, "NULL argument");
+  EX_ARG(tol > 0 && maxiter >= 0, "tolerance must be positive and maxiter non-negative");
+  StreamGuard g;
+  int s;
+  if ((s = g.init(stream))) return s;
+  return multi_pcg(b, Ke, nrhs, B, X, tol, maxiter, iters, relres, g.work);
+}
+
 int exfem_ebe_matvec(exfem_block b, const double* Ke, const double* v, double* y, int apply_bc, void* stream) {
   EX_ARG(b && Ke && v && y, "NULL argument");
   return launch_ebe_matvec(b, Ke, v, y, nullptr, as_stream(stream), apply_bc != 0);

@@ -296,61 +296,6 @@ ebe_tc_kernel(int64_t ne, const int32_t* __restrict__ conn, const __nv_bfloat16*
   }
 }
 
-// y[3n+c, r] = fixed ? v : sum over node n's gather-plan slots of the element rows;
-// one thread per node and group of four right-hand sides (16-byte loads and stores)
-// when nrhs is a multiple of 4, else per node and right-hand side
-__global__ void gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32_t* __restrict__ plan,
-                                    int64_t sentinel, const float* __restrict__ ys, const uint8_t* __restrict__ fixed,
-                                    const float* __restrict__ V, int nrhs, float* __restrict__ Y) {
-  const int nd = 3 * nnode;
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if ((nrhs & 3) == 0) {
-    const int nq = nrhs >> 2;
-    if (t >= nn * nq) return;
-    const int64_t n = t / nq;
-    const int r4 = (int)(t - n * nq) * 4;
-    float4 s[3] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0)};
-    for (int k = 0; k < vmax; ++k) {
-      const int64_t slot = plan[n * vmax + k];
-      if (slot == sentinel) break;
-      const int64_t e = slot / nnode;
-      const int a = (int)(slot - e * nnode);
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float4 w = *reinterpret_cast<const float4*>(ys + (e * nd + 3 * a + c) * nrhs + r4);
-        s[c].x += w.x;
-        s[c].y += w.y;
-        s[c].z += w.z;
-        s[c].w += w.w;
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const int64_t d = 3 * n + c;
-      float4* out = reinterpret_cast<float4*>(Y + d * nrhs + r4);
-      *out = (fixed && fixed[d]) ? *reinterpret_cast<const float4*>(V + d * nrhs + r4) : s[c];
-    }
-    return;
-  }
-  if (t >= nn * nrhs) return;
-  const int64_t n = t / nrhs;
-  const int r = (int)(t - n * nrhs);
-  float s[3] = {0.f, 0.f, 0.f};
-  for (int k = 0; k < vmax; ++k) {
-    const int64_t slot = plan[n * vmax + k];
-    if (slot == sentinel) break;
-    const int64_t e = slot / nnode;
-    const int a = (int)(slot - e * nnode);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) s[c] += ys[(e * nd + 3 * a + c) * nrhs + r];
-  }
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const int64_t d = 3 * n + c;
-    Y[d * nrhs + r] = (fixed && fixed[d]) ? V[d * nrhs + r] : s[c];
-  }
-}
-
 template <int ET>
 static int tc_launch(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, const float* V, const uint8_t* fx,
                      cudaStream_t s) {
@@ -394,13 +339,7 @@ int launch_ebe_matvec_tc(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, co
                                           : tc_launch<EXFEM_C3D10>(b, Ke, nrhs, V, fx, s);
     if (st) return st;
   }
-  const int64_t work = (nrhs & 3) == 0 ? b->nn * (nrhs / 4) : b->nn * nrhs;
-  if (work) {
-    gather_multi_kernel<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(
-        b->nn, b->vmax, b->nnode, b->plan.p, b->ne * b->nnode, b->ys_tc.p, bc ? b->fixed.p : nullptr, V, nrhs, Y);
-    EX_LAUNCH_CHECK();
-  }
-  return EXFEM_OK;
+  return launch_gather_multi<float>(b, b->ys_tc.p, V, Y, nrhs, bc, s);
 }
 
 }  // namespace exfem

@@ -68,6 +68,8 @@ struct exfem_block_s {
   uint64_t tan_gen = 0, bc_gen = 0;
   // scratch
   exfem::DevBuf<double> ys;           // (ne*nnode*3) element vectors for gather assembly
+  exfem::DevBuf<double> mp_work;      // multi-case Jacobi PCG: inverse diagonal, R, P, Q, partial sums, scalars
+  exfem::DevBuf<double> ys_m64;       // (ne*nnode*3*nrhs) element rows of the FP64 multi-right-hand-side product
   exfem::DevBuf<float> ys_tc;         // (ne*nnode*3*nrhs) element rows of the tensor-core stored-Ke product
   int64_t ndof() const { return 3 * nn; }
 };
@@ -109,6 +111,15 @@ int launch_wait_selftest(int polls, int* err, cudaStream_t s);
 // stored-Ke product for several right-hand sides on the tensor cores (ebe_tc.cu)
 int launch_ebe_matvec_tc(exfem_block_s* b, const __nv_bfloat16* Ke, int nrhs, const float* V, float* Y,
                          cudaStream_t s, bool bc);
+// multi-right-hand-side stored-Ke product on the CUDA cores (ebe_multi.cu); Ke in
+// EXFEM_BF16 / EXFEM_F32 (V, Y FP32) or EXFEM_F64 (V, Y FP64)
+int launch_ebe_matvec_multi(exfem_block_s* b, const void* Ke, int ke_dtype, int nrhs, const void* V, void* Y,
+                            bool bc, cudaStream_t s);
+// multi-case Jacobi PCG with stored FP64 Ke (ebe_multi.cu): B, X (ndof, nrhs) FP64
+int multi_pcg(exfem_block_s* b, const double* Ke, int nrhs, const double* B, double* X, double tol, int maxiter,
+              int* iters, double* relres, cudaStream_t s);
+template <class VT>
+int launch_gather_multi(exfem_block_s* b, const VT* ys, const VT* V, VT* Y, int nrhs, bool bc, cudaStream_t s);
 
 // reductions and vector kernels (krylov.cu)
 enum ModeForce { FORCE_FULL = 0, FORCE_TANGENT = 1, FORCE_STRESS = 2 };

@@ -10,8 +10,10 @@ the stiffness K0 at u = 0; T = a device V-cycle of K0), lambda = -1/mu.
 K phi = w^2 M phi for the smallest eigenvalues: A = the block's FP64 matrix-free
 tangent product (prescribed DOFs held at zero), B = the HRZ-lumped mass matrix
 (gfem/model.py:120-124, 501-510), T = one smoothed-aggregation V-cycle of the
-stiffness (hierarchy set up on the device).  Every A and T application is a call of
-the library per column; the block Rayleigh-Ritz steps are small dense products on
+stiffness (hierarchy set up on the device).  The modal A and every T application is
+a call of the library per column; the buckling A and B (stored element matrices)
+apply one multi-right-hand-side product per 16 columns, so each Ke is read once per
+block step; the block Rayleigh-Ritz steps are small dense products on
 the device and a small symmetric eigenproblem on the host, as in the reference
 (Knyazev's LOBPCG with SVQB orthonormalisation).
 """
@@ -175,17 +177,19 @@ def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=Non
 
 def _ops_block(ops, free):
     """(n, m) -> (n, m): V -> free * sum_b K_b (free * V) of stored element ops
-    [(dofs, Ke)] on their blocks, column by column (gfem/eigen.py:97-110)."""
+    [(dofs, Ke)] on their blocks (gfem/eigen.py:97-110), up to 16 columns per
+    stored-Ke product (one read of each block's Ke serves all of them)."""
     def apply(V):
-        cols = []
-        for j in range(V.shape[1]):
-            v = (V[:, j] * free).contiguous()
+        W = (V * free[:, None]).contiguous()
+        out = torch.empty_like(W)
+        for j in range(0, W.shape[1], 16):
+            Wj = W[:, j:j + 16].contiguous()
             y = None
             for blk, K in ops:
-                t = blk.ebe_matvec(K, v, apply_bc=False)
+                t = blk.ebe_matvec_multi(K, Wj, apply_bc=False)
                 y = t if y is None else y + t
-            cols.append(y * free)
-        return torch.stack(cols, 1)
+            out[:, j:j + 16] = y * free[:, None]
+        return out
     return apply
 
 

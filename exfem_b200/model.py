@@ -59,6 +59,16 @@ def _dev(x, dtype=torch.float64):
     return torch.as_tensor(np.asarray(x), dtype=dtype, device="cuda").contiguous()
 
 
+def _case_groups(nc):
+    """Load cases in groups the multi-case PCG takes (16, 8, 4, 3, 2, 1 at a time)."""
+    out = []
+    while nc > 0:
+        g = next(k for k in (16, 8, 4, 3, 2, 1) if k <= nc)
+        out.append(g)
+        nc -= g
+    return out
+
+
 class Block:
     """Element block: connectivity, element type and material (gfem/model.py:21-26,
     same positional arguments).  The global operators need the block bound to the
@@ -237,15 +247,49 @@ class Block:
         check(lib.exfem_tangent_diagonal(self.handle, ptr(d), stream_ptr()))
         return d
 
-    def ebe_matvec_multi(self, Ke_bf16, V, apply_bc=True):
-        """Stored-Ke product of several right-hand sides on the tensor cores: Ke
-        (ne, nd, nd) BF16, V (ndof, nrhs <= 16) FP32 -> (ndof, nrhs) FP32 (V rounded
-        to BF16, FP32 accumulation)."""
-        V = V.to(torch.float32).contiguous()
+    def ebe_matvec_multi(self, Ke, V, apply_bc=True, engine="cuda"):
+        """Stored-Ke product of several right-hand sides, V (ndof, nrhs <= 16) ->
+        (ndof, nrhs).  engine "cuda": Ke (ne, nd, nd) BF16 or FP32 with FP32 V and
+        accumulation, or FP64 Ke with FP64 V; "tc": the tensor-core form, BF16 Ke,
+        V rounded to BF16, FP32 accumulation."""
+        if engine == "tc":
+            V = V.to(torch.float32).contiguous()
+            Y = torch.empty_like(V)
+            check(lib.exfem_ebe_matvec_bf16_multi(self.handle, ptr(Ke.contiguous()), V.shape[1], ptr(V), ptr(Y),
+                                                  1 if apply_bc else 0, stream_ptr()))
+            return Y
+        if engine != "cuda":
+            raise ValueError(f"unknown engine {engine!r}")
+        code = {torch.float64: _lib.F64, torch.float32: _lib.F32, torch.bfloat16: _lib.BF16}[Ke.dtype]
+        V = V.to(torch.float64 if Ke.dtype == torch.float64 else torch.float32).contiguous()
         Y = torch.empty_like(V)
-        check(lib.exfem_ebe_matvec_bf16_multi(self.handle, ptr(Ke_bf16.contiguous()), V.shape[1], ptr(V), ptr(Y),
-                                              1 if apply_bc else 0, stream_ptr()))
+        check(lib.exfem_ebe_matvec_multi(self.handle, ptr(Ke.contiguous()), code, V.shape[1], ptr(V), ptr(Y),
+                                         1 if apply_bc else 0, stream_ptr()))
         return Y
+
+    def multi_pcg(self, Ke, B, tol=1e-8, maxiter=20000):
+        """Jacobi PCG over the columns of B (ndof, ncase) at once with the stored
+        FP64 Ke and this block's prescribed DOFs (gfem/optimize.py:116-143): one
+        product per iteration for every case, each case with its own scalars and
+        stopping test.  Returns (X, iters, relres) per case."""
+        B = B.to(torch.float64)
+        nc = B.shape[1]
+        X = torch.empty_like(B)
+        iters, rel = np.zeros(nc, np.int32), np.zeros(nc)
+        j = 0
+        for size in _case_groups(nc):
+            Bg = B[:, j:j + size].contiguous()
+            Xg = torch.empty_like(Bg)
+            it = np.zeros(size, np.int32)
+            rr = np.zeros(size)
+            st = lib.exfem_multi_pcg(self.handle, ptr(Ke.contiguous()), size, ptr(Bg), ptr(Xg), float(tol),
+                                     int(maxiter), it.ctypes.data, rr.ctypes.data, stream_ptr())
+            if st < 0:
+                check(st)
+            X[:, j:j + size] = Xg
+            iters[j:j + size], rel[j:j + size] = it, rr
+            j += size
+        return X, iters, rel
 
     def ebe_matvec(self, Ke, v, apply_bc=True):
         v = _dev(v)

@@ -11,7 +11,10 @@ FP64 refinement to ``cg_tol``, every instance with its own scalars and stopping
 test).  A model of several blocks (materials or element types) solves its cases one
 after another with the same FP32/FP64 mixed solver over all of its blocks and one
 device hierarchy.  ``method="jacobi"`` keeps the reference's algorithm: FP64
-stored-Ke Jacobi-PCG per case, to ``cg_tol``.
+stored-Ke Jacobi-PCG for every case, to ``cg_tol`` — on a one-block model all cases
+(up to 16 per call) share each stored-Ke product (``Block.multi_pcg``: one read of
+Ke per iteration for every case, each case with its own scalars and stopping test,
+the loop on the device), on a model of several blocks one case after another.
 """
 import numpy as np
 import torch
@@ -48,6 +51,10 @@ def multi_load_cases(model, step, cases, cg_tol=1e-8, method="batch"):
         S = NativeSolver(model.blocks, "mf32", "amg", linalg.DeviceAMG(model.blocks, Kes))
         del Kes
         return torch.stack([S.mixed(torch.as_tensor(f, device="cuda"), tol=cg_tol)[0] for f in rhs])
+    if len(model.blocks) == 1:
+        B = torch.as_tensor(rhs.T.copy(), device="cuda")
+        X, iters, rel = model.blocks[0].multi_pcg(Kes[0], B, tol=cg_tol, maxiter=20000)
+        return X.T.contiguous()
     S = NativeSolver(model.blocks, "ebe64", "jacobi", None)
     S.set_ke(Kes)
     out = []

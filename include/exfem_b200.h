@@ -181,6 +181,28 @@ int exfem_ebe_matvec(exfem_block b, const double* Ke, const double* v, double* y
  * vmaps the single product over load cases). */
 int exfem_ebe_matvec_bf16_multi(exfem_block b, const void* Ke_bf16, int nrhs, const float* V, float* Y,
                                 int apply_bc, void* stream);
+/* Stored-Ke product for nrhs (1..16) right-hand sides at once on the CUDA cores:
+ * Ke (ne, nd, nd) in ke_dtype (EXFEM_BF16, EXFEM_F32 or EXFEM_F64, as written by
+ * exfem_element_stiffness), V and Y (ndof, nrhs) with the right-hand sides fastest,
+ * FP32 for BF16 / FP32 Ke (FP32 accumulation) and FP64 for FP64 Ke.  One read of Ke
+ * serves every right-hand side; element rows are summed per node through the
+ * gather plan in the reference's order.  apply_bc as exfem_ebe_matvec.  The
+ * multi-load-case form of gfem/model.py:264-267 (gfem/optimize.py:116-143 vmaps the
+ * single product over load cases). */
+int exfem_ebe_matvec_multi(exfem_block b, const void* Ke, int ke_dtype, int nrhs, const void* V, void* Y,
+                           int apply_bc, void* stream);
+/* Jacobi PCG over nrhs (1, 2, 3, 4, 8 or 16) load cases at once with the stored FP64
+ * element matrices Ke and the block's prescribed DOFs (gfem/optimize.py:116-143:
+ * linalg.pcg, gfem/linalg.py:21-47, vmapped over the cases, with A(v) = free K
+ * (free v) + (1 - free) v and the inverse assembled diagonal, 1 on prescribed
+ * rows): B, X (ndof, nrhs) FP64 with the cases fastest; B should be zero on
+ * prescribed DOFs (the reference passes free * f).  One product per iteration for
+ * all cases; each case keeps its own scalars and stops on its own test (r.r <=
+ * tol^2 max(b.b, 1e-300) or k >= maxiter); iters and relres (nrhs) per case.  The
+ * loop runs on the device (one graph launch).  EXFEM_NOT_CONVERGED if a case
+ * stopped on maxiter.  Synchronises the stream. */
+int exfem_multi_pcg(exfem_block b, const double* Ke, int nrhs, const double* B, double* X, double tol, int maxiter,
+                    int* iters, double* relres, void* stream);
 /* Diagonal of stored Ke (gfem/model.py:169-173 ops_diagonal), FP64 (ndof). */
 int exfem_ebe_diagonal(exfem_block b, const double* Ke, double* diag, void* stream);
 /* Initial-stress (geometric) stiffness of every element under its constant

@@ -156,3 +156,44 @@ def test_multi_load_cases_matches_oracle(cuda):
         assert U.shape == (3, m.ndof)
         for k in range(3):
             assert _rel(U[k], ref[k]) < 1e-8, (method, k, _rel(U[k], ref[k]))
+
+
+@pytest.mark.parametrize("ncase", [5, 16])
+def test_multi_case_jacobi_pcg_matches_oracle(cuda, ncase):
+    """Block.multi_pcg (gfem/optimize.py:116-143, the vmapped Jacobi PCG): every case
+    of one call — one stored-Ke product per iteration for all of them — converges to
+    the oracle's sparse direct solution (1e-8), in the oracle's own Jacobi-PCG
+    iteration count (within one iteration: the sums run in another order)."""
+    import scipy.sparse.linalg as spla
+    import torch
+
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    from oracle import fem as ofem
+    from oracle import linalg as olin
+    from oracle import solvers as osol
+    X, c = mesh.box_hex(40.0, 10.0, 10.0, 8, 2, 2)
+    X = mesh.jitter_interior(X, 5.0, 0.1, 4)
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)]
+    m = xf.Model(X)
+    blk = m.add_block(c, xf.HEX8, xf.LinearElastic(210e3, 0.3))
+    om = ofem.Model(X)
+    om.add_block(c, ofem.HEX8, ofem.LinearElastic(210e3, 0.3))
+    setup = osol.Setup(om, osol.Step(bcs=bcs))
+    ops = [(d, K.numpy()) for d, K in om.stiffness_ops(torch.zeros(om.ndof, dtype=torch.float64), om.init_state())]
+    A = olin.bc_matrix(ofem.ops_assemble(ops, om.ndof), setup.free).tocsr()
+    d = A.diagonal()                       # the assembled diagonal on the free rows
+    inv = np.where(setup.free > 0, 1.0 / np.where(np.abs(d) > 0, d, 1.0), 1.0)
+    F = np.random.default_rng(ncase).standard_normal((ncase, m.ndof)) * setup.free[None, :]
+    blk.set_fixed(~setup.free.astype(bool))
+    K = blk.stiffness(torch.zeros(m.ndof, dtype=torch.float64, device="cuda"), blk.init_state())
+    Xs, iters, rel = blk.multi_pcg(K, torch.as_tensor(F.T.copy(), device="cuda"), tol=1e-10)
+    for k in range(ncase):
+        xo, ko, ro = olin.pcg(lambda v: A @ v, F[k], lambda r: inv * r, tol=1e-10, maxiter=20000)
+        xd = spla.spsolve(A.tocsc(), F[k])
+        assert _rel(Xs[:, k], xd) < 1e-8, (k, _rel(Xs[:, k], xd))
+        assert abs(int(iters[k]) - ko) <= 1, (k, iters[k], ko)
+        assert rel[k] <= 1e-10
+    blk.set_fixed(None)
+

@@ -219,7 +219,7 @@ def test_tensor_core_stored_ke_multi_rhs(cuda, kind, nrhs):
     K64 = blk.stiffness(zero, blk.init_state())
     rng = np.random.default_rng(nrhs)
     V = torch.as_tensor(rng.standard_normal((pmod.ndof, nrhs)), dtype=torch.float32, device="cuda")
-    Y = blk.ebe_matvec_multi(Kb, V)
+    Y = blk.ebe_matvec_multi(Kb, V, engine="tc")
     Vb = V.to(torch.bfloat16).double()
     for r in range(nrhs):
         yb = blk.ebe_matvec(Kb.double(), Vb[:, r].contiguous())
@@ -229,3 +229,33 @@ def test_tensor_core_stored_ke_multi_rhs(cuda, kind, nrhs):
         assert rel_err(Y[:, r].double(), yb) < 1e-5
         assert rel_err(Y[:, r].double(), y64) < 2e-2
     blk.set_fixed(None)
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+@pytest.mark.parametrize("nrhs", [1, 4, 5, 16])
+def test_multi_rhs_stored_ke_product(cuda, kind, nrhs):
+    """CUDA-core stored-Ke product of several right-hand sides: FP64 Ke against the
+    single-right-hand-side FP64 product of each column (1e-13), FP32 Ke (1e-6) and
+    BF16 Ke (against the BF16-rounded Ke in FP64, 1e-5) — prescribed rows included."""
+    X, c, pmod, omod = _pair(kind, "el", n=(5, 4, 3))
+    blk = pmod.blocks[0]
+    fixed = np.zeros(pmod.ndof, bool)
+    fixed[::7] = True
+    blk.set_fixed(fixed)
+    zero = torch.zeros(pmod.ndof, dtype=torch.float64, device="cuda")
+    K64 = blk.stiffness(zero, blk.init_state())
+    rng = np.random.default_rng(100 + nrhs)
+    V = torch.as_tensor(rng.standard_normal((pmod.ndof, nrhs)), device="cuda")
+    Y64 = blk.ebe_matvec_multi(K64, V)
+    Y32 = blk.ebe_matvec_multi(K64.float(), V.float())
+    Kb = K64.to(torch.bfloat16)
+    Yb = blk.ebe_matvec_multi(Kb, V.float())
+    assert Y64.dtype == torch.float64 and Y32.dtype == torch.float32 and Yb.dtype == torch.float32
+    for r in range(nrhs):
+        y = blk.ebe_matvec(K64, V[:, r].contiguous())
+        assert rel_err(Y64[:, r], y) < 1e-13
+        assert rel_err(Y32[:, r].double(), y) < 1e-6
+        yb = blk.ebe_matvec(Kb.double(), V[:, r].float().double().contiguous())
+        assert rel_err(Yb[:, r].double(), yb) < 1e-5
+    blk.set_fixed(None)
+
