@@ -81,14 +81,20 @@ constexpr int MW = 8;  // warps per CTA
 //
 // Each warp takes EP elements per pass (EP = 2 for BF16 / FP32 Ke, 1 for FP64): the
 // Ke rows of all of them are requested first, then their nodal values are gathered
-// together, so that every lane has EP rows and EP gathers in flight at once.
+// together (16-byte vectors of right-hand sides where nrhs allows), so that every
+// lane has EP rows and EP gathers in flight at once.  FP32 products of an even
+// number of right-hand sides issue packed FFMA2 (two right-hand sides per
+// instruction, each rounded as its own FMA).
 template <int ET, int NR, class KT, class VT>
 __global__ void __launch_bounds__(32 * MW)
 ebe_multi_kernel(int64_t ne, const int32_t* __restrict__ conn, const KT* __restrict__ Ke,
-                 const VT* __restrict__ V, const uint8_t* __restrict__ fixed, VT* __restrict__ ys) {
+                 const VT* __restrict__ V, const uint8_t* __restrict__ fixed, VT* __restrict__ ys, int vecv) {
   constexpr int NN = ElemTraits<ET>::nnode, ND = 3 * NN;
   constexpr int EP = sizeof(KT) <= 4 ? 2 : 1;
-  __shared__ VT us[MW][EP][ND * NR];
+  constexpr int W = (NR * sizeof(VT)) % 16 == 0 ? 16 / (int)sizeof(VT) : 1;  // values per gathered vector
+  constexpr int NV = ND * NR / W;
+  constexpr bool PAIRED = sizeof(VT) == 4 && NR % 2 == 0;
+  __shared__ __align__(16) VT us[MW][EP][ND * NR];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * MW;
   for (int64_t e0 = (int64_t)blockIdx.x * MW + warp; e0 < ne; e0 += EP * stride) {
@@ -102,11 +108,26 @@ ebe_multi_kernel(int64_t ne, const int32_t* __restrict__ conn, const KT* __restr
     for (int p = 0; p < EP; ++p) {
       const int64_t e = e0 + p * stride;
       if (e < ne) {
-        for (int q = lane; q < ND * NR; q += 32) {
-          const int i = q / NR, r = q - i * NR;
+        for (int q = lane; q < NV; q += 32) {
+          const int i = (q * W) / NR, r = (q * W) % NR;
           const int64_t d = 3 * (int64_t)__ldg(conn + e * NN + i / 3) + i % 3;
-          const VT v = __ldg(V + d * NR + r);
-          us[warp][p][q] = (fixed && __ldg(fixed + d)) ? VT(0) : v;
+          const bool off = fixed && __ldg(fixed + d);
+          if constexpr (W > 1) {
+            uint4 v;
+            if (vecv) {  // V 16-byte aligned (checked on the host)
+              v = __ldg(reinterpret_cast<const uint4*>(V + d * NR + r));
+            } else {
+              VT t[W];
+#pragma unroll
+              for (int k = 0; k < W; ++k) t[k] = __ldg(V + d * NR + r + k);
+              memcpy(&v, t, 16);
+            }
+            if (off) v = make_uint4(0, 0, 0, 0);
+            *reinterpret_cast<uint4*>(&us[warp][p][q * W]) = v;
+          } else {
+            const VT v = __ldg(V + d * NR + r);
+            us[warp][p][q] = off ? VT(0) : v;
+          }
         }
       }
     }
@@ -117,13 +138,32 @@ ebe_multi_kernel(int64_t ne, const int32_t* __restrict__ conn, const KT* __restr
       if (e < ne && lane < ND) {
         const VT* u = us[warp][p];
         VT y[NR];
+        if constexpr (PAIRED) {
+          float2 y2[NR / 2];
 #pragma unroll
-        for (int r = 0; r < NR; ++r) y[r] = VT(0);
+          for (int j = 0; j < NR / 2; ++j) y2[j] = make_float2(0.f, 0.f);
 #pragma unroll
-        for (int c = 0; c < ND; ++c) {
-          const VT k = to_acc(row[p][c], VT(0));
+          for (int c = 0; c < ND; ++c) {
+            const float k = to_acc(row[p][c], 0.f);
+            const float2 k2 = make_float2(k, k);
+            const float2* u2 = reinterpret_cast<const float2*>(u + c * NR);
 #pragma unroll
-          for (int r = 0; r < NR; ++r) y[r] += k * u[c * NR + r];
+            for (int j = 0; j < NR / 2; ++j) y2[j] = __ffma2_rn(k2, u2[j], y2[j]);
+          }
+#pragma unroll
+          for (int j = 0; j < NR / 2; ++j) {
+            y[2 * j] = y2[j].x;
+            y[2 * j + 1] = y2[j].y;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < NR; ++r) y[r] = VT(0);
+#pragma unroll
+          for (int c = 0; c < ND; ++c) {
+            const VT k = to_acc(row[p][c], VT(0));
+#pragma unroll
+            for (int r = 0; r < NR; ++r) y[r] += k * u[c * NR + r];
+          }
         }
         VT* out = ys + (e * ND + lane) * NR;
         if constexpr ((NR * sizeof(VT)) % 16 == 0) {
@@ -146,11 +186,13 @@ ebe_multi_kernel(int64_t ne, const int32_t* __restrict__ conn, const KT* __restr
 // Y[3n+c, r] = fixed ? V : sum over node n's gather-plan slots of the element rows,
 // the slots in the plan's order; one thread per node and group of four right-hand
 // sides (16-byte loads and stores) for FP32 with nrhs a multiple of 4 and aligned
-// V, Y (vec4), else per node and right-hand side
+// V, Y (vec4), else per node and right-hand side.  The plan entries are read four
+// at a time and the rows of all four slots requested before any is added.
 template <class VT>
-__global__ void gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32_t* __restrict__ plan,
+__global__ void __launch_bounds__(256) gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32_t* __restrict__ plan,
                                     int64_t sentinel, const VT* __restrict__ ys, const uint8_t* __restrict__ fixed,
                                     const VT* __restrict__ V, int nrhs, VT* __restrict__ Y, int vec4) {
+  constexpr int K = 4;
   const int nd = 3 * nnode;
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if constexpr (sizeof(VT) == 4) {
@@ -160,18 +202,35 @@ __global__ void gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32
       const int64_t n = t / nq;
       const int r4 = (int)(t - n * nq) * 4;
       float4 s[3] = {make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0), make_float4(0, 0, 0, 0)};
-      for (int k = 0; k < vmax; ++k) {
-        const int64_t slot = plan[n * vmax + k];
-        if (slot == sentinel) break;
-        const int64_t e = slot / nnode;
-        const int a = (int)(slot - e * nnode);
+      bool more = true;
+      for (int k0 = 0; k0 < vmax && more; k0 += K) {
+        int64_t sl[K];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float4 w = *reinterpret_cast<const float4*>(ys + (e * nd + 3 * a + c) * nrhs + r4);
-          s[c].x += w.x;
-          s[c].y += w.y;
-          s[c].z += w.z;
-          s[c].w += w.w;
+        for (int u = 0; u < K; ++u) sl[u] = k0 + u < vmax ? (int64_t)plan[n * vmax + k0 + u] : sentinel;
+        float4 w[K][3];
+#pragma unroll
+        for (int u = 0; u < K; ++u) {
+          if (sl[u] != sentinel) {
+            const int64_t e = sl[u] / nnode;
+            const int a = (int)(sl[u] - e * nnode);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+              w[u][c] = *reinterpret_cast<const float4*>(ys + (e * nd + 3 * a + c) * nrhs + r4);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < K; ++u) {
+          if (sl[u] == sentinel) {
+            more = false;
+            break;
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            s[c].x += w[u][c].x;
+            s[c].y += w[u][c].y;
+            s[c].z += w[u][c].z;
+            s[c].w += w[u][c].w;
+          }
         }
       }
 #pragma unroll
@@ -187,13 +246,30 @@ __global__ void gather_multi_kernel(int64_t nn, int vmax, int nnode, const int32
   const int64_t n = t / nrhs;
   const int r = (int)(t - n * nrhs);
   VT s[3] = {VT(0), VT(0), VT(0)};
-  for (int k = 0; k < vmax; ++k) {
-    const int64_t slot = plan[n * vmax + k];
-    if (slot == sentinel) break;
-    const int64_t e = slot / nnode;
-    const int a = (int)(slot - e * nnode);
+  bool more = true;
+  for (int k0 = 0; k0 < vmax && more; k0 += K) {
+    int64_t sl[K];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) s[c] += ys[(e * nd + 3 * a + c) * nrhs + r];
+    for (int u = 0; u < K; ++u) sl[u] = k0 + u < vmax ? (int64_t)plan[n * vmax + k0 + u] : sentinel;
+    VT w[K][3];
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+      if (sl[u] != sentinel) {
+        const int64_t e = sl[u] / nnode;
+        const int a = (int)(sl[u] - e * nnode);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) w[u][c] = ys[(e * nd + 3 * a + c) * nrhs + r];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+      if (sl[u] == sentinel) {
+        more = false;
+        break;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s[c] += w[u][c];
+    }
   }
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -226,9 +302,10 @@ int multi_launch(exfem_block_s* b, const KT* Ke, int nrhs, const VT* V, VT* ys, 
   EX_CUDA(cudaGetDevice(&dev));
   EX_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b->ne + MW - 1) / MW, (int64_t)nsm * 8));
-#define EXF_MULTI(NR)                                                                             \
-  case NR:                                                                                        \
-    ebe_multi_kernel<ET, NR, KT, VT><<<grid, 32 * MW, 0, s>>>(b->ne, b->conn.p, Ke, V, fx, ys); \
+  const int vecv = (uintptr_t)V % 16 == 0;  // 16-byte gathers of V need it aligned
+#define EXF_MULTI(NR)                                                                                   \
+  case NR:                                                                                              \
+    ebe_multi_kernel<ET, NR, KT, VT><<<grid, 32 * MW, 0, s>>>(b->ne, b->conn.p, Ke, V, fx, ys, vecv); \
     break;
   switch (nrhs) {
     EXF_MULTI(1) EXF_MULTI(2) EXF_MULTI(3) EXF_MULTI(4) EXF_MULTI(5) EXF_MULTI(6) EXF_MULTI(7) EXF_MULTI(8)
@@ -491,14 +568,16 @@ int mp_solve(exfem_block_s* b, const double* Ke, const double* Bm, double* X, do
   const int64_t n = b->ndof();
   int st;
   // workspace: dinv (n), R, P, Q (n NR each), partial sums, scalars, counter
+  // (every array starts on 256 bytes: the product reads P with 16-byte loads)
   DevBuf<double>& w = b->mp_work;
-  const size_t need = (size_t)n * (1 + 3 * NR) + (size_t)MP_MAX_BLOCKS * 16 + sizeof(MultiScal) / 8 + 64;
+  const int64_t np = (n + 31) / 32 * 32;
+  const size_t need = (size_t)np * (1 + 3 * NR) + (size_t)MP_MAX_BLOCKS * 16 + sizeof(MultiScal) / 8 + 64;
   if (w.n < need && (st = w.alloc(need))) return st;
   double* dinv = w.p;
-  double* R = dinv + n;
-  double* P = R + n * NR;
-  double* Q = P + n * NR;
-  double* partial = Q + n * NR;
+  double* R = dinv + np;
+  double* P = R + np * NR;
+  double* Q = P + np * NR;
+  double* partial = Q + np * NR;
   MultiScal* sc = reinterpret_cast<MultiScal*>(partial + MP_MAX_BLOCKS * 16);
   unsigned* counter = reinterpret_cast<unsigned*>(sc + 1);
   const unsigned grid =

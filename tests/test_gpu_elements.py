@@ -259,3 +259,25 @@ def test_multi_rhs_stored_ke_product(cuda, kind, nrhs):
         assert rel_err(Yb[:, r].double(), yb) < 1e-5
     blk.set_fixed(None)
 
+
+def test_multi_rhs_product_with_unaligned_operands(cuda):
+    """The C ABI takes V and Y at any element-aligned address: a V and a Y four bytes
+    off a 16-byte boundary give the same product as aligned copies (the 16-byte
+    loads and stores are used only where the addresses allow them)."""
+    from exfem_b200 import _lib
+    from exfem_b200._lib import lib
+    X, c, pmod, omod = _pair("hex", "el", n=(5, 4, 3))
+    blk = pmod.blocks[0]
+    zero = torch.zeros(pmod.ndof, dtype=torch.float64, device="cuda")
+    Kb = blk.stiffness(zero, blk.init_state(), dtype=torch.bfloat16)
+    nr = 4
+    V = torch.randn(pmod.ndof, nr, dtype=torch.float32, device="cuda")
+    Y = blk.ebe_matvec_multi(Kb, V)
+    buf = torch.zeros(2, pmod.ndof * nr + 1, dtype=torch.float32, device="cuda")
+    Vu, Yu = buf[0, 1:], buf[1, 1:]
+    Vu.copy_(V.reshape(-1))
+    assert Vu.data_ptr() % 16 != 0 and Yu.data_ptr() % 16 != 0
+    _lib.check(lib.exfem_ebe_matvec_multi(blk.handle, _lib.ptr(Kb), _lib.BF16, nr, Vu.data_ptr(), Yu.data_ptr(), 1,
+                                          _lib.stream_ptr()))
+    torch.testing.assert_close(Yu.reshape(pmod.ndof, nr), Y, rtol=0, atol=0)
+
