@@ -36,6 +36,8 @@ int host_face_once(int64_t nface, const int64_t* keys, uint8_t* once);
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm, int& maxu);
 int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters, double* relres, cudaStream_t st);
+int solver_mixed_graph(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
+                       int maxiter, int* iters, int* updates, double* relres, cudaStream_t st);
 int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
                     int maxiter, int* iters, int* updates, double* relres, cudaStream_t st);
 int solver_mixed(exfem_solver_s* S, const double* b, double* x, double tol, double inner_tol, int max_pass,
@@ -724,6 +726,7 @@ int exfem_solver_set_graph(exfem_solver s, int enable, int chunk) {
   EX_ARG(chunk >= 1 && chunk <= 1024, "chunk must be in 1..1024");
   for (auto& g : s->gexec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (s->gmixed) { cudaGraphExecDestroy(s->gmixed); s->gmixed = nullptr; }
   s->use_graph = enable ? 1 : 0;
   s->chunk = chunk;
   return EXFEM_OK;
@@ -733,6 +736,7 @@ int exfem_solver_set_loop(exfem_solver s, int device_loop) {
   EX_ARG(s, "solver is NULL");
   for (auto& g : s->gexec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  if (s->gmixed) { cudaGraphExecDestroy(s->gmixed); s->gmixed = nullptr; }
   s->device_loop = device_loop ? 1 : 0;
   return EXFEM_OK;
 }
@@ -757,9 +761,13 @@ int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, d
   StreamGuard g;
   int st;
   if ((st = g.init(stream))) return st;
+  // reliable updates run as one graph when the PCG loop runs on the device
   const int r = s->mixed_mode == 1
-                    ? solver_mixed_ru(s, b, x, tol, s->mixed_delta, 100 * max_pass, maxiter, iters, passes, relres,
-                                      g.work)
+                    ? (s->use_graph && s->device_loop
+                           ? solver_mixed_graph(s, b, x, tol, s->mixed_delta, 100 * max_pass, maxiter, iters, passes,
+                                                relres, g.work)
+                           : solver_mixed_ru(s, b, x, tol, s->mixed_delta, 100 * max_pass, maxiter, iters, passes,
+                                             relres, g.work))
                     : solver_mixed(s, b, x, tol, inner_tol, max_pass, maxiter, iters, passes, relres, g.work);
   if (r < 0) return r;
   const int w = block_wait_status(s->blk, g.work);

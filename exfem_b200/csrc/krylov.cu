@@ -12,6 +12,10 @@
 // Mixed refinement follows gfem/solvers.py:344-384 (_LinearSystem._mixed): an
 // FP32 inner PCG on the normalised residual, the correction accumulated in FP64,
 // and the FP64 residual b - A x recomputed with the FP64 operator each pass.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "solver.h"
 
 namespace exfem {
@@ -633,6 +637,7 @@ static int pcg_prepare(exfem_solver_s* S, cudaStream_t st) {
       cudaGraphDestroy(g);
       EX_CUDA(ce);
       S->gloop[gi] = S->device_loop != 0;
+      ++S->graph_gen;
       S->g_Ke[gi] = keptr;
       S->g_lmax[gi] = S->cheb_lmax;
     }
@@ -862,6 +867,303 @@ int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, d
   return (std::isfinite(rn) && rn <= tol * bn) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
 }
 
+// ---------------------------------------------------------------- reliable updates as one graph
+//
+// The same recursion as solver_mixed_ru with every decision taken on the device:
+// the replacement segments are a conditional while node whose body holds the
+// segment start (scaled FP32 residual, fresh or rescaled direction), the PCG loop
+// (a nested conditional while node over one captured iteration), the FP64
+// replacement x += sc x32, r64 = b - A64 x, and the test for the next segment.  The
+// scalars (||b||, ||r||, the scale, the restart flag, iteration and replacement
+// counts) live in a MixedScal in device memory; every formula is the host path's, in
+// the same order and precision, so both give the same iterates.  One graph per
+// solver handle, built on first use and rebuilt with the PCG graph (prescribed DOFs,
+// element matrices, Chebyshev bound); b and x pass through the handle's own vectors
+// so that the graph's addresses stay fixed.
+
+__global__ void mx_params_kernel(MixedScal* ms, double tol, double delta, int maxiter, int max_updates) {
+  ms->tol = tol;
+  ms->delta = delta;
+  ms->maxiter = maxiter;
+  ms->max_updates = max_updates;
+}
+
+// after ||b||^2 landed in nrm2: the recursion's starting scalars
+__global__ void mx_start_kernel(MixedScal* ms) {
+  const double bn = sqrt(ms->nrm2);
+  ms->bn = bn;
+  ms->rn = bn;
+  ms->rn_prev = bn;
+  ms->sc = bn;
+  ms->restart = 1;
+  ms->its = 0;
+  ms->nup = 0;
+  ms->done = bn == 0.0;
+}
+
+// segment start: 1/sc for the scaled residual, the segment's tolerance and budget
+// (segment_scal_kernel's fields)
+__global__ void mx_seg_begin_kernel(MixedScal* ms, PcgScal* sc) {
+  ms->inv_sc = 1.0 / ms->sc;
+  const double seg_tol = fmax(ms->delta, ms->tol * ms->bn / ms->rn);
+  sc->spare = seg_tol * seg_tol;
+  sc->k = 0;
+  sc->maxiter = max(ms->maxiter - ms->its, 0);
+  sc->done = 0;
+}
+
+__global__ void mx_scale_down_kernel(int64_t n, const double* __restrict__ r64, float* __restrict__ r32,
+                                     const MixedScal* ms) {
+  const double s = ms->inv_sc;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    r32[i] = (float)((double)r64[i] * s);
+}
+
+// direction of the new segment: the preconditioned residual after a restart, else
+// the skipped update of the last iteration, p = z + beta p
+__global__ void mx_dir_kernel(int64_t n, float* __restrict__ p, const float* __restrict__ z, const PcgScal* sc,
+                              const MixedScal* ms) {
+  const bool fresh = ms->restart != 0;
+  const float beta = (float)sc->beta;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = fresh ? z[i] : z[i] + beta * p[i];
+}
+
+__global__ void mx_count_kernel(MixedScal* ms, const PcgScal* sc) { ms->its += sc->k; }
+
+__global__ void mx_axpy_kernel(int64_t n, double* __restrict__ x, const float* __restrict__ d, const MixedScal* ms) {
+  const double sc = ms->sc;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] += (double)d[i] * sc;
+}
+
+// after ||r64||^2 landed in nrm2: stop, or prepare the next segment (restart when the
+// replacement did not halve the residual, else rescale the kept direction)
+__global__ void mx_seg_end_kernel(MixedScal* ms) {
+  const double rn = sqrt(ms->nrm2);
+  ms->rn = rn;
+  ms->nup += 1;
+  ms->done = !isfinite(rn) || rn <= ms->tol * ms->bn || ms->its >= ms->maxiter || ms->nup >= ms->max_updates;
+  if (!ms->done) {
+    ms->restart = !(rn <= 0.5 * ms->rn_prev);
+    ms->pscale = ms->restart ? 1.0f : (float)(ms->sc / rn);
+    ms->rn_prev = rn;
+    ms->sc = rn;
+  }
+}
+
+__global__ void mx_rescale_kernel(int64_t n, float* __restrict__ p, const MixedScal* ms) {
+  if (ms->done || ms->restart) return;
+  const float a = ms->pscale;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    p[i] *= a;
+}
+
+// segment loop condition: another segment while not done, at most max_updates + 1
+__global__ void mx_cond_kernel(cudaGraphConditionalHandle h, MixedScal* ms, int head) {
+  if (head) ms->loops = 0;
+  else ms->loops += 1;
+  const bool more = !ms->done && (long long)ms->loops <= (long long)ms->max_updates;
+  cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
+// nodes of g that no edge leaves
+static int graph_leaves(cudaGraph_t g, std::vector<cudaGraphNode_t>& out) {
+  size_t nn = 0, ne = 0;
+  EX_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  if (nn) EX_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  EX_CUDA(cudaGraphGetEdges(g, nullptr, nullptr, &ne));
+  std::vector<cudaGraphNode_t> from(ne), to(ne);
+  if (ne) EX_CUDA(cudaGraphGetEdges(g, from.data(), to.data(), &ne));
+  out.clear();
+  for (auto nd : nodes)
+    if (std::find(from.begin(), from.end(), nd) == from.end()) out.push_back(nd);
+  return EXFEM_OK;
+}
+
+// capture the work of f on stream st into g after the nodes deps
+template <class F>
+static int capture_into(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cudaStream_t st, F f) {
+  cudaError_t e = cudaStreamBeginCaptureToGraph(st, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                                cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    set_error("graph capture could not start: %s", cudaGetErrorString(e));
+    return EXFEM_ERR_CUDA;
+  }
+  int cs = f();
+  if (!cs && cudaGetLastError() != cudaSuccess) cs = EXFEM_ERR_CUDA;
+  cudaGraph_t out = nullptr;
+  e = cudaStreamEndCapture(st, &out);
+  if (cs) return cs;
+  if (e != cudaSuccess) {
+    set_error("graph capture failed: %s", cudaGetErrorString(e));
+    return EXFEM_ERR_CUDA;
+  }
+  return EXFEM_OK;
+}
+
+static int mixed_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* out) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  MixedScal* ms = S->mx_scal.p;
+  PcgScal* sc = S->scal.p;
+  float *x32 = S->x32.p, *r32 = S->r32.p, *z32 = S->z32.p, *p32 = S->p32.p;
+  const double* b = S->mx_b.p;
+  double* x = S->mx_x.p;
+  cudaGraph_t g = nullptr;
+  EX_CUDA(cudaGraphCreate(&g, 0));
+  auto fail = [&](int s) {
+    cudaGraphDestroy(g);
+    return s;
+  };
+  int s;
+  cudaGraphConditionalHandle hs, hp;
+  cudaGraph_t seg, body;
+  cudaGraphNode_t n_seg, n_pcg;
+  // head: x = 0, r64 = b, ||b||, start scalars, the PCG scalars' reset
+  s = capture_into(g, {}, st, [&]() -> int {
+    EX_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    EX_CUDA(cudaMemcpyAsync(S->r64.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    int q;
+    if ((q = dot<double>(S, b, b, FIN_STORE, &ms->nrm2, 0, st))) return q;
+    mx_start_kernel<<<1, 1, 0, st>>>(ms);
+    init_scal_kernel<<<1, 1, 0, st>>>(sc, 1.0, 0);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  // the segment loop
+  std::vector<cudaGraphNode_t> leaves;
+  if ((s = graph_leaves(g, leaves))) return fail(s);
+  {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&hs, g, 0, 0);
+    if (e != cudaSuccess) return fail((set_error("condition handle: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+  }
+  s = capture_into(g, leaves, st, [&]() -> int {
+    mx_cond_kernel<<<1, 1, 0, st>>>(hs, ms, 1);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  {
+    std::vector<cudaGraphNode_t> deps;
+    if ((s = graph_leaves(g, deps))) return fail(s);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hs;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(&n_seg, g, deps.data(), deps.size(), &cp);
+    if (e != cudaSuccess) return fail((set_error("while node: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+    seg = cp.conditional.phGraph_out[0];
+  }
+  // segment start
+  s = capture_into(seg, {}, st, [&]() -> int {
+    mx_seg_begin_kernel<<<1, 1, 0, st>>>(ms, sc);
+    mx_scale_down_kernel<<<eg, 256, 0, st>>>(n, S->r64.p, r32, ms);
+    EX_CUDA(cudaMemsetAsync(x32, 0, sizeof(float) * n, st));
+    int q;
+    if ((q = dot<float>(S, r32, r32, FIN_BB, nullptr, 0, st))) return q;
+    if ((q = pc_apply<float>(S, r32, z32, nullptr, st))) return q;
+    mx_dir_kernel<<<grid_for(n, 256), 256, 0, st>>>(n, p32, z32, sc, ms);
+    if ((q = dot<float>(S, r32, z32, FIN_RZ0, nullptr, 0, st))) return q;
+    if ((q = dot<float>(S, r32, r32, FIN_RR0, nullptr, 0, st))) return q;
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  // the PCG loop of the segment
+  if ((s = graph_leaves(seg, leaves))) return fail(s);
+  {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&hp, seg, 0, 0);
+    if (e != cudaSuccess) return fail((set_error("condition handle: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+  }
+  s = capture_into(seg, leaves, st, [&]() -> int {
+    loop_cond_kernel<<<1, 1, 0, st>>>(hp, sc, 1);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  {
+    std::vector<cudaGraphNode_t> deps;
+    if ((s = graph_leaves(seg, deps))) return fail(s);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hp;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(&n_pcg, seg, deps.data(), deps.size(), &cp);
+    if (e != cudaSuccess) return fail((set_error("while node: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+    body = cp.conditional.phGraph_out[0];
+  }
+  s = capture_into(body, {}, st, [&]() -> int {
+    int q;
+    if ((q = pcg_iteration<float>(S, st))) return q;
+    loop_cond_kernel<<<1, 1, 0, st>>>(hp, sc, 0);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  // segment end: replacement, FP64 residual, test, rescale, loop condition
+  s = capture_into(seg, {n_pcg}, st, [&]() -> int {
+    mx_count_kernel<<<1, 1, 0, st>>>(ms, sc);
+    mx_axpy_kernel<<<eg, 256, 0, st>>>(n, x, x32, ms);
+    int q;
+    if ((q = mf_apply_all<double>(S, x, S->Ap64.p, nullptr, st))) return q;
+    sub64_kernel<<<eg, 256, 0, st>>>(n, b, S->Ap64.p, S->r64.p);
+    if ((q = dot<double>(S, S->r64.p, S->r64.p, FIN_STORE, &ms->nrm2, 0, st))) return q;
+    mx_seg_end_kernel<<<1, 1, 0, st>>>(ms);
+    mx_rescale_kernel<<<eg, 256, 0, st>>>(n, p32, ms);
+    mx_cond_kernel<<<1, 1, 0, st>>>(hs, ms, 0);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  *out = g;
+  return EXFEM_OK;
+}
+
+int solver_mixed_graph(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
+                       int maxiter, int* iters, int* updates, double* relres, cudaStream_t st) {
+  const int64_t n = S->n;
+  if (S->op == EXFEM_OP_EBE_F64 || S->op == EXFEM_OP_CSR_F64) {
+    set_error("mixed refinement needs a matrix-free operator (EXFEM_OP_MF_F32)");
+    return EXFEM_ERR_ARG;
+  }
+  int s;
+  if ((s = pcg_prepare<float>(S, st))) return s;
+  if (!S->mx_b.p && ((s = S->mx_b.alloc(std::max<int64_t>(n, 1))) || (s = S->mx_x.alloc(std::max<int64_t>(n, 1))) ||
+                     (s = S->mx_scal.alloc(1))))
+    return s;
+  // the PCG graph's validity covers this one (same captured iteration)
+  if (S->gmixed && S->gmixed_gen != S->graph_gen) {
+    cudaGraphExecDestroy(S->gmixed);
+    S->gmixed = nullptr;
+  }
+  if (!S->gmixed) {
+    CaptureScope cap;
+    cudaGraph_t g = nullptr;
+    if ((s = mixed_graph_build(S, st, &g))) return s;
+    cudaError_t e = cudaGraphInstantiate(&S->gmixed, g, 0);
+    cudaGraphDestroy(g);
+    EX_CUDA(e);
+    S->gmixed_gen = S->graph_gen;
+  }
+  EX_CUDA(cudaMemcpyAsync(S->mx_b.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  mx_params_kernel<<<1, 1, 0, st>>>(S->mx_scal.p, tol, delta, maxiter, max_updates);
+  EX_LAUNCH_CHECK();
+  EX_CUDA(cudaGraphLaunch(S->gmixed, st));
+  EX_CUDA(cudaMemcpyAsync(x, S->mx_x.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  MixedScal h;
+  EX_CUDA(cudaMemcpyAsync(&h, S->mx_scal.p, sizeof(MixedScal), cudaMemcpyDeviceToHost, st));
+  EX_CUDA(cudaStreamSynchronize(st));
+  if (h.bn == 0.0) {
+    if (iters) *iters = 0;
+    if (updates) *updates = 0;
+    if (relres) *relres = 0.0;
+    return EXFEM_OK;
+  }
+  if (iters) *iters = h.its;
+  if (updates) *updates = h.nup;
+  if (relres) *relres = h.rn / h.bn;
+  return (std::isfinite(h.rn) && h.rn <= tol * h.bn) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
+}
+
 int solver_alloc(exfem_solver_s* S) {
   const int64_t n = S->n;
   int s;
@@ -894,5 +1196,6 @@ int solver_alloc(exfem_solver_s* S) {
 exfem_solver_s::~exfem_solver_s() {
   for (auto& g : gexec)
     if (g) cudaGraphExecDestroy(g);
+  if (gmixed) cudaGraphExecDestroy(gmixed);
   if (h_scal) exfem::outside_captures([&] { return cudaFreeHost(h_scal); });
 }

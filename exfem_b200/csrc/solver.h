@@ -79,6 +79,13 @@ struct PcgScal {
   int k, maxiter, done, pad;
 };
 
+// device scalars of the reliable-update mixed solve run as one graph
+struct MixedScal {
+  double tol, delta, bn, rn, rn_prev, sc, inv_sc, nrm2;
+  float pscale;
+  int maxiter, max_updates, its, nup, restart, done, loops;
+};
+
 }  // namespace exfem
 
 struct exfem_amg_s {
@@ -130,6 +137,12 @@ struct exfem_solver_s {
   int use_graph = 1, chunk = 8, device_loop = 1;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   bool gloop[2] = {false, false};
+  uint64_t graph_gen = 0;  // counts (re)builds of the PCG graphs
+  // the reliable-update mixed solve as one graph (built with device_loop)
+  cudaGraphExec_t gmixed = nullptr;
+  uint64_t gmixed_gen = 0;
+  exfem::DevBuf<exfem::MixedScal> mx_scal;
+  exfem::DevBuf<double> mx_b, mx_x;
   std::vector<const double*> g_Ke[2];
   ~exfem_solver_s();
 };
