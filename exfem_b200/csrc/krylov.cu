@@ -1003,7 +1003,9 @@ static int capture_into(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
   return EXFEM_OK;
 }
 
-static int mixed_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* out) {
+// the nodes of one reliable-update solve of mx_b into mx_x, appended to g after its
+// current leaves (g may be the body of an enclosing conditional node)
+static int mixed_nodes(exfem_solver_s* S, cudaStream_t st, cudaGraph_t g) {
   const int64_t n = S->n;
   const unsigned eg = grid_for(n, 256);
   MixedScal* ms = S->mx_scal.p;
@@ -1011,18 +1013,15 @@ static int mixed_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* ou
   float *x32 = S->x32.p, *r32 = S->r32.p, *z32 = S->z32.p, *p32 = S->p32.p;
   const double* b = S->mx_b.p;
   double* x = S->mx_x.p;
-  cudaGraph_t g = nullptr;
-  EX_CUDA(cudaGraphCreate(&g, 0));
-  auto fail = [&](int s) {
-    cudaGraphDestroy(g);
-    return s;
-  };
+  auto fail = [&](int s) { return s; };
   int s;
   cudaGraphConditionalHandle hs, hp;
   cudaGraph_t seg, body;
   cudaGraphNode_t n_seg, n_pcg;
+  std::vector<cudaGraphNode_t> leaves;
+  if ((s = graph_leaves(g, leaves))) return s;
   // head: x = 0, r64 = b, ||b||, start scalars, the PCG scalars' reset
-  s = capture_into(g, {}, st, [&]() -> int {
+  s = capture_into(g, leaves, st, [&]() -> int {
     EX_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
     EX_CUDA(cudaMemcpyAsync(S->r64.p, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     int q;
@@ -1033,7 +1032,6 @@ static int mixed_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* ou
   });
   if (s) return fail(s);
   // the segment loop
-  std::vector<cudaGraphNode_t> leaves;
   if ((s = graph_leaves(g, leaves))) return fail(s);
   {
     cudaError_t e = cudaGraphConditionalHandleCreate(&hs, g, 0, 0);
@@ -1113,7 +1111,17 @@ static int mixed_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* ou
     mx_cond_kernel<<<1, 1, 0, st>>>(hs, ms, 0);
     return EXFEM_OK;
   });
-  if (s) return fail(s);
+  return s;
+}
+
+static int mixed_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* out) {
+  cudaGraph_t g = nullptr;
+  EX_CUDA(cudaGraphCreate(&g, 0));
+  int s = mixed_nodes(S, st, g);
+  if (s) {
+    cudaGraphDestroy(g);
+    return s;
+  }
   *out = g;
   return EXFEM_OK;
 }
@@ -1162,6 +1170,382 @@ int solver_mixed_graph(exfem_solver_s* S, const double* b, double* x, double tol
   if (updates) *updates = h.nup;
   if (relres) *relres = h.rn / h.bn;
   return (std::isfinite(h.rn) && h.rn <= tol * h.bn) ? EXFEM_OK : EXFEM_NOT_CONVERGED;
+}
+
+// ---------------------------------------------------------------- Newton increment as one graph
+//
+// One increment of StaticSolver (gfem/solvers.py:607-683: the tangent predictor,
+// then Newton corrections with the reference's convergence test and its 4-step
+// backtracking line search) for a single-block model with the matrix-free tangent
+// and the reliable-update mixed solve, as one graph launch: every norm, test and
+// step length is computed on the device, the Newton loop and the line search are
+// conditional while nodes, each correction's linear solve sits under a conditional
+// if node (skipped once the increment has converged) and is the graph form of the
+// mixed solve (mixed_nodes).  Elementwise updates use unfused multiply and add, as
+// the host driver's array arithmetic does; norms are fixed-order device sums.
+
+__global__ void nw_init_kernel(NewtonScal* ns, double rtol, int max_iter, int line_search, double qref) {
+  ns->rtol = rtol;
+  ns->max_iter = max_iter;
+  ns->line_search = line_search;
+  ns->qref = qref;
+  ns->it = 0;
+  ns->done = 0;
+  ns->converged = 0;
+  ns->failed = 0;
+  ns->corrections = max_iter;
+  ns->dut = 0.0;
+  ns->loops = 0;
+}
+
+// d = a - b
+__global__ void nw_sub_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                              double* __restrict__ d) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    d[i] = __dsub_rn(a[i], b[i]);
+}
+
+// r = free * (f [+ k] - fext); with neg also rhs = -r
+__global__ void nw_residual_kernel(int64_t n, const uint8_t* __restrict__ fixed, const double* __restrict__ f,
+                                   const double* __restrict__ k, const double* __restrict__ fext, double* __restrict__ r) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double a = k ? __dadd_rn(f[i], k[i]) : f[i];
+    const double fr = (fixed && fixed[i]) ? 0.0 : 1.0;
+    r[i] = __dmul_rn(fr, __dsub_rn(a, fext[i]));
+  }
+}
+
+__global__ void nw_neg_kernel(int64_t n, const double* __restrict__ r, double* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = -r[i];
+}
+
+// predictor: qref = max(qref, ||r||)
+__global__ void nw_pred_kernel(NewtonScal* ns) { ns->qref = fmax(ns->qref, sqrt(ns->nrm_r)); }
+
+// u = ut + free * du
+__global__ void nw_pred_step_kernel(int64_t n, const uint8_t* __restrict__ fixed, const double* __restrict__ ut,
+                                    const double* __restrict__ du, double* __restrict__ u) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const double fr = (fixed && fixed[i]) ? 0.0 : 1.0;
+    u[i] = __dadd_rn(ut[i], __dmul_rn(fr, du[i]));
+  }
+}
+
+__global__ void nw_fn_kernel(NewtonScal* ns) { ns->fn_t = sqrt(ns->nrm_t); }
+
+// the convergence test of one Newton iteration (gfem/solvers.py:640-660); sets the
+// condition of the correction that follows
+__global__ void nw_test_kernel(NewtonScal* ns, cudaGraphConditionalHandle h_solve) {
+  ns->it += 1;
+  const double rt = sqrt(ns->nrm_r), ft = sqrt(ns->nrm_f), utn = sqrt(ns->nrm_u);
+  ns->rt = rt;
+  ns->ft = ft;
+  const double ref = fmax(fmax(ns->fn_t, ft), fmax(1e-3 * ns->qref, 1e-30));
+  ns->qref = fmax(ns->qref, fmax(ns->fn_t, ft));
+  const double ratio = rt / ref;
+  ns->ratio = ratio;
+  if (ns->it <= 64) ns->hist[ns->it - 1] = ratio;
+  if (!isfinite(rt)) {
+    ns->failed = 1;
+    ns->done = 1;
+  } else {
+    const bool small_du = ns->dut <= 1e-2 * fmax(utn, 1e-30);
+    if (ratio <= ns->rtol * 1e-2 || (ns->it > 1 && ratio <= ns->rtol && small_du)) {
+      ns->converged = 1;
+      ns->done = 1;
+      ns->corrections = ns->it - 1;
+    }
+  }
+  ns->alpha = 1.0;
+  ns->rls = rt;
+  ns->ls_count = 0;
+  ns->ls_done = !ns->line_search;
+  cudaGraphSetConditional(h_solve, ns->done ? 0u : 1u);
+}
+
+// trial point of the line search: ut = u + alpha du
+__global__ void nw_trial_kernel(int64_t n, const double* __restrict__ u, const double* __restrict__ du,
+                                double* __restrict__ ut, const NewtonScal* ns) {
+  const double a = ns->alpha;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    ut[i] = __dadd_rn(u[i], __dmul_rn(a, du[i]));
+}
+
+// accept the step when the trial residual fell below the current one or alpha < 0.2
+__global__ void nw_ls_test_kernel(NewtonScal* ns, cudaGraphConditionalHandle h) {
+  ns->ls_count += 1;
+  const double n2 = sqrt(ns->nrm_r);
+  ns->n2 = n2;
+  if (n2 < ns->rls || ns->alpha < 0.2) ns->ls_done = 1;
+  else ns->alpha *= 0.5;
+  cudaGraphSetConditional(h, (!ns->ls_done && ns->ls_count < 4) ? 1u : 0u);
+}
+
+__global__ void nw_ls_head_kernel(NewtonScal* ns, cudaGraphConditionalHandle h) {
+  cudaGraphSetConditional(h, ns->ls_done ? 0u : 1u);
+}
+
+// u = u + alpha du; dut = |alpha| ||du|| (alpha is a power of two: the same as ||alpha du||)
+__global__ void nw_step_kernel(int64_t n, double* __restrict__ u, const double* __restrict__ du,
+                               const NewtonScal* ns) {
+  const double a = ns->alpha;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    u[i] = __dadd_rn(u[i], __dmul_rn(a, du[i]));
+}
+
+__global__ void nw_dut_kernel(NewtonScal* ns) { ns->dut = fabs(ns->alpha) * sqrt(ns->nrm_du); }
+
+// Newton loop condition: another iteration while not done, at most max_iter
+__global__ void nw_cond_kernel(cudaGraphConditionalHandle h, NewtonScal* ns, int head) {
+  if (head) ns->loops = 0;
+  else ns->loops += 1;
+  cudaGraphSetConditional(h, (!ns->done && ns->it < ns->max_iter && ns->loops <= ns->max_iter) ? 1u : 0u);
+}
+
+// internal force f (and, for J2, the new states and the consistent tangent data) at u
+static int nw_fint(exfem_solver_s* S, const double* u, double* s_new, double* f, cudaStream_t st) {
+  exfem_block_s* b = S->blk;
+  const bool j2 = b->mat.kind == EXFEM_J2;
+  int s;
+  if ((s = launch_force(b, FORCE_FULL, u, j2 ? S->nw_s_old.p : nullptr, j2 ? s_new : nullptr, b->ys.p, nullptr,
+                        nullptr, nullptr, st)))
+    return s;
+  return launch_gather_assemble(b, b->ys.p, f, nullptr, nullptr, st);
+}
+
+static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* out) {
+  const int64_t n = S->n;
+  const unsigned eg = grid_for(n, 256);
+  exfem_block_s* b = S->blk;
+  const bool j2 = b->mat.kind == EXFEM_J2;
+  const uint8_t* fx = b->fixed.p;
+  NewtonScal* ns = S->nw_scal.p;
+  double *U = S->nw_u.p, *UT = S->nw_ut.p, *DU = S->nw_du.p, *R = S->nw_r.p, *F = S->nw_f.p, *T = S->nw_t.p;
+  const double *FEXT = S->nw_fext.p, *START = S->nw_start.p;
+  cudaGraph_t g = nullptr;
+  EX_CUDA(cudaGraphCreate(&g, 0));
+  auto fail = [&](int s) {
+    cudaGraphDestroy(g);
+    return s;
+  };
+  int s;
+  std::vector<cudaGraphNode_t> leaves;
+  // predictor (gfem/solvers.py:607-624): r = free (fint(uc) + K(uc)(ut - uc) - fext),
+  // du from the mixed solve of -r (a zero r solves to zero), u = ut + free du
+  s = capture_into(g, {}, st, [&]() -> int {
+    int q;
+    EX_CUDA(cudaMemcpyAsync(UT, START, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    nw_sub_kernel<<<eg, 256, 0, st>>>(n, UT, U, DU);
+    if ((q = nw_fint(S, U, S->nw_s_trial.p, F, st))) return q;
+    if (j2 && (q = launch_force(b, FORCE_TANGENT, U, S->nw_s_old.p, nullptr, nullptr, nullptr, nullptr, nullptr, st)))
+      return q;
+    if ((q = launch_mf_matvec<double>(b, DU, T, nullptr, st, false))) return q;
+    nw_residual_kernel<<<eg, 256, 0, st>>>(n, fx, F, T, FEXT, R);
+    if ((q = dot<double>(S, R, R, FIN_STORE, &ns->nrm_r, 0, st))) return q;
+    nw_pred_kernel<<<1, 1, 0, st>>>(ns);
+    if ((q = solver_refresh_diagonal(S, st))) return q;
+    nw_neg_kernel<<<eg, 256, 0, st>>>(n, R, S->mx_b.p);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  if ((s = mixed_nodes(S, st, g))) return fail(s);
+  if ((s = graph_leaves(g, leaves))) return fail(s);
+  s = capture_into(g, leaves, st, [&]() -> int {
+    nw_pred_step_kernel<<<eg, 256, 0, st>>>(n, fx, UT, S->mx_x.p, U);
+    int q;
+    if ((q = dot<double>(S, FEXT, FEXT, FIN_STORE, &ns->nrm_t, 0, st))) return q;
+    nw_fn_kernel<<<1, 1, 0, st>>>(ns);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  // Newton loop
+  cudaGraphConditionalHandle h_loop, h_solve, h_ls;
+  cudaGraph_t loop, solve, ls;
+  cudaGraphNode_t n_loop, n_solve, n_ls;
+  if ((s = graph_leaves(g, leaves))) return fail(s);
+  {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h_loop, g, 0, 0);
+    if (e != cudaSuccess) return fail((set_error("condition handle: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+  }
+  s = capture_into(g, leaves, st, [&]() -> int {
+    nw_cond_kernel<<<1, 1, 0, st>>>(h_loop, ns, 1);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  {
+    std::vector<cudaGraphNode_t> deps;
+    if ((s = graph_leaves(g, deps))) return fail(s);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(&n_loop, g, deps.data(), deps.size(), &cp);
+    if (e != cudaSuccess) return fail((set_error("while node: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+    loop = cp.conditional.phGraph_out[0];
+  }
+  // residual and convergence test; the if node's handle belongs to the loop body
+  {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h_solve, loop, 0, 0);
+    if (e != cudaSuccess) return fail((set_error("condition handle: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+  }
+  s = capture_into(loop, {}, st, [&]() -> int {
+    int q;
+    if ((q = nw_fint(S, U, S->nw_s_new.p, F, st))) return q;
+    nw_residual_kernel<<<eg, 256, 0, st>>>(n, fx, F, nullptr, FEXT, R);
+    if ((q = dot<double>(S, R, R, FIN_STORE, &ns->nrm_r, 0, st))) return q;
+    if ((q = dot<double>(S, F, F, FIN_STORE, &ns->nrm_f, 0, st))) return q;
+    if ((q = dot<double>(S, U, U, FIN_STORE, &ns->nrm_u, 0, st))) return q;
+    nw_test_kernel<<<1, 1, 0, st>>>(ns, h_solve);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  {
+    std::vector<cudaGraphNode_t> deps;
+    if ((s = graph_leaves(loop, deps))) return fail(s);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_solve;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(&n_solve, loop, deps.data(), deps.size(), &cp);
+    if (e != cudaSuccess) return fail((set_error("if node: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+    solve = cp.conditional.phGraph_out[0];
+  }
+  // the correction: tangent and diagonal at (u, states of the last converged
+  // increment), du from the mixed solve of -r
+  s = capture_into(solve, {}, st, [&]() -> int {
+    int q;
+    if (j2 && (q = launch_force(b, FORCE_TANGENT, U, S->nw_s_old.p, nullptr, nullptr, nullptr, nullptr, nullptr, st)))
+      return q;
+    if ((q = solver_refresh_diagonal(S, st))) return q;
+    nw_neg_kernel<<<eg, 256, 0, st>>>(n, R, S->mx_b.p);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  if ((s = mixed_nodes(S, st, solve))) return fail(s);
+  // line search (gfem/solvers.py:670-677): up to four trial points
+  if ((s = graph_leaves(solve, leaves))) return fail(s);
+  {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h_ls, solve, 0, 0);
+    if (e != cudaSuccess) return fail((set_error("condition handle: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+  }
+  s = capture_into(solve, leaves, st, [&]() -> int {
+    nw_ls_head_kernel<<<1, 1, 0, st>>>(ns, h_ls);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  {
+    std::vector<cudaGraphNode_t> deps;
+    if ((s = graph_leaves(solve, deps))) return fail(s);
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_ls;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(&n_ls, solve, deps.data(), deps.size(), &cp);
+    if (e != cudaSuccess) return fail((set_error("while node: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
+    ls = cp.conditional.phGraph_out[0];
+  }
+  s = capture_into(ls, {}, st, [&]() -> int {
+    int q;
+    nw_trial_kernel<<<eg, 256, 0, st>>>(n, U, S->mx_x.p, UT, ns);
+    if ((q = nw_fint(S, UT, S->nw_s_trial.p, T, st))) return q;
+    nw_residual_kernel<<<eg, 256, 0, st>>>(n, fx, T, nullptr, FEXT, DU);
+    if ((q = dot<double>(S, DU, DU, FIN_STORE, &ns->nrm_r, 0, st))) return q;
+    nw_ls_test_kernel<<<1, 1, 0, st>>>(ns, h_ls);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  s = capture_into(solve, {n_ls}, st, [&]() -> int {
+    nw_step_kernel<<<eg, 256, 0, st>>>(n, U, S->mx_x.p, ns);
+    int q;
+    if ((q = dot<double>(S, S->mx_x.p, S->mx_x.p, FIN_STORE, &ns->nrm_du, 0, st))) return q;
+    nw_dut_kernel<<<1, 1, 0, st>>>(ns);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  // loop condition after the (possibly skipped) correction
+  s = capture_into(loop, {n_solve}, st, [&]() -> int {
+    nw_cond_kernel<<<1, 1, 0, st>>>(h_loop, ns, 0);
+    return EXFEM_OK;
+  });
+  if (s) return fail(s);
+  *out = g;
+  return EXFEM_OK;
+}
+
+int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, const double* fext,
+                     const double* start, double rtol, int max_iter, int line_search, double cg_tol, int cg_maxiter,
+                     double* qref, double* u_out, double* s_out, int* corrections, int* converged, double* hist,
+                     cudaStream_t st) {
+  exfem_block_s* b = S->blk;
+  const int64_t n = S->n;
+  const bool j2 = b->mat.kind == EXFEM_J2;
+  if (S->op != EXFEM_OP_MF_F32 || S->pc != EXFEM_PC_AMG || !S->amg || !S->more.empty()) {
+    set_error("the device Newton increment needs a one-block solver with the FP32 matrix-free operator and an "
+              "AMG hierarchy");
+    return EXFEM_ERR_ARG;
+  }
+  if (max_iter < 1 || max_iter > 64) {
+    set_error("max_iter must lie in 1..64, got %d", max_iter);
+    return EXFEM_ERR_ARG;
+  }
+  const int64_t nst = j2 ? b->ne * b->ngp * b->nstate : 0;
+  int s;
+  // everything the captured work touches exists before the capture
+  if ((s = pcg_prepare<float>(S, st))) return s;
+  if (!S->mx_b.p && ((s = S->mx_b.alloc(std::max<int64_t>(n, 1))) || (s = S->mx_x.alloc(std::max<int64_t>(n, 1))) ||
+                     (s = S->mx_scal.alloc(1))))
+    return s;
+  if (!S->nw_scal.p) {
+    DevBuf<double>* v[] = {&S->nw_u, &S->nw_ut, &S->nw_du, &S->nw_r, &S->nw_f, &S->nw_t, &S->nw_fext, &S->nw_start};
+    for (auto* p : v)
+      if ((s = p->alloc(std::max<int64_t>(n, 1)))) return s;
+    if ((s = S->nw_scal.alloc(1))) return s;
+  }
+  if (j2 && S->nw_s_old.n < (size_t)nst) {
+    DevBuf<double>* v[] = {&S->nw_s_old, &S->nw_s_new, &S->nw_s_trial};
+    for (auto* p : v)
+      if ((s = p->alloc(nst))) return s;
+  }
+  if (b->ys.n < (size_t)(b->ne * b->nnode * 3) && (s = b->ys.alloc(b->ne * b->nnode * 3))) return s;
+  if (S->gnewton && S->gnewton_gen != S->graph_gen) {
+    cudaGraphExecDestroy(S->gnewton);
+    S->gnewton = nullptr;
+  }
+  if (!S->gnewton) {
+    // one eager FP64 product sets up the matrix-free operator's maps before the capture
+    if ((s = launch_mf_matvec<double>(b, S->nw_u.p, S->nw_t.p, nullptr, st, false))) return s;
+    CaptureScope cap;
+    cudaGraph_t g = nullptr;
+    if ((s = newton_graph_build(S, st, &g))) return s;
+    cudaError_t e = cudaGraphInstantiate(&S->gnewton, g, 0);
+    cudaGraphDestroy(g);
+    EX_CUDA(e);
+    S->gnewton_gen = S->graph_gen;
+  }
+  EX_CUDA(cudaMemcpyAsync(S->nw_u.p, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  EX_CUDA(cudaMemcpyAsync(S->nw_fext.p, fext, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  EX_CUDA(cudaMemcpyAsync(S->nw_start.p, start, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  if (j2) EX_CUDA(cudaMemcpyAsync(S->nw_s_old.p, s_old, sizeof(double) * nst, cudaMemcpyDeviceToDevice, st));
+  nw_init_kernel<<<1, 1, 0, st>>>(S->nw_scal.p, rtol, max_iter, line_search, *qref);
+  mx_params_kernel<<<1, 1, 0, st>>>(S->mx_scal.p, cg_tol, S->mixed_delta, cg_maxiter, 1200);
+  EX_LAUNCH_CHECK();
+  EX_CUDA(cudaGraphLaunch(S->gnewton, st));
+  EX_CUDA(cudaMemcpyAsync(u_out, S->nw_u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  if (j2) EX_CUDA(cudaMemcpyAsync(s_out, S->nw_s_new.p, sizeof(double) * nst, cudaMemcpyDeviceToDevice, st));
+  NewtonScal h;
+  EX_CUDA(cudaMemcpyAsync(&h, S->nw_scal.p, sizeof(NewtonScal), cudaMemcpyDeviceToHost, st));
+  EX_CUDA(cudaStreamSynchronize(st));
+  ++b->tan_gen;  // the graph changed the tangent data: the next host solve refreshes its diagonal
+  *qref = h.qref;
+  if (corrections) *corrections = h.corrections;
+  if (converged) *converged = h.converged && !h.failed;
+  if (hist)
+    for (int k = 0; k < std::min(h.it, 64); ++k) hist[k] = h.hist[k];
+  return EXFEM_OK;
 }
 
 int solver_alloc(exfem_solver_s* S) {

@@ -79,6 +79,13 @@ struct PcgScal {
   int k, maxiter, done, pad;
 };
 
+// device scalars of the Newton increment run as one graph
+struct NewtonScal {
+  double rtol, fn_t, qref, rt, ft, ut_n, ratio, dut, alpha, rls, n2, nrm_r, nrm_f, nrm_u, nrm_du, nrm_t;
+  int it, max_iter, done, converged, failed, corrections, line_search, ls_count, ls_done, loops;
+  double hist[64];
+};
+
 // device scalars of the reliable-update mixed solve run as one graph
 struct MixedScal {
   double tol, delta, bn, rn, rn_prev, sc, inv_sc, nrm2;
@@ -143,6 +150,11 @@ struct exfem_solver_s {
   uint64_t gmixed_gen = 0;
   exfem::DevBuf<exfem::MixedScal> mx_scal;
   exfem::DevBuf<double> mx_b, mx_x;
+  // the Newton increment as one graph (exfem_newton_increment)
+  cudaGraphExec_t gnewton = nullptr;
+  uint64_t gnewton_gen = 0;
+  exfem::DevBuf<exfem::NewtonScal> nw_scal;
+  exfem::DevBuf<double> nw_u, nw_ut, nw_du, nw_r, nw_f, nw_t, nw_fext, nw_start, nw_s_old, nw_s_new, nw_s_trial;
   std::vector<const double*> g_Ke[2];
   ~exfem_solver_s();
 };

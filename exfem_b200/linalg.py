@@ -494,6 +494,26 @@ class NativeSolver:
         self.last_iters = k.value
         return x, k.value, rr.value
 
+    def newton_increment(self, u, state, fext, start, qref, rtol, max_iter, line_search, cg_tol, cg_maxiter):
+        """One Newton increment (predictor and corrections, gfem/solvers.py:607-683)
+        as one graph launch on this solver (one block, FP32 matrix-free operator, AMG,
+        reliable updates): (converged, corrections, u, state, qref, ratios)."""
+        u = u.to(torch.float64).contiguous()
+        fext = fext.to(torch.float64).contiguous()
+        start = start.to(torch.float64).contiguous()
+        s_old = state.contiguous() if state is not None else None
+        u_out = torch.empty_like(u)
+        s_out = torch.empty_like(s_old) if s_old is not None else None
+        q = C.c_double(float(qref))
+        k, ok = C.c_int(), C.c_int()
+        ratios = np.zeros(max(int(max_iter), 1))
+        check(lib.exfem_newton_increment(self._h, ptr(u), ptr(s_old), ptr(fext), ptr(start), float(rtol), int(max_iter),
+                                         1 if line_search else 0, float(cg_tol), int(cg_maxiter), C.byref(q),
+                                         ptr(u_out), ptr(s_out), C.byref(k), C.byref(ok), ratios.ctypes.data,
+                                         stream_ptr()))
+        n_it = k.value + 1 if ok.value else int(max_iter)
+        return bool(ok.value), k.value, u_out, s_out, q.value, ratios[:n_it]
+
     def mixed(self, b, tol=1e-8, inner_tol=2e-5, max_pass=12, maxiter=20000):
         b = b.to(torch.float64).contiguous()
         x = torch.empty_like(b)

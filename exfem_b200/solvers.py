@@ -322,11 +322,17 @@ class _LinearSystem:                                                    # solver
 class StaticSolver:                                                     # solvers.py:481-683
     def __init__(self, model, rtol=5e-3, max_iter=16, linear_solver="auto", tangent="ebe", cg_tol=1e-9,
                  cg_maxiter=20000, verbose=True, monitor=None, line_search=True, graph=True, amg=None,
-                 amg_setup="auto", mixed_mode="reliable", operator="gather", async_amg=150000):
+                 amg_setup="auto", mixed_mode="reliable", operator="gather", async_amg=150000,
+                 device_newton=True):
         """``amg``: a prebuilt :class:`linalg.AMG` that every step starts from instead
         of assembling and setting up its own (the serving path keeps one resident
-        per mesh); the rebuild rule still applies."""
+        per mesh); the rebuild rule still applies.  ``device_newton``: run each
+        increment (predictor, Newton corrections, line search, linear solves) as one
+        graph launch on the device where the configuration allows it (one block,
+        matrix-free tangent, mixed solver with reliable updates and graphs); the
+        host loop otherwise."""
         self.m, self.rtol, self.max_iter = model, rtol, max_iter
+        self.device_newton = device_newton
         self.mon = monitor or Monitor(verbose)
         self.line_search = line_search
         self.lin = _LinearSystem(model, linear_solver, tangent, cg_tol, cg_maxiter, self.mon, graph, amg_setup,
@@ -361,12 +367,45 @@ class StaticSolver:                                                     # solver
         (converged, corrections, u, states); a non-finite residual fails it."""
         fext = setup.fext(t_new)
         start = torch.where(setup.fixed_j, setup.prescribed(t_new), u)
+        if self._device_increment_ok():
+            return self._device_increment(u, states, start, fext, fields, setup, inc)
         try:
             start = self._predictor(u, states, start, fext, fields, setup)
             ok, its, u_new, s_new, _ = self._newton(start, states, fext, fields, setup, inc)
         except FloatingPointError:
             return False, 0, u, states
         return ok, its, u_new, s_new
+
+    _HOOKS = ("_fint", "_ops", "_linsolve", "_predictor", "_residual", "_newton")
+
+    def _device_increment_ok(self):
+        """The increment can run as one device graph: one block, matrix-free tangent,
+        the mixed solver with reliable updates and graphs, and none of the host
+        loop's hooks replaced by a subclass."""
+        lin = self.lin
+        return (self.device_newton and len(self.m.blocks) == 1 and lin.method == "mixed" and lin.tangent == "mf"
+                and lin.mixed_mode == "reliable" and lin.graph and 1 <= self.max_iter <= 64
+                and all(getattr(type(self), h) is getattr(StaticSolver, h) for h in self._HOOKS))
+
+    def _device_increment(self, u, states, start, fext, fields, setup, inc):
+        """_predictor + _newton of one increment in one graph launch
+        (exfem_newton_increment): the same steps and tests, evaluated on the device."""
+        lin = self.lin
+        self.m._apply_fields(fields)
+        blk = self.m.blocks[0]
+        blk.set_fixed(setup.fixed)
+        if lin.amg is None:                     # the hierarchy the first linear solve would set up
+            lin._build_amg(None, setup, (u, states, fields))
+        S = lin._solver("mf32", "amg")
+        j2 = blk.material.nstate > 1
+        ok, its, u_new, s_new, self.qref, ratios = S.newton_increment(
+            u, states[0] if j2 else None, fext, start, self.qref, self.rtol, self.max_iter, self.line_search,
+            lin.cg_tol, lin.cg_maxiter)
+        for it, r in enumerate(ratios, 1):
+            self.mon.iteration(inc=inc, it=it, residual=float(r), du=None)
+        if not ok:
+            return False, its, u, states
+        return True, its, u_new, ([s_new] if j2 else states)
 
     def solve(self, step, u0=None, states=None, fext0=None, callback=None, state=None, scale=None):
         m = self.m

@@ -145,6 +145,32 @@ def _j2_case(dt):
     return X, bcs, om, uo, so, io, pm
 
 
+@pytest.mark.parametrize("dt", [1.0, 0.2])
+def test_device_newton_increment_matches_host_loop(cuda, dt):
+    """The increment as one graph launch (exfem_newton_increment: predictor, Newton
+    corrections, line search and mixed solves on the device) against the host
+    driver's loop on the same solver configuration: the same Newton corrections
+    in every increment, displacements and von Mises stresses equal to the linear
+    solves' tolerance, and both within the reference's bars of the oracle."""
+    import exfem_b200 as xf
+    X, bcs, om, uo, so, io, pm = _j2_case(dt)
+    res = []
+    for device in (True, False):
+        m = xf.Model(X)
+        m.add_block(pm.blocks[0].conn, xf.HEX8, xf.J2Plasticity(E, NU, [[250.0, 0.0], [1250.0, 1.0]]))
+        s = xf.StaticSolver(m, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-10, verbose=False,
+                            device_newton=device)
+        assert s._device_increment_ok() == device
+        u, st, info = s.solve(xf.Step(bcs=bcs, dt_init=dt, dt_max=dt))
+        res.append((u, m.stresses(u, st)[0]["MISES"], [h[1] for h in info["history"]]))
+    (ud, md, cd), (uh, mh, ch) = res
+    assert cd == ch, (cd, ch)
+    assert rel_err(ud, uh) < 1e-9 and rel_err(md, mh) < 1e-8
+    co = [h[1] for h in io["history"]]
+    assert len(cd) == len(co) and all(abs(a - b) <= 1 for a, b in zip(cd, co)), (cd, co)
+    assert rel_err(ud, uo) < 1e-5
+
+
 @pytest.mark.parametrize("method,tangent", [("amg", "ebe"), ("mixed", "mf")])
 def test_j2_newton_counts_single_increment(cuda, method, tangent):
     """One increment from the virgin state: no Gauss point starts on the yield
