@@ -12,12 +12,13 @@
 // Per element the work is Ke (nd x nd) times U_e (nd x nrhs): 2 FMA per byte of
 // BF16 Ke at four right-hand sides, far below what the tensor cores need to be the
 // bound, so the contraction runs on the CUDA cores and the kernel is bound by
-// streaming Ke.  One warp per element at a time (grid-stride): the warp gathers the
-// element's nodal values (prescribed DOFs zeroed) into its shared-memory slice,
-// lane i < nd multiplies row i of Ke — read with the widest aligned loads — by them
-// (broadcast reads) and stores the nrhs results of its row; the element rows are
-// then summed per node through the gather plan in the reference's order
-// (gfem/model.py:241-267) and opA's prescribed rows applied (gather_multi_kernel).
+// streaming Ke.  Each warp takes elements in turn (grid-stride, two per pass for BF16
+// and FP32 Ke): it gathers their nodal values (prescribed DOFs zeroed) into its
+// shared-memory slice, lane i < nd multiplies row i of Ke — read with the widest
+// aligned loads — by them (broadcast reads) and stores the nrhs results of its row;
+// the element rows are then summed per node through the gather plan in the
+// reference's order (gfem/model.py:241-267) and opA's prescribed rows applied
+// (gather_multi_kernel).
 #include <cuda_bf16.h>
 
 #include <algorithm>
