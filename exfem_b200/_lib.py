@@ -90,7 +90,7 @@ _SIGS = {
     "exfem_solver_set_graph": ([VP, C.c_int, C.c_int], C.c_int),
     "exfem_solver_set_loop": ([VP, C.c_int], C.c_int),
     "exfem_newton_increment": ([VP, VP, VP, VP, VP, C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, VP, VP, VP,
-                                VP, VP, VP, VP], C.c_int),
+                                VP, VP, VP, VP, VP], C.c_int),
     "exfem_solver_pcg": ([VP, P, P, D, C.c_int, C.POINTER(I32), C.POINTER(D), VP], C.c_int),
     "exfem_solver_mixed": ([VP, P, P, D, D, C.c_int, C.c_int, C.POINTER(I32), C.POINTER(I32), C.POINTER(D), VP],
                            C.c_int),

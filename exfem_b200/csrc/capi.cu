@@ -39,7 +39,7 @@ int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int ma
 int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, const double* fext,
                      const double* start, double rtol, int max_iter, int line_search, double cg_tol, int cg_maxiter,
                      double* qref, double* u_out, double* s_out, int* corrections, int* converged, double* hist,
-                     cudaStream_t st);
+                     int* lin_stats, cudaStream_t st);
 int solver_mixed_graph(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
                        int maxiter, int* iters, int* updates, double* relres, cudaStream_t st);
 int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
@@ -781,7 +781,7 @@ int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, d
 int exfem_newton_increment(exfem_solver s, const double* u, const double* state_old, const double* fext,
                            const double* start, double rtol, int max_iter, int line_search, double cg_tol,
                            int cg_maxiter, double* qref, double* u_out, double* state_out, int* corrections,
-                           int* converged, double* ratios, void* stream) {
+                           int* converged, double* ratios, int* lin_stats, void* stream) {
   EX_ARG(s && u && fext && start && qref && u_out, "NULL argument");
   EX_ARG(s->blk->mat.kind != EXFEM_J2 || (state_old && state_out), "J2 material needs state_old and state_out");
   EX_ARG(rtol > 0 && cg_tol > 0 && cg_maxiter >= 0, "invalid tolerances");
@@ -791,7 +791,7 @@ int exfem_newton_increment(exfem_solver s, const double* u, const double* state_
   int st;
   if ((st = g.init(stream))) return st;
   const int r = newton_increment(s, u, state_old, fext, start, rtol, max_iter, line_search != 0, cg_tol, cg_maxiter,
-                                 qref, u_out, state_out, corrections, converged, ratios, g.work);
+                                 qref, u_out, state_out, corrections, converged, ratios, lin_stats, g.work);
   if (r < 0) return r;
   const int w = block_wait_status(s->blk, g.work);
   return w < 0 ? w : r;

@@ -1234,6 +1234,11 @@ __global__ void nw_pred_step_kernel(int64_t n, const uint8_t* __restrict__ fixed
 
 __global__ void nw_fn_kernel(NewtonScal* ns) { ns->fn_t = sqrt(ns->nrm_t); }
 
+__global__ void nw_lin_kernel(NewtonScal* ns, const MixedScal* ms) {
+  ns->lin_its = ms->its;
+  ns->lin_nup = ms->nup;
+}
+
 // the convergence test of one Newton iteration (gfem/solvers.py:640-660); sets the
 // condition of the correction that follows
 __global__ void nw_test_kernel(NewtonScal* ns, cudaGraphConditionalHandle h_solve) {
@@ -1344,7 +1349,9 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
     nw_residual_kernel<<<eg, 256, 0, st>>>(n, fx, F, T, FEXT, R);
     if ((q = dot<double>(S, R, R, FIN_STORE, &ns->nrm_r, 0, st))) return q;
     nw_pred_kernel<<<1, 1, 0, st>>>(ns);
-    if ((q = solver_refresh_diagonal(S, st))) return q;
+    // the tangent of a J2 block changes with u and the states: its diagonal with it
+    // (an elastic block's diagonal is refreshed before the launch when stale)
+    if (j2 && (q = solver_refresh_diagonal(S, st))) return q;
     nw_neg_kernel<<<eg, 256, 0, st>>>(n, R, S->mx_b.p);
     return EXFEM_OK;
   });
@@ -1352,6 +1359,7 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
   if ((s = mixed_nodes(S, st, g))) return fail(s);
   if ((s = graph_leaves(g, leaves))) return fail(s);
   s = capture_into(g, leaves, st, [&]() -> int {
+    nw_lin_kernel<<<1, 1, 0, st>>>(ns, S->mx_scal.p);
     nw_pred_step_kernel<<<eg, 256, 0, st>>>(n, fx, UT, S->mx_x.p, U);
     int q;
     if ((q = dot<double>(S, FEXT, FEXT, FIN_STORE, &ns->nrm_t, 0, st))) return q;
@@ -1419,7 +1427,7 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
     int q;
     if (j2 && (q = launch_force(b, FORCE_TANGENT, U, S->nw_s_old.p, nullptr, nullptr, nullptr, nullptr, nullptr, st)))
       return q;
-    if ((q = solver_refresh_diagonal(S, st))) return q;
+    if (j2 && (q = solver_refresh_diagonal(S, st))) return q;
     nw_neg_kernel<<<eg, 256, 0, st>>>(n, R, S->mx_b.p);
     return EXFEM_OK;
   });
@@ -1432,6 +1440,7 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
     if (e != cudaSuccess) return fail((set_error("condition handle: %s", cudaGetErrorString(e)), EXFEM_ERR_CUDA));
   }
   s = capture_into(solve, leaves, st, [&]() -> int {
+    nw_lin_kernel<<<1, 1, 0, st>>>(ns, S->mx_scal.p);
     nw_ls_head_kernel<<<1, 1, 0, st>>>(ns, h_ls);
     return EXFEM_OK;
   });
@@ -1479,7 +1488,7 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
 int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, const double* fext,
                      const double* start, double rtol, int max_iter, int line_search, double cg_tol, int cg_maxiter,
                      double* qref, double* u_out, double* s_out, int* corrections, int* converged, double* hist,
-                     cudaStream_t st) {
+                     int* lin_stats, cudaStream_t st) {
   exfem_block_s* b = S->blk;
   const int64_t n = S->n;
   const bool j2 = b->mat.kind == EXFEM_J2;
@@ -1531,6 +1540,7 @@ int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, co
   EX_CUDA(cudaMemcpyAsync(S->nw_start.p, start, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   if (j2) EX_CUDA(cudaMemcpyAsync(S->nw_s_old.p, s_old, sizeof(double) * nst, cudaMemcpyDeviceToDevice, st));
   nw_init_kernel<<<1, 1, 0, st>>>(S->nw_scal.p, rtol, max_iter, line_search, *qref);
+  EX_CUDA(cudaMemsetAsync(&S->nw_scal.p->lin_its, 0, 2 * sizeof(int), st));
   mx_params_kernel<<<1, 1, 0, st>>>(S->mx_scal.p, cg_tol, S->mixed_delta, cg_maxiter, 1200);
   EX_LAUNCH_CHECK();
   EX_CUDA(cudaGraphLaunch(S->gnewton, st));
@@ -1539,12 +1549,16 @@ int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, co
   NewtonScal h;
   EX_CUDA(cudaMemcpyAsync(&h, S->nw_scal.p, sizeof(NewtonScal), cudaMemcpyDeviceToHost, st));
   EX_CUDA(cudaStreamSynchronize(st));
-  ++b->tan_gen;  // the graph changed the tangent data: the next host solve refreshes its diagonal
+  if (j2) ++b->tan_gen;  // the graph changed the tangent data: the next host solve refreshes its diagonal
   *qref = h.qref;
   if (corrections) *corrections = h.corrections;
   if (converged) *converged = h.converged && !h.failed;
   if (hist)
     for (int k = 0; k < std::min(h.it, 64); ++k) hist[k] = h.hist[k];
+  if (lin_stats) {
+    lin_stats[0] = h.lin_its;
+    lin_stats[1] = h.lin_nup;
+  }
   return EXFEM_OK;
 }
 

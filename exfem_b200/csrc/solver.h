@@ -83,6 +83,7 @@ struct PcgScal {
 struct NewtonScal {
   double rtol, fn_t, qref, rt, ft, ut_n, ratio, dut, alpha, rls, n2, nrm_r, nrm_f, nrm_u, nrm_du, nrm_t;
   int it, max_iter, done, converged, failed, corrections, line_search, ls_count, ls_done, loops;
+  int lin_its, lin_nup;  // FP32 iterations and replacements of the last linear solve
   double hist[64];
 };
 

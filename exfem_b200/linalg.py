@@ -507,10 +507,12 @@ class NativeSolver:
         q = C.c_double(float(qref))
         k, ok = C.c_int(), C.c_int()
         ratios = np.zeros(max(int(max_iter), 1))
+        lin = np.zeros(2, np.int32)
         check(lib.exfem_newton_increment(self._h, ptr(u), ptr(s_old), ptr(fext), ptr(start), float(rtol), int(max_iter),
                                          1 if line_search else 0, float(cg_tol), int(cg_maxiter), C.byref(q),
                                          ptr(u_out), ptr(s_out), C.byref(k), C.byref(ok), ratios.ctypes.data,
-                                         stream_ptr()))
+                                         lin.ctypes.data, stream_ptr()))
+        self.last_iters, self.last_passes = int(lin[0]), int(lin[1])
         n_it = k.value + 1 if ok.value else int(max_iter)
         return bool(ok.value), k.value, u_out, s_out, q.value, ratios[:n_it]
 

@@ -401,6 +401,7 @@ class StaticSolver:                                                     # solver
         ok, its, u_new, s_new, self.qref, ratios = S.newton_increment(
             u, states[0] if j2 else None, fext, start, self.qref, self.rtol, self.max_iter, self.line_search,
             lin.cg_tol, lin.cg_maxiter)
+        lin.last_iters, lin.last_passes = S.last_iters, S.last_passes
         for it, r in enumerate(ratios, 1):
             self.mon.iteration(inc=inc, it=it, residual=float(r), du=None)
         if not ok:

@@ -382,11 +382,13 @@ int exfem_solver_set_mixed_mode(exfem_solver s, int mode, double delta);
  * state_out at the last residual evaluation, corrections (Newton corrections when
  * converged, max_iter otherwise), converged (0 when the increment failed: not
  * converged in max_iter <= 64 iterations or a non-finite residual), ratios (the
- * residual ratio of every iteration, max_iter values at most). */
+ * residual ratio of every iteration, max_iter values at most), lin_stats (2: FP32
+ * iterations and FP64 replacements of the increment's last linear solve; may be
+ * NULL). */
 int exfem_newton_increment(exfem_solver s, const double* u, const double* state_old, const double* fext,
                            const double* start, double rtol, int max_iter, int line_search, double cg_tol,
                            int cg_maxiter, double* qref, double* u_out, double* state_out, int* corrections,
-                           int* converged, double* ratios, void* stream);
+                           int* converged, double* ratios, int* lin_stats, void* stream);
 
 /* ------------------------------------------------------------ batched solves
  * Many independent linear-elastic systems in one set of launches (no counterpart
