@@ -117,6 +117,7 @@ class _Entry:
             self.block = Block(spec.conn, spec.etype, spec.material, X=spec.X)
             self.block.set_fixed(spec.fixed)
             self.solver = linalg.NativeSolver(self.block, "mf32", "amg", self.amg, graph=graph)
+        self.static = None              # the J2 entry's StaticSolver, made by its first request
         self.bytes = spec.device_bytes_estimate()
         self.busy = False
         self.last_used = time.time()
@@ -313,9 +314,10 @@ class SolveServer:
                 raise RuntimeError(f"request {req.id}: refinement did not converge (rel. residual {rel:.2e})")
             return x.cpu().numpy(), dict(iters=k, passes=p, relres=rel)
         from .solvers import StaticSolver
-        s = StaticSolver(entry.model, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-6, verbose=False,
-                         graph=self.graph, amg=entry.amg)
-        u, states, info = s.solve(req.step)
+        if entry.static is None:        # kept with the entry: its solver handle and captured graphs are reused
+            entry.static = StaticSolver(entry.model, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-6,
+                                        verbose=False, graph=self.graph, amg=entry.amg)
+        u, states, info = entry.static.solve(req.step)
         return u.cpu().numpy(), dict(newton=info["iterations"], increments=info["increments"])
 
     def _worker(self, slot):
