@@ -401,7 +401,7 @@ def setup_section(n=80):
                 complexity=amg.complexity)
 
 
-def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), j2_frac=0.2, slots=8, seed=0,
+def serve_section(nmesh=24, rates=(50.0, 200.0), duration=15.0, dof=(1e3, 2e6), j2_frac=0.2, slots=24, seed=0,
                   nplain=32):
     """Served request stream: a catalogue of seeded C3D8 / C3D10 jittered
     cantilever meshes (DOF log-uniform in `dof`), a fraction `j2_frac` of them J2
