@@ -171,6 +171,54 @@ def test_device_newton_increment_matches_host_loop(cuda, dt):
     assert rel_err(ud, uo) < 1e-5
 
 
+def test_device_newton_failed_increment_cuts_back(cuda):
+    """An increment that the device graph cannot converge (max_iter = 2 where the
+    oracle needs more Newton corrections) comes back as failed and the host cuts the
+    increment back, as for the host loop: both paths take the same increments; without
+    line search both also take the same corrections."""
+    import exfem_b200 as xf
+    X, bcs, om, uo, so, io, pm = _j2_case(1.0)
+    assert max(h[1] for h in io["history"]) >= 2
+    res = []
+    for device in (True, False):
+        m = xf.Model(X)
+        m.add_block(pm.blocks[0].conn, xf.HEX8, xf.J2Plasticity(E, NU, [[250.0, 0.0], [1250.0, 1.0]]))
+        s = xf.StaticSolver(m, rtol=1e-6, max_iter=2, linear_solver="mixed", tangent="mf", cg_tol=1e-10,
+                            verbose=False, device_newton=device, line_search=False)
+        try:
+            u, st, info = s.solve(xf.Step(bcs=bcs, dt_init=1.0, dt_max=1.0, dt_min=1e-3, max_inc=50))
+            out = ("done", [round(h[0], 12) for h in info["history"]], info["increments"])
+        except RuntimeError as e:
+            out = ("failed", str(e).split(":")[0], None)
+        res.append(out)
+        m2 = xf.Model(X)
+        m2.add_block(pm.blocks[0].conn, xf.HEX8, xf.J2Plasticity(E, NU, [[250.0, 0.0], [1250.0, 1.0]]))
+        s2 = xf.StaticSolver(m2, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-10, verbose=False,
+                             device_newton=device, line_search=False)
+        u, st, info = s2.solve(xf.Step(bcs=bcs, dt_init=1.0, dt_max=1.0))
+        res.append((u, [h[1] for h in info["history"]]))
+    (cut_d, full_d), (cut_h, full_h) = res[0:2], res[2:4]
+    assert cut_d == cut_h, (cut_d, cut_h)
+    assert cut_d[0] == "failed" or cut_d[2] > len(cut_d[1])      # at least one increment was cut back
+    assert full_d[1] == full_h[1]
+    assert rel_err(full_d[0], full_h[0]) < 1e-9
+
+
+def test_device_newton_nonfinite_load_fails(cuda):
+    """A non-finite external force makes every device increment report failure (the
+    residual test sees a non-finite norm) and the step ends with the dt_min error,
+    with no fault on the GPU."""
+    import exfem_b200 as xf
+    X, bcs, om, uo, so, io, pm = _j2_case(1.0)
+    m = xf.Model(X)
+    m.add_block(pm.blocks[0].conn, xf.HEX8, xf.J2Plasticity(E, NU, [[250.0, 0.0], [1250.0, 1.0]]))
+    s = xf.StaticSolver(m, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-10, verbose=False)
+    assert s._device_increment_ok()
+    tip = np.nonzero(X[:, 0] > 100.0 - 1e-9)[0]
+    with pytest.raises(RuntimeError):
+        s.solve(xf.Step(bcs=bcs[:3], loads=[(tip, 2, float("nan"))], dt_init=1.0, dt_max=1.0, dt_min=0.1))
+
+
 @pytest.mark.parametrize("method,tangent", [("amg", "ebe"), ("mixed", "mf")])
 def test_j2_newton_counts_single_increment(cuda, method, tangent):
     """One increment from the virgin state: no Gauss point starts on the yield
