@@ -36,10 +36,10 @@ int host_face_once(int64_t nface, const int64_t* keys, uint8_t* once);
 int host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, std::vector<int32_t>& ptr,
                    std::vector<int32_t>& nodes, std::vector<uint16_t>& nend, std::vector<uint16_t>& perm, int& maxu);
 int solver_pcg(exfem_solver_s* S, const double* b, double* x, double tol, int maxiter, int* iters, double* relres, cudaStream_t st);
-int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, const double* fext,
+int newton_increment(exfem_solver_s* S, const double* u, const double* const* s_old, const double* fext,
                      const double* start, double rtol, int max_iter, int line_search, double cg_tol, int cg_maxiter,
-                     double* qref, double* u_out, double* s_out, int* corrections, int* converged, double* hist,
-                     int* lin_stats, cudaStream_t st);
+                     double* qref, double* u_out, double* const* s_out, int* corrections, int* converged,
+                     double* hist, int* lin_stats, cudaStream_t st);
 int solver_mixed_graph(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
                        int maxiter, int* iters, int* updates, double* relres, cudaStream_t st);
 int solver_mixed_ru(exfem_solver_s* S, const double* b, double* x, double tol, double delta, int max_updates,
@@ -778,20 +778,19 @@ int exfem_solver_mixed(exfem_solver s, const double* b, double* x, double tol, d
   return w < 0 ? w : r;
 }
 
-int exfem_newton_increment(exfem_solver s, const double* u, const double* state_old, const double* fext,
+int exfem_newton_increment(exfem_solver s, const double* u, const double* const* states_old, const double* fext,
                            const double* start, double rtol, int max_iter, int line_search, double cg_tol,
-                           int cg_maxiter, double* qref, double* u_out, double* state_out, int* corrections,
+                           int cg_maxiter, double* qref, double* u_out, double* const* states_out, int* corrections,
                            int* converged, double* ratios, int* lin_stats, void* stream) {
   EX_ARG(s && u && fext && start && qref && u_out, "NULL argument");
-  EX_ARG(s->blk->mat.kind != EXFEM_J2 || (state_old && state_out), "J2 material needs state_old and state_out");
   EX_ARG(rtol > 0 && cg_tol > 0 && cg_maxiter >= 0, "invalid tolerances");
   EX_ARG(s->mixed_mode == 1 && s->use_graph && s->device_loop,
          "the device Newton increment runs the reliable-update mixed solve with graphs and the device loop");
   StreamGuard g;
   int st;
   if ((st = g.init(stream))) return st;
-  const int r = newton_increment(s, u, state_old, fext, start, rtol, max_iter, line_search != 0, cg_tol, cg_maxiter,
-                                 qref, u_out, state_out, corrections, converged, ratios, lin_stats, g.work);
+  const int r = newton_increment(s, u, states_old, fext, start, rtol, max_iter, line_search != 0, cg_tol, cg_maxiter,
+                                 qref, u_out, states_out, corrections, converged, ratios, lin_stats, g.work);
   if (r < 0) return r;
   const int w = block_wait_status(s->blk, g.work);
   return w < 0 ? w : r;

@@ -1308,22 +1308,86 @@ __global__ void nw_cond_kernel(cudaGraphConditionalHandle h, NewtonScal* ns, int
   cudaGraphSetConditional(h, (!ns->done && ns->it < ns->max_iter && ns->loops <= ns->max_iter) ? 1u : 0u);
 }
 
-// internal force f (and, for J2, the new states and the consistent tangent data) at u
+// a += b
+__global__ void nw_add_kernel(int64_t n, double* __restrict__ a, const double* __restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    a[i] = __dadd_rn(a[i], b[i]);
+}
+
+// the model's blocks in order (the solver's first block, then the further ones)
+static exfem_block_s* nw_block(const exfem_solver_s* S, size_t i) { return i ? S->more[i - 1] : S->blk; }
+static size_t nw_nblock(const exfem_solver_s* S) { return 1 + S->more.size(); }
+static bool nw_j2(const exfem_block_s* b) { return b->mat.kind == EXFEM_J2; }
+// offset of block i's J2 states in the concatenated state buffers (0 entries for an
+// elastic block)
+static int64_t nw_state_off(const exfem_solver_s* S, size_t i) {
+  int64_t o = 0;
+  for (size_t k = 0; k < i; ++k) {
+    const exfem_block_s* b = nw_block(S, k);
+    if (nw_j2(b)) o += b->ne * b->ngp * b->nstate;
+  }
+  return o;
+}
+
+// internal force f = sum over the blocks, in block order (and, for J2 blocks, the
+// new states and the consistent tangent data) at u
 static int nw_fint(exfem_solver_s* S, const double* u, double* s_new, double* f, cudaStream_t st) {
-  exfem_block_s* b = S->blk;
-  const bool j2 = b->mat.kind == EXFEM_J2;
   int s;
-  if ((s = launch_force(b, FORCE_FULL, u, j2 ? S->nw_s_old.p : nullptr, j2 ? s_new : nullptr, b->ys.p, nullptr,
-                        nullptr, nullptr, st)))
-    return s;
-  return launch_gather_assemble(b, b->ys.p, f, nullptr, nullptr, st);
+  for (size_t i = 0; i < nw_nblock(S); ++i) {
+    exfem_block_s* b = nw_block(S, i);
+    const bool j2 = nw_j2(b);
+    const int64_t o = nw_state_off(S, i);
+    double* fb = i ? S->mb64.p : f;
+    if ((s = launch_force(b, FORCE_FULL, u, j2 ? S->nw_s_old.p + o : nullptr, j2 ? s_new + o : nullptr, b->ys.p,
+                          nullptr, nullptr, nullptr, st)))
+      return s;
+    if ((s = launch_gather_assemble(b, b->ys.p, fb, nullptr, nullptr, st))) return s;
+    if (i) {
+      nw_add_kernel<<<grid_for(S->n, 256), 256, 0, st>>>(S->n, f, fb);
+      EX_LAUNCH_CHECK();
+    }
+  }
+  return EXFEM_OK;
+}
+
+// consistent tangent data of every J2 block at (u, states of the last converged increment)
+static int nw_tangent(exfem_solver_s* S, const double* u, cudaStream_t st) {
+  int s;
+  for (size_t i = 0; i < nw_nblock(S); ++i) {
+    exfem_block_s* b = nw_block(S, i);
+    if (nw_j2(b) && (s = launch_force(b, FORCE_TANGENT, u, S->nw_s_old.p + nw_state_off(S, i), nullptr, nullptr,
+                                      nullptr, nullptr, nullptr, st)))
+      return s;
+  }
+  return EXFEM_OK;
+}
+
+// y = sum over the blocks of their FP64 matrix-free tangent products of v (no
+// prescribed rows), in block order
+static int nw_jvp(exfem_solver_s* S, const double* v, double* y, cudaStream_t st) {
+  int s;
+  for (size_t i = 0; i < nw_nblock(S); ++i) {
+    double* yb = i ? S->mb64.p : y;
+    if ((s = launch_mf_matvec<double>(nw_block(S, i), v, yb, nullptr, st, false))) return s;
+    if (i) {
+      nw_add_kernel<<<grid_for(S->n, 256), 256, 0, st>>>(S->n, y, yb);
+      EX_LAUNCH_CHECK();
+    }
+  }
+  return EXFEM_OK;
+}
+
+static bool nw_any_j2(const exfem_solver_s* S) {
+  for (size_t i = 0; i < nw_nblock(S); ++i)
+    if (nw_j2(nw_block(S, i))) return true;
+  return false;
 }
 
 static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* out) {
   const int64_t n = S->n;
   const unsigned eg = grid_for(n, 256);
   exfem_block_s* b = S->blk;
-  const bool j2 = b->mat.kind == EXFEM_J2;
+  const bool j2 = nw_any_j2(S);
   const uint8_t* fx = b->fixed.p;
   NewtonScal* ns = S->nw_scal.p;
   double *U = S->nw_u.p, *UT = S->nw_ut.p, *DU = S->nw_du.p, *R = S->nw_r.p, *F = S->nw_f.p, *T = S->nw_t.p;
@@ -1343,9 +1407,8 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
     EX_CUDA(cudaMemcpyAsync(UT, START, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     nw_sub_kernel<<<eg, 256, 0, st>>>(n, UT, U, DU);
     if ((q = nw_fint(S, U, S->nw_s_trial.p, F, st))) return q;
-    if (j2 && (q = launch_force(b, FORCE_TANGENT, U, S->nw_s_old.p, nullptr, nullptr, nullptr, nullptr, nullptr, st)))
-      return q;
-    if ((q = launch_mf_matvec<double>(b, DU, T, nullptr, st, false))) return q;
+    if ((q = nw_tangent(S, U, st))) return q;
+    if ((q = nw_jvp(S, DU, T, st))) return q;
     nw_residual_kernel<<<eg, 256, 0, st>>>(n, fx, F, T, FEXT, R);
     if ((q = dot<double>(S, R, R, FIN_STORE, &ns->nrm_r, 0, st))) return q;
     nw_pred_kernel<<<1, 1, 0, st>>>(ns);
@@ -1425,8 +1488,7 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
   // increment), du from the mixed solve of -r
   s = capture_into(solve, {}, st, [&]() -> int {
     int q;
-    if (j2 && (q = launch_force(b, FORCE_TANGENT, U, S->nw_s_old.p, nullptr, nullptr, nullptr, nullptr, nullptr, st)))
-      return q;
+    if ((q = nw_tangent(S, U, st))) return q;
     if (j2 && (q = solver_refresh_diagonal(S, st))) return q;
     nw_neg_kernel<<<eg, 256, 0, st>>>(n, R, S->mx_b.p);
     return EXFEM_OK;
@@ -1485,23 +1547,27 @@ static int newton_graph_build(exfem_solver_s* S, cudaStream_t st, cudaGraph_t* o
   return EXFEM_OK;
 }
 
-int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, const double* fext,
+int newton_increment(exfem_solver_s* S, const double* u, const double* const* s_old, const double* fext,
                      const double* start, double rtol, int max_iter, int line_search, double cg_tol, int cg_maxiter,
-                     double* qref, double* u_out, double* s_out, int* corrections, int* converged, double* hist,
-                     int* lin_stats, cudaStream_t st) {
-  exfem_block_s* b = S->blk;
+                     double* qref, double* u_out, double* const* s_out, int* corrections, int* converged,
+                     double* hist, int* lin_stats, cudaStream_t st) {
   const int64_t n = S->n;
-  const bool j2 = b->mat.kind == EXFEM_J2;
-  if (S->op != EXFEM_OP_MF_F32 || S->pc != EXFEM_PC_AMG || !S->amg || !S->more.empty()) {
-    set_error("the device Newton increment needs a one-block solver with the FP32 matrix-free operator and an "
-              "AMG hierarchy");
+  const size_t nb = nw_nblock(S);
+  const bool j2 = nw_any_j2(S);
+  if (S->op != EXFEM_OP_MF_F32 || S->pc != EXFEM_PC_AMG || !S->amg) {
+    set_error("the device Newton increment needs a solver with the FP32 matrix-free operator and an AMG hierarchy");
     return EXFEM_ERR_ARG;
   }
   if (max_iter < 1 || max_iter > 64) {
     set_error("max_iter must lie in 1..64, got %d", max_iter);
     return EXFEM_ERR_ARG;
   }
-  const int64_t nst = j2 ? b->ne * b->ngp * b->nstate : 0;
+  for (size_t i = 0; i < nb; ++i)
+    if (nw_j2(nw_block(S, i)) && (!s_old || !s_out || !s_old[i] || !s_out[i])) {
+      set_error("block %zu is J2: its state_old and state_out are needed", i);
+      return EXFEM_ERR_ARG;
+    }
+  const int64_t nst = nw_state_off(S, nb);
   int s;
   // everything the captured work touches exists before the capture
   if ((s = pcg_prepare<float>(S, st))) return s;
@@ -1514,19 +1580,24 @@ int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, co
       if ((s = p->alloc(std::max<int64_t>(n, 1)))) return s;
     if ((s = S->nw_scal.alloc(1))) return s;
   }
+  if (nb > 1 && S->mb64.n < (size_t)n && (s = S->mb64.alloc(std::max<int64_t>(n, 1)))) return s;
   if (j2 && S->nw_s_old.n < (size_t)nst) {
     DevBuf<double>* v[] = {&S->nw_s_old, &S->nw_s_new, &S->nw_s_trial};
     for (auto* p : v)
       if ((s = p->alloc(nst))) return s;
   }
-  if (b->ys.n < (size_t)(b->ne * b->nnode * 3) && (s = b->ys.alloc(b->ne * b->nnode * 3))) return s;
+  for (size_t i = 0; i < nb; ++i) {
+    exfem_block_s* b = nw_block(S, i);
+    if (b->ys.n < (size_t)(b->ne * b->nnode * 3) && (s = b->ys.alloc(b->ne * b->nnode * 3))) return s;
+  }
   if (S->gnewton && S->gnewton_gen != S->graph_gen) {
     cudaGraphExecDestroy(S->gnewton);
     S->gnewton = nullptr;
   }
   if (!S->gnewton) {
-    // one eager FP64 product sets up the matrix-free operator's maps before the capture
-    if ((s = launch_mf_matvec<double>(b, S->nw_u.p, S->nw_t.p, nullptr, st, false))) return s;
+    // one eager FP64 product per block sets up the matrix-free operators' maps before the capture
+    for (size_t i = 0; i < nb; ++i)
+      if ((s = launch_mf_matvec<double>(nw_block(S, i), S->nw_u.p, S->nw_t.p, nullptr, st, false))) return s;
     CaptureScope cap;
     cudaGraph_t g = nullptr;
     if ((s = newton_graph_build(S, st, &g))) return s;
@@ -1538,18 +1609,30 @@ int newton_increment(exfem_solver_s* S, const double* u, const double* s_old, co
   EX_CUDA(cudaMemcpyAsync(S->nw_u.p, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   EX_CUDA(cudaMemcpyAsync(S->nw_fext.p, fext, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   EX_CUDA(cudaMemcpyAsync(S->nw_start.p, start, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  if (j2) EX_CUDA(cudaMemcpyAsync(S->nw_s_old.p, s_old, sizeof(double) * nst, cudaMemcpyDeviceToDevice, st));
+  for (size_t i = 0; i < nb; ++i) {
+    const exfem_block_s* b = nw_block(S, i);
+    if (nw_j2(b))
+      EX_CUDA(cudaMemcpyAsync(S->nw_s_old.p + nw_state_off(S, i), s_old[i],
+                              sizeof(double) * b->ne * b->ngp * b->nstate, cudaMemcpyDeviceToDevice, st));
+  }
   nw_init_kernel<<<1, 1, 0, st>>>(S->nw_scal.p, rtol, max_iter, line_search, *qref);
   EX_CUDA(cudaMemsetAsync(&S->nw_scal.p->lin_its, 0, 2 * sizeof(int), st));
   mx_params_kernel<<<1, 1, 0, st>>>(S->mx_scal.p, cg_tol, S->mixed_delta, cg_maxiter, 1200);
   EX_LAUNCH_CHECK();
   EX_CUDA(cudaGraphLaunch(S->gnewton, st));
   EX_CUDA(cudaMemcpyAsync(u_out, S->nw_u.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  if (j2) EX_CUDA(cudaMemcpyAsync(s_out, S->nw_s_new.p, sizeof(double) * nst, cudaMemcpyDeviceToDevice, st));
+  for (size_t i = 0; i < nb; ++i) {
+    const exfem_block_s* b = nw_block(S, i);
+    if (nw_j2(b))
+      EX_CUDA(cudaMemcpyAsync(s_out[i], S->nw_s_new.p + nw_state_off(S, i),
+                              sizeof(double) * b->ne * b->ngp * b->nstate, cudaMemcpyDeviceToDevice, st));
+  }
   NewtonScal h;
   EX_CUDA(cudaMemcpyAsync(&h, S->nw_scal.p, sizeof(NewtonScal), cudaMemcpyDeviceToHost, st));
   EX_CUDA(cudaStreamSynchronize(st));
-  if (j2) ++b->tan_gen;  // the graph changed the tangent data: the next host solve refreshes its diagonal
+  // the graph changed the J2 blocks' tangent data: the next host solve refreshes its diagonal
+  for (size_t i = 0; i < nb; ++i)
+    if (nw_j2(nw_block(S, i))) ++nw_block(S, i)->tan_gen;
   *qref = h.qref;
   if (corrections) *corrections = h.corrections;
   if (converged) *converged = h.converged && !h.failed;

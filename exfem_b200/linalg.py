@@ -494,23 +494,26 @@ class NativeSolver:
         self.last_iters = k.value
         return x, k.value, rr.value
 
-    def newton_increment(self, u, state, fext, start, qref, rtol, max_iter, line_search, cg_tol, cg_maxiter):
+    def newton_increment(self, u, states, fext, start, qref, rtol, max_iter, line_search, cg_tol, cg_maxiter):
         """One Newton increment (predictor and corrections, gfem/solvers.py:607-683)
-        as one graph launch on this solver (one block, FP32 matrix-free operator, AMG,
-        reliable updates): (converged, corrections, u, state, qref, ratios)."""
+        as one graph launch on this solver (FP32 matrix-free operator, AMG, reliable
+        updates; one or several blocks).  states: per block its J2 state tensor or
+        None (elastic).  Returns (converged, corrections, u, states, qref, ratios)."""
         u = u.to(torch.float64).contiguous()
         fext = fext.to(torch.float64).contiguous()
         start = start.to(torch.float64).contiguous()
-        s_old = state.contiguous() if state is not None else None
+        s_old = [s.contiguous() if s is not None else None for s in states]
+        s_out = [torch.empty_like(s) if s is not None else None for s in s_old]
+        arr_old = (C.c_void_p * max(len(s_old), 1))(*[ptr(s) for s in s_old])
+        arr_out = (C.c_void_p * max(len(s_out), 1))(*[ptr(s) for s in s_out])
         u_out = torch.empty_like(u)
-        s_out = torch.empty_like(s_old) if s_old is not None else None
         q = C.c_double(float(qref))
         k, ok = C.c_int(), C.c_int()
         ratios = np.zeros(max(int(max_iter), 1))
         lin = np.zeros(2, np.int32)
-        check(lib.exfem_newton_increment(self._h, ptr(u), ptr(s_old), ptr(fext), ptr(start), float(rtol), int(max_iter),
+        check(lib.exfem_newton_increment(self._h, ptr(u), arr_old, ptr(fext), ptr(start), float(rtol), int(max_iter),
                                          1 if line_search else 0, float(cg_tol), int(cg_maxiter), C.byref(q),
-                                         ptr(u_out), ptr(s_out), C.byref(k), C.byref(ok), ratios.ctypes.data,
+                                         ptr(u_out), arr_out, C.byref(k), C.byref(ok), ratios.ctypes.data,
                                          lin.ctypes.data, stream_ptr()))
         self.last_iters, self.last_passes = int(lin[0]), int(lin[1])
         n_it = k.value + 1 if ok.value else int(max_iter)

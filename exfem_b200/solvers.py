@@ -379,11 +379,11 @@ class StaticSolver:                                                     # solver
     _HOOKS = ("_fint", "_ops", "_linsolve", "_predictor", "_residual", "_newton")
 
     def _device_increment_ok(self):
-        """The increment can run as one device graph: one block, matrix-free tangent,
-        the mixed solver with reliable updates and graphs, and none of the host
-        loop's hooks replaced by a subclass."""
+        """The increment can run as one device graph: matrix-free tangent, the mixed
+        solver with reliable updates and graphs, and none of the host loop's hooks
+        replaced by a subclass."""
         lin = self.lin
-        return (self.device_newton and len(self.m.blocks) == 1 and lin.method == "mixed" and lin.tangent == "mf"
+        return (self.device_newton and lin.method == "mixed" and lin.tangent == "mf"
                 and lin.mixed_mode == "reliable" and lin.graph and 1 <= self.max_iter <= 64
                 and all(getattr(type(self), h) is getattr(StaticSolver, h) for h in self._HOOKS))
 
@@ -392,21 +392,21 @@ class StaticSolver:                                                     # solver
         (exfem_newton_increment): the same steps and tests, evaluated on the device."""
         lin = self.lin
         self.m._apply_fields(fields)
-        blk = self.m.blocks[0]
-        blk.set_fixed(setup.fixed)
+        for blk in self.m.blocks:
+            blk.set_fixed(setup.fixed)
         if lin.amg is None:                     # the hierarchy the first linear solve would set up
             lin._build_amg(None, setup, (u, states, fields))
         S = lin._solver("mf32", "amg")
-        j2 = blk.material.nstate > 1
+        j2 = [blk.material.nstate > 1 for blk in self.m.blocks]
         ok, its, u_new, s_new, self.qref, ratios = S.newton_increment(
-            u, states[0] if j2 else None, fext, start, self.qref, self.rtol, self.max_iter, self.line_search,
-            lin.cg_tol, lin.cg_maxiter)
+            u, [s if f else None for s, f in zip(states, j2)], fext, start, self.qref, self.rtol, self.max_iter,
+            self.line_search, lin.cg_tol, lin.cg_maxiter)
         lin.last_iters, lin.last_passes = S.last_iters, S.last_passes
         for it, r in enumerate(ratios, 1):
             self.mon.iteration(inc=inc, it=it, residual=float(r), du=None)
         if not ok:
             return False, its, u, states
-        return True, its, u_new, ([s_new] if j2 else states)
+        return True, its, u_new, [n if f else s for s, n, f in zip(states, s_new, j2)]
 
     def solve(self, step, u0=None, states=None, fext0=None, callback=None, state=None, scale=None):
         m = self.m

@@ -372,22 +372,25 @@ int exfem_solver_set_mixed_mode(exfem_solver s, int mode, double delta);
  * 4-step backtracking line search) as one graph launch: the residual norms, the
  * convergence test, the step lengths and every linear solve (the reliable-update
  * mixed solve, FP32 matrix-free with the AMG V-cycle inside FP64 replacements, to
- * cg_tol) run on the device; the host reads the result once.  For a solver of one
- * block with EXFEM_OP_MF_F32, EXFEM_PC_AMG, reliable updates, graphs and the device
- * loop on; the block's prescribed DOFs are the step's.  u: converged displacements
- * of the previous increment (the predictor's start), state_old: its J2 states (ne,
- * ngp, nstate; NULL for elastic blocks), fext: the external force at the end of the
- * increment, start: u with the prescribed values of the increment's end on the
- * prescribed DOFs; qref: the running force scale (in and out).  Out: u_out and
- * state_out at the last residual evaluation, corrections (Newton corrections when
+ * cg_tol) run on the device; the host reads the result once.  For a solver with
+ * EXFEM_OP_MF_F32, EXFEM_PC_AMG, reliable updates, graphs and the device loop on, of
+ * one block or several (exfem_solver_add_block: forces, tangents and products are
+ * summed over the blocks in order); the blocks' prescribed DOFs are the step's.  u:
+ * converged displacements of the previous increment (the predictor's start),
+ * states_old: per block its J2 states (ne, ngp, nstate; the entry of an elastic block
+ * is ignored and may be NULL, as may the whole array for a model without J2 blocks),
+ * fext: the external force at the end of the increment, start: u with the prescribed
+ * values of the increment's end on the prescribed DOFs; qref: the running force
+ * scale (in and out).  Out: u_out and states_out (per block, like states_old) at the
+ * last residual evaluation, corrections (Newton corrections when
  * converged, max_iter otherwise), converged (0 when the increment failed: not
  * converged in max_iter <= 64 iterations or a non-finite residual), ratios (the
  * residual ratio of every iteration, max_iter values at most), lin_stats (2: FP32
  * iterations and FP64 replacements of the increment's last linear solve; may be
  * NULL). */
-int exfem_newton_increment(exfem_solver s, const double* u, const double* state_old, const double* fext,
+int exfem_newton_increment(exfem_solver s, const double* u, const double* const* states_old, const double* fext,
                            const double* start, double rtol, int max_iter, int line_search, double cg_tol,
-                           int cg_maxiter, double* qref, double* u_out, double* state_out, int* corrections,
+                           int cg_maxiter, double* qref, double* u_out, double* const* states_out, int* corrections,
                            int* converged, double* ratios, int* lin_stats, void* stream);
 
 /* ------------------------------------------------------------ batched solves

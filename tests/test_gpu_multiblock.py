@@ -117,6 +117,37 @@ def test_elastic_and_j2_blocks_newton_matches_oracle(cuda):
             assert rel_err(a["MISES"], b["MISES"]) < 1e-5
 
 
+def test_multi_block_device_newton_matches_host_loop(cuda):
+    """The device Newton increment over a J2 block and an elastic block (forces,
+    tangent products and states summed block by block) against the host loop, over
+    four increments so that the J2 block carries plastic history: the same Newton
+    counts, displacements and states to the Newton tolerance."""
+    import exfem_b200 as xf
+    from exfem_b200 import mesh
+    X, c = mesh.box_hex(100.0, 20.0, 20.0, 10, 2, 2)
+    X = mesh.jitter_interior(X, [10.0, 10.0, 10.0], 0.1, 6)
+    near = X[c].mean(1)[:, 0] < 30.0
+    fix = mesh.nodes_where(X, lambda x, y, z: x < 1e-9)
+    tip = mesh.nodes_where(X, lambda x, y, z: x > 100.0 - 1e-9)
+    bcs = [(fix, d, 0.0) for d in range(3)] + [(tip, 2, -1.5)]
+    table = [[250.0, 0.0], [1250.0, 1.0]]
+    out = {}
+    for device in (False, True):
+        pm = xf.Model(X)
+        pm.add_block(c[near], xf.HEX8, xf.J2Plasticity(*STEEL, table))
+        pm.add_block(c[~near], xf.HEX8, xf.LinearElastic(*STEEL))
+        sv = xf.StaticSolver(pm, rtol=1e-6, linear_solver="mixed", tangent="mf", cg_tol=1e-11, verbose=False,
+                             device_newton=device)
+        assert sv._device_increment_ok() == device
+        out[device] = sv.solve(xf.Step(bcs=bcs, dt_init=0.25))
+    (uh, sh, ih), (ud, sd, idv) = out[False], out[True]
+    assert float(sh[0][..., 9].max()) > 0
+    assert [h[1] for h in idv["history"]] == [h[1] for h in ih["history"]], (idv["history"], ih["history"])
+    assert rel_err(ud, uh) < 1e-6
+    for a, b in zip(sd, sh):
+        assert rel_err(a, b) < 1e-5
+
+
 def _write_two_section_deck(path, X, ca, cb):
     out = ["*HEADING", "two sections, two materials", "*NODE"]
     out += [f"{i + 1}, {X[i, 0]:.17g}, {X[i, 1]:.17g}, {X[i, 2]:.17g}" for i in range(len(X))]
