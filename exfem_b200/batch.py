@@ -109,11 +109,37 @@ def host_setups(problems, max_coarse=300, workers=None, stiffness=None):
         return list(ex.map(_setup_worker, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
 
 
-def _csr(M):
+def _canonical(M):
     M = M.tocsr()
+    M.sum_duplicates()
     M.sort_indices()
-    return (np.ascontiguousarray(M.indptr.astype(np.int64)), np.ascontiguousarray(M.indices.astype(np.int32)),
-            np.ascontiguousarray(M.data.astype(np.float64)))
+    return M
+
+
+def _block_diag_csr(blocks):
+    """Block-diagonal CSR arrays (indptr int64, indices int32, data float64) of
+    ``blocks`` (sparse matrices or ``(rows, cols)`` for an all-zero block), written
+    by shifting each block's CSR arrays: the rows of a block-diagonal matrix are its
+    blocks' rows with the column indices moved by the block's column offset."""
+    ncols = sum(b[1] if isinstance(b, tuple) else b.shape[1] for b in blocks)
+    if ncols >= 2 ** 31:
+        raise ValueError(f"union level of {ncols} columns exceeds 32-bit column indices")
+    ptrs, idx, val = [np.zeros(1, np.int64)], [], []
+    nnz = col0 = 0
+    for b in blocks:
+        if isinstance(b, tuple):
+            ptrs.append(np.full(b[0], nnz, np.int64))
+            col0 += b[1]
+            continue
+        b = _canonical(b)
+        ptrs.append(b.indptr[1:].astype(np.int64) + nnz)
+        idx.append(b.indices.astype(np.int32, copy=False) + np.int32(col0))
+        val.append(b.data.astype(np.float64, copy=False))
+        nnz += b.nnz
+        col0 += b.shape[1]
+    indices = np.concatenate(idx) if idx else np.zeros(0, np.int32)
+    data = np.concatenate(val) if val else np.zeros(0, np.float64)
+    return np.concatenate(ptrs), indices, data
 
 
 def union_hierarchy(setups):
@@ -142,16 +168,11 @@ def union_hierarchy(setups):
                 rho.append(np.full(lv["n"], lv["rho"]))
         sizes = [P.shape[0] for P in Ps]
         offsets.append(np.concatenate([[0], np.cumsum(sizes)]))
-        P = sp.block_diag(Ps, format="csr")
-        n, nc = P.shape
-        if l == 0:                                           # no stored level-0 matrix
-            A = sp.csr_matrix((n, n))
-        else:
-            A = sp.block_diag(As, format="csr")
-        R = P.T.tocsr()
-        Ap, Ai, Av = _csr(A)
-        Pp, Pi, Pv = _csr(P)
-        Rp, Ri, Rv = _csr(R)
+        n, nc = int(sum(sizes)), int(sum(P.shape[1] for P in Ps))
+        # no stored level-0 matrix: level 0 is smoothed with the matrix-free product
+        Ap, Ai, Av = _block_diag_csr([(P.shape[0], P.shape[0]) for P in Ps] if l == 0 else As)
+        Pp, Pi, Pv = _block_diag_csr(Ps)
+        Rp, Ri, Rv = _block_diag_csr([P.T for P in Ps])
         d = np.ascontiguousarray(np.concatenate(dinv))
         r = np.ascontiguousarray(np.concatenate(rho))
         check(lib.exfem_amg_add_level(h_amg, n, nc, Ap.ctypes.data, Ai.ctypes.data, Av.ctypes.data, Pp.ctypes.data,
