@@ -7,13 +7,14 @@ Buckling: K0 phi = -lambda KG phi through the smallest mu of KG phi = mu K0 phi
 step's loads, element matrices from the library's geometric-stiffness kernel; B =
 the stiffness K0 at u = 0; T = a device V-cycle of K0), lambda = -1/mu.
 
-K phi = w^2 M phi for the smallest eigenvalues: A = the block's FP64 matrix-free
-tangent product (prescribed DOFs held at zero), B = the HRZ-lumped mass matrix
-(gfem/model.py:120-124, 501-510), T = one smoothed-aggregation V-cycle of the
-stiffness (hierarchy set up on the device).  The modal A and every T application is
-a call of the library per column; the buckling A and B (stored element matrices)
-apply one multi-right-hand-side product per 16 columns, so each Ke is read once per
-block step; the block Rayleigh-Ritz steps are small dense products on
+K phi = w^2 M phi for the smallest eigenvalues: A = the stiffness (prescribed DOFs
+held at zero) from the stored FP64 element matrices, or the FP64 matrix-free product
+column by column, B = the HRZ-lumped mass matrix (gfem/model.py:120-124, 501-510),
+T = one smoothed-aggregation V-cycle of the stiffness (hierarchy set up on the
+device).  Every T application is a call of the library per column; the stored-Ke
+operators (the modal A, the buckling A and B) apply one multi-right-hand-side
+product per 16 columns, so each Ke is read once per block step; the block
+Rayleigh-Ritz steps are small dense products on
 the device and a small symmetric eigenproblem on the host, as in the reference
 (Knyazev's LOBPCG with SVQB orthonormalisation).
 """
@@ -137,10 +138,17 @@ def lobpcg(A, B, T, X0, k, tol=1e-6, maxiter=500, log=None):
     return np.asarray(lam[:k]), X[:, :k], it
 
 
-def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=None):
+def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=None, operator="stored"):
     """(w^2 (nmodes,), modes (nmodes, ndof)) of a model under the step's prescribed
     DOFs (gfem/eigen.py:99-124; ``nmodes`` is the reference step's ``nmodes``); the
-    stiffness of a model of several blocks is the sum over its blocks."""
+    stiffness of a model of several blocks is the sum over its blocks.  operator:
+    "stored" (default) keeps the FP64 element matrices the hierarchy is set up from
+    and applies them to up to 16 columns per product (the reference's block EbE
+    operator, gfem/eigen.py:97-110), each Ke read once per block step; "mf" applies
+    the FP64 matrix-free product column by column and keeps no element matrices
+    (ne x nd^2 doubles less on the device, about 13% slower)."""
+    if operator not in ("mf", "stored"):
+        raise ValueError(f"unknown modal operator {operator!r}")
     setup = _Setup(model, step, state or State(model))
     free = setup.free
     for blk in model.blocks:
@@ -149,6 +157,7 @@ def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=Non
     zero = torch.zeros(nd, dtype=torch.float64, device="cuda")
     Kes = [blk.stiffness(zero, blk.init_state()) for blk in model.blocks]
     amg = linalg.DeviceAMG(model.blocks, Kes, keep_level0=True)
+    stored = _ops_block(list(zip(model.blocks, Kes)), free) if operator == "stored" else None
     del Kes
     M = lumped_mass(model) * free
 
@@ -160,6 +169,8 @@ def modal_lobpcg(model, step, nmodes, state=None, tol=1e-6, maxiter=500, log=Non
         return out
 
     def A(V):
+        if stored is not None:
+            return stored(V)
         return torch.stack([K(V[:, j].contiguous()) for j in range(V.shape[1])], 1) * free[:, None]
 
     def B(V):
