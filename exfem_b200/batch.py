@@ -110,9 +110,12 @@ def host_setups(problems, max_coarse=300, workers=None, stiffness=None):
 
 
 def _canonical(M):
+    """M as CSR with sorted, summed entries (a copy where M is not, so that the
+    caller's matrix is left as it was)."""
     M = M.tocsr()
-    M.sum_duplicates()
-    M.sort_indices()
+    if not M.has_canonical_format:
+        M = M.copy()
+        M.sum_duplicates()
     return M
 
 

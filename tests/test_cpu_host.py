@@ -228,6 +228,46 @@ def test_batch_host_setups_in_spawned_workers():
             assert (la["P"] != lb["P"]).nnz == 0 and la["rho"] == lb["rho"]
 
 
+def test_batch_union_levels_equal_scipy_block_diag():
+    """The union level arrays written by shifting each problem's CSR arrays equal
+    SciPy's block_diag of the same blocks (canonicalised: summed duplicates, sorted
+    indices, explicit zeros kept), for unsorted and duplicated entries, identity
+    relays, empty rows and all-zero blocks given by their shape; the transpose
+    blocks give the union's transpose."""
+    from exfem_b200 import batch
+    rng = np.random.default_rng(5)
+    blocks = []
+    for n, m in ((7, 3), (1, 1), (12, 5), (4, 4), (9, 2)):
+        nnz = 3 * n
+        r, c = rng.integers(0, n, nnz), rng.integers(0, m, nnz)
+        v = rng.standard_normal(nnz)
+        v[::5] = 0.0                                         # explicit zeros stay
+        o = np.argsort(r, kind="stable")                     # rows in order, columns as drawn
+        blocks.append(sp.csr_matrix((v[o], c[o], np.searchsorted(r[o], np.arange(n + 1))), shape=(n, m)))
+    blocks.insert(2, sp.identity(3, format="csr"))
+    blocks.append(sp.csr_matrix((4, 2)))                     # empty rows
+    before = [(B.indptr.copy(), B.indices.copy(), B.data.copy()) for B in blocks]
+    ref = sp.block_diag(blocks, format="csr")
+    ref.sum_duplicates()
+    ref.sort_indices()
+    p, i, v = batch._block_diag_csr(blocks)
+    for B, (bp, bi, bv) in zip(blocks, before):               # the inputs are left as they were
+        assert np.array_equal(B.indptr, bp) and np.array_equal(B.indices, bi) and np.array_equal(B.data, bv)
+    assert p.dtype == np.int64 and i.dtype == np.int32 and v.dtype == np.float64
+    np.testing.assert_array_equal(p, ref.indptr)
+    np.testing.assert_array_equal(i, ref.indices)
+    np.testing.assert_array_equal(v, ref.data)
+    rt = ref.T.tocsr()
+    rt.sort_indices()
+    p, i, v = batch._block_diag_csr([B.T for B in blocks])
+    np.testing.assert_array_equal(p, rt.indptr)
+    np.testing.assert_array_equal(i, rt.indices)
+    np.testing.assert_array_equal(v, rt.data)
+    p, i, v = batch._block_diag_csr([(3, 3), (2, 2)])
+    np.testing.assert_array_equal(p, np.zeros(6, np.int64))
+    assert i.size == 0 and v.size == 0
+
+
 def test_random_cantilevers_follow_the_stated_ranges():
     from exfem_b200 import batch
     probs = batch.random_cantilevers(40, seed=3)
