@@ -499,6 +499,12 @@ class NativeSolver:
         as one graph launch on this solver (FP32 matrix-free operator, AMG, reliable
         updates; one or several blocks).  states: per block its J2 state tensor or
         None (elastic).  Returns (converged, corrections, u, states, qref, ratios)."""
+        if len(states) != len(self.blocks):
+            raise ValueError(f"one state entry per block: got {len(states)} for {len(self.blocks)} blocks")
+        for b, st in zip(self.blocks, states):
+            want = b.ne * b.etype.ngp * b.material.nstate
+            if b.material.nstate > 1 and (st is None or st.numel() != want or st.dtype != torch.float64):
+                raise ValueError(f"block {b.name}: J2 states need {want} FP64 values (ne, ngp, nstate)")
         u = u.to(torch.float64).contiguous()
         fext = fext.to(torch.float64).contiguous()
         start = start.to(torch.float64).contiguous()

@@ -734,3 +734,20 @@ def test_host_tile_maps_bit_exact(kind):
     for tile in (128, 256):
         for g, w in zip(_host_tile_maps(ct, len(X), tile), ofem.tile_maps(ct, tile)):
             np.testing.assert_array_equal(g, w)
+
+
+def test_newton_increment_checks_states_before_any_device_work():
+    """The device Newton increment takes one state entry per block, and a J2 block's
+    entry must hold its ne x ngp x nstate FP64 values: anything else is refused on
+    the host, before a pointer reaches the library."""
+    from types import SimpleNamespace as NS
+    import torch
+    j2 = NS(ne=2, etype=NS(ngp=8), material=NS(nstate=10), name="plastic")
+    el = NS(ne=3, etype=NS(ngp=8), material=NS(nstate=1), name="elastic")
+    fake = NS(blocks=[j2, el])
+    u = torch.zeros(12, dtype=torch.float64)
+    args = (u, u, 0.0, 1e-6, 4, True, 1e-6, 100)
+    for states in ([None], [None, None], [torch.zeros(2, 8, 9, dtype=torch.float64), None],
+                   [torch.zeros(2, 8, 10, dtype=torch.float32), None]):
+        with pytest.raises(ValueError):
+            linalg.NativeSolver.newton_increment(fake, u, states, *args)
