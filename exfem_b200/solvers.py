@@ -328,9 +328,9 @@ class StaticSolver:                                                     # solver
         of assembling and setting up its own (the serving path keeps one resident
         per mesh); the rebuild rule still applies.  ``device_newton``: run each
         increment (predictor, Newton corrections, line search, linear solves) as one
-        graph launch on the device where the configuration allows it (one block,
-        matrix-free tangent, mixed solver with reliable updates and graphs); the
-        host loop otherwise."""
+        graph launch on the device where the configuration allows it (matrix-free
+        tangent, mixed solver with reliable updates and graphs, any number of
+        blocks); the host loop otherwise."""
         self.m, self.rtol, self.max_iter = model, rtol, max_iter
         self.device_newton = device_newton
         self.mon = monitor or Monitor(verbose)
