@@ -1,6 +1,7 @@
 """CPU: mesh fixtures, host index builders through the C ABI, exported symbols,
 host smoothed-aggregation set-up, and the world-size-2 replicas path (gloo)."""
 import ctypes as C
+import json
 import os
 import re
 import subprocess
@@ -751,3 +752,37 @@ def test_newton_increment_checks_states_before_any_device_work():
                    [torch.zeros(2, 8, 10, dtype=torch.float32), None]):
         with pytest.raises(ValueError):
             linalg.NativeSolver.newton_increment(fake, u, states, *args)
+
+
+_NULL_CALLS = r'''
+import ctypes as C, json, sys
+from exfem_b200 import _lib
+out = {}
+for name, (argt, _) in sorted(_lib._SIGS.items()):
+    if name in ("exfem_version", "exfem_last_error"):
+        continue
+    args = [0 if t in (C.c_int, C.c_int64) else 0.0 if t is C.c_double else None for t in argt]
+    st = getattr(_lib.lib, name)(*args)
+    msg = _lib.lib.exfem_last_error()
+    out[name] = [st, msg.decode() if msg else ""]
+print(json.dumps(out))
+'''
+
+
+def test_every_export_refuses_null_arguments():
+    """Every export called with NULL pointers and zero sizes (no GPU needed) returns
+    a status without touching memory: an error with a message, except the destroy
+    calls (NULL is a no-op, like free) and the host builders given nothing to do.
+    Run in a child process, so that a crash fails the test instead of the run."""
+    env = dict(os.environ, PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    p = subprocess.run([sys.executable, "-c", _NULL_CALLS], capture_output=True, text=True, timeout=300, env=env,
+                       cwd=ROOT)
+    assert p.returncode == 0, p.stderr[-2000:]
+    res = json.loads(p.stdout.strip().splitlines()[-1])
+    ok_zero = {n for n in res if n.endswith("_destroy")} | {"exfem_host_face_once", "exfem_host_tile_pairs"}
+    assert len(res) > 70
+    for name, (st, msg) in res.items():
+        if name in ok_zero:
+            assert st == 0, (name, st, msg)
+        else:
+            assert st < 0 and msg, (name, st, msg)
