@@ -2,6 +2,8 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
+#include <new>
+#include <stdexcept>
 
 #include "sa.h"
 #include "solver.h"
@@ -154,6 +156,23 @@ struct StreamGuard {
   }
 };
 
+// Host work behind a C entry point: a C++ exception must not cross the C ABI, so
+// an allocation that fails (or a size no host array can hold) becomes a status
+template <class F>
+static int host_guard(F&& f) {
+  try {
+    return f();
+  } catch (const std::bad_alloc&) {
+    set_error("host memory exhausted");
+    return EXFEM_ERR_OOM;
+  } catch (const std::length_error&) {
+    set_error("size too large for a host array");
+    return EXFEM_ERR_ARG;
+  } catch (const std::exception& e) {
+    set_error("host error: %s", e.what());
+    return EXFEM_ERR_UNSUPPORTED;
+  }
+}
 
 extern "C" {
 
@@ -913,95 +932,124 @@ int exfem_selftest_bounded_wait(int polls, void* stream) {
 // ---------------------------------------------------------------- host builders
 int exfem_host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* plan, int* vmax) {
   EX_ARG(conn && vmax, "NULL argument");
-  std::vector<int32_t> p;
-  int v = 0, s;
-  if ((s = host_gather_plan(nn, ne, nnode, conn, p, v))) return s;
-  *vmax = v;
-  if (plan) memcpy(plan, p.data(), p.size() * sizeof(int32_t));
-  return EXFEM_OK;
+  EX_ARG(nn >= 0 && ne >= 0 && nnode >= 0, "invalid sizes (nn %lld, ne %lld, nnode %d)", (long long)nn,
+         (long long)ne, nnode);
+  return host_guard([&]() -> int {
+    std::vector<int32_t> p;
+    int v = 0, s;
+    if ((s = host_gather_plan(nn, ne, nnode, conn, p, v))) return s;
+    *vmax = v;
+    if (plan) memcpy(plan, p.data(), p.size() * sizeof(int32_t));
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int32_t* colour, int* ncolour) {
   EX_ARG(conn && colour && ncolour, "NULL argument");
-  std::vector<int32_t> c;
-  int s;
-  if ((s = host_colouring(nn, ne, nnode, conn, c, *ncolour))) return s;
-  memcpy(colour, c.data(), c.size() * sizeof(int32_t));
-  return EXFEM_OK;
+  EX_ARG(nn >= 0 && ne >= 0 && nnode >= 0, "invalid sizes (nn %lld, ne %lld, nnode %d)", (long long)nn,
+         (long long)ne, nnode);
+  for (int64_t k = 0; k < ne * nnode; ++k)
+    EX_ARG(conn[k] >= 0 && conn[k] < nn, "connectivity entry %d at slot %lld is outside [0, %lld)", conn[k],
+           (long long)k, (long long)nn);
+  return host_guard([&]() -> int {
+    std::vector<int32_t> c;
+    int s;
+    if ((s = host_colouring(nn, ne, nnode, conn, c, *ncolour))) return s;
+    memcpy(colour, c.data(), c.size() * sizeof(int32_t));
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_node_adjacency(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int64_t* nnz, int64_t* ptr,
                               int32_t* idx) {
   EX_ARG(nn >= 0 && ne >= 0 && nnode > 0 && (ne == 0 || conn) && nnz && ptr, "invalid arguments");
-  Rows r;
-  int st;
-  if ((st = host_node_adjacency(nn, ne, nnode, conn, r))) return st;
-  *nnz = (int64_t)r.idx.size();
-  std::copy(r.ptr.begin(), r.ptr.end(), ptr);
-  if (idx) std::copy(r.idx.begin(), r.idx.end(), idx);
-  return EXFEM_OK;
+  return host_guard([&]() -> int {
+    Rows r;
+    int st;
+    if ((st = host_node_adjacency(nn, ne, nnode, conn, r))) return st;
+    *nnz = (int64_t)r.idx.size();
+    std::copy(r.ptr.begin(), r.ptr.end(), ptr);
+    if (idx) std::copy(r.idx.begin(), r.idx.end(), idx);
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_fit_candidates(int64_t nb, int bs, int K, const int32_t* agg, int64_t nagg, const double* B,
                               double* Q, double* Bc) {
   EX_ARG(nb >= 0 && bs > 0 && K > 0 && nagg >= 0 && agg && B && Q && Bc, "invalid arguments");
-  for (int64_t n = 0; n < nb; ++n) EX_ARG(agg[n] < nagg, "aggregate %d of node %lld out of range", agg[n], (long long)n);
-  std::vector<double> q, bc;
-  host_fit_candidates(nb, bs, K, agg, nagg, B, q, bc);
-  std::copy(q.begin(), q.end(), Q);
-  std::copy(bc.begin(), bc.end(), Bc);
-  return EXFEM_OK;
+  for (int64_t n = 0; n < nb; ++n)
+    EX_ARG(agg[n] >= 0 && agg[n] < nagg, "aggregate %d of node %lld out of range", agg[n], (long long)n);
+  return host_guard([&]() -> int {
+    std::vector<double> q, bc;
+    host_fit_candidates(nb, bs, K, agg, nagg, B, q, bc);
+    std::copy(q.begin(), q.end(), Q);
+    std::copy(bc.begin(), bc.end(), Bc);
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_coarse_inverse(int64_t n, const double* A, double* Ainv) {
-  EX_ARG(n > 0 && A && Ainv, "invalid arguments");
-  std::vector<double> a(A, A + n * n), inv;
-  int st;
-  if ((st = host_coarse_inverse(n, a, inv))) return st;
-  std::copy(inv.begin(), inv.end(), Ainv);
-  return EXFEM_OK;
+  EX_ARG(n > 0 && n <= (int64_t(1) << 20) && A && Ainv, "invalid arguments");
+  return host_guard([&]() -> int {
+    std::vector<double> a(A, A + n * n), inv;
+    int st;
+    if ((st = host_coarse_inverse(n, a, inv))) return st;
+    std::copy(inv.begin(), inv.end(), Ainv);
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
   EX_ARG(ptr && idx && agg && nagg, "NULL argument");
-  return host_standard_aggregation(n, ptr, idx, agg, *nagg);
+  EX_ARG(n >= 0, "negative size %lld", (long long)n);
+  return host_guard([&]() -> int { return host_standard_aggregation(n, ptr, idx, agg, *nagg); });
 }
 
 int exfem_host_tile_maps(int64_t nn, int64_t ne, int nnode, const int32_t* conn, int tile, int64_t* ntile,
                          int64_t* nlist, int32_t* ptr, int32_t* nodes, uint16_t* nend, uint16_t* perm) {
-  EX_ARG(ne >= 0 && nnode > 0 && (conn || ne == 0) && ntile && nlist, "NULL argument");
+  EX_ARG(nn >= 0 && ne >= 0 && nnode > 0 && (conn || ne == 0) && ntile && nlist, "NULL argument or invalid sizes");
   EX_ARG(tile == 128 || tile == 256, "tile must be 128 or 256, got %d", tile);
   for (int64_t k = 0; k < ne * nnode; ++k)
     EX_ARG(conn[k] >= 0 && conn[k] < nn, "connectivity entry %d at slot %lld is outside [0, %lld)", conn[k],
            (long long)k, (long long)nn);
-  std::vector<int32_t> tp, tn;
-  std::vector<uint16_t> te, tq;
-  int maxu = 0, s;
-  if ((s = host_tile_maps(nn, ne, nnode, conn, tile, tp, tn, te, tq, maxu))) return s;
-  *ntile = (int64_t)tp.size() - 1;
-  *nlist = (int64_t)tn.size();
-  if (ptr) memcpy(ptr, tp.data(), tp.size() * sizeof(int32_t));
-  if (nodes) memcpy(nodes, tn.data(), tn.size() * sizeof(int32_t));
-  if (nend) memcpy(nend, te.data(), te.size() * sizeof(uint16_t));
-  if (perm) memcpy(perm, tq.data(), tq.size() * sizeof(uint16_t));
-  return EXFEM_OK;
+  return host_guard([&]() -> int {
+    std::vector<int32_t> tp, tn;
+    std::vector<uint16_t> te, tq;
+    int maxu = 0, s;
+    if ((s = host_tile_maps(nn, ne, nnode, conn, tile, tp, tn, te, tq, maxu))) return s;
+    *ntile = (int64_t)tp.size() - 1;
+    *nlist = (int64_t)tn.size();
+    if (ptr) memcpy(ptr, tp.data(), tp.size() * sizeof(int32_t));
+    if (nodes) memcpy(nodes, tn.data(), tn.size() * sizeof(int32_t));
+    if (nend) memcpy(nend, te.data(), te.size() * sizeof(uint16_t));
+    if (perm) memcpy(perm, tq.data(), tq.size() * sizeof(uint16_t));
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_face_once(int64_t nface, const int64_t* keys, uint8_t* once) {
   EX_ARG(nface >= 0 && ((keys && once) || nface == 0), "NULL argument");
-  return host_face_once(nface, keys, once);
+  return host_guard([&]() -> int { return host_face_once(nface, keys, once); });
 }
 
 int exfem_host_tile_pairs(int64_t ne, const int32_t* conn, int32_t* order, int32_t* conn_tile) {
   EX_ARG(ne >= 0 && (conn || ne == 0) && (order || ne == 0) && (conn_tile || ne == 0), "NULL argument");
-  std::vector<int32_t> o(order, order + ne), ct;
-  int s;
-  if ((s = host_tile_pairs(ne, conn, o, ct))) return s;
-  if (ne) {
-    memcpy(order, o.data(), ne * sizeof(int32_t));
-    memcpy(conn_tile, ct.data(), ct.size() * sizeof(int32_t));
-  }
-  return EXFEM_OK;
+  return host_guard([&]() -> int {
+    std::vector<char> seen(ne, 0);
+    for (int64_t k = 0; k < ne; ++k) {
+      EX_ARG(order[k] >= 0 && order[k] < ne && !seen[order[k]], "order is not a permutation of [0, %lld) at %lld",
+             (long long)ne, (long long)k);
+      seen[order[k]] = 1;
+    }
+    std::vector<int32_t> o(order, order + ne), ct;
+    int s;
+    if ((s = host_tile_pairs(ne, conn, o, ct))) return s;
+    if (ne) {
+      memcpy(order, o.data(), ne * sizeof(int32_t));
+      memcpy(conn_tile, ct.data(), ct.size() * sizeof(int32_t));
+    }
+    return EXFEM_OK;
+  });
 }
 
 int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
@@ -1011,11 +1059,13 @@ int exfem_host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const 
   for (int64_t k = 0; k < ne * nnode; ++k)
     EX_ARG(conn[k] >= 0 && conn[k] < nn, "connectivity entry %d at slot %lld is outside [0, %lld)", conn[k],
            (long long)k, (long long)nn);
-  std::vector<int32_t> o;
-  int s;
-  if ((s = host_tile_order(nn, ne, nnode, ncorner, X, conn, o))) return s;
-  if (ne) memcpy(order, o.data(), ne * sizeof(int32_t));
-  return EXFEM_OK;
+  return host_guard([&]() -> int {
+    std::vector<int32_t> o;
+    int s;
+    if ((s = host_tile_order(nn, ne, nnode, ncorner, X, conn, o))) return s;
+    if (ne) memcpy(order, o.data(), ne * sizeof(int32_t));
+    return EXFEM_OK;
+  });
 }
 
 }  // extern "C"

@@ -786,3 +786,35 @@ def test_every_export_refuses_null_arguments():
             assert st == 0, (name, st, msg)
         else:
             assert st < 0 and msg, (name, st, msg)
+
+
+def test_host_builders_refuse_invalid_sizes():
+    """The host index builders given negative sizes, an unknown tile size, a tile
+    order that is not a permutation or a dense block too large for the host return
+    an argument error with a message instead of building a huge host array (an
+    allocation error never leaves the library as a C++ exception)."""
+    lib = _lib.lib
+    buf = np.zeros(1 << 12, np.int64)
+    b = buf.ctypes.data
+    i64, i32 = C.c_int64(), C.c_int()
+    calls = [
+        lambda: lib.exfem_host_gather_plan(-1, 1, 8, b, b, C.byref(i32)),
+        lambda: lib.exfem_host_gather_plan(8, -1, 8, b, b, C.byref(i32)),
+        lambda: lib.exfem_host_colouring(-5, 1, 8, b, b, C.byref(i32)),
+        lambda: lib.exfem_host_colouring(8, 1, -8, b, b, C.byref(i32)),
+        lambda: lib.exfem_host_tile_order(-1, 1, 8, 8, b, b, b),
+        lambda: lib.exfem_host_tile_pairs(-3, b, b, b),
+        lambda: lib.exfem_host_tile_pairs(3, b, np.array([0, 0, 1], np.int32).ctypes.data, b),
+        lambda: lib.exfem_host_tile_pairs(3, b, np.array([0, 5, 1], np.int32).ctypes.data, b),
+        lambda: lib.exfem_host_tile_maps(8, 1, 8, b, 0, C.byref(i64), C.byref(i64), None, None, None, None),
+        lambda: lib.exfem_host_tile_maps(-8, 0, 8, b, 256, C.byref(i64), C.byref(i64), None, None, None, None),
+        lambda: lib.exfem_host_node_adjacency(-1, 1, 8, b, C.byref(i64), b, None),
+        lambda: lib.exfem_host_standard_aggregation(-1, b, b, b, C.byref(i64)),
+        lambda: lib.exfem_host_fit_candidates(2, 0, 6, b, 1, b, b, b),
+        lambda: lib.exfem_host_coarse_inverse(1 << 21, b, b),
+        lambda: lib.exfem_host_face_once(-4, b, b),
+    ]
+    for k, f in enumerate(calls):
+        assert f() == _lib.ERR_ARG and _lib.last_error(), k
+    # an empty slot list is a valid (empty) plan
+    assert lib.exfem_host_gather_plan(4, 1, 0, b, None, C.byref(i32)) == 0 and i32.value == 1
