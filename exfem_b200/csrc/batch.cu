@@ -407,7 +407,7 @@ using namespace exfem;
 
 extern "C" {
 
-int exfem_batch_create(exfem_block blk, exfem_amg amg, int ninst, const int64_t* dof_offsets, exfem_batch* out) {
+int exfem_batch_create(exfem_block blk, exfem_amg amg, int ninst, const int64_t* dof_offsets, exfem_batch* out) try {
   EX_ARG(blk && amg && dof_offsets && out, "NULL argument");
   *out = nullptr;
   EX_ARG(ninst >= 1, "need at least one instance");
@@ -424,6 +424,8 @@ int exfem_batch_create(exfem_block blk, exfem_amg amg, int ninst, const int64_t*
   if ((s = batch_alloc(B.get(), dof_offsets))) return s;
   *out = B.release();
   return EXFEM_OK;
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_batch_destroy(exfem_batch b) {
@@ -432,7 +434,7 @@ int exfem_batch_destroy(exfem_batch b) {
 }
 
 int exfem_batch_solve(exfem_batch b, const double* rhs, double* x, double tol, double inner_tol, int max_pass,
-                      int maxiter, int* iters, int* passes, double* relres, void* stream) {
+                      int maxiter, int* iters, int* passes, double* relres, void* stream) try {
   EX_ARG(b && rhs && x, "NULL argument");
   EX_ARG(tol >= 0 && inner_tol > 0 && max_pass >= 1 && maxiter >= 1, "invalid refinement parameters");
   cudaStream_t user = (cudaStream_t)stream, work = user;
@@ -452,6 +454,8 @@ int exfem_batch_solve(exfem_batch b, const double* rhs, double* x, double tol, d
     cudaStreamDestroy(work);
   }
   return s;
+} catch (...) {
+  return host_exception();
 }
 
 }  // extern "C"

@@ -28,6 +28,24 @@ int cuda_status(cudaError_t e, const char* what, const char* file, int line) {
   return e == cudaErrorMemoryAllocation ? EXFEM_ERR_OOM : EXFEM_ERR_CUDA;
 }
 
+int host_exception() {
+  try {
+    throw;
+  } catch (const std::bad_alloc&) {
+    set_error("host memory exhausted");
+    return EXFEM_ERR_OOM;
+  } catch (const std::length_error&) {
+    set_error("size too large for a host array");
+    return EXFEM_ERR_ARG;
+  } catch (const std::exception& e) {
+    set_error("host error: %s", e.what());
+    return EXFEM_ERR_UNSUPPORTED;
+  } catch (...) {
+    set_error("unknown host error");
+    return EXFEM_ERR_UNSUPPORTED;
+  }
+}
+
 int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan, int& vmax);
 int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& colour, int& ncolour);
 int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg);
@@ -162,15 +180,8 @@ template <class F>
 static int host_guard(F&& f) {
   try {
     return f();
-  } catch (const std::bad_alloc&) {
-    set_error("host memory exhausted");
-    return EXFEM_ERR_OOM;
-  } catch (const std::length_error&) {
-    set_error("size too large for a host array");
-    return EXFEM_ERR_ARG;
-  } catch (const std::exception& e) {
-    set_error("host error: %s", e.what());
-    return EXFEM_ERR_UNSUPPORTED;
+  } catch (...) {
+    return host_exception();
   }
 }
 
@@ -180,7 +191,7 @@ int exfem_version(void) { return 1000; }
 const char* exfem_last_error(void) { return g_err.c_str(); }
 
 int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const double* X_host, int64_t ne,
-                       const int32_t* conn_host, exfem_block* out) {
+                       const int32_t* conn_host, exfem_block* out) try {
   EX_ARG(out, "out is NULL");
   *out = nullptr;
   EX_ARG(etype == EXFEM_C3D8 || etype == EXFEM_C3D10, "unknown element type %d", etype);
@@ -315,6 +326,8 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
   if ((s = b->ys.alloc(std::max<int64_t>(ne * b->nnode * 3, 1)))) return s;
   *out = b.release();
   return EXFEM_OK;
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_block_destroy(exfem_block b) {
@@ -440,7 +453,7 @@ int exfem_block_set_lame(exfem_block b, const double* lam_host, const double* mu
   return build_geometry(b);
 }
 
-int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
+int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) try {
   EX_ARG(b, "block is NULL");
   int s;
   ++b->bc_gen;
@@ -487,6 +500,8 @@ int exfem_block_set_fixed(exfem_block b, const uint8_t* fixed_host) {
   }
   if ((s = b->fixed.upload(f.data(), f.size()))) return s;
   return b->node_fixed.upload(nf.data(), nf.size());
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_internal_force(exfem_block b, const double* u, const double* state_old, double* state_new, double* fe,
@@ -602,7 +617,7 @@ int exfem_amg_destroy(exfem_amg h) {
 int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc, const int64_t* A_ptr, const int32_t* A_idx,
                         const double* A_val, const int64_t* P_ptr, const int32_t* P_idx, const double* P_val,
                         const int64_t* R_ptr, const int32_t* R_idx, const double* R_val, const double* dinv,
-                        double rho) {
+                        double rho) try {
   EX_ARG(h && A_ptr && P_ptr && R_ptr && dinv, "NULL argument");
   EX_ARG(n > 0 && nc > 0, "empty level");
   EX_ARG(h->levels.empty() || h->levels.back()->nc == n, "level size %lld does not match the previous coarse size",
@@ -610,6 +625,8 @@ int exfem_amg_add_level(exfem_amg h, int64_t n, int64_t nc, const int64_t* A_ptr
   EX_ARG(rho > 0 && std::isfinite(rho), "invalid spectral bound %g", rho);
   EX_ARG(!h->replicated, "hierarchy already replicated");
   return amg_add_level(h, n, nc, A_ptr, A_idx, A_val, P_ptr, P_idx, P_val, R_ptr, R_idx, R_val, dinv, rho);
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_amg_set_coarse(exfem_amg h, int64_t nc, const double* Ainv) {
@@ -630,7 +647,7 @@ int exfem_amg_set_level_rows(exfem_amg h, int level, const double* rho_rows) {
   return amg_set_level_rows(h, (size_t)level, rho_rows);
 }
 
-int exfem_amg_set_coarse_blocks(exfem_amg h, int64_t nblk, const int64_t* offsets, const double* Ainv_blocks) {
+int exfem_amg_set_coarse_blocks(exfem_amg h, int64_t nblk, const int64_t* offsets, const double* Ainv_blocks) try {
   EX_ARG(h && offsets && Ainv_blocks && nblk > 0, "NULL argument or no blocks");
   EX_ARG(!h->replicated, "hierarchy already replicated");
   const int64_t nc = offsets[nblk];
@@ -650,6 +667,8 @@ int exfem_amg_set_coarse_blocks(exfem_amg h, int64_t nblk, const int64_t* offset
   if ((st = h->crow_s.upload(rs.data(), nc))) return st;
   if ((st = h->crow_m.upload(rm.data(), nc))) return st;
   return h->crow_a.upload(ra.data(), nc);
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_amg_replicate(exfem_amg h, int nblk, const int64_t* level_offsets, int ninst, const int32_t* inst_block) {
@@ -678,7 +697,7 @@ int exfem_amg_vcycle(exfem_amg h, int dtype, const void* r, void* z, exfem_block
 }
 
 // ---------------------------------------------------------------- solvers
-int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out) {
+int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, exfem_solver* out) try {
   EX_ARG(b && out, "NULL argument");
   *out = nullptr;
   EX_ARG(op_kind >= EXFEM_OP_EBE_F64 && op_kind <= EXFEM_OP_CSR_F64, "unknown operator kind %d", op_kind);
@@ -697,6 +716,8 @@ int exfem_solver_create(exfem_block b, int op_kind, int pc_kind, exfem_amg amg, 
   if ((s = solver_alloc(S.get()))) return s;
   *out = S.release();
   return EXFEM_OK;
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_solver_destroy(exfem_solver s) {
@@ -839,7 +860,7 @@ int exfem_amg_setup_block(exfem_amg h, exfem_block b, const double* Ke, int max_
 }
 
 int exfem_amg_setup_blocks(exfem_amg h, int nblk, const exfem_block* blocks, const double* const* Kes,
-                           int max_coarse, int keep_level0, void* stream) {
+                           int max_coarse, int keep_level0, void* stream) try {
   EX_ARG(h && nblk >= 1 && blocks && Kes, "NULL argument");
   std::vector<exfem_block_s*> bl(blocks, blocks + nblk);
   std::vector<const double*> ke(Kes, Kes + nblk);
@@ -855,6 +876,8 @@ int exfem_amg_setup_blocks(exfem_amg h, int nblk, const exfem_block* blocks, con
     h->Ainv.release();
   }
   return st;
+} catch (...) {
+  return host_exception();
 }
 
 int exfem_amg_export_level(exfem_amg h, int level, int what, int64_t* rows, int64_t* cols, int64_t* nnz,

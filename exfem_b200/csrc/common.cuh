@@ -18,6 +18,10 @@ namespace exfem {
 // ---------------------------------------------------------------- errors
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what, const char* file, int line);
+// status of the C++ exception being handled (call inside a catch clause): a C++
+// exception never crosses the C ABI; host allocations that fail become
+// EXFEM_ERR_OOM, sizes no host array can hold EXFEM_ERR_ARG
+int host_exception();
 
 #define EX_CUDA(call)                                                              \
   do {                                                                             \

@@ -112,7 +112,7 @@ void exfem_queue_s::worker() {
 
 extern "C" {
 
-int exfem_queue_create(int workers, exfem_queue* out) {
+int exfem_queue_create(int workers, exfem_queue* out) try {
   EX_ARG(out, "out is NULL");
   *out = nullptr;
   EX_ARG(workers >= 1 && workers <= 64, "workers must lie in 1..64, got %d", workers);
@@ -121,6 +121,8 @@ int exfem_queue_create(int workers, exfem_queue* out) {
   for (int i = 0; i < workers; ++i) q->threads.emplace_back([p = q.get()] { p->worker(); });
   *out = q.release();
   return EXFEM_OK;
+} catch (...) {
+  return ::exfem::host_exception();
 }
 
 int exfem_queue_destroy(exfem_queue q) {
@@ -137,7 +139,7 @@ int exfem_queue_destroy(exfem_queue q) {
   return EXFEM_OK;
 }
 
-int exfem_queue_submit(exfem_queue q, exfem_solver s, const double* rhs_host, double tol, int64_t* id) {
+int exfem_queue_submit(exfem_queue q, exfem_solver s, const double* rhs_host, double tol, int64_t* id) try {
   EX_ARG(q && s && rhs_host && id, "NULL argument");
   EX_ARG(s->op == EXFEM_OP_MF_F32, "queued solves run the mixed solver: the handle needs EXFEM_OP_MF_F32");
   EX_ARG(tol > 0, "tolerance must be positive, got %g", tol);
@@ -155,6 +157,8 @@ int exfem_queue_submit(exfem_queue q, exfem_solver s, const double* rhs_host, do
   }
   q->cv.notify_all();
   return EXFEM_OK;
+} catch (...) {
+  return ::exfem::host_exception();
 }
 
 int exfem_queue_poll(exfem_queue q, int64_t id, int* state, int* iters, double* relres) {
