@@ -46,7 +46,7 @@ int host_exception() {
   }
 }
 
-int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan, int& vmax);
+int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>* plan, int& vmax);
 int host_colouring(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& colour, int& ncolour);
 int host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t& nagg);
 int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double* X, const int32_t* conn,
@@ -210,7 +210,7 @@ int exfem_block_create(int etype, const exfem_material* mat, int64_t nn, const d
   int s;
   if ((s = set_material(b.get(), mat))) return s;
   b->nstate = mat->kind == EXFEM_J2 ? 19 : 1;
-  if ((s = host_gather_plan(nn, ne, b->nnode, conn_host, b->plan_host, b->vmax))) return s;
+  if ((s = host_gather_plan(nn, ne, b->nnode, conn_host, &b->plan_host, b->vmax))) return s;
   std::vector<int32_t> colours;
   if ((s = host_colouring(nn, ne, b->nnode, conn_host, colours, b->ncolour))) return s;
   b->colour_host = colours;
@@ -960,7 +960,7 @@ int exfem_host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* con
   return host_guard([&]() -> int {
     std::vector<int32_t> p;
     int v = 0, s;
-    if ((s = host_gather_plan(nn, ne, nnode, conn, p, v))) return s;
+    if ((s = host_gather_plan(nn, ne, nnode, conn, plan ? &p : nullptr, v))) return s;
     *vmax = v;
     if (plan) memcpy(plan, p.data(), p.size() * sizeof(int32_t));
     return EXFEM_OK;

@@ -36,9 +36,8 @@
 
 namespace exfem {
 
-int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>& plan,
+int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std::vector<int32_t>* plan_out,
                      int& vmax) {
-  std::vector<int32_t> cnt(nn, 0);
   const int64_t nslot = ne * nnode;
   for (int64_t k = 0; k < nslot; ++k) {
     const int32_t n = conn[k];
@@ -46,21 +45,51 @@ int host_gather_plan(int64_t nn, int64_t ne, int nnode, const int32_t* conn, std
       set_error("connectivity entry %d at slot %lld is outside [0, %lld)", n, (long long)k, (long long)nn);
       return EXFEM_ERR_ARG;
     }
-    ++cnt[n];
   }
-  int32_t m = 1;
-  for (int64_t n = 0; n < nn; ++n) m = cnt[n] > m ? cnt[n] : m;
-  vmax = m;
   if (nslot >= (int64_t)INT32_MAX) {
     set_error("gather plan needs int64 slots (ne*nnode >= 2^31)");
     return EXFEM_ERR_UNSUPPORTED;
   }
-  plan.assign((size_t)nn * vmax, (int32_t)nslot);
-  std::fill(cnt.begin(), cnt.end(), 0);
-  for (int64_t k = 0; k < nslot; ++k) {
-    const int32_t n = conn[k];
-    plan[(size_t)n * vmax + cnt[n]++] = (int32_t)k;
-  }
+  // threads own contiguous node ranges and each scans every slot in increasing
+  // order, so a row lists its slots in increasing order exactly as one counting
+  // sort does, and each thread's counters and plan rows stay within its range
+  const int nth = (int)std::max<int64_t>(
+      1, std::min<int64_t>(std::min<int>((int)std::thread::hardware_concurrency(), 16), nslot / (1 << 20)));
+  std::vector<int32_t> cnt(nn, 0);
+  auto range = [&](int t, int64_t& lo, int64_t& hi) {
+    lo = nn * t / nth;
+    hi = nn * (t + 1) / nth;
+  };
+  auto run = [&](auto&& f) {
+    if (nth == 1) { f(0); return; }
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; ++t) pool.emplace_back(f, t);
+    for (auto& th : pool) th.join();
+  };
+  run([&](int t) {
+    int64_t lo, hi;
+    range(t, lo, hi);
+    for (int64_t k = 0; k < nslot; ++k) {
+      const int32_t n = conn[k];
+      if (n >= lo && n < hi) ++cnt[n];
+    }
+  });
+  int32_t m = 1;
+  for (int64_t n = 0; n < nn; ++n) m = cnt[n] > m ? cnt[n] : m;
+  vmax = m;
+  if (!plan_out) return EXFEM_OK;  // the width alone
+  std::vector<int32_t>& plan = *plan_out;
+  plan.resize((size_t)nn * vmax);
+  run([&](int t) {
+    int64_t lo, hi;
+    range(t, lo, hi);
+    std::fill(plan.begin() + lo * vmax, plan.begin() + hi * vmax, (int32_t)nslot);
+    std::fill(cnt.begin() + lo, cnt.begin() + hi, 0);
+    for (int64_t k = 0; k < nslot; ++k) {
+      const int32_t n = conn[k];
+      if (n >= lo && n < hi) plan[(size_t)n * vmax + cnt[n]++] = (int32_t)k;
+    }
+  });
   return EXFEM_OK;
 }
 
