@@ -818,3 +818,14 @@ def test_host_builders_refuse_invalid_sizes():
         assert f() == _lib.ERR_ARG and _lib.last_error(), k
     # an empty slot list is a valid (empty) plan
     assert lib.exfem_host_gather_plan(4, 1, 0, b, None, C.byref(i32)) == 0 and i32.value == 1
+
+
+def test_host_gather_plan_threaded_bit_exact():
+    """A plan large enough to be built by several threads (over 2^21 slots, node
+    numbers shuffled so that every thread's node range takes slots from all over
+    the connectivity) equals the oracle's stable argsort plan."""
+    X, c = mesh.box_hex(1, 1, 1, 66, 64, 64)
+    perm = np.random.default_rng(4).permutation(len(X)).astype(np.int32)
+    c = perm[c]
+    assert c.size > 2 ** 21
+    np.testing.assert_array_equal(_host_plan(c, len(X)), fem.gather_plan([c], len(X)))
