@@ -174,25 +174,55 @@ int host_tile_order(int64_t nn, int64_t ne, int nnode, int ncorner, const double
       if (e == 0 || v < lo[d]) lo[d] = v;
       if (e == 0 || v > hi[d]) hi[d] = v;
     }
-  std::vector<uint64_t> key(ne);
-  for (int64_t e = 0; e < ne; ++e) {
-    uint64_t k = 0;
-    for (int d = 0; d < 3; ++d) {
-      uint64_t q = 0;
-      if (hi[d] > lo[d]) {
-        const double f = std::floor((s[3 * e + d] - lo[d]) / (hi[d] - lo[d]) * 2097152.0);
-        q = f >= 2097151.0 ? 2097151u : (f > 0.0 ? (uint64_t)f : 0u);
-      }
-      for (int b = 0; b < 21; ++b) k |= ((q >> b) & 1ull) << (3 * b + d);
+  // sort records (component, Morton key, element): the order is strict, so chunks
+  // sorted by separate threads and merged give the one sorted sequence
+  struct Rec {
+    int64_t comp;
+    uint64_t key;
+    int32_t e;
+    bool operator<(const Rec& o) const {
+      if (comp != o.comp) return comp < o.comp;
+      if (key != o.key) return key < o.key;
+      return e < o.e;
     }
-    key[e] = k;
+  };
+  std::vector<Rec> rec(ne);
+  const int nth = (int)std::max<int64_t>(
+      1, std::min<int64_t>(std::min<int>((int)std::thread::hardware_concurrency(), 16), ne / (1 << 16)));
+  std::vector<int64_t> cut(nth + 1);
+  for (int t = 0; t <= nth; ++t) cut[t] = ne * t / nth;
+  auto chunk = [&](int t) {
+    for (int64_t e = cut[t]; e < cut[t + 1]; ++e) {
+      uint64_t k = 0;
+      for (int d = 0; d < 3; ++d) {
+        uint64_t q = 0;
+        if (hi[d] > lo[d]) {
+          const double f = std::floor((s[3 * e + d] - lo[d]) / (hi[d] - lo[d]) * 2097152.0);
+          q = f >= 2097151.0 ? 2097151u : (f > 0.0 ? (uint64_t)f : 0u);
+        }
+        for (int b = 0; b < 21; ++b) k |= ((q >> b) & 1ull) << (3 * b + d);
+      }
+      rec[e] = Rec{comp[e], k, (int32_t)e};
+    }
+    std::sort(rec.begin() + cut[t], rec.begin() + cut[t + 1]);
+  };
+  if (nth == 1) {
+    chunk(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nth; ++t) pool.emplace_back(chunk, t);
+    for (auto& th : pool) th.join();
+    // pairwise merges of neighbouring runs, the merges of one round in parallel
+    for (int w = 1; w < nth; w *= 2) {
+      std::vector<std::thread> mp;
+      for (int t = 0; t + w < nth; t += 2 * w) {
+        const int64_t a = cut[t], m = cut[t + w], b = cut[std::min(t + 2 * w, nth)];
+        mp.emplace_back([&rec, a, m, b]() { std::inplace_merge(rec.begin() + a, rec.begin() + m, rec.begin() + b); });
+      }
+      for (auto& th : mp) th.join();
+    }
   }
-  for (int64_t e = 0; e < ne; ++e) order[e] = (int32_t)e;
-  std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
-    if (comp[a] != comp[b]) return comp[a] < comp[b];
-    if (key[a] != key[b]) return key[a] < key[b];
-    return a < b;
-  });
+  for (int64_t p = 0; p < ne; ++p) order[p] = rec[p].e;
   return EXFEM_OK;
 }
 

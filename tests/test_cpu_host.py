@@ -829,3 +829,17 @@ def test_host_gather_plan_threaded_bit_exact():
     c = perm[c]
     assert c.size > 2 ** 21
     np.testing.assert_array_equal(_host_plan(c, len(X)), fem.gather_plan([c], len(X)))
+
+
+def test_host_tile_order_threaded_bit_exact():
+    """A tile order large enough to be sorted in several chunks and merged (three
+    mesh components, jittered coordinates, over 2^17 elements) equals the oracle's
+    restatement."""
+    X1, c1 = mesh.box_hex(2.0, 1.0, 1.0, 64, 32, 32)
+    X1 = mesh.jitter_interior(X1, 1.0 / 32, 0.1, 7)
+    X2, c2 = mesh.box_hex(1.0, 1.0, 1.0, 20, 20, 20)
+    X = np.concatenate([X1, X2 + 3.0, X1 - 5.0])
+    c = np.concatenate([c1, c2 + len(X1), c1 + len(X1) + len(X2)])
+    assert len(c) > 2 ** 17
+    order = _host_order(X, c, 8)
+    np.testing.assert_array_equal(order, fem.tile_order(X, c, 8))
