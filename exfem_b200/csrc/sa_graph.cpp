@@ -72,16 +72,31 @@ void build_rows(int64_t nrows, int64_t ncols, Rows& R, F fn) {
     }
     for (auto& x : th) x.join();
   }
-  R.ptr.assign(nrows + 1, 0);
-  int64_t r = 0, tot = 0;
-  for (int t = 0; t < T; ++t)
-    for (int64_t l : len[t]) { R.ptr[r + 1] = R.ptr[r] + l; ++r; tot += l; }
-  R.idx.resize(tot);
-  int64_t o = 0;
+  // concatenation: each thread's rows and entries land at offsets known from the
+  // part sizes, so the threads write their ranges of ptr and idx side by side
+  std::vector<int64_t> row0(T + 1, 0), off(T + 1, 0);
   for (int t = 0; t < T; ++t) {
-    if (!part[t].empty()) std::memcpy(R.idx.data() + o, part[t].data(), part[t].size() * sizeof(int32_t));
-    o += (int64_t)part[t].size();
+    row0[t + 1] = row0[t] + (int64_t)len[t].size();
+    off[t + 1] = off[t] + (int64_t)part[t].size();
+  }
+  R.ptr.resize(nrows + 1);
+  R.ptr[0] = 0;
+  R.idx.resize(off[T]);
+  auto place = [&](int t) {
+    int64_t o = off[t];
+    for (size_t i = 0; i < len[t].size(); ++i) {
+      o += len[t][i];
+      R.ptr[row0[t] + (int64_t)i + 1] = o;
+    }
+    if (!part[t].empty()) std::memcpy(R.idx.data() + off[t], part[t].data(), part[t].size() * sizeof(int32_t));
     std::vector<int32_t>().swap(part[t]);
+  };
+  if (T == 1) {
+    place(0);
+  } else {
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(place, t);
+    for (auto& x : th) x.join();
   }
 }
 

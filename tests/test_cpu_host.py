@@ -843,3 +843,23 @@ def test_host_tile_order_threaded_bit_exact():
     assert len(c) > 2 ** 17
     order = _host_order(X, c, 8)
     np.testing.assert_array_equal(order, fem.tile_order(X, c, 8))
+
+
+def test_host_node_adjacency_threaded():
+    """Node adjacency of a mesh large enough to be built by several threads (69k
+    nodes, numbering shuffled) equals the sparsity pattern of the node-element
+    incidence product, rows ascending."""
+    X, c = mesh.box_hex(1, 1, 1, 40, 40, 40)
+    perm = np.random.default_rng(8).permutation(len(X)).astype(np.int32)
+    c = np.ascontiguousarray(perm[c])
+    nn, ne = len(X), len(c)
+    nnz, ptr = C.c_int64(), np.zeros(nn + 1, np.int64)
+    _lib.check(_lib.lib.exfem_host_node_adjacency(nn, ne, 8, c.ctypes.data, C.byref(nnz), ptr.ctypes.data, None))
+    idx = np.zeros(nnz.value, np.int32)
+    _lib.check(_lib.lib.exfem_host_node_adjacency(nn, ne, 8, c.ctypes.data, C.byref(nnz), ptr.ctypes.data,
+                                                  idx.ctypes.data))
+    inc = sp.csr_matrix((np.ones(c.size), (c.ravel(), np.repeat(np.arange(ne), 8))), shape=(nn, ne))
+    A = (inc @ inc.T + sp.identity(nn)).tocsr()
+    A.sort_indices()
+    np.testing.assert_array_equal(ptr, A.indptr)
+    np.testing.assert_array_equal(idx, A.indices)
