@@ -104,6 +104,7 @@ _SIGS = {
     "exfem_host_node_adjacency": ([I64, I64, I32, P, C.POINTER(I64), P, P], C.c_int),
     "exfem_host_fit_candidates": ([I64, I32, I32, P, I64, P, P, P], C.c_int),
     "exfem_host_coarse_inverse": ([I64, P, P], C.c_int),
+    "exfem_host_filter_pattern": ([I64, P, P, P, C.POINTER(I64), P, P, P], C.c_int),
     "exfem_host_tile_order": ([I64, I64, I32, I32, P, P, P], C.c_int),
     "exfem_host_tile_pairs": ([I64, P, P, P], C.c_int),
     "exfem_host_face_once": ([I64, P, P], C.c_int),

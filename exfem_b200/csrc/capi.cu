@@ -1022,6 +1022,30 @@ int exfem_host_coarse_inverse(int64_t n, const double* A, double* Ainv) {
   });
 }
 
+int exfem_host_filter_pattern(int64_t nrows, const int64_t* ptr, const int32_t* idx, const uint8_t* flag,
+                              int64_t* nnz, int64_t* ptr_out, int32_t* idx_out, int64_t* keep_out) {
+  EX_ARG(nrows >= 0 && ptr && nnz, "NULL argument or negative row count");
+  EX_ARG(ptr[0] == 0, "ptr[0] must be 0");
+  for (int64_t r = 0; r < nrows; ++r) EX_ARG(ptr[r + 1] >= ptr[r], "ptr decreases at row %lld", (long long)r);
+  EX_ARG(ptr[nrows] == 0 || (idx && flag), "NULL idx or flag");
+  return host_guard([&]() -> int {
+    int64_t c = 0;
+    for (int64_t q = 0; q < ptr[nrows]; ++q) c += flag[q] ? 1 : 0;
+    *nnz = c;
+    if (!idx_out) return EXFEM_OK;
+    EX_ARG(ptr_out && (keep_out || c == 0), "NULL output");
+    Rows pat, S;
+    std::vector<int64_t> keep;
+    pat.ptr.assign(ptr, ptr + nrows + 1);
+    pat.idx.assign(idx, idx + ptr[nrows]);
+    host_filter_pattern(pat, flag, S, keep);
+    std::copy(S.ptr.begin(), S.ptr.end(), ptr_out);
+    std::copy(S.idx.begin(), S.idx.end(), idx_out);
+    std::copy(keep.begin(), keep.end(), keep_out);
+    return EXFEM_OK;
+  });
+}
+
 int exfem_host_standard_aggregation(int64_t n, const int64_t* ptr, const int32_t* idx, int32_t* agg, int64_t* nagg) {
   EX_ARG(ptr && idx && agg && nagg, "NULL argument");
   EX_ARG(n >= 0, "negative size %lld", (long long)n);

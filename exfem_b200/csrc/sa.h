@@ -18,6 +18,9 @@ struct Rows {
 // node adjacency of a mesh: row n lists, ascending, every node that shares an
 // element with n (n itself included)
 int host_node_adjacency(int64_t nn, int64_t ne, int nnode, const int32_t* conn, Rows& out);
+// the entries q of pattern `pat` whose flag[q] is set, row by row in their order:
+// S holds their columns, keep their positions in pat (rows filtered on threads)
+void host_filter_pattern(const Rows& pat, const uint8_t* flag, Rows& S, std::vector<int64_t>& keep);
 // six rigid-body modes of nodes X (nn, 3) centred at their mean: (3 nn, 6) row-major
 void host_rigid_body_modes(int64_t nn, const double* X, std::vector<double>& B);
 // tentative prolongator of an aggregation: per aggregate, modified Gram-Schmidt of

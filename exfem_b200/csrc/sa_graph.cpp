@@ -131,6 +131,32 @@ int host_node_adjacency(int64_t nn, int64_t ne, int nnode, const int32_t* conn, 
   return EXFEM_OK;
 }
 
+void host_filter_pattern(const Rows& pat, const uint8_t* flag, Rows& S, std::vector<int64_t>& keep) {
+  const int64_t nr = pat.nrows();
+  S.ptr.assign(nr + 1, 0);
+  parallel_ranges(nr, [&](int, int64_t lo, int64_t hi) {
+    for (int64_t r = lo; r < hi; ++r) {
+      int64_t c = 0;
+      for (int64_t q = pat.ptr[r]; q < pat.ptr[r + 1]; ++q) c += flag[q] ? 1 : 0;
+      S.ptr[r + 1] = c;
+    }
+  });
+  for (int64_t r = 0; r < nr; ++r) S.ptr[r + 1] += S.ptr[r];
+  S.idx.resize(S.ptr[nr]);
+  keep.resize(S.ptr[nr]);
+  parallel_ranges(nr, [&](int, int64_t lo, int64_t hi) {
+    for (int64_t r = lo; r < hi; ++r) {
+      int64_t o = S.ptr[r];
+      for (int64_t q = pat.ptr[r]; q < pat.ptr[r + 1]; ++q)
+        if (flag[q]) {
+          S.idx[o] = pat.idx[q];
+          keep[o] = q;
+          ++o;
+        }
+    }
+  });
+}
+
 void host_rigid_body_modes(int64_t nn, const double* X, std::vector<double>& B) {
   double m[3] = {0, 0, 0};
   for (int64_t i = 0; i < nn; ++i)

@@ -725,14 +725,8 @@ int amg_setup_blocks(exfem_amg_s* h, const std::vector<exfem_block_s*>& blks, co
       std::vector<uint8_t> f;
       if ((st = down(f, flag.p, (size_t)nblk, s))) return st;
       Rows S;
-      S.ptr.assign(A.nb + 1, 0);
       std::vector<int64_t> keep;
-      keep.reserve(nblk);
-      for (int64_t r = 0; r < A.nb; ++r) {
-        for (int64_t q = A.pat.ptr[r]; q < A.pat.ptr[r + 1]; ++q)
-          if (f[q]) { keep.push_back(q); S.idx.push_back(A.pat.idx[q]); }
-        S.ptr[r + 1] = (int64_t)S.idx.size();
-      }
+      host_filter_pattern(A.pat, f.data(), S, keep);
       if ((int64_t)keep.size() < nblk) {
         DevBuf<int64_t> dkeep;
         DevBuf<double> v;

@@ -465,6 +465,15 @@ int exfem_host_node_adjacency(int64_t nn, int64_t ne, int nnode, const int32_t* 
 int exfem_host_fit_candidates(int64_t nb, int bs, int K, const int32_t* agg, int64_t nagg, const double* B,
                               double* Q, double* Bc);
 int exfem_host_coarse_inverse(int64_t n, const double* A, double* Ainv);
+/* Strength filter of the device set-up (theta = 0: the blocks of a level matrix that
+ * are not all zero), exported for checking: the entries q of the pattern (nrows,
+ * ptr, idx) with flag[q] set, row by row in their order.  *nnz = their count;
+ * ptr_out (nrows + 1), idx_out (their columns) and keep_out (their positions in
+ * idx) are written when idx_out is not NULL.  No counterpart in the reference
+ * (pyamg's classical strength with theta = 0 inside smoothed_aggregation_solver,
+ * gfem/linalg.py:113-116). */
+int exfem_host_filter_pattern(int64_t nrows, const int64_t* ptr, const int32_t* idx, const uint8_t* flag,
+                              int64_t* nnz, int64_t* ptr_out, int32_t* idx_out, int64_t* keep_out);
 /* tile order of the matrix-free operator (see exfem_block_tile_order) for a mesh
  * of ne elements with nnode nodes each, the first ncorner of them corners:
  * order (ne,) position -> element.  No counterpart in the reference. */

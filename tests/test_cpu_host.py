@@ -863,3 +863,31 @@ def test_host_node_adjacency_threaded():
     A.sort_indices()
     np.testing.assert_array_equal(ptr, A.indptr)
     np.testing.assert_array_equal(idx, A.indices)
+
+
+@pytest.mark.parametrize("nrows", [7, 120_000])
+def test_host_filter_pattern(nrows):
+    """The strength filter of the device set-up (the entries whose flag is set, row
+    by row in order, with their positions) equals NumPy's boolean selection, on one
+    thread and on several (120k rows), with empty rows and rows filtered empty."""
+    rng = np.random.default_rng(nrows)
+    cnt = rng.integers(0, 9, nrows)
+    ptr = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+    idx = rng.integers(0, nrows, ptr[-1]).astype(np.int32)
+    flag = (rng.random(ptr[-1]) < 0.7).astype(np.uint8)
+    nnz = C.c_int64()
+    _lib.check(_lib.lib.exfem_host_filter_pattern(nrows, ptr.ctypes.data, idx.ctypes.data, flag.ctypes.data,
+                                                  C.byref(nnz), None, None, None))
+    assert nnz.value == int(flag.sum())
+    po, io, ko = np.empty(nrows + 1, np.int64), np.empty(nnz.value, np.int32), np.empty(nnz.value, np.int64)
+    _lib.check(_lib.lib.exfem_host_filter_pattern(nrows, ptr.ctypes.data, idx.ctypes.data, flag.ctypes.data,
+                                                  C.byref(nnz), po.ctypes.data, io.ctypes.data, ko.ctypes.data))
+    rows = np.repeat(np.arange(nrows), cnt)
+    sel = flag.astype(bool)
+    np.testing.assert_array_equal(po, np.concatenate([[0], np.cumsum(np.bincount(rows[sel], minlength=nrows))]))
+    np.testing.assert_array_equal(io, idx[sel])
+    np.testing.assert_array_equal(ko, np.nonzero(sel)[0])
+    bad = ptr.copy()
+    bad[3] = bad[2] - 1
+    assert _lib.lib.exfem_host_filter_pattern(nrows, bad.ctypes.data, idx.ctypes.data, flag.ctypes.data,
+                                              C.byref(nnz), None, None, None) == _lib.ERR_ARG
